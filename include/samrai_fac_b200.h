@@ -1,0 +1,210 @@
+/*
+ * samrai_fac_b200.h -- C ABI of the B200-native FAC Poisson hot path.
+ *
+ * Plain C: opaque context, plain pointers and sizes, int status returns
+ * (0 = success; see fac_status).  No CUDA or C++ types cross this boundary.
+ *
+ * Each entry point replaces one piece of SAMRAI's cell-centred FAC path
+ * (paths relative to the SAMRAI source tree):
+ *   solv/CellPoissonFACSolver.{h,C}   solver wrapper      -> fac_solve*
+ *   solv/FACPreconditioner.{h,C}      FAC cycling         -> fac_fac_cycle
+ *   solv/CellPoissonFACOps.{h,C}      level operators     -> fac_smooth,
+ *                                     fac_comp_residual, fac_restrict,
+ *                                     fac_prolong_correct, fac_rms_norm ...
+ *   xfer/RefineSchedule::fillData     ghost fill          -> fac_ghost_fill
+ * The reference reaches its numerical kernels through the F77 ABI
+ * (SAMRAI_F77_FUNC, every argument by pointer, no return value); this ABI
+ * instead works one level of the whole hierarchy per call.
+ *
+ * One context holds a batch of independent problems ("problems") that share
+ * the dimension and the number of levels; every level operation acts on
+ * that level of every active problem at once.
+ *
+ * Cell data use SAMRAI's ArrayData layout (pdat/ArrayData.C:79-127):
+ * column-major over the ghosted box, i fastest.  Host buffers passed to the
+ * upload/download calls hold one level of one problem: the patches' ghosted
+ * arrays concatenated in patch order.  Side data (D): per patch, axis
+ * 0..dim-1, the side box (upper+1 along the axis), ghost width 0.
+ */
+#ifndef SAMRAI_FAC_B200_H
+#define SAMRAI_FAC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fac_ctx fac_ctx;
+
+enum fac_status {
+   FAC_OK = 0,
+   FAC_ERR_ARG = 1,        /* bad argument (reference: TBOX_ERROR/TBOX_ASSERT) */
+   FAC_ERR_STATE = 2,      /* call out of order (e.g. before fac_initialize) */
+   FAC_ERR_CUDA = 3,       /* a CUDA runtime call failed */
+   FAC_ERR_NESTING = 4,    /* hierarchy not properly nested */
+   FAC_ERR_NOMEM = 5,      /* device allocation failed */
+   FAC_ERR_DEVICE = 6      /* device-side error flag was set */
+};
+
+/* Cell field ids (ghost width): the vectors of FACPreconditioner and the
+ * Poisson C coefficient. */
+enum fac_field {
+   FAC_U = 0,   /* solution u            (1) */
+   FAC_F = 1,   /* right-hand side f     (0) */
+   FAC_E = 2,   /* error e               (1) */
+   FAC_R = 3,   /* residual r            (0) */
+   FAC_TR = 4,  /* coarser-level residual (0) */
+   FAC_W = 5,   /* control volume weight (0) */
+   FAC_C = 6    /* Poisson C field       (0) */
+};
+
+/* Last error message of this thread (never NULL). */
+const char *fac_last_error(void);
+
+/* ---- context and hierarchy (CellPoissonFACSolver ctor,
+ *      FACPreconditioner::initializeSolverState FACPreconditioner.C:158-229) */
+
+/* Create an empty context of dimension dim (2 or 3) on CUDA device `device`.
+ * device = -1 makes a host-only context: fac_initialize builds and checks
+ * every device table without touching a GPU; operations then fail with
+ * FAC_ERR_STATE. */
+int fac_ctx_create(fac_ctx **ctx, int dim, int device);
+int fac_ctx_destroy(fac_ctx *ctx);
+
+/* Add one problem.  n0: level-0 cells per axis (physical domain is the
+ * box [0,n0-1]); xlo/xup: physical extent; ratio: nlev x 3 refinement
+ * ratios to the next coarser level (level 0: 1 1 1); npatch: patches per
+ * level; boxes: lo0 lo1 lo2 hi0 hi1 hi2 per patch in level order.
+ * Returns the problem index through *problem. */
+int fac_add_problem(fac_ctx *ctx, const int *n0, const double *xlo,
+                    const double *xup, int nlev, const int *ratio,
+                    const int *npatch, const int *boxes, int *problem);
+
+/* PoissonSpecifications (solv/PoissonSpecifications.h:51-345):
+ * div(D grad u) + C u = f.  d_variable: D is side data (fac_upload_side);
+ * c_kind 0 = zero, 1 = constant c_const, 2 = cell field FAC_C. */
+int fac_set_poisson(fac_ctx *ctx, int d_variable, double d_const,
+                    int c_kind, double c_const);
+
+/* Robin boundary coefficients a u + b du/dn = g per location index
+ * 0..2*dim-1 (solv/RobinBcCoefStrategy.h; Dirichlet a=1,b=0 as
+ * SimpleCellRobinBcCoefs::setBcCoefs, SimpleCellRobinBcCoefs.C:283-290). */
+int fac_set_bc(fac_ctx *ctx, const double *a, const double *b,
+               const double *g);
+
+/* Input keys of FACPreconditioner (FACPreconditioner.C:80-114) and
+ * CellPoissonFACOps (CellPoissonFACOps.C:692-739).  ewing: 1 selects
+ * cf_discretization "Ewing" (0 is rejected: only Ewing is implemented). */
+int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol,
+                   double relative_residual_tol, int pre_sweeps,
+                   int post_sweeps, double coarse_tol, int coarse_max_it,
+                   int ewing);
+
+/* Build device tables and allocate device state
+ * (CellPoissonFACOps::initializeOperatorState, CellPoissonFACOps.C:751-1106). */
+int fac_initialize(fac_ctx *ctx);
+
+/* Sizes (doubles) of one level of one problem in the host layout. */
+int fac_field_size(fac_ctx *ctx, int fid, int problem, int ln, size_t *n);
+int fac_side_size(fac_ctx *ctx, int problem, int ln, size_t *n);
+int fac_oside_size(fac_ctx *ctx, int problem, int ln, size_t *n);
+
+/* Host <-> device copies of one level of one problem (host layout above).
+ * Synchronous with respect to the context's stream. */
+int fac_upload_field(fac_ctx *ctx, int fid, int problem, int ln,
+                     const double *host);
+int fac_download_field(fac_ctx *ctx, int fid, int problem, int ln,
+                       double *host);
+int fac_upload_side(fac_ctx *ctx, int problem, int ln, const double *host);
+int fac_download_side(fac_ctx *ctx, int problem, int ln, double *host);
+/* Flux scratch (side layout) as left by the last fac_comp_residual on ln:
+ * D grad u with the Ewing fix and the coarsened finer-level flux. */
+int fac_download_flux(fac_ctx *ctx, int problem, int ln, double *host);
+/* Saved outer-side flux of a refined level (CellPoissonFACOps.C:1933-1948):
+ * per patch, axis, lower then upper side. */
+int fac_download_oside(fac_ctx *ctx, int problem, int ln, double *host);
+
+/* ---- level operators (FACOperatorStrategy, FACOperatorStrategy.h:83-364) */
+
+/* xeqScheduleGhostFill (with_coarse=1) / xeqScheduleGhostFillNoCoarse
+ * (CellPoissonFACOps.C:2861-2900). */
+int fac_ghost_fill(fac_ctx *ctx, int fid, int ln, int with_coarse,
+                   int homogeneous);
+/* smoothErrorByRedBlack (CellPoissonFACOps.C:1339-1514): nsweeps red-black
+ * Gauss-Seidel sweeps of field fid_e against right-hand side fid_r; tol < 0
+ * disables the convergence test.  sweeps (optional, one int per problem)
+ * receives the sweeps taken. */
+int fac_smooth(fac_ctx *ctx, int fid_e, int fid_r, int ln, int nsweeps,
+               double tol, int *sweeps);
+/* computeCompositeResidualOnLevel (CellPoissonFACOps.C:1792-1956). */
+int fac_comp_residual(fac_ctx *ctx, int fid_r, int fid_u, int fid_f, int ln,
+                      int error_equation);
+/* restrictResidual / restrictSolution without the ghost fill
+ * (CellPoissonFACOps.C:1197-1242): volume-weighted average of level
+ * dest_ln+1 into level dest_ln. */
+int fac_restrict(fac_ctx *ctx, int fid_src, int fid_dst, int dest_ln);
+/* restrictSolution (CellPoissonFACOps.C:1197-1220). */
+int fac_restrict_solution(fac_ctx *ctx, int fid, int dest_ln);
+/* prolongErrorAndCorrect (CellPoissonFACOps.C:1254-1304). */
+int fac_prolong_correct(fac_ctx *ctx, int fid_src, int fid_dst, int dest_ln);
+/* computeVectorWeights (CellPoissonFACOps.C:2005-2102) into FAC_W. */
+int fac_compute_weights(fac_ctx *ctx);
+/* SAMRAIVectorReal::RMSNorm (SAMRAIVectorReal.C:821-840) over all levels;
+ * norms: one double per problem. */
+int fac_rms_norm(fac_ctx *ctx, int fid, double *norms);
+/* solveCoarsestLevel (CellPoissonFACOps.C:1681-1730). */
+int fac_solve_coarsest(fac_ctx *ctx, int *sweeps);
+/* One FACPreconditioner::facCycle_Recursive V-cycle (FACPreconditioner.C:
+ * 462-518) on e = FAC_E, r = FAC_R. */
+int fac_fac_cycle(fac_ctx *ctx);
+
+/* ---- solver (CellPoissonFACSolver::solveSystem, CellPoissonFACSolver.C:
+ *      310-352, over FACPreconditioner::solveSystem FACPreconditioner.C:
+ *      277-452).  u (FAC_U) and f (FAC_F) must be resident.
+ * converged, iterations, residual: one entry per problem (may be NULL). */
+int fac_solve(fac_ctx *ctx, int *converged, int *iterations,
+              double *residual);
+
+/* Solve from host memory: uploads f (and u0, when not NULL) for every
+ * problem and level, solves, and downloads u.  Array k of f_host/u_host
+ * holds level (k % nlev) of problem (k / nlev) in the host layout. */
+int fac_solve_host(fac_ctx *ctx, const double *const *f_host,
+                   const double *const *u0_host, double *const *u_host,
+                   int *converged, int *iterations, double *residual);
+
+/* Per-cycle residual norms of the last fac_solve for one problem:
+ * hist[0] = before the first cycle, hist[k] after cycle k; *n entries. */
+int fac_residual_history(fac_ctx *ctx, int problem, double *hist, int cap,
+                         int *n);
+
+/* Red-black sweeps taken by coarsest-level solves since the last reset,
+ * per problem (long long each). */
+int fac_coarse_sweeps(fac_ctx *ctx, long long *sweeps);
+int fac_reset_stats(fac_ctx *ctx);
+
+/* Synchronise the context's stream. */
+int fac_synchronize(fac_ctx *ctx);
+
+/* ---- instrumentation (the reference's tbox::Timer around each FAC op,
+ *      CellPoissonFACOps.C:626-639, as CUDA events on the context stream). */
+
+/* Kernels launched by this process so far, over all contexts. */
+int fac_kernel_launches(long long *n);
+/* Record CUDA events around every red-black colour pass (kind 0) and
+ * ghost fill (kind 1) from now on; clears earlier records. */
+int fac_profile_enable(fac_ctx *ctx, int on);
+/* Totals over the records of one kind: launches, device milliseconds and
+ * algorithmic bytes (colour pass: 8*(ghosted cells + cells) + 8*dim*cells
+ * when D is variable; ghost fill: 16 bytes per ghost cell written). */
+int fac_profile_read(fac_ctx *ctx, int kind, long long *launches, double *ms,
+                     double *bytes);
+int fac_profile_reset(fac_ctx *ctx);
+/* Device timer on the context stream: stop = 0 records the start event;
+ * stop = 1 records the end event, waits for it and returns milliseconds. */
+int fac_timer(fac_ctx *ctx, int stop, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,2021 @@
+// Host side of the FAC hot path: hierarchy tables (the device form of
+// SAMRAI's refine/coarsen schedules), the FAC algorithm
+// (FACPreconditioner + CellPoissonFACOps) and the C ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/samrai_fac_b200.h"
+#include "fac_internal.h"
+#include "fac_kernels.h"
+
+namespace samrai_b200 {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_last_error;
+// Host-only mode (device index -1): tables are built and validated but no
+// device memory is allocated and no kernel can run.
+static thread_local bool g_dry = false;
+
+struct FacError : std::runtime_error {
+   int code;
+   FacError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CUDA_CHECK(x)                                                             \
+   do {                                                                           \
+      cudaError_t _e = (x);                                                       \
+      if (_e != cudaSuccess)                                                      \
+         throw FacError(FAC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); \
+   } while (0)
+
+// ---------------------------------------------------------------------------
+// box algebra (hier::Box semantics: inclusive lower/upper corners)
+// ---------------------------------------------------------------------------
+
+struct Box {
+   int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+   bool empty() const { return lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]; }
+   long long size() const
+   {
+      if (empty()) return 0;
+      return (long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+   }
+   bool contains(int i, int j, int k) const
+   {
+      return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+   }
+};
+
+static Box isect(const Box &a, const Box &b)
+{
+   Box r;
+   for (int d = 0; d < 3; ++d) {
+      r.lo[d] = std::max(a.lo[d], b.lo[d]);
+      r.hi[d] = std::min(a.hi[d], b.hi[d]);
+   }
+   return r;
+}
+
+static Box grow(Box b, int dim, int g)
+{
+   for (int a = 0; a < dim; ++a) {
+      b.lo[a] -= g;
+      b.hi[a] += g;
+   }
+   return b;
+}
+
+static int coarsen_index(int i, int r) { return i < 0 ? (i + 1) / r - 1 : i / r; }
+
+static Box coarsen(Box b, int dim, const int *r)
+{
+   for (int a = 0; a < dim; ++a) {
+      b.lo[a] = coarsen_index(b.lo[a], r[a]);
+      b.hi[a] = coarsen_index(b.hi[a], r[a]);
+   }
+   return b;
+}
+
+static Box refine(Box b, int dim, const int *r)
+{
+   for (int a = 0; a < dim; ++a) {
+      b.lo[a] = b.lo[a] * r[a];
+      b.hi[a] = (b.hi[a] + 1) * r[a] - 1;
+   }
+   return b;
+}
+
+// a minus b as a list of disjoint boxes
+static void subtract(const Box &a, const Box &b, std::vector<Box> &out)
+{
+   Box I = isect(a, b);
+   if (I.empty()) {
+      out.push_back(a);
+      return;
+   }
+   Box rem = a;
+   for (int d = 0; d < 3; ++d) {
+      if (rem.lo[d] < I.lo[d]) {
+         Box piece = rem;
+         piece.hi[d] = I.lo[d] - 1;
+         out.push_back(piece);
+         rem.lo[d] = I.lo[d];
+      }
+      if (rem.hi[d] > I.hi[d]) {
+         Box piece = rem;
+         piece.lo[d] = I.hi[d] + 1;
+         out.push_back(piece);
+         rem.hi[d] = I.hi[d];
+      }
+   }
+}
+
+static void subtract_all(std::vector<Box> &region, const Box &b)
+{
+   std::vector<Box> out;
+   for (const Box &r : region) subtract(r, b, out);
+   region.swap(out);
+}
+
+static ArrDesc make_desc(long long base, const Box &gb)
+{
+   ArrDesc d;
+   d.base = base;
+   for (int a = 0; a < 3; ++a) {
+      d.lo[a] = gb.lo[a];
+      d.n[a] = gb.hi[a] - gb.lo[a] + 1;
+   }
+   return d;
+}
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+
+template <class T>
+struct DevArray {
+   T *p = nullptr;
+   size_t n = 0;
+   void alloc(size_t count)
+   {
+      free();
+      n = count;
+      if (g_dry) return;
+      if (count) {
+         cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+         if (e != cudaSuccess) {
+            p = nullptr;
+            throw FacError(FAC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+         }
+      }
+   }
+   void upload(const std::vector<T> &v, cudaStream_t s)
+   {
+      alloc(v.size());
+      if (!v.empty() && !g_dry)
+         CUDA_CHECK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+   }
+   void free()
+   {
+      if (p) cudaFree(p);
+      p = nullptr;
+      n = 0;
+   }
+   ~DevArray() { free(); }
+   DevArray() = default;
+   DevArray(const DevArray &) = delete;
+   DevArray &operator=(const DevArray &) = delete;
+};
+
+template <class I>
+struct ItemList {
+   std::vector<I> items;
+   std::vector<Chunk> chunks;
+   DevArray<I> d_items;
+   DevArray<Chunk> d_chunks;
+   void add(const I &it, long long ncells, int aux = 0)
+   {
+      const int id = (int)items.size();
+      items.push_back(it);
+      for (long long b = 0; b < ncells; b += kChunk) {
+         Chunk c;
+         c.patch = id;
+         c.begin = (int)b;
+         c.count = (int)std::min<long long>(kChunk, ncells - b);
+         c.aux = aux;
+         chunks.push_back(c);
+      }
+   }
+   void upload(cudaStream_t s)
+   {
+      d_items.upload(items, s);
+      d_chunks.upload(chunks, s);
+   }
+   int nchunks() const { return (int)chunks.size(); }
+   void clear()
+   {
+      items.clear();
+      chunks.clear();
+      d_items.free();
+      d_chunks.free();
+   }
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+struct HostProblem {
+   int n0[3];
+   double xlo[3], xup[3];
+   int nlev;
+   int ratio[kMaxLevels][3];
+   std::vector<Box> boxes[kMaxLevels];
+};
+
+struct LevelState {
+   int npatch = 0;
+   std::vector<PatchDesc> hp;
+   std::vector<Box> box;               // patch boxes
+   std::vector<int> prob_patch_begin;  // size nprob+1
+   long long n1 = 0, n0 = 0, ns = 0, no = 0;
+   std::vector<long long> prob_off1, prob_off0, prob_offs, prob_offo;  // size nprob+1
+   int ratio[3] = {1, 1, 1};
+   double tranwt[3] = {0, 0, 0}, longwt[3] = {0, 0, 0};
+   double rb_bytes = 0, fill_bytes = 0;  // algorithmic bytes per launch
+   std::vector<Box> domain;            // per problem
+   std::vector<double> dx;             // per problem x3
+
+   DevArray<PatchDesc> d_patches;
+   DevArray<double> u, e, f, r, tr, w, c, d, flux, oflux, cfflux;
+   DevArray<unsigned char> cfmask;
+   DevArray<int> d_ratio;
+
+   // work chunks
+   std::vector<Chunk> cell_chunks, slot_chunks, flux_chunks;
+   DevArray<Chunk> d_cell_chunks, d_slot_chunks, d_flux_chunks;
+   std::vector<int> prob_cell_chunk_begin;
+   DevArray<int> d_prob_cell_chunk_begin;
+   DevArray<double2> norm_partial;
+
+   ItemList<FillItem> fill_nc, fill_wc;   // ghost fill without / with coarser level
+   std::vector<CfFace> cf;
+   DevArray<CfFace> d_cf;
+   ItemList<RestrictItem> restrict_g1, restrict_g0;  // from level ln+1 into this
+   ItemList<FluxCoarsenItem> fcoarsen;               // from level ln+1 into this
+   ItemList<FillItem> tmp_fill;                      // coarse interpolation arrays
+   ItemList<ProlongItem> prolong;                    // from level ln-1 into this
+   DevArray<double> tmp;
+   DevArray<double> dxc_prob;                        // per problem dx of level ln-1
+   DevArray<unsigned long long> maxres_red, maxres_blk;
+   DevArray<int> last_patch;
+   std::vector<long long> dir_idx;
+   DevArray<long long> d_dir_idx;
+   DevArray<double> dir_cache;
+};
+
+}  // namespace samrai_b200
+
+using namespace samrai_b200;
+
+struct fac_ctx {
+   int dim = 2;
+   int device = 0;
+   cudaStream_t stream = nullptr;
+   bool initialized = false;
+   std::vector<HostProblem> probs;
+   int nlev = 0;
+   PoissonSpec spec{0, 0, 1.0, 0.0};
+   BcCoefs bc;
+   // FACPreconditioner / CellPoissonFACOps parameters (reference defaults,
+   // FACPreconditioner.C:37-48 and CellPoissonFACOps.C:588-600)
+   int max_cycles = 10;
+   double residual_tol = 1e-6;
+   double rel_residual_tol = -1.0;
+   int pre_sweeps = 1, post_sweeps = 1;
+   double coarse_tol = 1e-8;
+   int coarse_max_it = 500;
+   int ewing = 1;
+   int check_interval = 8;   // sweeps between host checks of convergence flags
+
+   // optional per-kernel timing with CUDA events on the context stream
+   struct ProfRec {
+      int kind;
+      cudaEvent_t a, b;
+      double bytes;
+   };
+   bool profiling = false;
+   std::vector<ProfRec> prof;
+   std::vector<cudaEvent_t> ev_pool;
+   size_t ev_next = 0;
+   cudaEvent_t t0 = nullptr, t1 = nullptr;
+
+   LevelState L[kMaxLevels];
+   DevArray<int> active, run;
+   DevArray<long long> sweeps_call, sweeps_coarse;
+   DevArray<double2> norm_acc;
+   std::vector<std::vector<double>> hist;  // per problem residual history
+
+   ~fac_ctx()
+   {
+      for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+      if (t0) cudaEventDestroy(t0);
+      if (t1) cudaEventDestroy(t1);
+   }
+};
+
+namespace {
+
+int nprob(const fac_ctx *c) { return (int)c->probs.size(); }
+
+cudaEvent_t next_event(fac_ctx *c)
+{
+   if (c->ev_next == c->ev_pool.size()) {
+      cudaEvent_t e;
+      CUDA_CHECK(cudaEventCreate(&e));
+      c->ev_pool.push_back(e);
+   }
+   return c->ev_pool[c->ev_next++];
+}
+
+// Record the start of a profiled launch; returns its index or -1.
+int prof_begin(fac_ctx *c, int kind, double bytes)
+{
+   if (!c->profiling) return -1;
+   fac_ctx::ProfRec r;
+   r.kind = kind;
+   r.bytes = bytes;
+   r.a = next_event(c);
+   r.b = next_event(c);
+   CUDA_CHECK(cudaEventRecord(r.a, c->stream));
+   c->prof.push_back(r);
+   return (int)c->prof.size() - 1;
+}
+
+void prof_end(fac_ctx *c, int idx)
+{
+   if (idx < 0) return;
+   CUDA_CHECK(cudaEventRecord(c->prof[idx].b, c->stream));
+}
+
+double *field_ptr(LevelState &L, int fid)
+{
+   switch (fid) {
+      case FAC_U: return L.u.p;
+      case FAC_F: return L.f.p;
+      case FAC_E: return L.e.p;
+      case FAC_R: return L.r.p;
+      case FAC_TR: return L.tr.p;
+      case FAC_W: return L.w.p;
+      case FAC_C: return L.c.p;
+   }
+   throw FacError(FAC_ERR_ARG, "bad field id");
+}
+
+int field_ghost(int fid)
+{
+   if (fid < 0 || fid > FAC_C) throw FacError(FAC_ERR_ARG, "bad field id");
+   return (fid == FAC_U || fid == FAC_E) ? 1 : 0;
+}
+
+Box ghost_box(int dim, const Box &b, int g) { return grow(b, dim, g); }
+
+long long cell_count(int dim, const Box &b, int g) { return ghost_box(dim, b, g).size(); }
+
+Box side_box(const Box &b, int a)
+{
+   Box s = b;
+   s.hi[a] += 1;
+   return s;
+}
+
+Box face_box(const Box &b, int a, int s)
+{
+   Box f = side_box(b, a);
+   if (s == 0) f.hi[a] = f.lo[a];
+   else f.lo[a] = f.hi[a];
+   return f;
+}
+
+void check_state(fac_ctx *c, bool need_init)
+{
+   if (!c) throw FacError(FAC_ERR_ARG, "null context");
+   if (need_init && !c->initialized) throw FacError(FAC_ERR_STATE, "fac_initialize not called");
+   if (!need_init && c->initialized) throw FacError(FAC_ERR_STATE, "context already initialized");
+}
+
+void check_ops(fac_ctx *c)
+{
+   check_state(c, true);
+   if (c->device < 0)
+      throw FacError(FAC_ERR_STATE, "host-only context (device -1) cannot run operations");
+}
+
+// ---------------------------------------------------------------------------
+// table construction (CellPoissonFACOps::initializeOperatorState)
+// ---------------------------------------------------------------------------
+
+void build_level_layout(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   const int np = nprob(c);
+   L.hp.clear();
+   L.box.clear();
+   L.prob_patch_begin.assign(np + 1, 0);
+   L.prob_off1.assign(np + 1, 0);
+   L.prob_off0.assign(np + 1, 0);
+   L.prob_offs.assign(np + 1, 0);
+   L.prob_offo.assign(np + 1, 0);
+   L.domain.resize(np);
+   L.dx.assign(3 * np, 1.0);
+   for (int a = 0; a < 3; ++a) L.ratio[a] = c->probs[0].ratio[ln][a];
+   long long o1 = 0, o0 = 0, os = 0, oo = 0;
+   for (int p = 0; p < np; ++p) {
+      const HostProblem &P = c->probs[p];
+      L.prob_patch_begin[p] = (int)L.hp.size();
+      L.prob_off1[p] = o1;
+      L.prob_off0[p] = o0;
+      L.prob_offs[p] = os;
+      L.prob_offo[p] = oo;
+      int rz[3] = {1, 1, 1};
+      for (int l = 1; l <= ln; ++l)
+         for (int a = 0; a < 3; ++a) rz[a] *= P.ratio[l][a];
+      Box dom;
+      for (int a = 0; a < 3; ++a) {
+         dom.lo[a] = 0;
+         dom.hi[a] = a < dim ? P.n0[a] * rz[a] - 1 : 0;
+         // CartesianGridGeometry.C:308-312, 373-379
+         const double dx0 = a < dim ? (P.xup[a] - P.xlo[a]) / ((double)P.n0[a]) : 1.0;
+         L.dx[3 * p + a] = a < dim ? dx0 / ((double)rz[a]) : 1.0;
+      }
+      L.domain[p] = dom;
+      for (const Box &b : P.boxes[ln]) {
+         PatchDesc d;
+         std::memset(&d, 0, sizeof(d));
+         for (int a = 0; a < 3; ++a) {
+            d.lo[a] = b.lo[a];
+            d.hi[a] = b.hi[a];
+            d.dx[a] = L.dx[3 * p + a];
+         }
+         d.prob = p;
+         d.flags = 0;
+         d.off1 = o1;
+         d.off0 = o0;
+         o1 += cell_count(dim, b, 1);
+         o0 += cell_count(dim, b, 0);
+         for (int a = 0; a < 3; ++a) {
+            d.offs[a] = os;
+            if (a < dim) os += side_box(b, a).size();
+         }
+         for (int a = 0; a < 3; ++a)
+            for (int s = 0; s < 2; ++s) {
+               d.offo[a][s] = oo;
+               if (a < dim) oo += face_box(b, a, s).size();
+            }
+         L.hp.push_back(d);
+         L.box.push_back(b);
+      }
+   }
+   L.prob_patch_begin[np] = (int)L.hp.size();
+   L.prob_off1[np] = o1;
+   L.prob_off0[np] = o0;
+   L.prob_offs[np] = os;
+   L.prob_offo[np] = oo;
+   L.npatch = (int)L.hp.size();
+   L.n1 = o1;
+   L.n0 = o0;
+   L.ns = os;
+   L.no = oo;
+   for (int a = 0; a < 3; ++a) {
+      // ewingfixflux*: tranwt = 1.0/(1+r) in REAL*4 (2d.f:502), longwt = 2*tranwt
+      L.tranwt[a] = (double)(1.0f / (float)(1 + L.ratio[a]));
+      L.longwt[a] = 2 * L.tranwt[a];
+   }
+}
+
+ArrDesc patch_desc(const fac_ctx *c, const LevelState &L, int ip, int g)
+{
+   const Box gb = ghost_box(c->dim, L.box[ip], g);
+   return make_desc(g ? L.hp[ip].off1 : L.hp[ip].off0, gb);
+}
+
+// Boxes of ghost cells of box b whose outside pattern is `side`
+// (physical boundary, trimmed to b's extent on the other axes).
+bool bc_box(int dim, const Box &b, const Box &dom, const int *side, Box &out)
+{
+   out = b;
+   for (int a = 0; a < 3; ++a) {
+      if (a >= dim) {
+         if (side[a]) return false;
+         continue;
+      }
+      if (side[a] < 0) {
+         if (b.lo[a] != dom.lo[a]) return false;
+         out.lo[a] = out.hi[a] = b.lo[a] - 1;
+      } else if (side[a] > 0) {
+         if (b.hi[a] != dom.hi[a]) return false;
+         out.lo[a] = out.hi[a] = b.hi[a] + 1;
+      }
+   }
+   return true;
+}
+
+std::vector<std::array<int, 3>> all_sides(int dim)
+{
+   std::vector<std::array<int, 3>> v;
+   for (int z = (dim == 3 ? -1 : 0); z <= (dim == 3 ? 1 : 0); ++z)
+      for (int y = -1; y <= 1; ++y)
+         for (int x = -1; x <= 1; ++x) {
+            if (!x && !y && !z) continue;
+            v.push_back({x, y, z});
+         }
+   return v;
+}
+
+void build_fill_tables(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   const int np = nprob(c);
+   L.fill_nc.clear();
+   L.fill_wc.clear();
+   auto sides = all_sides(dim);
+   for (int p = 0; p < np; ++p) {
+      const int pb = L.prob_patch_begin[p], pe = L.prob_patch_begin[p + 1];
+      for (int ip = pb; ip < pe; ++ip) {
+         const Box gb = ghost_box(dim, L.box[ip], 1);
+         const ArrDesc dst = patch_desc(c, L, ip, 1);
+         // same-level copies (CellGeometry overlap: dst ghost box x src box)
+         for (int iq = pb; iq < pe; ++iq) {
+            if (iq == ip) continue;
+            Box ov = isect(gb, L.box[iq]);
+            if (ov.empty()) continue;
+            FillItem it;
+            std::memset(&it, 0, sizeof(it));
+            it.kind = kFillCopy;
+            it.prob = p;
+            for (int a = 0; a < 3; ++a) {
+               it.lo[a] = ov.lo[a];
+               it.hi[a] = ov.hi[a];
+            }
+            it.dst = dst;
+            it.src = patch_desc(c, L, iq, 1);
+            L.fill_nc.add(it, ov.size());
+            L.fill_wc.add(it, ov.size());
+         }
+         // physical boundary
+         for (auto &s : sides) {
+            Box bb;
+            if (!bc_box(dim, L.box[ip], L.domain[p], s.data(), bb)) continue;
+            FillItem it;
+            std::memset(&it, 0, sizeof(it));
+            it.kind = kFillBc;
+            it.prob = p;
+            for (int a = 0; a < 3; ++a) {
+               it.lo[a] = bb.lo[a];
+               it.hi[a] = bb.hi[a];
+               it.side[a] = s[a];
+               it.h[a] = L.dx[3 * p + a];
+            }
+            it.dst = dst;
+            it.src = dst;
+            L.fill_nc.add(it, bb.size());
+            L.fill_wc.add(it, bb.size());
+         }
+         // coarse-level fill of ghost cells not covered by the level
+         if (ln > 0) {
+            const LevelState &C = c->L[ln - 1];
+            std::vector<Box> region{isect(gb, L.domain[p])};
+            for (int iq = pb; iq < pe; ++iq) subtract_all(region, L.box[iq]);
+            const int cb = C.prob_patch_begin[p], ce = C.prob_patch_begin[p + 1];
+            for (const Box &rg : region) {
+               if (rg.empty()) continue;
+               std::vector<Box> left{rg};
+               for (int iq = cb; iq < ce; ++iq) {
+                  Box fr = refine(C.box[iq], dim, L.ratio);
+                  Box sub = isect(rg, fr);
+                  if (sub.empty()) continue;
+                  subtract_all(left, fr);
+                  FillItem it;
+                  std::memset(&it, 0, sizeof(it));
+                  it.kind = kFillCoarse;
+                  it.prob = p;
+                  for (int a = 0; a < 3; ++a) {
+                     it.lo[a] = sub.lo[a];
+                     it.hi[a] = sub.hi[a];
+                     it.ratio[a] = L.ratio[a];
+                  }
+                  it.dst = dst;
+                  it.src = patch_desc(c, C, iq, 1);
+                  it.src_is_coarse = 1;
+                  L.fill_wc.add(it, sub.size());
+               }
+               for (const Box &lb : left)
+                  if (!lb.empty())
+                     throw FacError(FAC_ERR_NESTING, "level " + std::to_string(ln) +
+                                                          " is not properly nested");
+            }
+         }
+      }
+   }
+}
+
+void build_cf_faces(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   std::vector<unsigned char> mask(L.no, 0);
+   L.cf.clear();
+   if (ln == 0) {
+      L.cfmask.upload(mask, c->stream);
+      return;
+   }
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      PatchDesc &d = L.hp[ip];
+      const int p = d.prob;
+      const int pb = L.prob_patch_begin[p], pe = L.prob_patch_begin[p + 1];
+      const Box &b = L.box[ip];
+      const Box gb1 = ghost_box(dim, b, 1);
+      auto c1 = [&](int i, int j, int k) {
+         const long long nx = gb1.hi[0] - gb1.lo[0] + 1, ny = gb1.hi[1] - gb1.lo[1] + 1;
+         return d.off1 + (i - gb1.lo[0]) + nx * ((j - gb1.lo[1]) + ny * (k - gb1.lo[2]));
+      };
+      for (int a = 0; a < dim; ++a)
+         for (int s = 0; s < 2; ++s) {
+            Box layer = b;
+            const int g = s == 0 ? b.lo[a] - 1 : b.hi[a] + 1;
+            layer.lo[a] = layer.hi[a] = g;
+            std::vector<Box> region{isect(layer, L.domain[p])};
+            for (int iq = pb; iq < pe; ++iq) subtract_all(region, L.box[iq]);
+            const Box fb = face_box(b, a, s);
+            const Box sb = side_box(b, a);
+            for (const Box &rg : region)
+               for (int k = rg.lo[2]; k <= rg.hi[2]; ++k)
+                  for (int j = rg.lo[1]; j <= rg.hi[1]; ++j)
+                     for (int i = rg.lo[0]; i <= rg.hi[0]; ++i) {
+                        int cc[3] = {i, j, k};
+                        cc[a] = s == 0 ? b.lo[a] : b.hi[a];
+                        int fc[3] = {cc[0], cc[1], cc[2]};
+                        if (s == 1) fc[a] += 1;
+                        int mq[3] = {cc[0], cc[1], cc[2]};
+                        for (int t = 0; t < dim; ++t) {
+                           if (t == a) continue;
+                           const int rr = L.ratio[t];
+                           const int base = coarsen_index(cc[t], rr) * rr;
+                           mq[t] = base + (rr - (cc[t] - base) - 1);
+                           if (mq[t] < b.lo[t] || mq[t] > b.hi[t])
+                              throw FacError(FAC_ERR_NESTING,
+                                             "patch box not aligned to the refinement ratio");
+                        }
+                        CfFace f;
+                        std::memset(&f, 0, sizeof(f));
+                        f.cell = c1(cc[0], cc[1], cc[2]);
+                        f.mirror = c1(mq[0], mq[1], mq[2]);
+                        f.ghost = c1(i, j, k);
+                        const long long fnx = fb.hi[0] - fb.lo[0] + 1, fny = fb.hi[1] - fb.lo[1] + 1;
+                        const int ti = cc[0] - fb.lo[0], tj = cc[1] - fb.lo[1], tk = cc[2] - fb.lo[2];
+                        long long tlin;
+                        if (a == 0) tlin = tj + (long long)(b.hi[1] - b.lo[1] + 1) * tk;
+                        else if (a == 1) tlin = ti + (long long)(b.hi[0] - b.lo[0] + 1) * tk;
+                        else tlin = ti + (long long)(b.hi[0] - b.lo[0] + 1) * tj;
+                        (void)fnx;
+                        (void)fny;
+                        f.oidx = d.offo[a][s] + tlin;
+                        const long long snx = sb.hi[0] - sb.lo[0] + 1, sny = sb.hi[1] - sb.lo[1] + 1;
+                        f.sidx = d.offs[a] + (fc[0] - sb.lo[0]) +
+                                 snx * ((fc[1] - sb.lo[1]) + sny * (fc[2] - sb.lo[2]));
+                        f.patch = ip;
+                        f.axis = a;
+                        f.side = s;
+                        L.cf.push_back(f);
+                        mask[f.oidx] = 1;
+                        d.flags |= 1;
+                     }
+         }
+   }
+   L.cfmask.upload(mask, c->stream);
+   L.d_cf.upload(L.cf, c->stream);
+}
+
+void build_chunks(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   const int np = nprob(c);
+   L.cell_chunks.clear();
+   L.slot_chunks.clear();
+   L.flux_chunks.clear();
+   L.prob_cell_chunk_begin.assign(np + 1, 0);
+   int cur_prob = -1;
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      const Box &b = L.box[ip];
+      while (cur_prob < L.hp[ip].prob) {
+         ++cur_prob;
+         L.prob_cell_chunk_begin[cur_prob] = (int)L.cell_chunks.size();
+      }
+      const long long n = b.size();
+      for (long long s = 0; s < n; s += kChunk)
+         L.cell_chunks.push_back({ip, (int)s, (int)std::min<long long>(kChunk, n - s), 0});
+      const long long nx = b.hi[0] - b.lo[0] + 1;
+      const long long slots = ((nx + 1) / 2) * (n / nx);
+      for (long long s = 0; s < slots; s += kChunk)
+         L.slot_chunks.push_back({ip, (int)s, (int)std::min<long long>(kChunk, slots - s), 0});
+      for (int a = 0; a < dim; ++a) {
+         const long long ns = side_box(b, a).size();
+         for (long long s = 0; s < ns; s += kChunk)
+            L.flux_chunks.push_back({ip, (int)s, (int)std::min<long long>(kChunk, ns - s), a});
+      }
+   }
+   while (cur_prob < np) {
+      ++cur_prob;
+      L.prob_cell_chunk_begin[cur_prob] = (int)L.cell_chunks.size();
+   }
+   L.d_cell_chunks.upload(L.cell_chunks, c->stream);
+   L.d_slot_chunks.upload(L.slot_chunks, c->stream);
+   L.d_flux_chunks.upload(L.flux_chunks, c->stream);
+   L.d_prob_cell_chunk_begin.upload(L.prob_cell_chunk_begin, c->stream);
+   L.norm_partial.alloc(std::max<size_t>(1, L.cell_chunks.size()));
+   std::vector<int> last(np, 0);
+   for (int p = 0; p < np; ++p) last[p] = L.prob_patch_begin[p + 1] - 1;
+   L.last_patch.upload(last, c->stream);
+   L.maxres_red.alloc(std::max(1, L.npatch));
+   L.maxres_blk.alloc(std::max(1, L.npatch));
+   // one colour pass reads u over the ghosted boxes, f at the active half,
+   // writes u at the active half, and reads D on all faces when variable
+   double n = 0, ng = 0;
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      n += (double)L.box[ip].size();
+      ng += (double)cell_count(dim, L.box[ip], 1);
+   }
+   L.rb_bytes = 8.0 * (ng + n) + (c->spec.d_variable ? 8.0 * dim * n : 0.0) +
+                (c->spec.c_kind == 2 ? 4.0 * n : 0.0);
+   double gcells = 0;
+   for (const FillItem &it : L.fill_nc.items) {
+      Box b;
+      for (int a = 0; a < 3; ++a) {
+         b.lo[a] = it.lo[a];
+         b.hi[a] = it.hi[a];
+      }
+      gcells += (double)b.size();
+   }
+   L.fill_bytes = 16.0 * gcells;
+}
+
+// Inter-level tables with the next finer level (restriction, flux coarsening).
+void build_coarsen_tables(fac_ctx *c, int ln)
+{
+   LevelState &C = c->L[ln];
+   LevelState &Fl = c->L[ln + 1];
+   const int dim = c->dim;
+   const int np = nprob(c);
+   C.restrict_g1.clear();
+   C.restrict_g0.clear();
+   C.fcoarsen.clear();
+   const int *r = Fl.ratio;
+   const int raux = r[0] | (r[1] << 8) | ((dim == 3 ? r[2] : 1) << 16);
+   for (int p = 0; p < np; ++p) {
+      const int fb = Fl.prob_patch_begin[p], fe = Fl.prob_patch_begin[p + 1];
+      const int cb = C.prob_patch_begin[p], ce = C.prob_patch_begin[p + 1];
+      for (int ip = fb; ip < fe; ++ip) {
+         const Box cbox = coarsen(Fl.box[ip], dim, r);
+         for (int iq = cb; iq < ce; ++iq) {
+            for (int g = 0; g < 2; ++g) {
+               Box ov = isect(cbox, ghost_box(dim, C.box[iq], g));
+               if (ov.empty()) continue;
+               RestrictItem it;
+               it.prob = p;
+               it.fine_patch = ip;
+               it.coarse_patch = iq;
+               for (int a = 0; a < 3; ++a) {
+                  it.lo[a] = ov.lo[a];
+                  it.hi[a] = ov.hi[a];
+               }
+               (g ? C.restrict_g1 : C.restrict_g0).add(it, ov.size(), raux);
+            }
+         }
+         for (int a = 0; a < dim; ++a) {
+            int t0 = -1, t1 = -1;
+            for (int t = 0; t < dim; ++t)
+               if (t != a) {
+                  if (t0 < 0) t0 = t;
+                  else t1 = t;
+               }
+            for (int s = 0; s < 2; ++s) {
+               Box T = cbox;
+               const int cf = s == 0 ? cbox.lo[a] : cbox.hi[a] + 1;
+               T.lo[a] = T.hi[a] = cf;
+               for (int iq = cb; iq < ce; ++iq) {
+                  Box ov = isect(T, side_box(C.box[iq], a));
+                  if (ov.empty()) continue;
+                  FluxCoarsenItem it;
+                  it.prob = p;
+                  it.axis = a;
+                  it.side = s;
+                  it.fine_patch = ip;
+                  it.coarse_patch = iq;
+                  for (int d = 0; d < 3; ++d) {
+                     it.lo[d] = ov.lo[d];
+                     it.hi[d] = ov.hi[d];
+                  }
+                  it.fface = s == 0 ? Fl.box[ip].lo[a] : Fl.box[ip].hi[a] + 1;
+                  it.t0 = t0;
+                  it.t1 = t1;
+                  const int aux = r[t0] | ((t1 >= 0 ? r[t1] : 1) << 8);
+                  C.fcoarsen.add(it, ov.size(), aux);
+               }
+            }
+         }
+      }
+   }
+   C.restrict_g1.upload(c->stream);
+   C.restrict_g0.upload(c->stream);
+   C.fcoarsen.upload(c->stream);
+}
+
+// Coarse interpolation arrays for prolongation into level ln
+// (RefineSchedule coarse interpolation level, RefineSchedule.C:1353-1560).
+void build_prolong_tables(fac_ctx *c, int ln)
+{
+   LevelState &Fl = c->L[ln];
+   LevelState &C = c->L[ln - 1];
+   const int dim = c->dim;
+   Fl.tmp_fill.clear();
+   Fl.prolong.clear();
+   auto sides = all_sides(dim);
+   long long toff = 0;
+   for (int ip = 0; ip < Fl.npatch; ++ip) {
+      const int p = Fl.hp[ip].prob;
+      const Box fill = ghost_box(dim, Fl.box[ip], 1);
+      const Box B = isect(coarsen(fill, dim, Fl.ratio), C.domain[p]);
+      const Box Bg = ghost_box(dim, B, 1);
+      const ArrDesc T = make_desc(toff, Bg);
+      toff += Bg.size();
+      const int cb = C.prob_patch_begin[p], ce = C.prob_patch_begin[p + 1];
+      for (int iq = cb; iq < ce; ++iq) {
+         Box ov = isect(Bg, C.box[iq]);
+         if (ov.empty()) continue;
+         FillItem it;
+         std::memset(&it, 0, sizeof(it));
+         it.kind = kFillCopy;
+         it.prob = p;
+         for (int a = 0; a < 3; ++a) {
+            it.lo[a] = ov.lo[a];
+            it.hi[a] = ov.hi[a];
+         }
+         it.dst = T;
+         it.src = patch_desc(c, C, iq, 1);
+         it.src_is_coarse = 1;
+         Fl.tmp_fill.add(it, ov.size());
+      }
+      for (auto &s : sides) {
+         Box bb;
+         if (!bc_box(dim, B, C.domain[p], s.data(), bb)) continue;
+         Box inward = bb;
+         for (int a = 0; a < 3; ++a) {
+            inward.lo[a] -= s[a];
+            inward.hi[a] -= s[a];
+         }
+         for (int iq = cb; iq < ce; ++iq) {
+            Box sub = isect(inward, C.box[iq]);
+            if (sub.empty()) continue;
+            FillItem it;
+            std::memset(&it, 0, sizeof(it));
+            it.kind = kFillBc;
+            it.prob = p;
+            for (int a = 0; a < 3; ++a) {
+               it.lo[a] = sub.lo[a] + s[a];
+               it.hi[a] = sub.hi[a] + s[a];
+               it.side[a] = s[a];
+               it.h[a] = C.dx[3 * p + a];
+            }
+            it.dst = T;
+            it.src = patch_desc(c, C, iq, 1);
+            it.src_is_coarse = 1;
+            Fl.tmp_fill.add(it, sub.size());
+         }
+      }
+      ProlongItem pi;
+      pi.prob = p;
+      pi.fine_patch = ip;
+      pi.tmp = T;
+      Fl.prolong.add(pi, Fl.box[ip].size());
+   }
+   Fl.tmp.alloc(std::max<long long>(1, toff));
+   // cells of the interpolation array that nothing fills stay NaN
+   if (!g_dry)
+      CUDA_CHECK(cudaMemsetAsync(Fl.tmp.p, 0xff, Fl.tmp.n * sizeof(double), c->stream));
+   Fl.tmp_fill.upload(c->stream);
+   Fl.prolong.upload(c->stream);
+   std::vector<double> dxc(3 * nprob(c));
+   for (int p = 0; p < nprob(c); ++p)
+      for (int a = 0; a < 3; ++a) dxc[3 * p + a] = C.dx[3 * p + a];
+   Fl.dxc_prob.upload(dxc, c->stream);
+}
+
+// Cells of the codimension-1 physical boundary boxes of u (untrimmed:
+// BaseGridGeometry::getBoundaryBoxes grows them one cell tangentially),
+// saved and restored by SimpleCellRobinBcCoefs::cacheDirichletData /
+// restoreDirichletData.
+void build_dirichlet_index(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   L.dir_idx.clear();
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      const int p = L.hp[ip].prob;
+      const Box &b = L.box[ip];
+      const Box &dom = L.domain[p];
+      const Box gb = ghost_box(dim, b, 1);
+      const long long nx = gb.hi[0] - gb.lo[0] + 1, ny = gb.hi[1] - gb.lo[1] + 1;
+      for (int k = gb.lo[2]; k <= gb.hi[2]; ++k)
+         for (int j = gb.lo[1]; j <= gb.hi[1]; ++j)
+            for (int i = gb.lo[0]; i <= gb.hi[0]; ++i) {
+               const int cc[3] = {i, j, k};
+               int out = 0;
+               bool ok = true;
+               for (int a = 0; a < dim; ++a)
+                  if (cc[a] < dom.lo[a] || cc[a] > dom.hi[a]) {
+                     ++out;
+                     if (!((cc[a] == b.lo[a] - 1 && b.lo[a] == dom.lo[a]) ||
+                           (cc[a] == b.hi[a] + 1 && b.hi[a] == dom.hi[a])))
+                        ok = false;
+                  }
+               if (!ok || out != 1) continue;
+               L.dir_idx.push_back(L.hp[ip].off1 + (i - gb.lo[0]) +
+                                   nx * ((j - gb.lo[1]) + ny * (k - gb.lo[2])));
+            }
+   }
+   L.d_dir_idx.upload(L.dir_idx, c->stream);
+   L.dir_cache.alloc(std::max<size_t>(1, L.dir_idx.size()));
+}
+
+// CellPoissonFACOps::computeVectorWeights (CellPoissonFACOps.C:2005-2102).
+void compute_weights_host(fac_ctx *c)
+{
+   if (g_dry) return;
+   const int dim = c->dim;
+   for (int ln = c->nlev - 1; ln >= 0; --ln) {
+      LevelState &L = c->L[ln];
+      std::vector<double> w(std::max<long long>(1, L.n0), 0.0);
+      for (int ip = 0; ip < L.npatch; ++ip) {
+         const int p = L.hp[ip].prob;
+         double vol = L.dx[3 * p + 0];
+         vol *= L.dx[3 * p + 1];
+         if (dim > 2) vol *= L.dx[3 * p + 2];
+         const Box &b = L.box[ip];
+         const long long n = b.size();
+         for (long long t = 0; t < n; ++t) w[L.hp[ip].off0 + t] = vol;
+         if (ln < c->nlev - 1) {
+            LevelState &Fl = c->L[ln + 1];
+            const long long nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+            for (int iq = Fl.prob_patch_begin[p]; iq < Fl.prob_patch_begin[p + 1]; ++iq) {
+               Box ov = isect(coarsen(Fl.box[iq], dim, Fl.ratio), b);
+               if (ov.empty()) continue;
+               for (int k = ov.lo[2]; k <= ov.hi[2]; ++k)
+                  for (int j = ov.lo[1]; j <= ov.hi[1]; ++j)
+                     for (int i = ov.lo[0]; i <= ov.hi[0]; ++i)
+                        w[L.hp[ip].off0 + (i - b.lo[0]) + nx * ((j - b.lo[1]) + ny * (k - b.lo[2]))] =
+                           0.0;
+            }
+         }
+      }
+      CUDA_CHECK(cudaMemcpyAsync(L.w.p, w.data(), L.n0 * sizeof(double), cudaMemcpyHostToDevice,
+                                 c->stream));
+   }
+}
+
+// Host-side bounds check of every device table before any kernel runs:
+// each transaction's destination and source cells must lie inside the
+// arrays they address, and every array inside its buffer.
+void vcheck(bool ok, const char *what)
+{
+   if (!ok) throw FacError(FAC_ERR_ARG, std::string("table validation failed: ") + what);
+}
+
+bool desc_contains(const ArrDesc &d, const Box &b, long long buflen)
+{
+   if (b.empty()) return true;
+   for (int a = 0; a < 3; ++a)
+      if (b.lo[a] < d.lo[a] || b.hi[a] > d.lo[a] + d.n[a] - 1) return false;
+   const long long n = (long long)d.n[0] * d.n[1] * d.n[2];
+   return d.base >= 0 && d.base + n <= buflen;
+}
+
+Box item_box(const int *lo, const int *hi)
+{
+   Box b;
+   for (int a = 0; a < 3; ++a) {
+      b.lo[a] = lo[a];
+      b.hi[a] = hi[a];
+   }
+   return b;
+}
+
+void validate_fill(const ItemList<FillItem> &L, long long dstlen, long long samelen,
+                   long long coarselen)
+{
+   for (const FillItem &it : L.items) {
+      const Box b = item_box(it.lo, it.hi);
+      vcheck(!b.empty(), "empty fill item");
+      vcheck(desc_contains(it.dst, b, dstlen), "fill destination");
+      Box sb = b;
+      if (it.kind == kFillCoarse) {
+         for (int a = 0; a < 3; ++a) {
+            vcheck(it.ratio[a] >= 1, "fill ratio");
+            sb.lo[a] = coarsen_index(b.lo[a], it.ratio[a]);
+            sb.hi[a] = coarsen_index(b.hi[a], it.ratio[a]);
+         }
+      } else if (it.kind == kFillBc) {
+         for (int a = 0; a < 3; ++a) {
+            sb.lo[a] -= it.side[a];
+            sb.hi[a] -= it.side[a];
+         }
+      }
+      vcheck(desc_contains(it.src, sb, it.src_is_coarse ? coarselen : samelen), "fill source");
+   }
+   for (const Chunk &ch : L.chunks) {
+      vcheck(ch.patch >= 0 && ch.patch < (int)L.items.size(), "fill chunk item");
+      const FillItem &it = L.items[ch.patch];
+      vcheck(ch.begin >= 0 && ch.count > 0 &&
+                ch.begin + ch.count <= item_box(it.lo, it.hi).size(),
+             "fill chunk range");
+   }
+}
+
+void validate_tables(fac_ctx *c)
+{
+   const int dim = c->dim;
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      const long long clen = ln > 0 ? c->L[ln - 1].n1 : 0;
+      validate_fill(L.fill_nc, L.n1, L.n1, clen);
+      validate_fill(L.fill_wc, L.n1, L.n1, clen);
+      for (int ip = 0; ip < L.npatch; ++ip) {
+         const PatchDesc &d = L.hp[ip];
+         vcheck(d.off1 + cell_count(dim, L.box[ip], 1) <= L.n1, "patch ghost-1 extent");
+         vcheck(d.off0 + cell_count(dim, L.box[ip], 0) <= L.n0, "patch ghost-0 extent");
+         for (int a = 0; a < dim; ++a) {
+            vcheck(d.offs[a] + side_box(L.box[ip], a).size() <= L.ns, "patch side extent");
+            for (int s = 0; s < 2; ++s)
+               vcheck(d.offo[a][s] + face_box(L.box[ip], a, s).size() <= L.no,
+                      "patch outer-side extent");
+         }
+      }
+      for (const CfFace &f : L.cf) {
+         vcheck(f.cell >= 0 && f.cell < L.n1 && f.mirror >= 0 && f.mirror < L.n1 &&
+                   f.ghost >= 0 && f.ghost < L.n1,
+                "cf cell index");
+         vcheck(f.oidx >= 0 && f.oidx < L.no && f.sidx >= 0 && f.sidx < L.ns, "cf face index");
+      }
+      for (const Chunk &ch : L.cell_chunks)
+         vcheck(ch.patch >= 0 && ch.patch < L.npatch &&
+                   ch.begin + ch.count <= L.box[ch.patch].size(),
+                "cell chunk");
+      for (const Chunk &ch : L.slot_chunks) {
+         const Box &b = L.box[ch.patch];
+         const long long nx = b.hi[0] - b.lo[0] + 1;
+         vcheck(ch.begin + ch.count <= ((nx + 1) / 2) * (b.size() / nx), "slot chunk");
+      }
+      for (const Chunk &ch : L.flux_chunks)
+         vcheck(ch.aux >= 0 && ch.aux < dim &&
+                   ch.begin + ch.count <= side_box(L.box[ch.patch], ch.aux).size(),
+                "flux chunk");
+      if (ln > 0) {
+         LevelState &C = c->L[ln - 1];
+         validate_fill(L.tmp_fill, (long long)L.tmp.n, 0, C.n1);
+         for (const ProlongItem &pi : L.prolong.items) {
+            // linear refine reads coarse cells coarsen(box) -1 .. +1
+            Box need = grow(coarsen(L.box[pi.fine_patch], dim, L.ratio), dim, 1);
+            vcheck(desc_contains(pi.tmp, need, (long long)L.tmp.n), "prolong stencil");
+         }
+      }
+      if (ln + 1 < c->nlev) {
+         LevelState &Fl = c->L[ln + 1];
+         for (int g = 0; g < 2; ++g) {
+            const ItemList<RestrictItem> &R = g ? L.restrict_g1 : L.restrict_g0;
+            for (const RestrictItem &it : R.items) {
+               const Box b = item_box(it.lo, it.hi);
+               vcheck(isect(b, ghost_box(dim, L.box[it.coarse_patch], g)).size() == b.size(),
+                      "restrict destination");
+               vcheck(isect(refine(b, dim, Fl.ratio), Fl.box[it.fine_patch]).size() ==
+                         refine(b, dim, Fl.ratio).size(),
+                      "restrict source");
+            }
+         }
+         for (const FluxCoarsenItem &it : L.fcoarsen.items) {
+            const Box b = item_box(it.lo, it.hi);
+            vcheck(isect(b, side_box(L.box[it.coarse_patch], it.axis)).size() == b.size(),
+                   "flux coarsen destination");
+            Box fb = refine(b, dim, Fl.ratio);
+            fb.lo[it.axis] = fb.hi[it.axis] = it.fface;
+            vcheck(isect(fb, face_box(Fl.box[it.fine_patch], it.axis, it.side)).size() ==
+                      fb.size(),
+                   "flux coarsen source");
+         }
+      }
+   }
+}
+
+void initialize(fac_ctx *c)
+{
+   if (c->probs.empty()) throw FacError(FAC_ERR_STATE, "no problems added");
+   if (!c->ewing) throw FacError(FAC_ERR_ARG, "only cf_discretization Ewing is implemented");
+   c->nlev = c->probs[0].nlev;
+   for (auto &P : c->probs) {
+      if (P.nlev != c->nlev) throw FacError(FAC_ERR_ARG, "problems must share the level count");
+      for (int ln = 0; ln < c->nlev; ++ln)
+         for (int a = 0; a < 3; ++a)
+            if (P.ratio[ln][a] != c->probs[0].ratio[ln][a])
+               throw FacError(FAC_ERR_ARG, "problems must share refinement ratios");
+   }
+   g_dry = c->device < 0;
+   struct DryReset {
+      ~DryReset() { g_dry = false; }
+   } dry_reset;
+   if (!g_dry) CUDA_CHECK(cudaSetDevice(c->device));
+   const int np = nprob(c);
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      build_level_layout(c, ln);
+      const size_t n1 = std::max<long long>(1, L.n1), n0 = std::max<long long>(1, L.n0);
+      L.u.alloc(n1);
+      L.e.alloc(n1);
+      L.f.alloc(n0);
+      L.r.alloc(n0);
+      L.tr.alloc(n0);
+      L.w.alloc(n0);
+      L.c.alloc(c->spec.c_kind == 2 ? n0 : 1);
+      L.d.alloc(c->spec.d_variable ? std::max<long long>(1, L.ns) : 1);
+      L.flux.alloc(std::max<long long>(1, L.ns));
+      L.oflux.alloc(std::max<long long>(1, L.no));
+      L.cfflux.alloc(std::max<long long>(1, L.no));
+      if (!g_dry)
+         for (auto *b : {&L.u, &L.e, &L.f, &L.r, &L.tr, &L.w, &L.c, &L.d, &L.flux, &L.oflux,
+                         &L.cfflux})
+            CUDA_CHECK(cudaMemsetAsync(b->p, 0, b->n * sizeof(double), c->stream));
+      std::vector<int> rr(L.ratio, L.ratio + 3);
+      L.d_ratio.upload(rr, c->stream);
+   }
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      build_fill_tables(c, ln);
+      build_cf_faces(c, ln);
+      build_chunks(c, ln);
+      build_dirichlet_index(c, ln);
+      if (ln > 0) build_prolong_tables(c, ln);
+   }
+   for (int ln = 0; ln + 1 < c->nlev; ++ln) build_coarsen_tables(c, ln);
+   validate_tables(c);
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      L.d_patches.upload(L.hp, c->stream);  // after cf flags are set
+      L.fill_nc.upload(c->stream);
+      L.fill_wc.upload(c->stream);
+   }
+   std::vector<int> ones(np, 1);
+   c->active.upload(ones, c->stream);
+   c->run.upload(ones, c->stream);
+   c->sweeps_call.alloc(np);
+   c->sweeps_coarse.alloc(np);
+   c->norm_acc.alloc(np);
+   c->hist.assign(np, {});
+   if (!g_dry) {
+      CUDA_CHECK(cudaMemsetAsync(c->sweeps_coarse.p, 0, np * sizeof(long long), c->stream));
+      compute_weights_host(c);
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   }
+   c->initialized = true;
+}
+
+// ---------------------------------------------------------------------------
+// level operators
+// ---------------------------------------------------------------------------
+
+void ghost_fill(fac_ctx *c, int fid, int ln, bool with_coarse, int homogeneous, const int *mask)
+{
+   LevelState &L = c->L[ln];
+   if (field_ghost(fid) != 1) return;  // ghost-0 fields have no ghosts to fill
+   double *dst = field_ptr(L, fid);
+   const double *coarse = ln > 0 ? field_ptr(c->L[ln - 1], fid) : nullptr;
+   ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
+   const int pi = prof_begin(c, 1, L.fill_bytes);
+   launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), dst, dst, coarse,
+               homogeneous, c->bc, mask);
+   prof_end(c, pi);
+}
+
+// CellPoissonFACOps::smoothErrorByRedBlack (CellPoissonFACOps.C:1339-1514).
+void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
+{
+   LevelState &L = c->L[ln];
+   const int np = nprob(c);
+   double *e = field_ptr(L, fid_e);
+   const double *r = field_ptr(L, fid_r);
+   CUDA_CHECK(cudaMemcpyAsync(c->run.p, c->active.p, np * sizeof(int), cudaMemcpyDeviceToDevice,
+                              c->stream));
+   CUDA_CHECK(cudaMemsetAsync(c->sweeps_call.p, 0, np * sizeof(long long), c->stream));
+   ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+   if (ln > 0) ghost_fill(c, fid_e, ln, true, 1, c->run.p);
+   std::vector<int> hrun(np);
+   for (int isweep = 0; isweep < nsweeps; ++isweep) {
+      if (tol >= 0.0 && isweep > 0 && isweep % c->check_interval == 0) {
+         CUDA_CHECK(cudaMemcpyAsync(hrun.data(), c->run.p, np * sizeof(int),
+                                    cudaMemcpyDeviceToHost, c->stream));
+         CUDA_CHECK(cudaStreamSynchronize(c->stream));
+         bool any = false;
+         for (int v : hrun) any = any || v;
+         if (!any) break;
+      }
+      CUDA_CHECK(cudaMemsetAsync(L.maxres_red.p, 0, L.maxres_red.n * sizeof(unsigned long long),
+                                 c->stream));
+      CUDA_CHECK(cudaMemsetAsync(L.maxres_blk.p, 0, L.maxres_blk.n * sizeof(unsigned long long),
+                                 c->stream));
+      for (int color = 0; color < 2; ++color) {
+         ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+         if (ln > 0)
+            launch_cf_flux(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, e, L.d.p,
+                           c->spec.d_variable, c->spec.d_const, L.tranwt, L.longwt, L.cfflux.p,
+                           c->run.p);
+         const int pi = prof_begin(c, 0, L.rb_bytes);
+         launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
+                     L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
+                     color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p);
+         prof_end(c, pi);
+      }
+      ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+      launch_sweep_check(c->stream, L.maxres_red.p, L.maxres_blk.p, L.last_patch.p, np, tol,
+                         c->run.p, c->sweeps_call.p);
+   }
+   CUDA_CHECK(cudaGetLastError());
+}
+
+// CellPoissonFACOps::computeCompositeResidualOnLevel (CellPoissonFACOps.C:1792-1956).
+void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int error_eq)
+{
+   LevelState &L = c->L[ln];
+   const int *run = c->active.p;
+   ghost_fill(c, fid_u, ln, ln > 0, error_eq, run);
+   const double *u = field_ptr(L, fid_u);
+   launch_flux(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
+               L.d_flux_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt, L.d_ratio.p,
+               L.flux.p, run);
+   if (ln < c->nlev - 1) {
+      LevelState &Fl = c->L[ln + 1];
+      launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
+                          L.fcoarsen.nchunks(), Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
+                          L.flux.p, run);
+   }
+   launch_residual(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
+                   L.d_cell_chunks.p, u, field_ptr(L, fid_f), L.flux.p, L.c.p,
+                   field_ptr(L, fid_r), ln > 0 ? L.oflux.p : nullptr, run);
+   CUDA_CHECK(cudaGetLastError());
+}
+
+void restrict_op(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
+{
+   LevelState &C = c->L[dest_ln];
+   LevelState &Fl = c->L[dest_ln + 1];
+   const int sg = field_ghost(fid_src), dg = field_ghost(fid_dst);
+   ItemList<RestrictItem> &it = dg ? C.restrict_g1 : C.restrict_g0;
+   launch_restrict(c->stream, c->dim, it.d_items.p, it.d_chunks.p, it.nchunks(), Fl.d_patches.p,
+                   C.d_patches.p, field_ptr(Fl, fid_src), sg, field_ptr(C, fid_dst), dg,
+                   c->active.p);
+   CUDA_CHECK(cudaGetLastError());
+}
+
+void restrict_solution(fac_ctx *c, int fid, int dest_ln)
+{
+   restrict_op(c, fid, fid, dest_ln);
+   ghost_fill(c, fid, dest_ln, dest_ln > 0, 0, c->active.p);
+}
+
+// CellPoissonFACOps::prolongErrorAndCorrect (CellPoissonFACOps.C:1254-1304).
+void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
+{
+   LevelState &Fl = c->L[dest_ln];
+   LevelState &C = c->L[dest_ln - 1];
+   if (field_ghost(fid_src) != 1 || field_ghost(fid_dst) != 1)
+      throw FacError(FAC_ERR_ARG, "prolongation needs ghosted cell fields");
+   launch_fill(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p, Fl.tmp_fill.nchunks(),
+               Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1, c->bc, c->active.p);
+   launch_prolong_add(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
+                      Fl.prolong.nchunks(), Fl.d_patches.p, Fl.tmp.p, Fl.dxc_prob.p, Fl.ratio,
+                      field_ptr(Fl, fid_dst), c->active.p);
+   CUDA_CHECK(cudaGetLastError());
+}
+
+void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
+{
+   const int np = nprob(c);
+   CUDA_CHECK(cudaMemsetAsync(c->norm_acc.p, 0, np * sizeof(double2), c->stream));
+   const int g = field_ghost(fid);
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      launch_norm(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p, L.d_cell_chunks.p,
+                  field_ptr(L, fid), g, L.w.p, L.norm_partial.p, L.d_prob_cell_chunk_begin.p, np,
+                  c->norm_acc.p);
+   }
+   std::vector<double2> acc(np);
+   CUDA_CHECK(cudaMemcpyAsync(acc.data(), c->norm_acc.p, np * sizeof(double2),
+                              cudaMemcpyDeviceToHost, c->stream));
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   out.resize(np);
+   for (int p = 0; p < np; ++p) {
+      const double num = std::sqrt(acc[p].x);
+      out[p] = acc[p].y > 0.0 ? num / std::sqrt(acc[p].y) : 0.0;
+   }
+}
+
+void solve_coarsest(fac_ctx *c)
+{
+   smooth(c, FAC_E, FAC_R, 0, c->coarse_max_it, c->coarse_tol);
+   // accumulate the per-call sweep counts
+   const int np = nprob(c);
+   std::vector<long long> a(np), b(np);
+   CUDA_CHECK(cudaMemcpyAsync(a.data(), c->sweeps_call.p, np * sizeof(long long),
+                              cudaMemcpyDeviceToHost, c->stream));
+   CUDA_CHECK(cudaMemcpyAsync(b.data(), c->sweeps_coarse.p, np * sizeof(long long),
+                              cudaMemcpyDeviceToHost, c->stream));
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   for (int p = 0; p < np; ++p) b[p] += a[p];
+   CUDA_CHECK(cudaMemcpyAsync(c->sweeps_coarse.p, b.data(), np * sizeof(long long),
+                              cudaMemcpyHostToDevice, c->stream));
+   ghost_fill(c, FAC_E, 0, false, 1, c->active.p);
+}
+
+// FACPreconditioner::facCycle_Recursive (FACPreconditioner.C:462-518).
+void fac_cycle_recursive(fac_ctx *c, int ln)
+{
+   if (ln == 0) {
+      solve_coarsest(c);
+   } else {
+      smooth(c, FAC_E, FAC_R, ln, c->pre_sweeps, -1.0);
+      comp_residual(c, FAC_TR, FAC_E, FAC_R, ln, 1);
+      restrict_op(c, FAC_TR, FAC_R, ln - 1);
+      fac_cycle_recursive(c, ln - 1);
+      prolong_correct(c, FAC_E, FAC_E, ln);
+      smooth(c, FAC_E, FAC_R, ln, c->post_sweeps, -1.0);
+   }
+}
+
+// FACPreconditioner::computeFullCompositeResidual (FACPreconditioner.C:775-814).
+void full_composite_residual(fac_ctx *c, std::vector<double> &norms)
+{
+   const int lmax = c->nlev - 1;
+   comp_residual(c, FAC_R, FAC_U, FAC_F, lmax, 0);
+   for (int ln = lmax - 1; ln >= 0; --ln) {
+      restrict_solution(c, FAC_U, ln);
+      comp_residual(c, FAC_R, FAC_U, FAC_F, ln, 0);
+      restrict_op(c, FAC_R, FAC_R, ln);
+   }
+   rms_norm(c, FAC_R, norms);
+}
+
+void zero_field(fac_ctx *c, int fid)
+{
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      const size_t n = field_ghost(fid) ? L.u.n : L.f.n;
+      CUDA_CHECK(cudaMemsetAsync(field_ptr(L, fid), 0, n * sizeof(double), c->stream));
+   }
+}
+
+void dirichlet(fac_ctx *c, bool restore)
+{
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      const long long n = (long long)L.dir_idx.size();
+      if (restore) launch_scatter(c->stream, L.d_dir_idx.p, n, L.dir_cache.p, L.u.p);
+      else launch_gather(c->stream, L.d_dir_idx.p, n, L.u.p, L.dir_cache.p);
+   }
+}
+
+// FACPreconditioner::solveSystem (FACPreconditioner.C:277-452) inside
+// CellPoissonFACSolver::solveSystem (CellPoissonFACSolver.C:310-352).
+void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
+{
+   const int np = nprob(c);
+   std::vector<int> act(np, 1);
+   CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int), cudaMemcpyHostToDevice,
+                              c->stream));
+   dirichlet(c, false);
+   zero_field(c, FAC_E);
+   zero_field(c, FAC_R);
+   std::vector<double> res, fnorm;
+   full_composite_residual(c, res);
+   rms_norm(c, FAC_F, fnorm);
+   std::vector<double> eff(np);
+   for (int p = 0; p < np; ++p) {
+      eff[p] = c->residual_tol;
+      if (c->rel_residual_tol >= 0) {
+         const double t = fnorm[p] * c->rel_residual_tol;
+         if (eff[p] < t) eff[p] = t;
+      }
+      c->hist[p].assign(1, res[p]);
+   }
+   std::vector<int> its(np, 0);
+   int it = 0;
+   bool any = true;
+   while (any) {
+      zero_field(c, FAC_E);
+      fac_cycle_recursive(c, c->nlev - 1);
+      for (int ln = 0; ln < c->nlev; ++ln) {
+         LevelState &L = c->L[ln];
+         launch_add_interior(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                             L.d_cell_chunks.p, L.u.p, L.e.p, c->active.p);
+      }
+      for (int ln = c->nlev - 2; ln >= 0; --ln) restrict_solution(c, FAC_U, ln);
+      std::vector<double> nr;
+      full_composite_residual(c, nr);
+      ++it;
+      any = false;
+      for (int p = 0; p < np; ++p) {
+         if (!act[p]) continue;
+         res[p] = nr[p];
+         its[p] = it;
+         c->hist[p].push_back(nr[p]);
+         if (!(nr[p] > eff[p] && it < c->max_cycles)) act[p] = 0;
+         any = any || act[p];
+      }
+      CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int),
+                                 cudaMemcpyHostToDevice, c->stream));
+   }
+   std::vector<int> ones(np, 1);
+   CUDA_CHECK(cudaMemcpyAsync(c->active.p, ones.data(), np * sizeof(int), cudaMemcpyHostToDevice,
+                              c->stream));
+   dirichlet(c, true);
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   for (int p = 0; p < np; ++p) {
+      if (converged) converged[p] = res[p] < eff[p];
+      if (iterations) iterations[p] = its[p];
+      if (residual) residual[p] = res[p];
+   }
+}
+
+size_t field_slice(const fac_ctx *c, int fid, int p, int ln, long long &off)
+{
+   const LevelState &L = c->L[ln];
+   if (fid == FAC_U || fid == FAC_E) {
+      off = L.prob_off1[p];
+      return (size_t)(L.prob_off1[p + 1] - L.prob_off1[p]);
+   }
+   off = L.prob_off0[p];
+   return (size_t)(L.prob_off0[p + 1] - L.prob_off0[p]);
+}
+
+void check_pl(fac_ctx *c, int p, int ln)
+{
+   if (p < 0 || p >= nprob(c)) throw FacError(FAC_ERR_ARG, "bad problem index");
+   if (ln < 0 || ln >= c->nlev) throw FacError(FAC_ERR_ARG, "bad level number");
+}
+
+template <class F>
+int guarded(F &&f)
+{
+   try {
+      f();
+      return FAC_OK;
+   } catch (const FacError &e) {
+      g_last_error = e.what();
+      return e.code;
+   } catch (const std::exception &e) {
+      g_last_error = e.what();
+      return FAC_ERR_ARG;
+   }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char *fac_last_error(void) { return g_last_error.c_str(); }
+
+int fac_ctx_create(fac_ctx **ctx, int dim, int device)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null output pointer");
+      if (dim != 2 && dim != 3) throw FacError(FAC_ERR_ARG, "dim must be 2 or 3");
+      if (device >= 0) {
+         int ndev = 0;
+         CUDA_CHECK(cudaGetDeviceCount(&ndev));
+         if (device >= ndev) throw FacError(FAC_ERR_ARG, "bad device index");
+         CUDA_CHECK(cudaSetDevice(device));
+      }
+      fac_ctx *c = new fac_ctx();
+      c->dim = dim;
+      c->device = device;
+      for (int l = 0; l < 6; ++l) {
+         c->bc.a[l] = 1.0;
+         c->bc.b[l] = 0.0;
+         c->bc.g[l] = 0.0;
+      }
+      if (device >= 0) {
+         cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+         if (e != cudaSuccess) {
+            delete c;
+            throw FacError(FAC_ERR_CUDA, cudaGetErrorString(e));
+         }
+      }
+      *ctx = c;
+   });
+}
+
+int fac_ctx_destroy(fac_ctx *ctx)
+{
+   return guarded([&] {
+      if (!ctx) return;
+      if (ctx->device < 0) {
+         g_dry = true;
+         delete ctx;
+         g_dry = false;
+         return;
+      }
+      cudaSetDevice(ctx->device);
+      cudaStreamSynchronize(ctx->stream);
+      cudaStream_t s = ctx->stream;
+      delete ctx;
+      cudaStreamDestroy(s);
+   });
+}
+
+int fac_add_problem(fac_ctx *ctx, const int *n0, const double *xlo, const double *xup, int nlev,
+                    const int *ratio, const int *npatch, const int *boxes, int *problem)
+{
+   return guarded([&] {
+      check_state(ctx, false);
+      if (!n0 || !xlo || !xup || !ratio || !npatch || !boxes)
+         throw FacError(FAC_ERR_ARG, "null argument");
+      if (nlev < 1 || nlev > kMaxLevels) throw FacError(FAC_ERR_ARG, "bad level count");
+      HostProblem P;
+      const int dim = ctx->dim;
+      for (int a = 0; a < 3; ++a) {
+         P.n0[a] = a < dim ? n0[a] : 1;
+         P.xlo[a] = a < dim ? xlo[a] : 0.0;
+         P.xup[a] = a < dim ? xup[a] : 1.0;
+         if (P.n0[a] < 1) throw FacError(FAC_ERR_ARG, "bad n0");
+      }
+      P.nlev = nlev;
+      int off = 0;
+      for (int ln = 0; ln < nlev; ++ln) {
+         for (int a = 0; a < 3; ++a) {
+            P.ratio[ln][a] = a < dim ? ratio[3 * ln + a] : 1;
+            if (P.ratio[ln][a] < 1 || P.ratio[ln][a] > 255)
+               throw FacError(FAC_ERR_ARG, "bad ratio");
+         }
+         if (npatch[ln] < 1) throw FacError(FAC_ERR_ARG, "empty level");
+         for (int ip = 0; ip < npatch[ln]; ++ip, ++off) {
+            Box b;
+            for (int a = 0; a < 3; ++a) {
+               b.lo[a] = boxes[6 * off + a];
+               b.hi[a] = boxes[6 * off + 3 + a];
+            }
+            if (dim == 2) b.lo[2] = b.hi[2] = 0;
+            if (b.empty()) throw FacError(FAC_ERR_ARG, "empty patch box");
+            P.boxes[ln].push_back(b);
+         }
+      }
+      ctx->probs.push_back(P);
+      if (problem) *problem = (int)ctx->probs.size() - 1;
+   });
+}
+
+int fac_set_poisson(fac_ctx *ctx, int d_variable, double d_const, int c_kind, double c_const)
+{
+   return guarded([&] {
+      check_state(ctx, false);
+      if (c_kind < 0 || c_kind > 2) throw FacError(FAC_ERR_ARG, "bad c_kind");
+      ctx->spec.d_variable = d_variable ? 1 : 0;
+      ctx->spec.d_const = d_const;
+      ctx->spec.c_kind = c_kind;
+      ctx->spec.c_const = c_const;
+   });
+}
+
+int fac_set_bc(fac_ctx *ctx, const double *a, const double *b, const double *g)
+{
+   return guarded([&] {
+      if (!ctx || !a || !b || !g) throw FacError(FAC_ERR_ARG, "null argument");
+      for (int l = 0; l < 2 * ctx->dim; ++l) {
+         ctx->bc.a[l] = a[l];
+         ctx->bc.b[l] = b[l];
+         ctx->bc.g[l] = g[l];
+      }
+   });
+}
+
+int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol, double relative_residual_tol,
+                   int pre_sweeps, int post_sweeps, double coarse_tol, int coarse_max_it, int ewing)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      // FACPreconditioner::getFromInput range checks (FACPreconditioner.C:80-114)
+      if (max_cycles < 1) throw FacError(FAC_ERR_ARG, "max_cycles");
+      if (!(residual_tol > 0)) throw FacError(FAC_ERR_ARG, "residual_tol");
+      if (pre_sweeps < 0 || post_sweeps < 0) throw FacError(FAC_ERR_ARG, "sweeps");
+      if (!(coarse_tol > 0)) throw FacError(FAC_ERR_ARG, "coarse_solver_tolerance");
+      if (coarse_max_it < 1) throw FacError(FAC_ERR_ARG, "coarse_solver_max_iterations");
+      ctx->max_cycles = max_cycles;
+      ctx->residual_tol = residual_tol;
+      ctx->rel_residual_tol = relative_residual_tol;
+      ctx->pre_sweeps = pre_sweeps;
+      ctx->post_sweeps = post_sweeps;
+      ctx->coarse_tol = coarse_tol;
+      ctx->coarse_max_it = coarse_max_it;
+      ctx->ewing = ewing;
+   });
+}
+
+int fac_initialize(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_state(ctx, false);
+      initialize(ctx);
+   });
+}
+
+int fac_field_size(fac_ctx *ctx, int fid, int problem, int ln, size_t *n)
+{
+   return guarded([&] {
+      check_state(ctx, true);
+      check_pl(ctx, problem, ln);
+      field_ghost(fid);
+      long long off;
+      *n = field_slice(ctx, fid, problem, ln, off);
+   });
+}
+
+int fac_side_size(fac_ctx *ctx, int problem, int ln, size_t *n)
+{
+   return guarded([&] {
+      check_state(ctx, true);
+      check_pl(ctx, problem, ln);
+      const LevelState &L = ctx->L[ln];
+      *n = (size_t)(L.prob_offs[problem + 1] - L.prob_offs[problem]);
+   });
+}
+
+int fac_oside_size(fac_ctx *ctx, int problem, int ln, size_t *n)
+{
+   return guarded([&] {
+      check_state(ctx, true);
+      check_pl(ctx, problem, ln);
+      const LevelState &L = ctx->L[ln];
+      *n = (size_t)(L.prob_offo[problem + 1] - L.prob_offo[problem]);
+   });
+}
+
+int fac_upload_field(fac_ctx *ctx, int fid, int problem, int ln, const double *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
+      if (fid == FAC_C && ctx->spec.c_kind != 2) throw FacError(FAC_ERR_ARG, "C is not variable");
+      long long off;
+      const size_t n = field_slice(ctx, fid, problem, ln, off);
+      CUDA_CHECK(cudaMemcpyAsync(field_ptr(ctx->L[ln], fid) + off, host, n * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_download_field(fac_ctx *ctx, int fid, int problem, int ln, double *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
+      long long off;
+      const size_t n = field_slice(ctx, fid, problem, ln, off);
+      CUDA_CHECK(cudaMemcpyAsync(host, field_ptr(ctx->L[ln], fid) + off, n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_upload_side(fac_ctx *ctx, int problem, int ln, const double *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!ctx->spec.d_variable) throw FacError(FAC_ERR_ARG, "D is not variable");
+      if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
+      const LevelState &L = ctx->L[ln];
+      const long long off = L.prob_offs[problem], n = L.prob_offs[problem + 1] - off;
+      CUDA_CHECK(cudaMemcpyAsync(ctx->L[ln].d.p + off, host, n * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_download_side(fac_ctx *ctx, int problem, int ln, double *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
+      const LevelState &L = ctx->L[ln];
+      const long long off = L.prob_offs[problem], n = L.prob_offs[problem + 1] - off;
+      CUDA_CHECK(cudaMemcpyAsync(host, ctx->L[ln].d.p + off, n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_download_flux(fac_ctx *ctx, int problem, int ln, double *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
+      const LevelState &L = ctx->L[ln];
+      const long long off = L.prob_offs[problem], n = L.prob_offs[problem + 1] - off;
+      CUDA_CHECK(cudaMemcpyAsync(host, ctx->L[ln].flux.p + off, n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_download_oside(fac_ctx *ctx, int problem, int ln, double *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
+      const LevelState &L = ctx->L[ln];
+      const long long off = L.prob_offo[problem], n = L.prob_offo[problem + 1] - off;
+      CUDA_CHECK(cudaMemcpyAsync(host, ctx->L[ln].oflux.p + off, n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_ghost_fill(fac_ctx *ctx, int fid, int ln, int with_coarse, int homogeneous)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, ln);
+      ghost_fill(ctx, fid, ln, with_coarse != 0, homogeneous ? 1 : 0, ctx->active.p);
+      CUDA_CHECK(cudaGetLastError());
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_smooth(fac_ctx *ctx, int fid_e, int fid_r, int ln, int nsweeps, double tol, int *sweeps)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, ln);
+      if (field_ghost(fid_e) != 1 || field_ghost(fid_r) != 0)
+         throw FacError(FAC_ERR_ARG, "smooth needs a ghosted unknown and a ghost-0 rhs");
+      smooth(ctx, fid_e, fid_r, ln, nsweeps, tol);
+      if (sweeps) {
+         std::vector<long long> s(nprob(ctx));
+         CUDA_CHECK(cudaMemcpyAsync(s.data(), ctx->sweeps_call.p, s.size() * sizeof(long long),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+         for (size_t p = 0; p < s.size(); ++p) sweeps[p] = (int)s[p];
+      }
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_comp_residual(fac_ctx *ctx, int fid_r, int fid_u, int fid_f, int ln, int error_equation)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, ln);
+      if (field_ghost(fid_u) != 1 || field_ghost(fid_r) != 0 || field_ghost(fid_f) != 0)
+         throw FacError(FAC_ERR_ARG, "bad field kinds for the residual");
+      comp_residual(ctx, fid_r, fid_u, fid_f, ln, error_equation ? 1 : 0);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_restrict(fac_ctx *ctx, int fid_src, int fid_dst, int dest_ln)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, dest_ln);
+      if (dest_ln + 1 >= ctx->nlev) throw FacError(FAC_ERR_ARG, "no finer level");
+      restrict_op(ctx, fid_src, fid_dst, dest_ln);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_restrict_solution(fac_ctx *ctx, int fid, int dest_ln)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, dest_ln);
+      if (dest_ln + 1 >= ctx->nlev) throw FacError(FAC_ERR_ARG, "no finer level");
+      restrict_solution(ctx, fid, dest_ln);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_prolong_correct(fac_ctx *ctx, int fid_src, int fid_dst, int dest_ln)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, dest_ln);
+      if (dest_ln < 1) throw FacError(FAC_ERR_ARG, "no coarser level");
+      prolong_correct(ctx, fid_src, fid_dst, dest_ln);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_compute_weights(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      compute_weights_host(ctx);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_rms_norm(fac_ctx *ctx, int fid, double *norms)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!norms) throw FacError(FAC_ERR_ARG, "null output");
+      std::vector<double> v;
+      rms_norm(ctx, fid, v);
+      for (size_t p = 0; p < v.size(); ++p) norms[p] = v[p];
+   });
+}
+
+int fac_solve_coarsest(fac_ctx *ctx, int *sweeps)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      solve_coarsest(ctx);
+      if (sweeps) {
+         std::vector<long long> s(nprob(ctx));
+         CUDA_CHECK(cudaMemcpyAsync(s.data(), ctx->sweeps_call.p, s.size() * sizeof(long long),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+         for (size_t p = 0; p < s.size(); ++p) sweeps[p] = (int)s[p];
+      }
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_fac_cycle(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      fac_cycle_recursive(ctx, ctx->nlev - 1);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_solve(fac_ctx *ctx, int *converged, int *iterations, double *residual)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      solve(ctx, converged, iterations, residual);
+   });
+}
+
+int fac_solve_host(fac_ctx *ctx, const double *const *f_host, const double *const *u0_host,
+                   double *const *u_host, int *converged, int *iterations, double *residual)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!f_host || !u_host) throw FacError(FAC_ERR_ARG, "null host array table");
+      const int np = nprob(ctx);
+      for (int p = 0; p < np; ++p)
+         for (int ln = 0; ln < ctx->nlev; ++ln) {
+            const int k = p * ctx->nlev + ln;
+            long long off;
+            size_t n = field_slice(ctx, FAC_F, p, ln, off);
+            CUDA_CHECK(cudaMemcpyAsync(ctx->L[ln].f.p + off, f_host[k], n * sizeof(double),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+            n = field_slice(ctx, FAC_U, p, ln, off);
+            if (u0_host && u0_host[k])
+               CUDA_CHECK(cudaMemcpyAsync(ctx->L[ln].u.p + off, u0_host[k], n * sizeof(double),
+                                          cudaMemcpyHostToDevice, ctx->stream));
+            else
+               CUDA_CHECK(cudaMemsetAsync(ctx->L[ln].u.p + off, 0, n * sizeof(double),
+                                          ctx->stream));
+         }
+      solve(ctx, converged, iterations, residual);
+      for (int p = 0; p < np; ++p)
+         for (int ln = 0; ln < ctx->nlev; ++ln) {
+            const int k = p * ctx->nlev + ln;
+            long long off;
+            const size_t n = field_slice(ctx, FAC_U, p, ln, off);
+            CUDA_CHECK(cudaMemcpyAsync(u_host[k], ctx->L[ln].u.p + off, n * sizeof(double),
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+         }
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_residual_history(fac_ctx *ctx, int problem, double *hist, int cap, int *n)
+{
+   return guarded([&] {
+      check_state(ctx, true);
+      check_pl(ctx, problem, 0);
+      const auto &h = ctx->hist[problem];
+      const int m = (int)std::min<size_t>(h.size(), (size_t)std::max(cap, 0));
+      for (int t = 0; t < m; ++t) hist[t] = h[t];
+      if (n) *n = (int)h.size();
+   });
+}
+
+int fac_coarse_sweeps(fac_ctx *ctx, long long *sweeps)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      CUDA_CHECK(cudaMemcpyAsync(sweeps, ctx->sweeps_coarse.p, nprob(ctx) * sizeof(long long),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_reset_stats(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      CUDA_CHECK(cudaMemsetAsync(ctx->sweeps_coarse.p, 0, nprob(ctx) * sizeof(long long),
+                                 ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_kernel_launches(long long *n)
+{
+   return guarded([&] {
+      if (!n) throw FacError(FAC_ERR_ARG, "null output");
+      *n = kernel_launch_count();
+   });
+}
+
+int fac_profile_enable(fac_ctx *ctx, int on)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      ctx->profiling = on != 0;
+      ctx->prof.clear();
+      ctx->ev_next = 0;
+   });
+}
+
+int fac_profile_read(fac_ctx *ctx, int kind, long long *launches, double *ms, double *bytes)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      long long n = 0;
+      double t = 0, b = 0;
+      for (const auto &r : ctx->prof) {
+         if (r.kind != kind) continue;
+         float e = 0.f;
+         CUDA_CHECK(cudaEventElapsedTime(&e, r.a, r.b));
+         ++n;
+         t += e;
+         b += r.bytes;
+      }
+      if (launches) *launches = n;
+      if (ms) *ms = t;
+      if (bytes) *bytes = b;
+   });
+}
+
+int fac_profile_reset(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      ctx->prof.clear();
+      ctx->ev_next = 0;
+   });
+}
+
+int fac_timer(fac_ctx *ctx, int stop, double *ms)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!ctx->t0) {
+         CUDA_CHECK(cudaEventCreate(&ctx->t0));
+         CUDA_CHECK(cudaEventCreate(&ctx->t1));
+      }
+      if (!stop) {
+         CUDA_CHECK(cudaEventRecord(ctx->t0, ctx->stream));
+         return;
+      }
+      CUDA_CHECK(cudaEventRecord(ctx->t1, ctx->stream));
+      CUDA_CHECK(cudaEventSynchronize(ctx->t1));
+      float e = 0.f;
+      CUDA_CHECK(cudaEventElapsedTime(&e, ctx->t0, ctx->t1));
+      if (ms) *ms = e;
+   });
+}
+
+int fac_synchronize(fac_ctx *ctx)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+}  // extern "C"

@@ -1,0 +1,969 @@
+// FP64 kernels of the FAC Poisson hot path (sm_100a).
+//
+// Built with --fmad=false: every multiply and add is rounded separately, in
+// the order of the reference's Fortran expressions, so results are
+// bit-identical to the reference arithmetic (solv_cellpoissonfacops{2,3}d.f,
+// geom_m4cart{refine,coarsen}ops{2,3}d.i, solv_cartesianrobinbchelper{2,3}d.f).
+//
+// All kernels are table driven: a level of every problem in the context is
+// processed by one launch whose blocks each take one Chunk (a run of cells of
+// one patch or one transaction), so patches of uneven size share the grid.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+
+#include "fac_internal.h"
+#include "fac_kernels.h"
+
+namespace samrai_b200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ long long aidx(const ArrDesc &A, int i, int j, int k)
+{
+   return A.base + (long long)(i - A.lo[0]) +
+          (long long)A.n[0] * ((long long)(j - A.lo[1]) +
+                               (long long)A.n[1] * (long long)(k - A.lo[2]));
+}
+
+// Index of cell (i,j,k) in a patch's array with ghost width g.
+template <int DIM>
+__device__ __forceinline__ long long cidx(const PatchDesc &p, long long off,
+                                          int g, int i, int j, int k)
+{
+   const int gz = DIM == 3 ? g : 0;
+   const long long nx = p.hi[0] - p.lo[0] + 1 + 2 * g;
+   const long long ny = p.hi[1] - p.lo[1] + 1 + 2 * g;
+   return off + (i - p.lo[0] + g) + nx * ((j - p.lo[1] + g) + ny * (k - p.lo[2] + gz));
+}
+
+// Index of face (i,j,k) of axis a in a patch's side array (ghost 0).
+__device__ __forceinline__ long long sidx(const PatchDesc &p, int a, int i, int j,
+                                          int k)
+{
+   const long long nx = p.hi[0] - p.lo[0] + 1 + (a == 0);
+   const long long ny = p.hi[1] - p.lo[1] + 1 + (a == 1);
+   return p.offs[a] + (i - p.lo[0]) + nx * ((j - p.lo[1]) + ny * (k - p.lo[2]));
+}
+
+// Index of the tangential position of cell (i,j,k) in a face array of axis a.
+__device__ __forceinline__ long long oidx(const PatchDesc &p, int a, int s, int i,
+                                          int j, int k)
+{
+   const long long nx = p.hi[0] - p.lo[0] + 1;
+   const long long ny = p.hi[1] - p.lo[1] + 1;
+   long long t;
+   if (a == 0) t = (j - p.lo[1]) + ny * (k - p.lo[2]);
+   else if (a == 1) t = (i - p.lo[0]) + nx * (k - p.lo[2]);
+   else t = (i - p.lo[0]) + nx * (j - p.lo[1]);
+   return p.offo[a][s] + t;
+}
+
+__device__ __forceinline__ int coarsen_index(int i, int r)
+{
+   return i < 0 ? (i + 1) / r - 1 : i / r;
+}
+
+// settype1cells{2,3}d (robinbchelper2d.f:10-72): ghost value from the
+// interior value next to the boundary.
+__device__ __forceinline__ double robin(double uin, int loc, double h, int hom,
+                                        const BcCoefs &bc)
+{
+   const double a = bc.a[loc], b = bc.b[loc];
+   if (hom) return (uin * (b - 0.5 * h * a)) / (b + 0.5 * h * a);
+   return (h * bc.g[loc] + uin * (b - 0.5 * h * a)) / (b + 0.5 * h * a);
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v)
+{
+   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// ---------------------------------------------------------------------------
+// ghost fill
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads)
+k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
+       double *__restrict__ dst, const double *__restrict__ src_same,
+       const double *__restrict__ src_coarse, int homogeneous, BcCoefs bc,
+       const int *__restrict__ active)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const FillItem &it = items[ch.patch];
+   if (active && !active[it.prob]) return;
+   const double *src = it.src_is_coarse ? src_coarse : src_same;
+   const int nx = it.hi[0] - it.lo[0] + 1;
+   const int ny = it.hi[1] - it.lo[1] + 1;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = it.lo[0] + lin % nx;
+      const int r = lin / nx;
+      const int j = it.lo[1] + r % ny;
+      const int k = it.lo[2] + r / ny;
+      double v;
+      if (it.kind == kFillCopy) {
+         v = src[aidx(it.src, i, j, k)];
+      } else if (it.kind == kFillCoarse) {
+         v = src[aidx(it.src, coarsen_index(i, it.ratio[0]),
+                      coarsen_index(j, it.ratio[1]),
+                      coarsen_index(k, it.ratio[2]))];
+      } else {
+         // Every ghost value of codimension m depends only on the interior
+         // cell reached by moving inward along all m outside axes
+         // (settype1/2/3cells{2,3}d applied in codimension order).
+         const double uin =
+            src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
+         double f[3];
+         int m = 0;
+         for (int a = 0; a < 3; ++a) {
+            if (it.side[a]) {
+               f[a] = robin(uin, 2 * a + (it.side[a] > 0), it.h[a], homogeneous, bc);
+               ++m;
+            } else {
+               f[a] = 0.0;
+            }
+         }
+         if (m == 1) {
+            v = it.side[0] ? f[0] : (it.side[1] ? f[1] : f[2]);
+         } else if (m == 2) {
+            double s0 = 0.0, s1 = 0.0;
+            int n = 0;
+            for (int a = 0; a < 3; ++a)
+               if (it.side[a]) {
+                  if (n == 0) s0 = f[a];
+                  else s1 = f[a];
+                  ++n;
+               }
+            v = -uin + (s1 + s0);
+         } else {
+            const double two3 = (double)(2.0f / 3.0f);
+            v = -uin + two3 * ((f[0] + f[1]) + f[2]);
+         }
+      }
+      dst[aidx(it.dst, i, j, k)] = v;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// Ewing coarse-fine flux (ewingfixflux{vardc,condc}{2,3}d, 2d.f:460-686,
+// 3d.f:604-1012), evaluated from the current u.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double ewing_flux(const double *__restrict__ u,
+                                             const double *__restrict__ dside,
+                                             const CfFace &cf, const PatchDesc &p,
+                                             int dvar, double dconst,
+                                             const double *tranwt,
+                                             const double *longwt)
+{
+   const int a = cf.axis;
+   const double d = dvar ? dside[cf.sidx] : dconst;
+   const double dxi = 1. / p.dx[a];
+   const double uc = u[cf.cell], ug = u[cf.ghost], um = u[cf.mirror];
+   double flux;
+   if (cf.side == 0) {
+      flux = dxi * d * (uc - ug);
+      return longwt[a] * flux + tranwt[a] * d * (um - uc) / p.dx[a];
+   }
+   flux = dxi * d * (ug - uc);
+   return longwt[a] * flux - tranwt[a] * d * (um - uc) / p.dx[a];
+}
+
+struct EwingWeights {
+   double tranwt[3];
+   double longwt[3];
+};
+
+__global__ void __launch_bounds__(kThreads)
+k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
+          const PatchDesc *__restrict__ patches, const double *__restrict__ u,
+          const double *__restrict__ dside, int dvar, double dconst,
+          EwingWeights w, double *__restrict__ cfflux,
+          const int *__restrict__ run)
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= nfaces) return;
+   const CfFace cf = faces[t];
+   const PatchDesc &p = patches[cf.patch];
+   if (run && !run[p.prob]) return;
+   cfflux[cf.oidx] = ewing_flux(u, dside, cf, p, dvar, dconst, w.tranwt, w.longwt);
+}
+
+// ---------------------------------------------------------------------------
+// red-black Gauss-Seidel colour pass with on-the-fly fluxes
+// (compflux* + rbgswithfluxmax*, 2d.f:10-364, 3d.f:10-484)
+// ---------------------------------------------------------------------------
+
+template <int DIM, bool DVAR, int CKIND>
+__global__ void __launch_bounds__(kThreads)
+k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+       double *__restrict__ u, const double *__restrict__ f,
+       const double *__restrict__ dside, const double *__restrict__ cfield,
+       const double *__restrict__ cfflux, const unsigned char *__restrict__ cfmask,
+       int offset, double dconst, double cconst,
+       unsigned long long *__restrict__ maxres_patch, const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   if (run && !run[p.prob]) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const int hx = (nx + 1) >> 1;
+   const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
+   const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+   const bool has_cf = (p.flags & 1) != 0;
+   const double rcoef = 1.0;
+   double maxres = 0.0;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int s = ch.begin + t;
+      const int row = s / hx;
+      const int mm = s - row * hx;
+      const int j = p.lo[1] + row % ny;
+      const int k = DIM == 3 ? p.lo[2] + row / ny : 0;
+      int ioffset;
+      if (DIM == 2) {
+         const int q = p.lo[1] + j;
+         ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
+      } else {
+         const int q = p.lo[0] + j + k;
+         ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
+      }
+      const int i = p.lo[0] + ioffset + 2 * mm;
+      if (i > p.hi[0]) continue;
+      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+      const long long sx = 1;
+      const long long sy = nx + 2;
+      const long long sz = (long long)(nx + 2) * (ny + 2);
+      const double uc = u[c];
+      double dx0, dx1, dy0, dy1, dz0 = 0.0, dz1 = 0.0;
+      if (DVAR) {
+         dx0 = dside[sidx(p, 0, i, j, k)];
+         dx1 = dside[sidx(p, 0, i + 1, j, k)];
+         dy0 = dside[sidx(p, 1, i, j, k)];
+         dy1 = dside[sidx(p, 1, i, j + 1, k)];
+         if (DIM == 3) {
+            dz0 = dside[sidx(p, 2, i, j, k)];
+            dz1 = dside[sidx(p, 2, i, j, k + 1)];
+         }
+      } else {
+         dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
+      }
+      double fxl = dxi * dx0 * (uc - u[c - sx]);
+      double fxh = dxi * dx1 * (u[c + sx] - uc);
+      double fyl = dyi * dy0 * (uc - u[c - sy]);
+      double fyh = dyi * dy1 * (u[c + sy] - uc);
+      double fzl = 0.0, fzh = 0.0;
+      if (DIM == 3) {
+         fzl = dzi * dz0 * (uc - u[c - sz]);
+         fzh = dzi * dz1 * (u[c + sz] - uc);
+      }
+      if (has_cf) {
+         if (i == p.lo[0]) {
+            const long long o = oidx(p, 0, 0, i, j, k);
+            if (cfmask[o]) fxl = cfflux[o];
+         }
+         if (i == p.hi[0]) {
+            const long long o = oidx(p, 0, 1, i, j, k);
+            if (cfmask[o]) fxh = cfflux[o];
+         }
+         if (j == p.lo[1]) {
+            const long long o = oidx(p, 1, 0, i, j, k);
+            if (cfmask[o]) fyl = cfflux[o];
+         }
+         if (j == p.hi[1]) {
+            const long long o = oidx(p, 1, 1, i, j, k);
+            if (cfmask[o]) fyh = cfflux[o];
+         }
+         if (DIM == 3) {
+            if (k == p.lo[2]) {
+               const long long o = oidx(p, 2, 0, i, j, k);
+               if (cfmask[o]) fzl = cfflux[o];
+            }
+            if (k == p.hi[2]) {
+               const long long o = oidx(p, 2, 1, i, j, k);
+               if (cfmask[o]) fzh = cfflux[o];
+            }
+         }
+      }
+      const double sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
+                                   : (CKIND == 1 ? cconst : 0.0);
+      const double fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
+      double residual, dudr;
+      if (DIM == 2) {
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
+         dudr = 1. / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
+      } else {
+         const double dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
+                    sf * uc;
+         dudr = 1. / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
+                      sf);
+      }
+      const double du = -residual * dudr;
+      u[c] = uc + du * rcoef;
+      const double ar = fabs(residual);
+      if (maxres < ar) maxres = ar;
+   }
+   // block max, then one atomic per block
+   __shared__ double red[kThreads / 32];
+   for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_down_sync(0xffffffffu, maxres, o);
+      maxres = other > maxres ? other : maxres;
+   }
+   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxres;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double m = red[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
+      if (maxres_patch) atomic_max_nonneg(&maxres_patch[ch.patch], m);
+   }
+}
+
+// ---------------------------------------------------------------------------
+// fluxes into side arrays, with the Ewing fix on coarse-fine faces
+// (computeFluxOnPatch, CellPoissonFACOps.C:2157-2267)
+// ---------------------------------------------------------------------------
+
+template <int DIM, bool DVAR>
+__global__ void __launch_bounds__(kThreads)
+k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+       const double *__restrict__ u, const double *__restrict__ dside,
+       double dconst, const unsigned char *__restrict__ cfmask, EwingWeights w,
+       const int *ratio_to_coarser, double *__restrict__ flux,
+       const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   if (run && !run[p.prob]) return;
+   const int a = ch.aux;
+   const int nx = p.hi[0] - p.lo[0] + 1 + (a == 0);
+   const int ny = p.hi[1] - p.lo[1] + 1 + (a == 1);
+   const double dai = 1. / p.dx[a];
+   const bool has_cf = (p.flags & 1) != 0;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int r = lin / nx;
+      const int j = p.lo[1] + r % ny;
+      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+      int cm[3] = {i, j, k};
+      cm[a] -= 1;
+      const long long cp = cidx<DIM>(p, p.off1, 1, i, j, k);
+      const long long cq = cidx<DIM>(p, p.off1, 1, cm[0], cm[1], cm[2]);
+      const long long si = sidx(p, a, i, j, k);
+      const double d = DVAR ? dside[si] : dconst;
+      double fl = dai * d * (u[cp] - u[cq]);
+      if (has_cf) {
+         const int fc[3] = {i, j, k};
+         int s = -1;
+         if (fc[a] == p.lo[a]) s = 0;
+         else if (fc[a] == p.hi[a] + 1) s = 1;
+         if (s >= 0) {
+            int cc[3] = {i, j, k};
+            if (s == 1) cc[a] -= 1;
+            const long long o = oidx(p, a, s, cc[0], cc[1], cc[2]);
+            if (cfmask[o]) {
+               int mq[3] = {cc[0], cc[1], cc[2]};
+               for (int tt = 0; tt < DIM; ++tt) {
+                  if (tt == a) continue;
+                  const int rr = ratio_to_coarser[tt];
+                  const int base = coarsen_index(cc[tt], rr) * rr;
+                  mq[tt] = base + (rr - (cc[tt] - base) - 1);
+               }
+               const double uc = u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
+               const double um = u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
+               if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
+               else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
+            }
+         }
+      }
+      flux[si] = fl;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// residual from side fluxes (compres{var,con}sca{2,3}d) and outer-side save
+// ---------------------------------------------------------------------------
+
+template <int DIM, int CKIND>
+__global__ void __launch_bounds__(kThreads)
+k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+           const double *__restrict__ u, const double *__restrict__ f,
+           const double *__restrict__ flux, const double *__restrict__ cfield,
+           double cconst, double *__restrict__ res, double *__restrict__ oflux,
+           const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   if (run && !run[p.prob]) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
+   const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int r = lin / nx;
+      const int j = p.lo[1] + r % ny;
+      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+      const double fxl = flux[sidx(p, 0, i, j, k)], fxh = flux[sidx(p, 0, i + 1, j, k)];
+      const double fyl = flux[sidx(p, 1, i, j, k)], fyh = flux[sidx(p, 1, i, j + 1, k)];
+      const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
+      const double uc = u[cidx<DIM>(p, p.off1, 1, i, j, k)];
+      const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
+      double rv;
+      if (DIM == 2) {
+         rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
+      } else {
+         const double fzl = flux[sidx(p, 2, i, j, k)], fzh = flux[sidx(p, 2, i, j, k + 1)];
+         rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - sf * uc;
+      }
+      res[c0] = rv;
+      if (oflux) {
+         if (i == p.lo[0]) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
+         if (i == p.hi[0]) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
+         if (j == p.lo[1]) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
+         if (j == p.hi[1]) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
+         if (DIM == 3) {
+            if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = flux[sidx(p, 2, i, j, k)];
+            if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = flux[sidx(p, 2, i, j, k + 1)];
+         }
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------
+// flux coarsening (cartwgtavgoutsidedoub*, OutersideData::copy2)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads)
+k_flux_coarsen(const FluxCoarsenItem *__restrict__ items, const Chunk *__restrict__ chunks,
+               const PatchDesc *__restrict__ fine, const PatchDesc *__restrict__ coarse,
+               const double *__restrict__ oflux_fine, double *__restrict__ flux_coarse,
+               const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const FluxCoarsenItem it = items[ch.patch];
+   if (run && !run[it.prob]) return;
+   const PatchDesc fp = fine[it.fine_patch];
+   const PatchDesc cp = coarse[it.coarse_patch];
+   const int a = it.axis;
+   const int nx = it.hi[0] - it.lo[0] + 1;
+   const int ny = it.hi[1] - it.lo[1] + 1;
+   // refinement ratios along the tangential axes come in the chunk's aux word
+   double wf, wc;
+   if (it.t1 < 0) {
+      wf = fp.dx[it.t0];
+      wc = cp.dx[it.t0];
+   } else {
+      wf = fp.dx[it.t0] * fp.dx[it.t1];
+      wc = cp.dx[it.t0] * cp.dx[it.t1];
+   }
+   const int r0 = ch.aux & 0xff;
+   const int r1 = (ch.aux >> 8) & 0xff;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      int c[3];
+      c[0] = it.lo[0] + lin % nx;
+      const int rr = lin / nx;
+      c[1] = it.lo[1] + rr % ny;
+      c[2] = it.lo[2] + rr / ny;
+      double acc = 0.0;
+      if (it.t1 < 0) {
+         for (int ir = 0; ir < r0; ++ir) {
+            int fc[3] = {0, 0, 0};
+            fc[a] = it.fface;
+            fc[it.t0] = c[it.t0] * r0 + ir;
+            int cc[3] = {fc[0], fc[1], fc[2]};
+            if (it.side == 1) cc[a] -= 1;
+            acc = acc + oflux_fine[oidx(fp, a, it.side, cc[0], cc[1], cc[2])] * wf;
+         }
+      } else {
+         for (int ro = 0; ro < r1; ++ro)
+            for (int ri = 0; ri < r0; ++ri) {
+               int fc[3];
+               fc[a] = it.fface;
+               fc[it.t0] = c[it.t0] * r0 + ri;
+               fc[it.t1] = c[it.t1] * r1 + ro;
+               int cc[3] = {fc[0], fc[1], fc[2]};
+               if (it.side == 1) cc[a] -= 1;
+               acc = acc + oflux_fine[oidx(fp, a, it.side, cc[0], cc[1], cc[2])] * wf;
+            }
+      }
+      acc = acc / wc;
+      flux_coarse[sidx(cp, a, c[0], c[1], c[2])] = acc;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// restriction (cartwgtavgcelldoub{2,3}d)
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chunks,
+           const PatchDesc *__restrict__ fine, const PatchDesc *__restrict__ coarse,
+           const double *__restrict__ src, int src_g, double *__restrict__ dst,
+           int dst_g, const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const RestrictItem it = items[ch.patch];
+   if (run && !run[it.prob]) return;
+   const PatchDesc fp = fine[it.fine_patch];
+   const PatchDesc cp = coarse[it.coarse_patch];
+   const int nx = it.hi[0] - it.lo[0] + 1;
+   const int ny = it.hi[1] - it.lo[1] + 1;
+   const int r0 = ch.aux & 0xff, r1 = (ch.aux >> 8) & 0xff, r2 = (ch.aux >> 16) & 0xff;
+   double dVf, dVc;
+   if (DIM == 2) {
+      dVf = fp.dx[0] * fp.dx[1];
+      dVc = cp.dx[0] * cp.dx[1];
+   } else {
+      dVf = fp.dx[0] * fp.dx[1] * fp.dx[2];
+      dVc = cp.dx[0] * cp.dx[1] * cp.dx[2];
+   }
+   const long long soff = src_g ? fp.off1 : fp.off0;
+   const long long doff = dst_g ? cp.off1 : cp.off0;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = it.lo[0] + lin % nx;
+      const int rr = lin / nx;
+      const int j = it.lo[1] + rr % ny;
+      const int k = it.lo[2] + rr / ny;
+      double acc = 0.0;
+      const int nr2 = DIM == 3 ? r2 : 1;
+      for (int i2 = 0; i2 < nr2; ++i2)
+         for (int i1 = 0; i1 < r1; ++i1)
+            for (int i0 = 0; i0 < r0; ++i0) {
+               const int fk = DIM == 3 ? k * r2 + i2 : 0;
+               acc = acc + src[cidx<DIM>(fp, soff, src_g, i * r0 + i0, j * r1 + i1, fk)] * dVf;
+            }
+      acc = acc / dVc;
+      dst[cidx<DIM>(cp, doff, dst_g, i, j, k)] = acc;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// linear refine of the coarse interpolation array + correction
+// (cartlinrefcelldoub{2,3}d, HierarchyCellDataOpsReal::add)
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ chunks,
+              const PatchDesc *__restrict__ fine, const double *__restrict__ tmp,
+              const double *__restrict__ dxc_prob, int ratio0, int ratio1, int ratio2,
+              double *__restrict__ e, const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const ProlongItem it = items[ch.patch];
+   if (run && !run[it.prob]) return;
+   const PatchDesc p = fine[it.fine_patch];
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const double half = 0.5, one = 1.0;
+   const double *dxc = dxc_prob + 3 * it.prob;
+   const int r[3] = {ratio0, ratio1, ratio2};
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int rr = lin / nx;
+      const int j = p.lo[1] + rr % ny;
+      const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
+      const int fi[3] = {i, j, k};
+      int ic[3];
+      double x[3];
+      for (int a = 0; a < DIM; ++a) {
+         ic[a] = coarsen_index(fi[a], r[a]);
+         const int ir = fi[a] - ic[a] * r[a];
+         const double deltax = ((double)ir + half) * p.dx[a] - dxc[a] * half;
+         x[a] = deltax / dxc[a];
+         if (x[a] < 0.0) {
+            ic[a] = ic[a] - 1;
+            x[a] = x[a] + one;
+         }
+      }
+      double v;
+      const ArrDesc &T = it.tmp;
+      if (DIM == 2) {
+         const double c00 = tmp[aidx(T, ic[0], ic[1], 0)];
+         const double c10 = tmp[aidx(T, ic[0] + 1, ic[1], 0)];
+         const double c01 = tmp[aidx(T, ic[0], ic[1] + 1, 0)];
+         const double c11 = tmp[aidx(T, ic[0] + 1, ic[1] + 1, 0)];
+         v = (c00 + (c10 - c00) * x[0]) * (one - x[1]) + (c01 + (c11 - c01) * x[0]) * x[1];
+      } else {
+         const double c000 = tmp[aidx(T, ic[0], ic[1], ic[2])];
+         const double c100 = tmp[aidx(T, ic[0] + 1, ic[1], ic[2])];
+         const double c010 = tmp[aidx(T, ic[0], ic[1] + 1, ic[2])];
+         const double c110 = tmp[aidx(T, ic[0] + 1, ic[1] + 1, ic[2])];
+         const double c001 = tmp[aidx(T, ic[0], ic[1], ic[2] + 1)];
+         const double c101 = tmp[aidx(T, ic[0] + 1, ic[1], ic[2] + 1)];
+         const double c011 = tmp[aidx(T, ic[0], ic[1] + 1, ic[2] + 1)];
+         const double c111 = tmp[aidx(T, ic[0] + 1, ic[1] + 1, ic[2] + 1)];
+         const double y = x[1], z = x[2], xx = x[0];
+         v = ((c000 + (c100 - c000) * xx) * (one - y) + (c010 + (c110 - c010) * xx) * y) *
+                (one - z) +
+             ((c001 + (c101 - c001) * xx) * (one - y) + (c011 + (c111 - c011) * xx) * y) * z;
+      }
+      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+      e[c] = e[c] + v;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// interior cell helpers
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_add_interior(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+               double *__restrict__ u, const double *__restrict__ e,
+               const int *__restrict__ run)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   if (run && !run[p.prob]) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int r = lin / nx;
+      const int j = p.lo[1] + r % ny;
+      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+      u[c] = u[c] + e[c];
+   }
+}
+
+// Weighted sums sum(w x^2), sum(w) per chunk.
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_norm_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+               const double *__restrict__ x, int xg, const double *__restrict__ w,
+               double2 *__restrict__ partial)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const long long xoff = xg ? p.off1 : p.off0;
+   double sd = 0.0, sv = 0.0;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int r = lin / nx;
+      const int j = p.lo[1] + r % ny;
+      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+      const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
+      const double wv = w[cidx<DIM>(p, p.off0, 0, i, j, k)];
+      sd += xv * xv * wv;
+      sv += wv;
+   }
+   __shared__ double rs[kThreads], rv[kThreads];
+   rs[threadIdx.x] = sd;
+   rv[threadIdx.x] = sv;
+   __syncthreads();
+   for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) {
+         rs[threadIdx.x] += rs[threadIdx.x + o];
+         rv[threadIdx.x] += rv[threadIdx.x + o];
+      }
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(rs[0], rv[0]);
+}
+
+// Per problem: sum the partials of its chunks (in chunk order) and add them
+// to acc[prob] (levels are summed in level order by the caller).
+__global__ void k_norm_reduce(const double2 *__restrict__ partial,
+                              const int *__restrict__ prob_chunk_begin, int nprob,
+                              double2 *__restrict__ acc)
+{
+   const int pr = blockIdx.x;
+   if (pr >= nprob) return;
+   const int b = prob_chunk_begin[pr], e = prob_chunk_begin[pr + 1];
+   __shared__ double rs[kThreads], rv[kThreads];
+   double sd = 0.0, sv = 0.0;
+   for (int c = b + threadIdx.x; c < e; c += blockDim.x) {
+      sd += partial[c].x;
+      sv += partial[c].y;
+   }
+   rs[threadIdx.x] = sd;
+   rv[threadIdx.x] = sv;
+   __syncthreads();
+   for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) {
+         rs[threadIdx.x] += rs[threadIdx.x + o];
+         rv[threadIdx.x] += rv[threadIdx.x + o];
+      }
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) {
+      acc[pr].x += rs[0];
+      acc[pr].y += rv[0];
+   }
+}
+
+// Convergence test of one red-black sweep per problem
+// (CellPoissonFACOps.C:1496-1508 with the last patch's max residuals).
+__global__ void k_sweep_check(const unsigned long long *__restrict__ red,
+                              const unsigned long long *__restrict__ blk,
+                              const int *__restrict__ last_patch, int nprob,
+                              double tol, int *__restrict__ run,
+                              long long *__restrict__ sweeps)
+{
+   const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+   if (pr >= nprob) return;
+   if (!run[pr]) return;
+   sweeps[pr] += 1;
+   if (tol >= 0.0) {
+      const int lp = last_patch[pr];
+      const double r = __longlong_as_double((long long)red[lp]);
+      const double b = __longlong_as_double((long long)blk[lp]);
+      const double m = r > b ? r : b;
+      run[pr] = m > tol ? 1 : 0;
+   }
+}
+
+__global__ void k_gather(const long long *__restrict__ idx, long long n,
+                         const double *__restrict__ src, double *__restrict__ dst)
+{
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) dst[t] = src[idx[t]];
+}
+
+__global__ void k_scatter(const long long *__restrict__ idx, long long n,
+                          const double *__restrict__ src, double *__restrict__ dst)
+{
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) dst[idx[t]] = src[t];
+}
+
+std::atomic<long long> g_launches{0};
+
+}  // namespace
+
+long long kernel_launch_count() { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
+                 double *dst, const double *src_same, const double *src_coarse,
+                 int homogeneous, const BcCoefs &bc, const int *active)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_fill<<<nchunks, kThreads, 0, s>>>(items, chunks, dst, src_same, src_coarse,
+                                       homogeneous, bc, active);
+}
+
+void launch_cf_flux(cudaStream_t s, const CfFace *faces, int nfaces, const PatchDesc *patches,
+                    const double *u, const double *dside, int dvar, double dconst,
+                    const double *tranwt, const double *longwt, double *cfflux,
+                    const int *run)
+{
+   if (nfaces <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   EwingWeights w;
+   for (int a = 0; a < 3; ++a) {
+      w.tranwt[a] = tranwt[a];
+      w.longwt[a] = longwt[a];
+   }
+   const int nb = (nfaces + kThreads - 1) / kThreads;
+   k_cf_flux<<<nb, kThreads, 0, s>>>(faces, nfaces, patches, u, dside, dvar, dconst, w,
+                                     cfflux, run);
+}
+
+template <int DIM, bool DVAR, int CK>
+static void rbgs_inst(cudaStream_t s, int nchunks, const PatchDesc *patches,
+                      const Chunk *chunks, double *u, const double *f, const double *dside,
+                      const double *cfield, const double *cfflux,
+                      const unsigned char *cfmask, int offset, double dconst,
+                      double cconst, unsigned long long *maxres, const int *run)
+{
+   k_rbgs<DIM, DVAR, CK><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, dside, cfield,
+                                                      cfflux, cfmask, offset, dconst,
+                                                      cconst, maxres, run);
+}
+
+void launch_rbgs(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                 const PatchDesc *patches, const Chunk *chunks, double *u, const double *f,
+                 const double *dside, const double *cfield, const double *cfflux,
+                 const unsigned char *cfmask, int offset, unsigned long long *maxres,
+                 const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+#define RB(D, V, C)                                                                   \
+   rbgs_inst<D, V, C>(s, nchunks, patches, chunks, u, f, dside, cfield, cfflux, cfmask, \
+                      offset, spec.d_const, spec.c_const, maxres, run)
+   if (dim == 2) {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RB(2, true, 2);
+         else if (spec.c_kind == 1) RB(2, true, 1);
+         else RB(2, true, 0);
+      } else {
+         if (spec.c_kind == 2) RB(2, false, 2);
+         else if (spec.c_kind == 1) RB(2, false, 1);
+         else RB(2, false, 0);
+      }
+   } else {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RB(3, true, 2);
+         else if (spec.c_kind == 1) RB(3, true, 1);
+         else RB(3, true, 0);
+      } else {
+         if (spec.c_kind == 2) RB(3, false, 2);
+         else if (spec.c_kind == 1) RB(3, false, 1);
+         else RB(3, false, 0);
+      }
+   }
+#undef RB
+}
+
+void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                 const PatchDesc *patches, const Chunk *chunks, const double *u,
+                 const double *dside, const unsigned char *cfmask, const double *tranwt,
+                 const double *longwt, const int *ratio_dev, double *flux, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   EwingWeights w;
+   for (int a = 0; a < 3; ++a) {
+      w.tranwt[a] = tranwt[a];
+      w.longwt[a] = longwt[a];
+   }
+   if (dim == 2) {
+      if (spec.d_variable)
+         k_flux<2, true><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
+                                                      cfmask, w, ratio_dev, flux, run);
+      else
+         k_flux<2, false><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
+                                                       cfmask, w, ratio_dev, flux, run);
+   } else {
+      if (spec.d_variable)
+         k_flux<3, true><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
+                                                      cfmask, w, ratio_dev, flux, run);
+      else
+         k_flux<3, false><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
+                                                       cfmask, w, ratio_dev, flux, run);
+   }
+}
+
+void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                     const PatchDesc *patches, const Chunk *chunks, const double *u,
+                     const double *f, const double *flux, const double *cfield,
+                     double *res, double *oflux, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+#define RS(D, C)                                                                         \
+   k_residual<D, C><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, flux, cfield,     \
+                                                 spec.c_const, res, oflux, run)
+   if (dim == 2) {
+      if (spec.c_kind == 2) RS(2, 2);
+      else if (spec.c_kind == 1) RS(2, 1);
+      else RS(2, 0);
+   } else {
+      if (spec.c_kind == 2) RS(3, 2);
+      else if (spec.c_kind == 1) RS(3, 1);
+      else RS(3, 0);
+   }
+#undef RS
+}
+
+void launch_flux_coarsen(cudaStream_t s, const FluxCoarsenItem *items, const Chunk *chunks,
+                         int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
+                         const double *oflux_fine, double *flux_coarse, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_flux_coarsen<<<nchunks, kThreads, 0, s>>>(items, chunks, fine, coarse, oflux_fine,
+                                               flux_coarse, run);
+}
+
+void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const Chunk *chunks,
+                     int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
+                     const double *src, int src_g, double *dst, int dst_g, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_restrict<2><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, coarse, src, src_g, dst,
+                                                 dst_g, run);
+   else
+      k_restrict<3><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, coarse, src, src_g, dst,
+                                                 dst_g, run);
+}
+
+void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const Chunk *chunks,
+                        int nchunks, const PatchDesc *fine, const double *tmp,
+                        const double *dxc_prob, const int *ratio, double *e, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_prolong_add<2><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
+                                                    ratio[0], ratio[1], ratio[2], e, run);
+   else
+      k_prolong_add<3><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
+                                                    ratio[0], ratio[1], ratio[2], e, run);
+}
+
+void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                         const Chunk *chunks, double *u, const double *e, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_add_interior<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+   else
+      k_add_interior<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+}
+
+void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                 const Chunk *chunks, const double *x, int xg, const double *w,
+                 double2 *partial, const int *prob_chunk_begin, int nprob, double2 *acc)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(2, std::memory_order_relaxed);
+   if (dim == 2)
+      k_norm_partial<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, x, xg, w, partial);
+   else
+      k_norm_partial<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, x, xg, w, partial);
+   k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
+}
+
+void launch_sweep_check(cudaStream_t s, const unsigned long long *red,
+                        const unsigned long long *blk, const int *last_patch, int nprob,
+                        double tol, int *run, long long *sweeps)
+{
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   const int nb = (nprob + 127) / 128;
+   k_sweep_check<<<nb, 128, 0, s>>>(red, blk, last_patch, nprob, tol, run, sweeps);
+}
+
+void launch_gather(cudaStream_t s, const long long *idx, long long n, const double *src,
+                   double *dst)
+{
+   if (n <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_gather<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(idx, n, src, dst);
+}
+
+void launch_scatter(cudaStream_t s, const long long *idx, long long n, const double *src,
+                    double *dst)
+{
+   if (n <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(idx, n, src, dst);
+}
+
+}  // namespace samrai_b200

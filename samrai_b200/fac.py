@@ -1,0 +1,430 @@
+"""Python binding of the B200 FAC library (C ABI in include/samrai_fac_b200.h).
+
+Two layers, mirroring the reference's own split:
+
+* :class:`FacContext` -- one-to-one with the C ABI: a batch of problems on
+  one GPU and the FACOperatorStrategy level operators
+  (solv/FACOperatorStrategy.h:83-364) plus the whole solve.
+* :class:`CellPoissonFACSolver` -- the drop-in for solv::CellPoissonFACSolver
+  (solv/CellPoissonFACSolver.h:116-475): same method names, input keys and
+  defaults, driving a FacContext.
+
+There is no CPU fallback: the CUDA library must be built
+(``python -m samrai_b200.build``) and a GPU present, or the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+
+U, F, E, R, TR, W, C = range(7)
+CELL_GHOST = [1, 0, 1, 0, 0, 0, 0]
+
+_lib = None
+
+
+class FacError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"FAC error {code}: {msg}")
+        self.code = code
+
+
+def library_path():
+    return _build.LIB
+
+
+def load_library(build_if_missing=True):
+    """Load libsamrai_fac_b200.so (building it in-tree if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise FileNotFoundError(f"{path} is missing; run python -m samrai_b200.build")
+        _build.build()
+    L = ctypes.CDLL(path)
+    vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    szp = ctypes.POINTER(ctypes.c_size_t)
+    sig = {
+        "fac_last_error": (ctypes.c_char_p, []),
+        "fac_ctx_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int]),
+        "fac_ctx_destroy": (ctypes.c_int, [vp]),
+        "fac_add_problem": (ctypes.c_int, [vp, ip, dp, dp, ctypes.c_int, ip, ip, ip, ip]),
+        "fac_set_poisson": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_double]),
+        "fac_set_bc": (ctypes.c_int, [vp, dp, dp, dp]),
+        "fac_set_params": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_int]),
+        "fac_initialize": (ctypes.c_int, [vp]),
+        "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
+        "fac_side_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
+        "fac_oside_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
+        "fac_upload_field": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_download_field": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_upload_side": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_download_side": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_download_flux": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_download_oside": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_ghost_fill": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int]),
+        "fac_smooth": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ip]),
+        "fac_comp_residual": (ctypes.c_int, [vp] + [ctypes.c_int] * 5),
+        "fac_restrict": (ctypes.c_int, [vp] + [ctypes.c_int] * 3),
+        "fac_restrict_solution": (ctypes.c_int, [vp] + [ctypes.c_int] * 2),
+        "fac_prolong_correct": (ctypes.c_int, [vp] + [ctypes.c_int] * 3),
+        "fac_compute_weights": (ctypes.c_int, [vp]),
+        "fac_rms_norm": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "fac_solve_coarsest": (ctypes.c_int, [vp, ip]),
+        "fac_fac_cycle": (ctypes.c_int, [vp]),
+        "fac_solve": (ctypes.c_int, [vp, ip, ip, dp]),
+        "fac_solve_host": (ctypes.c_int, [vp, ctypes.POINTER(dp), ctypes.POINTER(dp),
+                                          ctypes.POINTER(dp), ip, ip, dp]),
+        "fac_residual_history": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, ip]),
+        "fac_coarse_sweeps": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
+        "fac_reset_stats": (ctypes.c_int, [vp]),
+        "fac_synchronize": (ctypes.c_int, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Names of the C ABI entry points this binding expects."""
+    load_library()
+    return [n for n in dir(_lib) if n.startswith("fac_")]
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _check(rc):
+    if rc != 0:
+        raise FacError(rc, load_library().fac_last_error().decode())
+
+
+class FacContext:
+    """A batch of FAC problems on one GPU (device=-1: host-only table check)."""
+
+    def __init__(self, problems: Sequence, params: Optional[dict] = None, device: int = 0,
+                 bc=None):
+        L = load_library()
+        problems = list(problems)
+        if not problems:
+            raise ValueError("no problems")
+        self.problems = problems
+        self.dim = problems[0].dim
+        self.nlev = problems[0].nlev
+        self.device = device
+        h = ctypes.c_void_p()
+        _check(L.fac_ctx_create(ctypes.byref(h), self.dim, device))
+        self.h = h
+        p0 = problems[0]
+        _check(L.fac_set_poisson(h, int(p0.d_variable), float(p0.d_const), int(p0.c_kind),
+                                 float(p0.c_const)))
+        if bc is not None:
+            a, b, g = (np.ascontiguousarray(x, dtype=np.float64) for x in bc)
+            _check(L.fac_set_bc(h, _dp(a), _dp(b), _dp(g)))
+        prm = dict(max_cycles=100, residual_tol=1e-300, relative_residual_tol=1e-10,
+                   pre_sweeps=2, post_sweeps=2, coarse_tol=1e-8, coarse_max_it=500, ewing=1)
+        if params:
+            prm.update(params)
+        self.params = prm
+        _check(L.fac_set_params(h, prm["max_cycles"], prm["residual_tol"],
+                                prm["relative_residual_tol"], prm["pre_sweeps"],
+                                prm["post_sweeps"], prm["coarse_tol"], prm["coarse_max_it"],
+                                prm["ewing"]))
+        for prob in problems:
+            n0 = np.array(prob.n0, dtype=np.int32)
+            xlo = np.array(prob.xlo, dtype=np.float64)
+            xup = np.array(prob.xup, dtype=np.float64)
+            ratio = np.array([lv.ratio for lv in prob.levels], dtype=np.int32).reshape(-1)
+            npatch = np.array([len(lv.boxes) for lv in prob.levels], dtype=np.int32)
+            boxes = np.ascontiguousarray(
+                np.concatenate([lv.boxes for lv in prob.levels]).astype(np.int32).reshape(-1))
+            idx = ctypes.c_int(0)
+            _check(L.fac_add_problem(h, _ip(n0), _dp(xlo), _dp(xup), prob.nlev, _ip(ratio),
+                                     _ip(npatch), _ip(boxes), ctypes.byref(idx)))
+        _check(L.fac_initialize(h))
+        if device >= 0:
+            for ip_, prob in enumerate(problems):
+                for ln in range(self.nlev):
+                    if prob.f:
+                        self.upload(F, ip_, ln, prob.f[ln])
+                    if prob.u0:
+                        self.upload(U, ip_, ln, prob.u0[ln])
+                    if prob.d_variable:
+                        self.upload_side(ip_, ln, prob.d[ln])
+                    if prob.c_kind == 2:
+                        self.upload(C, ip_, ln, prob.c[ln])
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().fac_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nprob(self):
+        return len(self.problems)
+
+    # sizes and transfers ----------------------------------------------------
+    def size(self, fid, prob, ln):
+        n = ctypes.c_size_t(0)
+        _check(load_library().fac_field_size(self.h, fid, prob, ln, ctypes.byref(n)))
+        return n.value
+
+    def upload(self, fid, prob, ln, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        if arr.size != self.size(fid, prob, ln):
+            raise ValueError(f"size {arr.size} != {self.size(fid, prob, ln)}")
+        _check(load_library().fac_upload_field(self.h, fid, prob, ln, _dp(arr)))
+
+    def download(self, fid, prob, ln):
+        out = np.empty(self.size(fid, prob, ln))
+        _check(load_library().fac_download_field(self.h, fid, prob, ln, _dp(out)))
+        return out
+
+    def upload_side(self, prob, ln, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        _check(load_library().fac_upload_side(self.h, prob, ln, _dp(arr)))
+
+    def _side_n(self, prob, ln):
+        n = ctypes.c_size_t(0)
+        _check(load_library().fac_side_size(self.h, prob, ln, ctypes.byref(n)))
+        return n.value
+
+    def download_flux(self, prob, ln):
+        out = np.empty(self._side_n(prob, ln))
+        _check(load_library().fac_download_flux(self.h, prob, ln, _dp(out)))
+        return out
+
+    def download_oside(self, prob, ln):
+        n = ctypes.c_size_t(0)
+        _check(load_library().fac_oside_size(self.h, prob, ln, ctypes.byref(n)))
+        out = np.empty(n.value)
+        _check(load_library().fac_download_oside(self.h, prob, ln, _dp(out)))
+        return out
+
+    # operators --------------------------------------------------------------
+    def ghost_fill(self, fid, ln, with_coarse, homogeneous):
+        _check(load_library().fac_ghost_fill(self.h, fid, ln, int(with_coarse), int(homogeneous)))
+
+    def smooth(self, fid_e, fid_r, ln, nsweeps, tol=-1.0):
+        sw = np.zeros(self.nprob, dtype=np.int32)
+        _check(load_library().fac_smooth(self.h, fid_e, fid_r, ln, nsweeps, tol, _ip(sw)))
+        return sw
+
+    def comp_residual(self, fid_r, fid_u, fid_f, ln, error_eq):
+        _check(load_library().fac_comp_residual(self.h, fid_r, fid_u, fid_f, ln, int(error_eq)))
+
+    def restrict(self, fid_src, fid_dst, dest_ln):
+        _check(load_library().fac_restrict(self.h, fid_src, fid_dst, dest_ln))
+
+    def restrict_solution(self, fid, dest_ln):
+        _check(load_library().fac_restrict_solution(self.h, fid, dest_ln))
+
+    def prolong_correct(self, fid_src, fid_dst, dest_ln):
+        _check(load_library().fac_prolong_correct(self.h, fid_src, fid_dst, dest_ln))
+
+    def compute_weights(self):
+        _check(load_library().fac_compute_weights(self.h))
+
+    def rms_norm(self, fid):
+        out = np.zeros(self.nprob)
+        _check(load_library().fac_rms_norm(self.h, fid, _dp(out)))
+        return out
+
+    def solve_coarsest(self):
+        sw = np.zeros(self.nprob, dtype=np.int32)
+        _check(load_library().fac_solve_coarsest(self.h, _ip(sw)))
+        return sw
+
+    def fac_cycle(self):
+        _check(load_library().fac_fac_cycle(self.h))
+
+    def solve(self):
+        conv = np.zeros(self.nprob, dtype=np.int32)
+        its = np.zeros(self.nprob, dtype=np.int32)
+        res = np.zeros(self.nprob)
+        _check(load_library().fac_solve(self.h, _ip(conv), _ip(its), _dp(res)))
+        return conv.astype(bool), its, res
+
+    def solve_host(self, f_arrays, u_out, u0_arrays=None):
+        """End-to-end solve from host buffers (one per problem x level)."""
+        n = self.nprob * self.nlev
+        DP = ctypes.POINTER(ctypes.c_double)
+        ftab = (DP * n)(*[_dp(a) for a in f_arrays])
+        utab = (DP * n)(*[_dp(a) for a in u_out])
+        u0tab = (DP * n)(*[_dp(a) for a in u0_arrays]) if u0_arrays is not None else None
+        conv = np.zeros(self.nprob, dtype=np.int32)
+        its = np.zeros(self.nprob, dtype=np.int32)
+        res = np.zeros(self.nprob)
+        _check(load_library().fac_solve_host(self.h, ftab, u0tab, utab, _ip(conv), _ip(its),
+                                             _dp(res)))
+        return conv.astype(bool), its, res
+
+    def residual_history(self, prob):
+        cap = self.params["max_cycles"] + 1
+        out = np.zeros(cap)
+        n = ctypes.c_int(0)
+        _check(load_library().fac_residual_history(self.h, prob, _dp(out), cap, ctypes.byref(n)))
+        return out[:min(n.value, cap)]
+
+    def coarse_sweeps(self):
+        out = np.zeros(self.nprob, dtype=np.int64)
+        _check(load_library().fac_coarse_sweeps(
+            self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
+        return out
+
+    def synchronize(self):
+        _check(load_library().fac_synchronize(self.h))
+
+
+class CellPoissonFACSolver:
+    """Drop-in for solv::CellPoissonFACSolver (CellPoissonFACSolver.h:116-475).
+
+    The reference identifies data by patch-data ids on a PatchHierarchy; here
+    a :class:`samrai_b200.configs.Problem` carries the hierarchy and its u,
+    f, D and C arrays, and the solver writes the converged u back into it.
+    Input keys and defaults follow FACPreconditioner (FACPreconditioner.C:
+    80-114) and CellPoissonFACOps (CellPoissonFACOps.C:692-739).
+    """
+
+    def __init__(self, dim: int, object_name: str = "CellPoissonFACSolver",
+                 input_db: Optional[dict] = None):
+        self.dim = dim
+        self.object_name = object_name
+        db = dict(input_db or {})
+        self._params = dict(max_cycles=db.get("max_cycles", 10),
+                            residual_tol=db.get("residual_tol", 1e-6),
+                            relative_residual_tol=db.get("relative_residual_tol", -1.0),
+                            pre_sweeps=db.get("num_pre_sweeps", 1),
+                            post_sweeps=db.get("num_post_sweeps", 1),
+                            coarse_tol=db.get("coarse_solver_tolerance", 1e-8),
+                            coarse_max_it=db.get("coarse_solver_max_iterations", 500),
+                            ewing=1)
+        if db.get("coarse_solver_choice", "redblack") not in ("redblack", "jacobi"):
+            raise ValueError("coarse_solver_choice must be redblack (hypre is not built)")
+        if db.get("cf_discretization", "Ewing") != "Ewing":
+            raise ValueError("only cf_discretization = Ewing is implemented")
+        if db.get("prolongation_method", "LINEAR_REFINE") != "LINEAR_REFINE":
+            raise ValueError("only prolongation_method = LINEAR_REFINE is implemented")
+        self._d_const = 1.0
+        self._d_variable = False
+        self._c_kind = 0
+        self._c_const = 0.0
+        self._bc = None
+        self._ctx: Optional[FacContext] = None
+        self._problems = None
+        self._device = 0
+        self._last = None
+
+    # PoissonSpecifications setters (CellPoissonFACSolver.h:312-365)
+    def setDConstant(self, d):
+        self._d_const, self._d_variable = float(d), False
+
+    def setDPatchDataId(self, flag=True):
+        self._d_variable = True
+
+    def setCConstant(self, c):
+        self._c_kind, self._c_const = (0, 0.0) if c == 0 else (1, float(c))
+
+    def setCPatchDataId(self, flag=True):
+        self._c_kind = 2
+
+    def setBoundaries(self, boundary_type="Dirichlet"):
+        """setBoundaries (CellPoissonFACSolver.h:264): only Dirichlet with
+        the cached ghost value g=0 or Robin coefficient triples."""
+        if boundary_type != "Dirichlet":
+            raise ValueError("only Dirichlet boundaries are supported here")
+        self._bc = None
+
+    def setBcObject(self, a, b, g):
+        self._bc = (a, b, g)
+
+    def setMaxCycles(self, n):
+        self._params["max_cycles"] = int(n)
+
+    def setResidualTolerance(self, tol, relative_tol=-1.0):
+        self._params["residual_tol"] = float(tol)
+        self._params["relative_residual_tol"] = float(relative_tol)
+
+    def setPresmoothingSweeps(self, n):
+        self._params["pre_sweeps"] = int(n)
+
+    def setPostsmoothingSweeps(self, n):
+        self._params["post_sweeps"] = int(n)
+
+    def setCoarsestLevelSolverTolerance(self, tol):
+        self._params["coarse_tol"] = float(tol)
+
+    def setCoarsestLevelSolverMaxIterations(self, n):
+        self._params["coarse_max_it"] = int(n)
+
+    def initializeSolverState(self, problems, device: int = 0):
+        """initializeSolverState (CellPoissonFACSolver.h:402): builds the
+        device state for one problem or a batch of problems."""
+        if not isinstance(problems, (list, tuple)):
+            problems = [problems]
+        for p in problems:
+            p.d_variable, p.d_const = self._d_variable or p.d_variable, self._d_const
+            if self._c_kind:
+                p.c_kind, p.c_const = self._c_kind, self._c_const
+        self._problems = list(problems)
+        self._ctx = FacContext(self._problems, self._params, device=device, bc=self._bc)
+
+    def deallocateSolverState(self):
+        if self._ctx:
+            self._ctx.close()
+        self._ctx = None
+
+    def solveSystem(self, problems=None):
+        """solveSystem (CellPoissonFACSolver.h:183/214).  Returns True when
+        every problem converged; the solution is stored in each problem's
+        ``u`` list."""
+        own = self._ctx is None
+        if own:
+            self.initializeSolverState(problems)
+        conv, its, res = self._ctx.solve()
+        for ip_, p in enumerate(self._problems):
+            p.u = [self._ctx.download(U, ip_, ln) for ln in range(p.nlev)]
+        self._last = (conv, its, res)
+        if own:
+            self.deallocateSolverState()
+        return bool(conv.all())
+
+    def getNumberOfIterations(self):
+        return int(self._last[1].max())
+
+    def getResidualNorm(self):
+        return float(self._last[2].max())
+
+    def getConvergenceFactors(self):
+        hist = self._ctx.residual_history(0) if self._ctx else None
+        if hist is None or len(hist) < 2:
+            return float("nan"), float("nan")
+        net = hist[-1] / (hist[0] + 1e-20)
+        avg = net ** (1.0 / (len(hist) - 1))
+        return avg, hist[-1] / hist[-2]

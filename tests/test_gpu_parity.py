@@ -1,0 +1,184 @@
+"""GPU parity of every FAC level operator and of the whole solve against the
+CPU oracle, through the C ABI.
+
+Bars: ghost fills are bit-exact; smoothing, residual, flux, restriction,
+prolongation and the converged solution match to 1e-12 relative (the FP64
+kernels use the reference's operation order with FMA contraction off, so in
+practice they are bit-exact too); norms to 1e-13 relative.
+"""
+import numpy as np
+import pytest
+
+from samrai_b200 import configs, fac
+from oracle.oracle import C, E, F, Oracle, R, TR, U, W, SD
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a - b).max() / scale)
+
+
+def pair(prob, params=None):
+    o = Oracle(prob, params=params)
+    g = fac.FacContext([prob], params=params)
+    return o, g
+
+
+def randomize(prob, o, g, rng, fields=(U, E, R, F, TR)):
+    for ln in range(prob.nlev):
+        for fid in fields:
+            v = rng.standard_normal(o.size(fid, ln))
+            o.set(fid, ln, v)
+            g.upload(fid, 0, ln, v)
+
+
+CONFIGS = [configs.config1, configs.config3, configs.small_3d]
+
+
+@pytest.mark.parametrize("mk", CONFIGS)
+@pytest.mark.parametrize("homogeneous", [0, 1])
+def test_ghost_fill_bit_exact(mk, homogeneous, require_gpu):
+    p = mk()
+    o, g = pair(p)
+    randomize(p, o, g, np.random.default_rng(1))
+    for ln in range(p.nlev):
+        for with_coarse in ([0, 1] if ln > 0 else [0]):
+            o.ghost_fill(U, ln, with_coarse, homogeneous)
+            g.ghost_fill(U, ln, with_coarse, homogeneous)
+            assert np.array_equal(g.download(U, 0, ln), o.get(U, ln)), (ln, with_coarse)
+
+
+@pytest.mark.parametrize("mk", CONFIGS)
+def test_smooth(mk, require_gpu):
+    p = mk()
+    o, g = pair(p)
+    randomize(p, o, g, np.random.default_rng(2))
+    for ln in range(p.nlev):
+        o.smooth(E, R, ln, 2, -1.0)
+        g.smooth(E, R, ln, 2, -1.0)
+        assert rel_err(g.download(E, 0, ln), o.get(E, ln)) <= REL
+        assert np.array_equal(g.download(E, 0, ln), o.get(E, ln))
+
+
+@pytest.mark.parametrize("mk", [configs.config1, configs.small_3d])
+def test_coarse_solve_sweep_count(mk, require_gpu):
+    p = mk()
+    o, g = pair(p, params=dict(coarse_tol=1e-3, coarse_max_it=200))
+    randomize(p, o, g, np.random.default_rng(3), fields=(E, R))
+    n_o, _ = o.smooth(E, R, 0, 200, 1e-3)
+    n_g = g.smooth(E, R, 0, 200, 1e-3)
+    assert int(n_g[0]) == n_o
+    assert rel_err(g.download(E, 0, 0), o.get(E, 0)) <= REL
+
+
+@pytest.mark.parametrize("mk", CONFIGS)
+@pytest.mark.parametrize("error_eq", [0, 1])
+def test_composite_residual(mk, error_eq, require_gpu):
+    p = mk()
+    o, g = pair(p)
+    randomize(p, o, g, np.random.default_rng(4))
+    for ln in range(p.nlev - 1, -1, -1):
+        o.comp_residual(R, U, F, ln, error_eq)
+        g.comp_residual(R, U, F, ln, error_eq)
+        assert rel_err(g.download(R, 0, ln), o.get(R, ln)) <= REL, ln
+        assert rel_err(g.download_flux(0, ln), o.get_side(1, ln)) <= REL, ln
+        if ln > 0:
+            assert rel_err(g.download_oside(0, ln), o.get_oside(ln)) <= REL, ln
+        assert np.array_equal(g.download(U, 0, ln), o.get(U, ln))
+
+
+@pytest.mark.parametrize("mk", CONFIGS)
+def test_restrict_and_prolong(mk, require_gpu):
+    p = mk()
+    o, g = pair(p)
+    randomize(p, o, g, np.random.default_rng(5))
+    for ln in range(p.nlev - 2, -1, -1):
+        o.restrict(TR, R, ln)
+        g.restrict(TR, R, ln)
+        assert rel_err(g.download(R, 0, ln), o.get(R, ln)) <= REL
+        o.restrict_solution(U, ln)
+        g.restrict_solution(U, ln)
+        assert rel_err(g.download(U, 0, ln), o.get(U, ln)) <= REL
+    for ln in range(1, p.nlev):
+        o.prolong_correct(E, E, ln)
+        g.prolong_correct(E, E, ln)
+        assert rel_err(g.download(E, 0, ln), o.get(E, ln)) <= REL
+
+
+@pytest.mark.parametrize("mk", CONFIGS)
+def test_rms_norm(mk, require_gpu):
+    p = mk()
+    o, g = pair(p)
+    randomize(p, o, g, np.random.default_rng(6), fields=(R,))
+    o.compute_weights()
+    g.compute_weights()
+    for ln in range(p.nlev):
+        assert np.array_equal(g.download(W, 0, ln), o.get(W, ln))
+    assert abs(g.rms_norm(R)[0] - o.rms_norm(R)) <= 1e-13 * o.rms_norm(R)
+
+
+def _solution_check(p, o, g, prob_index=0):
+    for ln in range(p.nlev):
+        assert rel_err(g.download(U, prob_index, ln), o.get(U, ln)) <= REL, ln
+
+
+def test_full_solve_config1(require_gpu):
+    p = configs.config1()
+    prm = dict(coarse_tol=1e-10)
+    o, g = pair(p, prm)
+    ok_o, it_o, res_o, hist_o = o.solve()
+    conv, its, res = g.solve()
+    assert ok_o and conv[0]
+    assert its[0] == it_o
+    hist_g = g.residual_history(0)
+    assert len(hist_g) == len(hist_o)
+    assert rel_err(hist_g, hist_o) <= 1e-11
+    _solution_check(p, o, g)
+    assert np.array_equal(g.coarse_sweeps(), [o.coarse_sweeps()])
+
+
+def test_full_solve_small_3d(require_gpu):
+    p = configs.small_3d()
+    prm = dict(coarse_tol=1e-10, max_cycles=6)
+    o, g = pair(p, prm)
+    o.solve()
+    g.solve()
+    assert len(g.residual_history(0)) == 7
+    _solution_check(p, o, g)
+
+
+def test_full_solve_varcoef_config3(require_gpu):
+    p = configs.config3()
+    prm = dict(coarse_tol=1e-10, max_cycles=8)
+    o, g = pair(p, prm)
+    ok_o, it_o, res_o, hist_o = o.solve()
+    conv, its, res = g.solve()
+    assert its[0] == it_o
+    assert rel_err(g.residual_history(0), hist_o) <= 1e-11
+    _solution_check(p, o, g)
+
+
+def test_batched_problems_match_individual_oracles(require_gpu):
+    probs = [configs.small_3d(seed=s) for s in (11, 12, 13)]
+    prm = dict(coarse_tol=1e-10, max_cycles=4)
+    g = fac.FacContext(probs, params=prm)
+    g.solve()
+    for i, p in enumerate(probs):
+        o = Oracle(p, params=prm)
+        o.solve()
+        _solution_check(p, o, g, prob_index=i)
+
+
+def test_config2_one_cycle(require_gpu):
+    p = configs.config2()
+    prm = dict(coarse_tol=1e-10, coarse_max_it=10, max_cycles=1)
+    o, g = pair(p, prm)
+    o.solve()
+    g.solve()
+    _solution_check(p, o, g)
