@@ -101,6 +101,14 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol,
                    int post_sweeps, double coarse_tol, int coarse_max_it,
                    int ewing);
 
+/* Precision of the FAC cycle (call before fac_initialize).  0: all FP64, the
+ * reference's arithmetic.  1: mixed -- red-black smoothing, prolongation
+ * and the error vector in FP32; composite residual with its coarse-fine
+ * flux sums, residual restriction, coarsest-level solve and the outer
+ * defect-correction loop in FP64.  No reference counterpart (the reference
+ * is FP64 throughout). */
+int fac_set_precision(fac_ctx *ctx, int mixed);
+
 /* Build device tables and allocate device state
  * (CellPoissonFACOps::initializeOperatorState, CellPoissonFACOps.C:751-1106). */
 int fac_initialize(fac_ctx *ctx);
@@ -173,6 +181,10 @@ int fac_solve_host(fac_ctx *ctx, const double *const *f_host,
                    const double *const *u0_host, double *const *u_host,
                    int *converged, int *iterations, double *residual);
 
+/* Set a cell field to zero on every level of every problem (ghosts
+ * included), e.g. u before a solve from a zero initial guess. */
+int fac_zero_field(fac_ctx *ctx, int fid);
+
 /* Per-cycle residual norms of the last fac_solve for one problem:
  * hist[0] = before the first cycle, hist[k] after cycle k; *n entries. */
 int fac_residual_history(fac_ctx *ctx, int problem, double *hist, int cap,
@@ -189,10 +201,16 @@ int fac_synchronize(fac_ctx *ctx);
 /* ---- instrumentation (the reference's tbox::Timer around each FAC op,
  *      CellPoissonFACOps.C:626-639, as CUDA events on the context stream). */
 
+/* Per-operation wall-clock totals with a stream synchronisation around each
+ * operation (tbox::Timer::barrierAndStart semantics); fac_trace_read writes
+ * a JSON object {"op@Lln": [calls, ms], ...}. */
+int fac_trace_enable(fac_ctx *ctx, int on);
+int fac_trace_read(fac_ctx *ctx, char *buf, int cap, int *len);
 /* Kernels launched by this process so far, over all contexts. */
 int fac_kernel_launches(long long *n);
-/* Record CUDA events around every red-black colour pass (kind 0) and
- * ghost fill (kind 1) from now on; clears earlier records. */
+/* Record CUDA events around every red-black colour pass (kind 0 FP64,
+ * kind 2 FP32) and ghost fill (kind 1 FP64, kind 3 FP32) from now on;
+ * clears earlier records.  Bytes count only problems still iterating. */
 int fac_profile_enable(fac_ctx *ctx, int on);
 /* Totals over the records of one kind: launches, device milliseconds and
  * algorithmic bytes (colour pass: 8*(ghosted cells + cells) + 8*dim*cells

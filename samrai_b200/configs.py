@@ -453,6 +453,123 @@ def small_3d(seed=7, n0=32) -> Problem:
     return p
 
 
-def config5(nprob=64):
-    """64 independent 3-D variable-coefficient problems (seeds 0..63)."""
-    return [config5_problem(s) for s in range(nprob)]
+def config5(nprob=64, first_seed=0, workers=None):
+    """64 independent 3-D variable-coefficient problems (seeds 0..63),
+    generated in parallel worker processes."""
+    seeds = list(range(first_seed, first_seed + nprob))
+    if workers is None:
+        import os
+        workers = min(len(seeds), os.cpu_count() or 1, 32)
+    if workers <= 1:
+        return [config5_problem(s) for s in seeds]
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_config5_worker, seeds)
+
+
+def _config5_worker(seed):
+    try:
+        from threadpoolctl import threadpool_limits
+        with threadpool_limits(1):
+            return config5_problem(seed)
+    except ImportError:
+        return config5_problem(seed)
+
+
+# ---------------------------------------------------------------------------
+# virtual coarse levels (multigrid coarsest-level solve for the fast variant)
+# ---------------------------------------------------------------------------
+
+def extend_hierarchy(prob: Problem, min_cells: int = 8, k: Optional[int] = None) -> Problem:
+    """Prepend k levels that coarsen the domain by 2 (default: until the
+    coarsest has fewer than 2*min_cells cells per side or an odd count).
+
+    The added levels each cover the whole domain, so every one of their
+    cells is covered by the next finer level: the composite problem, its
+    weights and its residual norm are unchanged, and the FAC cycle becomes
+    a full multigrid V-cycle whose coarsest solve is cheap (SAMRAI reaches
+    the same effect with its hypre coarse solver, CellPoissonFACOps.C:
+    1741-1781).  D on an added level is the mean of the finer faces on each
+    coarse face; f and u0 there are zero (fully covered cells)."""
+    dim = prob.dim
+    n = list(prob.n0[:dim])
+    if k is None:
+        k = 0
+        while all(x % 2 == 0 and x // 2 >= min_cells for x in n):
+            n = [x // 2 for x in n]
+            k += 1
+    else:
+        assert all(x % (2 ** k) == 0 for x in n), "domain not divisible by 2^k"
+    if k == 0:
+        return prob
+    # level 0 of the input must cover the domain
+    b0 = prob.levels[0].boxes
+    cov = int(np.prod(b0[:, 3:] - b0[:, :3] + 1, axis=1).sum())
+    assert cov == int(np.prod([prob.n0[a] for a in range(dim)])), "level 0 must cover the domain"
+    levels = []
+    for j in range(k, 0, -1):
+        m = [x // (2 ** j) for x in prob.n0[:dim]]
+        hi = [m[a] - 1 if a < dim else 0 for a in range(3)]
+        ratio = (1, 1, 1) if j == k else tuple(2 if a < dim else 1 for a in range(3))
+        levels.append(Level(ratio, np.array([[0, 0, 0] + hi], dtype=np.int32)))
+    first_orig = Level(tuple(2 if a < dim else 1 for a in range(3)), prob.levels[0].boxes)
+    levels.append(first_orig)
+    levels.extend(prob.levels[1:])
+    n0 = tuple(prob.n0[a] // (2 ** k) if a < dim else 1 for a in range(3))
+    ext = Problem(dim=dim, n0=n0, xlo=prob.xlo, xup=prob.xup, levels=levels,
+                  d_variable=prob.d_variable, d_const=prob.d_const, c_kind=prob.c_kind,
+                  c_const=prob.c_const, name=prob.name + f"+{k}mg")
+    ext.virtual_levels = k
+    ext.f = [np.zeros(field_size(ext, ln, 0)) for ln in range(k)] + list(prob.f)
+    ext.u0 = [np.zeros(field_size(ext, ln, 1)) for ln in range(k)] + list(prob.u0)
+    if prob.c_kind == 2:
+        ext.c = [np.zeros(field_size(ext, ln, 0)) for ln in range(k)] + list(prob.c)
+    if prob.d_variable:
+        dk = [None] * k + list(prob.d)
+        # dense side grids of the original level 0 (covers the domain)
+        dense = _dense_side(prob, 0, prob.d[0])
+        for ln in range(k - 1, -1, -1):
+            dense = [_coarsen_dense_side(dense[a], a, dim) for a in range(dim)]
+            dk[ln] = np.concatenate([dense[a].reshape(-1) for a in range(dim)])
+        ext.d = dk
+    return ext
+
+
+def _dense_side(prob: Problem, ln: int, d: np.ndarray):
+    """Per-axis dense side arrays (z, y, x) over the domain of level ln from
+    the patch side data of a level that covers the domain."""
+    dim = prob.dim
+    lo, hi = prob.domain(ln)
+    n = [hi[a] - lo[a] + 1 for a in range(3)]
+    out = []
+    for a in range(dim):
+        e = list(n)
+        e[a] += 1
+        out.append(np.zeros((e[2], e[1], e[0])))
+    off = 0
+    for b in prob.levels[ln].boxes:
+        for a in range(dim):
+            lo_b = b[:3].copy()
+            hi_b = b[3:].copy()
+            hi_b[a] += 1
+            ext = hi_b - lo_b + 1
+            cnt = int(np.prod(ext))
+            v = d[off:off + cnt].reshape(ext[2], ext[1], ext[0])
+            out[a][lo_b[2]:hi_b[2] + 1, lo_b[1]:hi_b[1] + 1, lo_b[0]:hi_b[0] + 1] = v
+            off += cnt
+    return out
+
+
+def _coarsen_dense_side(s: np.ndarray, a: int, dim: int):
+    """Mean of the 2^(dim-1) fine faces on each coarse face of axis a."""
+    ax = {0: 2, 1: 1, 2: 0}[a]          # numpy axis of index a
+    # keep every other face along the normal axis
+    sl = [slice(None)] * 3
+    sl[ax] = slice(0, None, 2)
+    t = s[tuple(sl)]
+    tang = [x for x in (0, 1, 2) if x != a and x < dim]
+    for tt in tang:
+        nax = {0: 2, 1: 1, 2: 0}[tt]
+        t = 0.5 * (np.take(t, range(0, t.shape[nax], 2), axis=nax) +
+                   np.take(t, range(1, t.shape[nax], 2), axis=nax))
+    return np.ascontiguousarray(t)

@@ -5,6 +5,8 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -233,12 +235,16 @@ struct LevelState {
    std::vector<long long> prob_off1, prob_off0, prob_offs, prob_offo;  // size nprob+1
    int ratio[3] = {1, 1, 1};
    double tranwt[3] = {0, 0, 0}, longwt[3] = {0, 0, 0};
-   double rb_bytes = 0, fill_bytes = 0;  // algorithmic bytes per launch
+   double rb_bytes = 0, fill_bytes = 0;  // algorithmic bytes per launch (all problems)
+   std::vector<double> rb_bytes_prob, fill_bytes_prob;  // per problem
    std::vector<Box> domain;            // per problem
    std::vector<double> dx;             // per problem x3
 
    DevArray<PatchDesc> d_patches;
    DevArray<double> u, e, f, r, tr, w, c, d, flux, oflux, cfflux;
+   // FP32 copies for the mixed-precision cycle (error, smoother rhs, D, C,
+   // Ewing fluxes, coarse interpolation arrays)
+   DevArray<float> e32, r32, d32, c32, cfflux32, tmp32;
    DevArray<unsigned char> cfmask;
    DevArray<int> d_ratio;
 
@@ -287,6 +293,8 @@ struct fac_ctx {
    double coarse_tol = 1e-8;
    int coarse_max_it = 500;
    int ewing = 1;
+   int mixed = 0;            // 1: FP32 smoothing and error transfer
+   std::vector<int> host_active;  // host copy of the active flags (instrumentation)
    int check_interval = 8;   // sweeps between host checks of convergence flags
 
    // optional per-kernel timing with CUDA events on the context stream
@@ -296,6 +304,10 @@ struct fac_ctx {
       double bytes;
    };
    bool profiling = false;
+   // per-operation wall time with a stream synchronisation on both sides
+   // (tbox::Timer::barrierAndStart semantics, tbox/Timer.C:174)
+   bool tracing = false;
+   std::map<std::string, std::pair<long long, double>> trace;
    std::vector<ProfRec> prof;
    std::vector<cudaEvent_t> ev_pool;
    size_t ev_next = 0;
@@ -319,6 +331,29 @@ namespace {
 
 int nprob(const fac_ctx *c) { return (int)c->probs.size(); }
 
+struct OpTimer {
+   fac_ctx *c;
+   std::string name;
+   std::chrono::steady_clock::time_point t0;
+   OpTimer(fac_ctx *ctx, const char *n, int ln) : c(ctx)
+   {
+      if (!c->tracing) return;
+      name = std::string(n) + "@L" + std::to_string(ln);
+      cudaStreamSynchronize(c->stream);
+      t0 = std::chrono::steady_clock::now();
+   }
+   ~OpTimer()
+   {
+      if (!c->tracing) return;
+      cudaStreamSynchronize(c->stream);
+      const double ms =
+         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      auto &e = c->trace[name];
+      e.first += 1;
+      e.second += ms;
+   }
+};
+
 cudaEvent_t next_event(fac_ctx *c)
 {
    if (c->ev_next == c->ev_pool.size()) {
@@ -327,6 +362,14 @@ cudaEvent_t next_event(fac_ctx *c)
       c->ev_pool.push_back(e);
    }
    return c->ev_pool[c->ev_next++];
+}
+
+double active_bytes(const fac_ctx *c, const std::vector<double> &per_prob)
+{
+   double b = 0;
+   for (size_t p = 0; p < per_prob.size(); ++p)
+      if (p >= c->host_active.size() || c->host_active[p]) b += per_prob[p];
+   return b;
 }
 
 // Record the start of a profiled launch; returns its index or -1.
@@ -741,7 +784,15 @@ void build_chunks(fac_ctx *c, int ln)
    }
    L.rb_bytes = 8.0 * (ng + n) + (c->spec.d_variable ? 8.0 * dim * n : 0.0) +
                 (c->spec.c_kind == 2 ? 4.0 * n : 0.0);
+   L.rb_bytes_prob.assign(np, 0.0);
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      const double pn = (double)L.box[ip].size(), pg = (double)cell_count(dim, L.box[ip], 1);
+      L.rb_bytes_prob[L.hp[ip].prob] += 8.0 * (pg + pn) +
+                                         (c->spec.d_variable ? 8.0 * dim * pn : 0.0) +
+                                         (c->spec.c_kind == 2 ? 4.0 * pn : 0.0);
+   }
    double gcells = 0;
+   L.fill_bytes_prob.assign(np, 0.0);
    for (const FillItem &it : L.fill_nc.items) {
       Box b;
       for (int a = 0; a < 3; ++a) {
@@ -749,6 +800,7 @@ void build_chunks(fac_ctx *c, int ln)
          b.hi[a] = it.hi[a];
       }
       gcells += (double)b.size();
+      L.fill_bytes_prob[it.prob] += 16.0 * (double)b.size();
    }
    L.fill_bytes = 16.0 * gcells;
 }
@@ -893,6 +945,11 @@ void build_prolong_tables(fac_ctx *c, int ln)
       Fl.prolong.add(pi, Fl.box[ip].size());
    }
    Fl.tmp.alloc(std::max<long long>(1, toff));
+   if (c->mixed) {
+      Fl.tmp32.alloc(std::max<long long>(1, toff));
+      if (!g_dry)
+         CUDA_CHECK(cudaMemsetAsync(Fl.tmp32.p, 0xff, Fl.tmp32.n * sizeof(float), c->stream));
+   }
    // cells of the interpolation array that nothing fills stay NaN
    if (!g_dry)
       CUDA_CHECK(cudaMemsetAsync(Fl.tmp.p, 0xff, Fl.tmp.n * sizeof(double), c->stream));
@@ -1147,6 +1204,16 @@ void initialize(fac_ctx *c)
             CUDA_CHECK(cudaMemsetAsync(b->p, 0, b->n * sizeof(double), c->stream));
       std::vector<int> rr(L.ratio, L.ratio + 3);
       L.d_ratio.upload(rr, c->stream);
+      if (c->mixed) {
+         L.e32.alloc(n1);
+         L.r32.alloc(n0);
+         L.d32.alloc(c->spec.d_variable ? std::max<long long>(1, L.ns) : 1);
+         L.c32.alloc(c->spec.c_kind == 2 ? n0 : 1);
+         L.cfflux32.alloc(std::max<long long>(1, L.no));
+         if (!g_dry)
+            for (auto *b : {&L.e32, &L.r32, &L.d32, &L.c32, &L.cfflux32})
+               CUDA_CHECK(cudaMemsetAsync(b->p, 0, b->n * sizeof(float), c->stream));
+      }
    }
    for (int ln = 0; ln < c->nlev; ++ln) {
       build_fill_tables(c, ln);
@@ -1189,7 +1256,7 @@ void ghost_fill(fac_ctx *c, int fid, int ln, bool with_coarse, int homogeneous, 
    double *dst = field_ptr(L, fid);
    const double *coarse = ln > 0 ? field_ptr(c->L[ln - 1], fid) : nullptr;
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
-   const int pi = prof_begin(c, 1, L.fill_bytes);
+   const int pi = prof_begin(c, 1, c->profiling ? active_bytes(c, L.fill_bytes_prob) : 0.0);
    launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), dst, dst, coarse,
                homogeneous, c->bc, mask);
    prof_end(c, pi);
@@ -1198,6 +1265,7 @@ void ghost_fill(fac_ctx *c, int fid, int ln, bool with_coarse, int homogeneous, 
 // CellPoissonFACOps::smoothErrorByRedBlack (CellPoissonFACOps.C:1339-1514).
 void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
 {
+   OpTimer ot(c, tol >= 0 ? "smooth_to_tol" : "smooth", ln);
    LevelState &L = c->L[ln];
    const int np = nprob(c);
    double *e = field_ptr(L, fid_e);
@@ -1227,7 +1295,7 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
             launch_cf_flux(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, e, L.d.p,
                            c->spec.d_variable, c->spec.d_const, L.tranwt, L.longwt, L.cfflux.p,
                            c->run.p);
-         const int pi = prof_begin(c, 0, L.rb_bytes);
+         const int pi = prof_begin(c, 0, c->profiling ? active_bytes(c, L.rb_bytes_prob) : 0.0);
          launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
                      L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
                      color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p);
@@ -1243,6 +1311,7 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
 // CellPoissonFACOps::computeCompositeResidualOnLevel (CellPoissonFACOps.C:1792-1956).
 void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int error_eq)
 {
+   OpTimer ot(c, "comp_residual", ln);
    LevelState &L = c->L[ln];
    const int *run = c->active.p;
    ghost_fill(c, fid_u, ln, ln > 0, error_eq, run);
@@ -1264,6 +1333,7 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
 
 void restrict_op(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
 {
+   OpTimer ot(c, "restrict", dest_ln);
    LevelState &C = c->L[dest_ln];
    LevelState &Fl = c->L[dest_ln + 1];
    const int sg = field_ghost(fid_src), dg = field_ghost(fid_dst);
@@ -1276,6 +1346,7 @@ void restrict_op(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
 
 void restrict_solution(fac_ctx *c, int fid, int dest_ln)
 {
+   OpTimer ot(c, "restrict_solution", dest_ln);
    restrict_op(c, fid, fid, dest_ln);
    ghost_fill(c, fid, dest_ln, dest_ln > 0, 0, c->active.p);
 }
@@ -1283,12 +1354,14 @@ void restrict_solution(fac_ctx *c, int fid, int dest_ln)
 // CellPoissonFACOps::prolongErrorAndCorrect (CellPoissonFACOps.C:1254-1304).
 void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
 {
+   OpTimer ot(c, "prolong", dest_ln);
    LevelState &Fl = c->L[dest_ln];
    LevelState &C = c->L[dest_ln - 1];
    if (field_ghost(fid_src) != 1 || field_ghost(fid_dst) != 1)
       throw FacError(FAC_ERR_ARG, "prolongation needs ghosted cell fields");
-   launch_fill(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p, Fl.tmp_fill.nchunks(),
-               Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1, c->bc, c->active.p);
+   launch_fill<double>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
+                       Fl.tmp_fill.nchunks(), Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1, c->bc,
+                       c->active.p);
    launch_prolong_add(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
                       Fl.prolong.nchunks(), Fl.d_patches.p, Fl.tmp.p, Fl.dxc_prob.p, Fl.ratio,
                       field_ptr(Fl, fid_dst), c->active.p);
@@ -1297,6 +1370,7 @@ void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
 
 void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
 {
+   OpTimer ot(c, "rms_norm", 0);
    const int np = nprob(c);
    CUDA_CHECK(cudaMemsetAsync(c->norm_acc.p, 0, np * sizeof(double2), c->stream));
    const int g = field_ghost(fid);
@@ -1319,6 +1393,7 @@ void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
 
 void solve_coarsest(fac_ctx *c)
 {
+   OpTimer ot(c, "solve_coarsest", 0);
    smooth(c, FAC_E, FAC_R, 0, c->coarse_max_it, c->coarse_tol);
    // accumulate the per-call sweep counts
    const int np = nprob(c);
@@ -1364,6 +1439,7 @@ void full_composite_residual(fac_ctx *c, std::vector<double> &norms)
 
 void zero_field(fac_ctx *c, int fid)
 {
+   OpTimer ot(c, "zero_field", fid);
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
       const size_t n = field_ghost(fid) ? L.u.n : L.f.n;
@@ -1381,12 +1457,124 @@ void dirichlet(fac_ctx *c, bool restore)
    }
 }
 
+// ---------------------------------------------------------------------------
+// mixed precision cycle: FP32 smoothing, prolongation and error storage;
+// FP64 composite residual (fluxes, Ewing fix, flux sums), residual
+// restriction and coarsest-level solve.  The outer FACPreconditioner loop
+// (u, f, full composite residual, norms) stays FP64, so each cycle is a
+// defect correction that recovers FP64 accuracy.
+// ---------------------------------------------------------------------------
+
+void ghost_fill32(fac_ctx *c, int ln, bool with_coarse, int homogeneous, const int *mask)
+{
+   LevelState &L = c->L[ln];
+   const float *coarse = ln > 0 ? c->L[ln - 1].e32.p : nullptr;
+   ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
+   const int pi =
+      prof_begin(c, 3, c->profiling ? 0.5 * active_bytes(c, L.fill_bytes_prob) : 0.0);
+   launch_fill<float>(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), L.e32.p, L.e32.p,
+                      coarse, homogeneous, c->bc, mask);
+   prof_end(c, pi);
+}
+
+void smooth32(fac_ctx *c, int ln, int nsweeps)
+{
+   OpTimer ot(c, "smooth32", ln);
+   LevelState &L = c->L[ln];
+   const int np = nprob(c);
+   const int *run = c->active.p;
+   ghost_fill32(c, ln, false, 1, run);
+   if (ln > 0) ghost_fill32(c, ln, true, 1, run);
+   for (int isweep = 0; isweep < nsweeps; ++isweep) {
+      for (int color = 0; color < 2; ++color) {
+         ghost_fill32(c, ln, false, 1, run);
+         if (ln > 0)
+            launch_cf_flux<float>(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, L.e32.p,
+                                  L.d32.p, c->spec.d_variable, c->spec.d_const, L.tranwt,
+                                  L.longwt, L.cfflux32.p, run);
+         const int pi =
+            prof_begin(c, 2, c->profiling ? 0.5 * active_bytes(c, L.rb_bytes_prob) : 0.0);
+         launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
+                            L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
+                            L.c32.p, L.cfflux32.p, L.cfmask.p, color, nullptr, run);
+         prof_end(c, pi);
+      }
+      ghost_fill32(c, ln, false, 1, run);
+   }
+   (void)np;
+   CUDA_CHECK(cudaGetLastError());
+}
+
+void comp_residual_mixed(fac_ctx *c, int ln)
+{
+   OpTimer ot(c, "comp_residual_mixed", ln);
+   LevelState &L = c->L[ln];
+   const int *run = c->active.p;
+   ghost_fill32(c, ln, ln > 0, 1, run);
+   launch_flux<float>(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
+                      L.d_flux_chunks.p, L.e32.p, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
+                      L.d_ratio.p, L.flux.p, run);
+   if (ln < c->nlev - 1) {
+      LevelState &Fl = c->L[ln + 1];
+      launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
+                          L.fcoarsen.nchunks(), Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
+                          L.flux.p, run);
+   }
+   launch_residual<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
+                          L.d_cell_chunks.p, L.e32.p, L.r.p, L.flux.p, L.c.p, L.tr.p,
+                          ln > 0 ? L.oflux.p : nullptr, run);
+   CUDA_CHECK(cudaGetLastError());
+}
+
+void prolong32(fac_ctx *c, int dest_ln)
+{
+   OpTimer ot(c, "prolong32", dest_ln);
+   LevelState &Fl = c->L[dest_ln];
+   LevelState &C = c->L[dest_ln - 1];
+   launch_fill<float>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
+                      Fl.tmp_fill.nchunks(), Fl.tmp32.p, nullptr, C.e32.p, 1, c->bc,
+                      c->active.p);
+   launch_prolong_add<float>(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
+                             Fl.prolong.nchunks(), Fl.d_patches.p, Fl.tmp32.p, Fl.dxc_prob.p,
+                             Fl.ratio, Fl.e32.p, c->active.p);
+   CUDA_CHECK(cudaGetLastError());
+}
+
+void fac_cycle_mixed(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   if (ln == 0) {
+      solve_coarsest(c);
+      launch_convert<double, float>(c->stream, L.e.p, L.e32.p, (long long)L.e.n);
+      return;
+   }
+   launch_convert<double, float>(c->stream, L.r.p, L.r32.p, (long long)L.r.n);
+   smooth32(c, ln, c->pre_sweeps);
+   comp_residual_mixed(c, ln);
+   restrict_op(c, FAC_TR, FAC_R, ln - 1);
+   fac_cycle_mixed(c, ln - 1);
+   prolong32(c, ln);
+   smooth32(c, ln, c->post_sweeps);
+}
+
+void mixed_prepare(fac_ctx *c)
+{
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      if (c->spec.d_variable)
+         launch_convert<double, float>(c->stream, L.d.p, L.d32.p, (long long)L.d.n);
+      if (c->spec.c_kind == 2)
+         launch_convert<double, float>(c->stream, L.c.p, L.c32.p, (long long)L.c.n);
+   }
+}
+
 // FACPreconditioner::solveSystem (FACPreconditioner.C:277-452) inside
 // CellPoissonFACSolver::solveSystem (CellPoissonFACSolver.C:310-352).
 void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
 {
    const int np = nprob(c);
    std::vector<int> act(np, 1);
+   c->host_active = act;
    CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int), cudaMemcpyHostToDevice,
                               c->stream));
    dirichlet(c, false);
@@ -1407,13 +1595,27 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
    std::vector<int> its(np, 0);
    int it = 0;
    bool any = true;
+   if (c->mixed) mixed_prepare(c);
    while (any) {
       zero_field(c, FAC_E);
-      fac_cycle_recursive(c, c->nlev - 1);
+      if (c->mixed) {
+         for (int ln = 0; ln < c->nlev; ++ln)
+            CUDA_CHECK(cudaMemsetAsync(c->L[ln].e32.p, 0, c->L[ln].e32.n * sizeof(float),
+                                       c->stream));
+         fac_cycle_mixed(c, c->nlev - 1);
+      } else {
+         fac_cycle_recursive(c, c->nlev - 1);
+      }
       for (int ln = 0; ln < c->nlev; ++ln) {
          LevelState &L = c->L[ln];
-         launch_add_interior(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
-                             L.d_cell_chunks.p, L.u.p, L.e.p, c->active.p);
+         if (c->mixed)
+            launch_add_interior<float>(c->stream, c->dim, (int)L.cell_chunks.size(),
+                                       L.d_patches.p, L.d_cell_chunks.p, L.u.p, L.e32.p,
+                                       c->active.p);
+         else
+            launch_add_interior<double>(c->stream, c->dim, (int)L.cell_chunks.size(),
+                                        L.d_patches.p, L.d_cell_chunks.p, L.u.p, L.e.p,
+                                        c->active.p);
       }
       for (int ln = c->nlev - 2; ln >= 0; --ln) restrict_solution(c, FAC_U, ln);
       std::vector<double> nr;
@@ -1430,7 +1632,9 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
       }
       CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int),
                                  cudaMemcpyHostToDevice, c->stream));
+      c->host_active = act;
    }
+   c->host_active.assign(np, 1);
    std::vector<int> ones(np, 1);
    CUDA_CHECK(cudaMemcpyAsync(c->active.p, ones.data(), np * sizeof(int), cudaMemcpyHostToDevice,
                               c->stream));
@@ -1617,6 +1821,15 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol, double rel
       ctx->coarse_tol = coarse_tol;
       ctx->coarse_max_it = coarse_max_it;
       ctx->ewing = ewing;
+   });
+}
+
+int fac_set_precision(fac_ctx *ctx, int mixed)
+{
+   return guarded([&] {
+      check_state(ctx, false);
+      if (mixed != 0 && mixed != 1) throw FacError(FAC_ERR_ARG, "precision must be 0 or 1");
+      ctx->mixed = mixed;
    });
 }
 
@@ -1937,6 +2150,46 @@ int fac_reset_stats(fac_ctx *ctx)
       CUDA_CHECK(cudaMemsetAsync(ctx->sweeps_coarse.p, 0, nprob(ctx) * sizeof(long long),
                                  ctx->stream));
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_zero_field(fac_ctx *ctx, int fid)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      zero_field(ctx, fid);
+   });
+}
+
+int fac_trace_enable(fac_ctx *ctx, int on)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      ctx->tracing = on != 0;
+      ctx->trace.clear();
+   });
+}
+
+int fac_trace_read(fac_ctx *ctx, char *buf, int cap, int *len)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      std::string j = "{";
+      bool first = true;
+      for (const auto &kv : ctx->trace) {
+         char tmp[256];
+         std::snprintf(tmp, sizeof(tmp), "%s\"%s\": [%lld, %.6f]", first ? "" : ", ",
+                       kv.first.c_str(), kv.second.first, kv.second.second);
+         j += tmp;
+         first = false;
+      }
+      j += "}";
+      if (len) *len = (int)j.size();
+      if (buf && cap > 0) {
+         const int n = std::min<int>(cap - 1, (int)j.size());
+         std::memcpy(buf, j.data(), n);
+         buf[n] = 0;
+      }
    });
 }
 

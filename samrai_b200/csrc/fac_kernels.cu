@@ -69,12 +69,12 @@ __device__ __forceinline__ int coarsen_index(int i, int r)
 
 // settype1cells{2,3}d (robinbchelper2d.f:10-72): ghost value from the
 // interior value next to the boundary.
-__device__ __forceinline__ double robin(double uin, int loc, double h, int hom,
-                                        const BcCoefs &bc)
+template <class T>
+__device__ __forceinline__ T robin(T uin, int loc, T h, int hom, const BcCoefs &bc)
 {
-   const double a = bc.a[loc], b = bc.b[loc];
-   if (hom) return (uin * (b - 0.5 * h * a)) / (b + 0.5 * h * a);
-   return (h * bc.g[loc] + uin * (b - 0.5 * h * a)) / (b + 0.5 * h * a);
+   const T a = (T)bc.a[loc], b = (T)bc.b[loc], half = (T)0.5;
+   if (hom) return (uin * (b - half * h * a)) / (b + half * h * a);
+   return (h * (T)bc.g[loc] + uin * (b - half * h * a)) / (b + half * h * a);
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v)
@@ -86,16 +86,17 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, doub
 // ghost fill
 // ---------------------------------------------------------------------------
 
+template <class T>
 __global__ void __launch_bounds__(kThreads)
 k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
-       double *__restrict__ dst, const double *__restrict__ src_same,
-       const double *__restrict__ src_coarse, int homogeneous, BcCoefs bc,
+       T *__restrict__ dst, const T *__restrict__ src_same,
+       const T *__restrict__ src_coarse, int homogeneous, BcCoefs bc,
        const int *__restrict__ active)
 {
    const Chunk ch = chunks[blockIdx.x];
    const FillItem &it = items[ch.patch];
    if (active && !active[it.prob]) return;
-   const double *src = it.src_is_coarse ? src_coarse : src_same;
+   const T *src = it.src_is_coarse ? src_coarse : src_same;
    const int nx = it.hi[0] - it.lo[0] + 1;
    const int ny = it.hi[1] - it.lo[1] + 1;
    for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -104,7 +105,7 @@ k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
       const int r = lin / nx;
       const int j = it.lo[1] + r % ny;
       const int k = it.lo[2] + r / ny;
-      double v;
+      T v;
       if (it.kind == kFillCopy) {
          v = src[aidx(it.src, i, j, k)];
       } else if (it.kind == kFillCoarse) {
@@ -115,22 +116,22 @@ k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
          // Every ghost value of codimension m depends only on the interior
          // cell reached by moving inward along all m outside axes
          // (settype1/2/3cells{2,3}d applied in codimension order).
-         const double uin =
+         const T uin =
             src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
-         double f[3];
+         T f[3];
          int m = 0;
          for (int a = 0; a < 3; ++a) {
             if (it.side[a]) {
-               f[a] = robin(uin, 2 * a + (it.side[a] > 0), it.h[a], homogeneous, bc);
+               f[a] = robin<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc);
                ++m;
             } else {
-               f[a] = 0.0;
+               f[a] = (T)0;
             }
          }
          if (m == 1) {
             v = it.side[0] ? f[0] : (it.side[1] ? f[1] : f[2]);
          } else if (m == 2) {
-            double s0 = 0.0, s1 = 0.0;
+            T s0 = (T)0, s1 = (T)0;
             int n = 0;
             for (int a = 0; a < 3; ++a)
                if (it.side[a]) {
@@ -140,7 +141,7 @@ k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
                }
             v = -uin + (s1 + s0);
          } else {
-            const double two3 = (double)(2.0f / 3.0f);
+            const T two3 = (T)(2.0f / 3.0f);
             v = -uin + two3 * ((f[0] + f[1]) + f[2]);
          }
       }
@@ -153,24 +154,24 @@ k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
 // 3d.f:604-1012), evaluated from the current u.
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ double ewing_flux(const double *__restrict__ u,
-                                             const double *__restrict__ dside,
-                                             const CfFace &cf, const PatchDesc &p,
-                                             int dvar, double dconst,
-                                             const double *tranwt,
-                                             const double *longwt)
+template <class T>
+__device__ __forceinline__ T ewing_flux(const T *__restrict__ u, const T *__restrict__ dside,
+                                        const CfFace &cf, const PatchDesc &p, int dvar,
+                                        T dconst, const double *tranwt, const double *longwt)
 {
    const int a = cf.axis;
-   const double d = dvar ? dside[cf.sidx] : dconst;
-   const double dxi = 1. / p.dx[a];
-   const double uc = u[cf.cell], ug = u[cf.ghost], um = u[cf.mirror];
-   double flux;
+   const T d = dvar ? dside[cf.sidx] : dconst;
+   const T h = (T)p.dx[a];
+   const T dxi = (T)1 / h;
+   const T uc = u[cf.cell], ug = u[cf.ghost], um = u[cf.mirror];
+   const T tw = (T)tranwt[a], lw = (T)longwt[a];
+   T flux;
    if (cf.side == 0) {
       flux = dxi * d * (uc - ug);
-      return longwt[a] * flux + tranwt[a] * d * (um - uc) / p.dx[a];
+      return lw * flux + tw * d * (um - uc) / h;
    }
    flux = dxi * d * (ug - uc);
-   return longwt[a] * flux - tranwt[a] * d * (um - uc) / p.dx[a];
+   return lw * flux - tw * d * (um - uc) / h;
 }
 
 struct EwingWeights {
@@ -178,11 +179,12 @@ struct EwingWeights {
    double longwt[3];
 };
 
+template <class T>
 __global__ void __launch_bounds__(kThreads)
 k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
-          const PatchDesc *__restrict__ patches, const double *__restrict__ u,
-          const double *__restrict__ dside, int dvar, double dconst,
-          EwingWeights w, double *__restrict__ cfflux,
+          const PatchDesc *__restrict__ patches, const T *__restrict__ u,
+          const T *__restrict__ dside, int dvar, T dconst,
+          EwingWeights w, T *__restrict__ cfflux,
           const int *__restrict__ run)
 {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -190,7 +192,7 @@ k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
    const CfFace cf = faces[t];
    const PatchDesc &p = patches[cf.patch];
    if (run && !run[p.prob]) return;
-   cfflux[cf.oidx] = ewing_flux(u, dside, cf, p, dvar, dconst, w.tranwt, w.longwt);
+   cfflux[cf.oidx] = ewing_flux<T>(u, dside, cf, p, dvar, dconst, w.tranwt, w.longwt);
 }
 
 // ---------------------------------------------------------------------------
@@ -198,13 +200,13 @@ k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
 // (compflux* + rbgswithfluxmax*, 2d.f:10-364, 3d.f:10-484)
 // ---------------------------------------------------------------------------
 
-template <int DIM, bool DVAR, int CKIND>
+template <int DIM, bool DVAR, int CKIND, class T>
 __global__ void __launch_bounds__(kThreads)
 k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
-       double *__restrict__ u, const double *__restrict__ f,
-       const double *__restrict__ dside, const double *__restrict__ cfield,
-       const double *__restrict__ cfflux, const unsigned char *__restrict__ cfmask,
-       int offset, double dconst, double cconst,
+       T *__restrict__ u, const T *__restrict__ f,
+       const T *__restrict__ dside, const T *__restrict__ cfield,
+       const T *__restrict__ cfflux, const unsigned char *__restrict__ cfmask,
+       int offset, T dconst, T cconst,
        unsigned long long *__restrict__ maxres_patch, const int *__restrict__ run)
 {
    const Chunk ch = chunks[blockIdx.x];
@@ -213,10 +215,11 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
    const int nx = p.hi[0] - p.lo[0] + 1;
    const int ny = p.hi[1] - p.lo[1] + 1;
    const int hx = (nx + 1) >> 1;
-   const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
-   const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+   const T one = (T)1;
+   const T dxi = one / (T)p.dx[0], dyi = one / (T)p.dx[1];
+   const T dzi = DIM == 3 ? one / (T)p.dx[2] : (T)0;
    const bool has_cf = (p.flags & 1) != 0;
-   const double rcoef = 1.0;
+   const T rcoef = one;
    double maxres = 0.0;
    for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
       const int s = ch.begin + t;
@@ -238,8 +241,8 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
       const long long sx = 1;
       const long long sy = nx + 2;
       const long long sz = (long long)(nx + 2) * (ny + 2);
-      const double uc = u[c];
-      double dx0, dx1, dy0, dy1, dz0 = 0.0, dz1 = 0.0;
+      const T uc = u[c];
+      T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
       if (DVAR) {
          dx0 = dside[sidx(p, 0, i, j, k)];
          dx1 = dside[sidx(p, 0, i + 1, j, k)];
@@ -252,11 +255,11 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
       } else {
          dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
       }
-      double fxl = dxi * dx0 * (uc - u[c - sx]);
-      double fxh = dxi * dx1 * (u[c + sx] - uc);
-      double fyl = dyi * dy0 * (uc - u[c - sy]);
-      double fyh = dyi * dy1 * (u[c + sy] - uc);
-      double fzl = 0.0, fzh = 0.0;
+      T fxl = dxi * dx0 * (uc - u[c - sx]);
+      T fxh = dxi * dx1 * (u[c + sx] - uc);
+      T fyl = dyi * dy0 * (uc - u[c - sy]);
+      T fyh = dyi * dy1 * (u[c + sy] - uc);
+      T fzl = (T)0, fzh = (T)0;
       if (DIM == 3) {
          fzl = dzi * dz0 * (uc - u[c - sz]);
          fzh = dzi * dz1 * (u[c + sz] - uc);
@@ -289,23 +292,23 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
             }
          }
       }
-      const double sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
-                                   : (CKIND == 1 ? cconst : 0.0);
-      const double fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
-      double residual, dudr;
+      const T sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
+                              : (CKIND == 1 ? cconst : (T)0);
+      const T fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
+      T residual, dudr;
       if (DIM == 2) {
          residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
-         dudr = 1. / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
+         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
       } else {
-         const double dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
+         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
          residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
                     sf * uc;
-         dudr = 1. / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
-                      sf);
+         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
+                       sf);
       }
-      const double du = -residual * dudr;
+      const T du = -residual * dudr;
       u[c] = uc + du * rcoef;
-      const double ar = fabs(residual);
+      const double ar = fabs((double)residual);
       if (maxres < ar) maxres = ar;
    }
    // block max, then one atomic per block
@@ -328,10 +331,10 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
 // (computeFluxOnPatch, CellPoissonFACOps.C:2157-2267)
 // ---------------------------------------------------------------------------
 
-template <int DIM, bool DVAR>
+template <int DIM, bool DVAR, class TU>
 __global__ void __launch_bounds__(kThreads)
 k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
-       const double *__restrict__ u, const double *__restrict__ dside,
+       const TU *__restrict__ u, const double *__restrict__ dside,
        double dconst, const unsigned char *__restrict__ cfmask, EwingWeights w,
        const int *ratio_to_coarser, double *__restrict__ flux,
        const int *__restrict__ run)
@@ -356,7 +359,7 @@ k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
       const long long cq = cidx<DIM>(p, p.off1, 1, cm[0], cm[1], cm[2]);
       const long long si = sidx(p, a, i, j, k);
       const double d = DVAR ? dside[si] : dconst;
-      double fl = dai * d * (u[cp] - u[cq]);
+      double fl = dai * d * ((double)u[cp] - (double)u[cq]);
       if (has_cf) {
          const int fc[3] = {i, j, k};
          int s = -1;
@@ -374,8 +377,8 @@ k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
                   const int base = coarsen_index(cc[tt], rr) * rr;
                   mq[tt] = base + (rr - (cc[tt] - base) - 1);
                }
-               const double uc = u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
-               const double um = u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
+               const double uc = (double)u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
+               const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
                if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
                else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
             }
@@ -389,10 +392,10 @@ k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
 // residual from side fluxes (compres{var,con}sca{2,3}d) and outer-side save
 // ---------------------------------------------------------------------------
 
-template <int DIM, int CKIND>
+template <int DIM, int CKIND, class TU>
 __global__ void __launch_bounds__(kThreads)
 k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
-           const double *__restrict__ u, const double *__restrict__ f,
+           const TU *__restrict__ u, const double *__restrict__ f,
            const double *__restrict__ flux, const double *__restrict__ cfield,
            double cconst, double *__restrict__ res, double *__restrict__ oflux,
            const int *__restrict__ run)
@@ -413,7 +416,7 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
       const double fxl = flux[sidx(p, 0, i, j, k)], fxh = flux[sidx(p, 0, i + 1, j, k)];
       const double fyl = flux[sidx(p, 1, i, j, k)], fyh = flux[sidx(p, 1, i, j + 1, k)];
       const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
-      const double uc = u[cidx<DIM>(p, p.off1, 1, i, j, k)];
+      const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
       const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
       double rv;
       if (DIM == 2) {
@@ -552,12 +555,12 @@ k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chu
 // (cartlinrefcelldoub{2,3}d, HierarchyCellDataOpsReal::add)
 // ---------------------------------------------------------------------------
 
-template <int DIM>
+template <int DIM, class T>
 __global__ void __launch_bounds__(kThreads)
 k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ chunks,
-              const PatchDesc *__restrict__ fine, const double *__restrict__ tmp,
+              const PatchDesc *__restrict__ fine, const T *__restrict__ tmp,
               const double *__restrict__ dxc_prob, int ratio0, int ratio1, int ratio2,
-              double *__restrict__ e, const int *__restrict__ run)
+              T *__restrict__ e, const int *__restrict__ run)
 {
    const Chunk ch = chunks[blockIdx.x];
    const ProlongItem it = items[ch.patch];
@@ -565,7 +568,7 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
    const PatchDesc p = fine[it.fine_patch];
    const int nx = p.hi[0] - p.lo[0] + 1;
    const int ny = p.hi[1] - p.lo[1] + 1;
-   const double half = 0.5, one = 1.0;
+   const T half = (T)0.5, one = (T)1;
    const double *dxc = dxc_prob + 3 * it.prob;
    const int r[3] = {ratio0, ratio1, ratio2};
    for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -576,35 +579,35 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
       const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
       const int fi[3] = {i, j, k};
       int ic[3];
-      double x[3];
+      T x[3];
       for (int a = 0; a < DIM; ++a) {
          ic[a] = coarsen_index(fi[a], r[a]);
          const int ir = fi[a] - ic[a] * r[a];
-         const double deltax = ((double)ir + half) * p.dx[a] - dxc[a] * half;
-         x[a] = deltax / dxc[a];
+         const T deltax = ((T)ir + half) * (T)p.dx[a] - (T)dxc[a] * half;
+         x[a] = deltax / (T)dxc[a];
          if (x[a] < 0.0) {
             ic[a] = ic[a] - 1;
             x[a] = x[a] + one;
          }
       }
-      double v;
-      const ArrDesc &T = it.tmp;
+      T v;
+      const ArrDesc &A = it.tmp;
       if (DIM == 2) {
-         const double c00 = tmp[aidx(T, ic[0], ic[1], 0)];
-         const double c10 = tmp[aidx(T, ic[0] + 1, ic[1], 0)];
-         const double c01 = tmp[aidx(T, ic[0], ic[1] + 1, 0)];
-         const double c11 = tmp[aidx(T, ic[0] + 1, ic[1] + 1, 0)];
+         const T c00 = tmp[aidx(A, ic[0], ic[1], 0)];
+         const T c10 = tmp[aidx(A, ic[0] + 1, ic[1], 0)];
+         const T c01 = tmp[aidx(A, ic[0], ic[1] + 1, 0)];
+         const T c11 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, 0)];
          v = (c00 + (c10 - c00) * x[0]) * (one - x[1]) + (c01 + (c11 - c01) * x[0]) * x[1];
       } else {
-         const double c000 = tmp[aidx(T, ic[0], ic[1], ic[2])];
-         const double c100 = tmp[aidx(T, ic[0] + 1, ic[1], ic[2])];
-         const double c010 = tmp[aidx(T, ic[0], ic[1] + 1, ic[2])];
-         const double c110 = tmp[aidx(T, ic[0] + 1, ic[1] + 1, ic[2])];
-         const double c001 = tmp[aidx(T, ic[0], ic[1], ic[2] + 1)];
-         const double c101 = tmp[aidx(T, ic[0] + 1, ic[1], ic[2] + 1)];
-         const double c011 = tmp[aidx(T, ic[0], ic[1] + 1, ic[2] + 1)];
-         const double c111 = tmp[aidx(T, ic[0] + 1, ic[1] + 1, ic[2] + 1)];
-         const double y = x[1], z = x[2], xx = x[0];
+         const T c000 = tmp[aidx(A, ic[0], ic[1], ic[2])];
+         const T c100 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2])];
+         const T c010 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2])];
+         const T c110 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2])];
+         const T c001 = tmp[aidx(A, ic[0], ic[1], ic[2] + 1)];
+         const T c101 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2] + 1)];
+         const T c011 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2] + 1)];
+         const T c111 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2] + 1)];
+         const T y = x[1], z = x[2], xx = x[0];
          v = ((c000 + (c100 - c000) * xx) * (one - y) + (c010 + (c110 - c010) * xx) * y) *
                 (one - z) +
              ((c001 + (c101 - c001) * xx) * (one - y) + (c011 + (c111 - c011) * xx) * y) * z;
@@ -618,10 +621,10 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
 // interior cell helpers
 // ---------------------------------------------------------------------------
 
-template <int DIM>
+template <int DIM, class T>
 __global__ void __launch_bounds__(kThreads)
 k_add_interior(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
-               double *__restrict__ u, const double *__restrict__ e,
+               double *__restrict__ u, const T *__restrict__ e,
                const int *__restrict__ run)
 {
    const Chunk ch = chunks[blockIdx.x];
@@ -636,7 +639,7 @@ k_add_interior(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ 
       const int j = p.lo[1] + r % ny;
       const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
       const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
-      u[c] = u[c] + e[c];
+      u[c] = u[c] + (double)e[c];
    }
 }
 
@@ -730,6 +733,13 @@ __global__ void k_sweep_check(const unsigned long long *__restrict__ red,
    }
 }
 
+template <class S, class D>
+__global__ void k_convert(const S *__restrict__ src, D *__restrict__ dst, long long n)
+{
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) dst[t] = (D)src[t];
+}
+
 __global__ void k_gather(const long long *__restrict__ idx, long long n,
                          const double *__restrict__ src, double *__restrict__ dst)
 {
@@ -754,20 +764,21 @@ long long kernel_launch_count() { return g_launches.load(); }
 // launchers
 // ---------------------------------------------------------------------------
 
+template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
-                 double *dst, const double *src_same, const double *src_coarse,
-                 int homogeneous, const BcCoefs &bc, const int *active)
+                 T *dst, const T *src_same, const T *src_coarse, int homogeneous,
+                 const BcCoefs &bc, const int *active)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_fill<<<nchunks, kThreads, 0, s>>>(items, chunks, dst, src_same, src_coarse,
-                                       homogeneous, bc, active);
+   k_fill<T><<<nchunks, kThreads, 0, s>>>(items, chunks, dst, src_same, src_coarse,
+                                          homogeneous, bc, active);
 }
 
+template <class T>
 void launch_cf_flux(cudaStream_t s, const CfFace *faces, int nfaces, const PatchDesc *patches,
-                    const double *u, const double *dside, int dvar, double dconst,
-                    const double *tranwt, const double *longwt, double *cfflux,
-                    const int *run)
+                    const T *u, const T *dside, int dvar, double dconst, const double *tranwt,
+                    const double *longwt, T *cfflux, const int *run)
 {
    if (nfaces <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -777,33 +788,33 @@ void launch_cf_flux(cudaStream_t s, const CfFace *faces, int nfaces, const Patch
       w.longwt[a] = longwt[a];
    }
    const int nb = (nfaces + kThreads - 1) / kThreads;
-   k_cf_flux<<<nb, kThreads, 0, s>>>(faces, nfaces, patches, u, dside, dvar, dconst, w,
-                                     cfflux, run);
+   k_cf_flux<T><<<nb, kThreads, 0, s>>>(faces, nfaces, patches, u, dside, dvar, (T)dconst, w,
+                                        cfflux, run);
 }
 
-template <int DIM, bool DVAR, int CK>
+template <int DIM, bool DVAR, int CK, class T>
 static void rbgs_inst(cudaStream_t s, int nchunks, const PatchDesc *patches,
-                      const Chunk *chunks, double *u, const double *f, const double *dside,
-                      const double *cfield, const double *cfflux,
-                      const unsigned char *cfmask, int offset, double dconst,
+                      const Chunk *chunks, T *u, const T *f, const T *dside, const T *cfield,
+                      const T *cfflux, const unsigned char *cfmask, int offset, double dconst,
                       double cconst, unsigned long long *maxres, const int *run)
 {
-   k_rbgs<DIM, DVAR, CK><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, dside, cfield,
-                                                      cfflux, cfmask, offset, dconst,
-                                                      cconst, maxres, run);
+   k_rbgs<DIM, DVAR, CK, T><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, dside, cfield,
+                                                         cfflux, cfmask, offset, (T)dconst,
+                                                         (T)cconst, maxres, run);
 }
 
+template <class T>
 void launch_rbgs(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
-                 const PatchDesc *patches, const Chunk *chunks, double *u, const double *f,
-                 const double *dside, const double *cfield, const double *cfflux,
+                 const PatchDesc *patches, const Chunk *chunks, T *u, const T *f,
+                 const T *dside, const T *cfield, const T *cfflux,
                  const unsigned char *cfmask, int offset, unsigned long long *maxres,
                  const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-#define RB(D, V, C)                                                                   \
-   rbgs_inst<D, V, C>(s, nchunks, patches, chunks, u, f, dside, cfield, cfflux, cfmask, \
-                      offset, spec.d_const, spec.c_const, maxres, run)
+#define RB(D, V, C)                                                                        \
+   rbgs_inst<D, V, C, T>(s, nchunks, patches, chunks, u, f, dside, cfield, cfflux, cfmask, \
+                         offset, spec.d_const, spec.c_const, maxres, run)
    if (dim == 2) {
       if (spec.d_variable) {
          if (spec.c_kind == 2) RB(2, true, 2);
@@ -828,8 +839,9 @@ void launch_rbgs(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
 #undef RB
 }
 
+template <class TU>
 void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
-                 const PatchDesc *patches, const Chunk *chunks, const double *u,
+                 const PatchDesc *patches, const Chunk *chunks, const TU *u,
                  const double *dside, const unsigned char *cfmask, const double *tranwt,
                  const double *longwt, const int *ratio_dev, double *flux, const int *run)
 {
@@ -842,31 +854,36 @@ void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
    }
    if (dim == 2) {
       if (spec.d_variable)
-         k_flux<2, true><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
-                                                      cfmask, w, ratio_dev, flux, run);
+         k_flux<2, true, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+                                                          spec.d_const, cfmask, w, ratio_dev,
+                                                          flux, run);
       else
-         k_flux<2, false><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
-                                                       cfmask, w, ratio_dev, flux, run);
+         k_flux<2, false, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+                                                           spec.d_const, cfmask, w,
+                                                           ratio_dev, flux, run);
    } else {
       if (spec.d_variable)
-         k_flux<3, true><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
-                                                      cfmask, w, ratio_dev, flux, run);
+         k_flux<3, true, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+                                                          spec.d_const, cfmask, w, ratio_dev,
+                                                          flux, run);
       else
-         k_flux<3, false><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside, spec.d_const,
-                                                       cfmask, w, ratio_dev, flux, run);
+         k_flux<3, false, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+                                                           spec.d_const, cfmask, w,
+                                                           ratio_dev, flux, run);
    }
 }
 
+template <class TU>
 void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
-                     const PatchDesc *patches, const Chunk *chunks, const double *u,
+                     const PatchDesc *patches, const Chunk *chunks, const TU *u,
                      const double *f, const double *flux, const double *cfield,
                      double *res, double *oflux, const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
 #define RS(D, C)                                                                         \
-   k_residual<D, C><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, flux, cfield,     \
-                                                 spec.c_const, res, oflux, run)
+   k_residual<D, C, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, flux, cfield, \
+                                                     spec.c_const, res, oflux, run)
    if (dim == 2) {
       if (spec.c_kind == 2) RS(2, 2);
       else if (spec.c_kind == 1) RS(2, 1);
@@ -903,29 +920,39 @@ void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const C
                                                  dst_g, run);
 }
 
+template <class T>
 void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const Chunk *chunks,
-                        int nchunks, const PatchDesc *fine, const double *tmp,
-                        const double *dxc_prob, const int *ratio, double *e, const int *run)
+                        int nchunks, const PatchDesc *fine, const T *tmp,
+                        const double *dxc_prob, const int *ratio, T *e, const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_prolong_add<2><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
-                                                    ratio[0], ratio[1], ratio[2], e, run);
+      k_prolong_add<2, T><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
+                                                       ratio[0], ratio[1], ratio[2], e, run);
    else
-      k_prolong_add<3><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
-                                                    ratio[0], ratio[1], ratio[2], e, run);
+      k_prolong_add<3, T><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
+                                                       ratio[0], ratio[1], ratio[2], e, run);
 }
 
+template <class T>
 void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                         const Chunk *chunks, double *u, const double *e, const int *run)
+                         const Chunk *chunks, double *u, const T *e, const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_add_interior<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+      k_add_interior<2, T><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
    else
-      k_add_interior<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+      k_add_interior<3, T><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+}
+
+template <class S, class D>
+void launch_convert(cudaStream_t s, const S *src, D *dst, long long n)
+{
+   if (n <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_convert<S, D><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
 }
 
 void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
@@ -965,5 +992,36 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
    g_launches.fetch_add(1, std::memory_order_relaxed);
    k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(idx, n, src, dst);
 }
+
+// explicit instantiations: FP64 (reference arithmetic) and FP32 (mixed
+// precision smoothing and transfer of the error)
+#define INST_T(T)                                                                          \
+   template void launch_fill<T>(cudaStream_t, const FillItem *, const Chunk *, int, T *,    \
+                                const T *, const T *, int, const BcCoefs &, const int *);   \
+   template void launch_cf_flux<T>(cudaStream_t, const CfFace *, int, const PatchDesc *,    \
+                                   const T *, const T *, int, double, const double *,       \
+                                   const double *, T *, const int *);                       \
+   template void launch_rbgs<T>(cudaStream_t, int, const PoissonSpec &, int,                \
+                                const PatchDesc *, const Chunk *, T *, const T *, const T *, \
+                                const T *, const T *, const unsigned char *, int,           \
+                                unsigned long long *, const int *);                         \
+   template void launch_flux<T>(cudaStream_t, int, const PoissonSpec &, int,                \
+                                const PatchDesc *, const Chunk *, const T *, const double *, \
+                                const unsigned char *, const double *, const double *,      \
+                                const int *, double *, const int *);                        \
+   template void launch_residual<T>(cudaStream_t, int, const PoissonSpec &, int,            \
+                                    const PatchDesc *, const Chunk *, const T *,            \
+                                    const double *, const double *, const double *,         \
+                                    double *, double *, const int *);                       \
+   template void launch_prolong_add<T>(cudaStream_t, int, const ProlongItem *,              \
+                                       const Chunk *, int, const PatchDesc *, const T *,    \
+                                       const double *, const int *, T *, const int *);      \
+   template void launch_add_interior<T>(cudaStream_t, int, int, const PatchDesc *,          \
+                                        const Chunk *, double *, const T *, const int *);
+INST_T(double)
+INST_T(float)
+#undef INST_T
+template void launch_convert<double, float>(cudaStream_t, const double *, float *, long long);
+template void launch_convert<float, double>(cudaStream_t, const float *, double *, long long);
 
 }  // namespace samrai_b200

@@ -10,28 +10,33 @@ namespace samrai_b200 {
 // Kernels launched by this process so far (all contexts).
 long long kernel_launch_count();
 
+template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
-                 double *dst, const double *src_same, const double *src_coarse,
-                 int homogeneous, const BcCoefs &bc, const int *active);
+                 T *dst, const T *src_same, const T *src_coarse, int homogeneous,
+                 const BcCoefs &bc, const int *active);
 
+template <class T>
 void launch_cf_flux(cudaStream_t s, const CfFace *faces, int nfaces, const PatchDesc *patches,
-                    const double *u, const double *dside, int dvar, double dconst,
-                    const double *tranwt, const double *longwt, double *cfflux,
-                    const int *run);
+                    const T *u, const T *dside, int dvar, double dconst, const double *tranwt,
+                    const double *longwt, T *cfflux, const int *run);
 
+template <class T>
 void launch_rbgs(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
-                 const PatchDesc *patches, const Chunk *chunks, double *u, const double *f,
-                 const double *dside, const double *cfield, const double *cfflux,
+                 const PatchDesc *patches, const Chunk *chunks, T *u, const T *f,
+                 const T *dside, const T *cfield, const T *cfflux,
                  const unsigned char *cfmask, int offset, unsigned long long *maxres,
                  const int *run);
 
+// Fluxes and residual are always FP64; the unknown may be FP32 (mixed).
+template <class TU>
 void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
-                 const PatchDesc *patches, const Chunk *chunks, const double *u,
+                 const PatchDesc *patches, const Chunk *chunks, const TU *u,
                  const double *dside, const unsigned char *cfmask, const double *tranwt,
                  const double *longwt, const int *ratio_dev, double *flux, const int *run);
 
+template <class TU>
 void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
-                     const PatchDesc *patches, const Chunk *chunks, const double *u,
+                     const PatchDesc *patches, const Chunk *chunks, const TU *u,
                      const double *f, const double *flux, const double *cfield,
                      double *res, double *oflux, const int *run);
 
@@ -43,12 +48,17 @@ void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const C
                      int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
                      const double *src, int src_g, double *dst, int dst_g, const int *run);
 
+template <class T>
 void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const Chunk *chunks,
-                        int nchunks, const PatchDesc *fine, const double *tmp,
-                        const double *dxc_prob, const int *ratio, double *e, const int *run);
+                        int nchunks, const PatchDesc *fine, const T *tmp,
+                        const double *dxc_prob, const int *ratio, T *e, const int *run);
 
+template <class T>
 void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                         const Chunk *chunks, double *u, const double *e, const int *run);
+                         const Chunk *chunks, double *u, const T *e, const int *run);
+
+template <class S, class D>
+void launch_convert(cudaStream_t s, const S *src, D *dst, long long n);
 
 void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                  const Chunk *chunks, const double *x, int xg, const double *w,

@@ -63,6 +63,7 @@ def load_library(build_if_missing=True):
                                           ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_int, ctypes.c_int]),
         "fac_initialize": (ctypes.c_int, [vp]),
+        "fac_set_precision": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
         "fac_side_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
         "fac_oside_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
@@ -91,6 +92,15 @@ def load_library(build_if_missing=True):
         "fac_coarse_sweeps": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
         "fac_reset_stats": (ctypes.c_int, [vp]),
         "fac_synchronize": (ctypes.c_int, [vp]),
+        "fac_zero_field": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_kernel_launches": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong)]),
+        "fac_profile_enable": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_profile_read": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong),
+                                            dp, dp]),
+        "fac_profile_reset": (ctypes.c_int, [vp]),
+        "fac_timer": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "fac_trace_enable": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_trace_read": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -123,7 +133,7 @@ class FacContext:
     """A batch of FAC problems on one GPU (device=-1: host-only table check)."""
 
     def __init__(self, problems: Sequence, params: Optional[dict] = None, device: int = 0,
-                 bc=None):
+                 bc=None, precision: str = "fp64"):
         L = load_library()
         problems = list(problems)
         if not problems:
@@ -161,6 +171,10 @@ class FacContext:
             idx = ctypes.c_int(0)
             _check(L.fac_add_problem(h, _ip(n0), _dp(xlo), _dp(xup), prob.nlev, _ip(ratio),
                                      _ip(npatch), _ip(boxes), ctypes.byref(idx)))
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        _check(L.fac_set_precision(h, 1 if precision == "mixed" else 0))
         _check(L.fac_initialize(h))
         if device >= 0:
             for ip_, prob in enumerate(problems):
@@ -300,6 +314,45 @@ class FacContext:
 
     def synchronize(self):
         _check(load_library().fac_synchronize(self.h))
+
+    def zero(self, fid):
+        _check(load_library().fac_zero_field(self.h, fid))
+
+    def profile(self, on=True):
+        _check(load_library().fac_profile_enable(self.h, int(on)))
+
+    def profile_read(self, kind):
+        n = ctypes.c_longlong(0)
+        ms = ctypes.c_double(0.0)
+        by = ctypes.c_double(0.0)
+        _check(load_library().fac_profile_read(self.h, kind, ctypes.byref(n), ctypes.byref(ms),
+                                               ctypes.byref(by)))
+        return n.value, ms.value, by.value
+
+    def trace(self, on=True):
+        _check(load_library().fac_trace_enable(self.h, int(on)))
+
+    def trace_read(self):
+        import json
+        n = ctypes.c_int(0)
+        _check(load_library().fac_trace_read(self.h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        _check(load_library().fac_trace_read(self.h, buf, n.value + 1, ctypes.byref(n)))
+        return json.loads(buf.value.decode())
+
+    def timer_start(self):
+        _check(load_library().fac_timer(self.h, 0, None))
+
+    def timer_stop(self):
+        ms = ctypes.c_double(0.0)
+        _check(load_library().fac_timer(self.h, 1, ctypes.byref(ms)))
+        return ms.value
+
+
+def kernel_launches():
+    n = ctypes.c_longlong(0)
+    _check(load_library().fac_kernel_launches(ctypes.byref(n)))
+    return n.value
 
 
 class CellPoissonFACSolver:

@@ -182,3 +182,28 @@ def test_config2_one_cycle(require_gpu):
     o.solve()
     g.solve()
     _solution_check(p, o, g)
+
+
+def test_mg_extended_hierarchy_matches_oracle(require_gpu):
+    """The fast variant (hierarchy extended by fully covered coarser levels)
+    against the oracle run on the same extended hierarchy, and its converged
+    solution against the plain solve's."""
+    p = configs.config3()
+    x = configs.extend_hierarchy(p)
+    prm = dict(coarse_tol=1e-300, coarse_max_it=20)
+    o = Oracle(x, params=prm)
+    g = fac.FacContext([x], params=prm)
+    ok_o, it_o, res_o, hist_o = o.solve()
+    conv, its, res = g.solve()
+    assert ok_o and conv[0] and its[0] == it_o
+    _solution_check(x, o, g)
+    op = Oracle(p, params=dict(coarse_tol=1e-10))
+    assert op.solve()[0]
+    k = x.virtual_levels
+    num = den = 0.0
+    for ln in range(p.nlev):
+        a = g.download(U, 0, ln + k)
+        b = op.get(U, ln)
+        num += float(np.sum((a - b) ** 2))
+        den += float(np.sum(b ** 2))
+    assert (num / den) ** 0.5 <= 1e-9

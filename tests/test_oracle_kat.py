@@ -205,3 +205,30 @@ def test_config1_converges_with_tight_coarse_tolerance():
     ok, it, res, hist = o.solve()
     assert ok and it <= 30
     assert res <= 1e-10 * hist[0] * 1.0000001
+
+
+def test_mg_extension_converges_to_plain_solution():
+    p = configs.config1()
+    x = configs.extend_hierarchy(p)
+    assert x.virtual_levels == 3 and x.nlev == 5
+    o = Oracle(x, params=dict(coarse_tol=1e-300, coarse_max_it=20))
+    ok, it, res, hist = o.solve()
+    assert ok and it < 15
+    op = Oracle(p, params=dict(coarse_tol=1e-10))
+    assert op.solve()[0]
+    for ln in range(p.nlev):
+        a, b = o.get(U, ln + 3), op.get(U, ln)
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+
+
+def test_mg_extension_coarsens_d_by_face_means():
+    p = configs.config3()
+    x = configs.extend_hierarchy(p)
+    # the coarsest extension level is 8x8; its x-faces average two finer faces
+    d16 = configs._dense_side(x, 1, x.d[1])
+    d8 = configs._dense_side(x, 0, x.d[0])
+    # arrays are (z, y, x); x-faces keep every other face along x and
+    # average the two finer faces along y
+    want = 0.5 * (d16[0][:, 0::2, 0::2] + d16[0][:, 1::2, 0::2])
+    assert d8[0].shape == want.shape == (1, 8, 9)
+    assert np.array_equal(d8[0], want)
