@@ -101,6 +101,23 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol,
                    int post_sweeps, double coarse_tol, int coarse_max_it,
                    int ewing);
 
+/* 1 (default): red-black colour passes read the value across a patch face
+ * from the neighbour patch's interior (or the physical-boundary formula, or
+ * the Ewing flux at a coarse-fine face) instead of from ghost cells, so the
+ * same-level ghost fills around every colour pass are skipped; one fill
+ * after the last sweep leaves the ghost cells as the reference leaves them.
+ * Results are bit-identical to 0 (fills as in CellPoissonFACOps.C:
+ * 1392-1495).  Used on a level only when its colouring is consistent across
+ * patches (always in 3-D). */
+int fac_set_fused(fac_ctx *ctx, int on);
+
+/* 1 (default): fac_solve captures one FAC cycle (V-cycle, correction,
+ * restriction, composite residual, norm kernels) into a CUDA graph on first
+ * use and replays it every cycle; converged problems are skipped on the
+ * device, and one host synchronisation per cycle reads the norms.  0: the
+ * same launches issued one by one.  Profiling and tracing use the latter. */
+int fac_set_graph(fac_ctx *ctx, int on);
+
 /* Precision of the FAC cycle (call before fac_initialize).  0: all FP64, the
  * reference's arithmetic.  1: mixed -- red-black smoothing, prolongation
  * and the error vector in FP32; composite residual with its coarse-fine
@@ -221,6 +238,53 @@ int fac_profile_reset(fac_ctx *ctx);
 /* Device timer on the context stream: stop = 0 records the start event;
  * stop = 1 records the end event, waits for it and returns milliseconds. */
 int fac_timer(fac_ctx *ctx, int stop, double *ms);
+
+/* ---- learned coarse-correction network.  No counterpart in the reference.
+ *
+ * Four 3x3x3 convolutions 1 -> 16 -> 16 -> 16 -> 1 channels, ReLU after the
+ * first three, no biases, zero padding; BF16 weights and activations, FP32
+ * accumulation (16 -> 16 layers on the tensor cores).  A sample is a patch
+ * plus a one-cell halo, zero-padded to FAC_CNN_BOX^3 cells, i fastest.
+ * Weights (FP32 masters, host arrays): w1 [27][16] (tap, out), w2, w3
+ * [27][16][16] (tap, in, out), w4 [27][16] (tap, in); tap = (dz+1)*9 +
+ * (dy+1)*3 + (dx+1).  x, y, target and mask are FP32 device arrays of
+ * nsamp*FAC_CNN_BOX^3 values. */
+#define FAC_CNN_BOX 18
+typedef struct fac_cnn fac_cnn;
+const char *fac_cnn_last_error(void);
+int fac_cnn_create(fac_cnn **net, int device, int max_batch, unsigned long long seed);
+int fac_cnn_destroy(fac_cnn *net);
+int fac_cnn_set_weights(fac_cnn *net, const float *w1, const float *w2,
+                        const float *w3, const float *w4);
+int fac_cnn_get_weights(fac_cnn *net, float *w1, float *w2, float *w3,
+                        float *w4);
+int fac_cnn_forward(fac_cnn *net, const float *x, long long nsamp, float *y);
+/* Masked mean squared error of the prediction and its weight gradients
+ * (host arrays; any may be NULL). */
+int fac_cnn_gradients(fac_cnn *net, const float *x, const float *target,
+                      const float *mask, long long nsamp, double *loss,
+                      float *g1, float *g2, float *g3, float *g4);
+/* One Adam step (beta 0.9/0.999) on the masked MSE; mask_sum = sum(mask). */
+int fac_cnn_train_step(fac_cnn *net, const float *x, const float *target,
+                       const float *mask, long long nsamp, double mask_sum,
+                       float lr, double *loss);
+
+/* Learned correction inside fac_solve (NULL disables it).  After every
+ * cycle the network predicts, from the composite residual on each patch of
+ * `level` (patch plus one-cell halo, scaled by the patch's RMS residual),
+ * the error on that patch (times the patch RMS residual and dx^2).  The
+ * prediction e is applied as u += alpha e with the per-problem
+ * minimal-residual step alpha = <r, A e> / <A e, A e> (weighted by the
+ * control volumes), and alpha = 0 whenever it would not lower the residual,
+ * so the FAC residual never grows.  Patches of `level` must have at most
+ * FAC_CNN_BOX-2 cells per side and the network a batch of at least the
+ * level's patch count. */
+int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level);
+/* The network's inputs for the current residual FAC_R of `level`: one
+ * FAC_CNN_BOX^3 FP32 sample per patch into the device array x, and the
+ * patch scales (RMS of r) into the host array scale (may be NULL).  Uses
+ * FAC_E of that level as scratch. */
+int fac_learned_samples(fac_ctx *ctx, int level, float *x, double *scale);
 
 #ifdef __cplusplus
 }

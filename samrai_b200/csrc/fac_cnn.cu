@@ -1,0 +1,707 @@
+// Learned coarse-correction network: forward, backward and Adam kernels.
+//
+// Four 3x3x3 convolutions 1 -> 16 -> 16 -> 16 -> 1 channels, ReLU after
+// the first three, no biases (so the network is positively homogeneous and
+// the residual's scale passes straight through), zero padding at the edge
+// of each sample.  Weights and stored activations are BF16; accumulation is
+// FP32.  One sample is a patch plus a one-cell halo padded to an S^3 box
+// (S = 18: patches of up to 16^3 cells).
+//
+// The 16 -> 16 layers run as implicit GEMMs on the tensor cores
+// (mma.sync m16n8k16, BF16 in, FP32 accumulate): for each of the 27 taps a
+// warp multiplies a 16-cell x 16-channel activation tile (gathered at the
+// tap's offset) by the tap's 16 x 16 weight block.  The same kernel computes
+// the backward pass with respect to the data (taps reversed, weights
+// transposed, gated by the forward ReLU mask).  Weight gradients of the
+// 16 -> 16 layers are 27 small GEMMs reducing over all cells, one warp per
+// tap.  The 1 -> 16 and 16 -> 1 layers are tiny and run on the FP32 cores.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/samrai_fac_b200.h"
+
+namespace {
+
+constexpr int S = FAC_CNN_BOX;       // sample box side (patch + halo)
+constexpr int S3 = S * S * S;
+constexpr int C = 16;                // hidden channels
+constexpr int T = 27;                // taps
+
+__device__ __forceinline__ void cell_coords(long long cell, int &x, int &y, int &z)
+{
+   const int rem = (int)(cell % S3);
+   x = rem % S;
+   y = (rem / S) % S;
+   z = rem / (S * S);
+}
+
+__device__ __forceinline__ int tap_dx(int t) { return t % 3 - 1; }
+__device__ __forceinline__ int tap_dy(int t) { return (t / 3) % 3 - 1; }
+__device__ __forceinline__ int tap_dz(int t) { return t / 9 - 1; }
+
+// Flat index of the neighbour of `cell` at tap t, or -1 outside the sample.
+__device__ __forceinline__ long long neighbour(long long cell, int x, int y, int z, int t)
+{
+   const int dx = tap_dx(t), dy = tap_dy(t), dz = tap_dz(t);
+   if (x + dx < 0 || x + dx >= S || y + dy < 0 || y + dy >= S || z + dz < 0 || z + dz >= S)
+      return -1;
+   return cell + dz * S * S + dy * S + dx;
+}
+
+__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16 *p, long long idx)
+{
+   return *reinterpret_cast<const uint32_t *>(p + idx);
+}
+
+__device__ __forceinline__ void mma_bf16(float *d, const uint32_t *a, uint32_t b0, uint32_t b1)
+{
+   asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// ---------------------------------------------------------------------------
+// layer 1: 1 -> 16, ReLU
+// ---------------------------------------------------------------------------
+__global__ void k_conv_in(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ w1,
+                          __nv_bfloat16 *__restrict__ y, long long ncells)
+{
+   __shared__ float w[T * C];
+   for (int i = threadIdx.x; i < T * C; i += blockDim.x) w[i] = w1[i];
+   __syncthreads();
+   const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (cell >= ncells) return;
+   int cx, cy, cz;
+   cell_coords(cell, cx, cy, cz);
+   float acc[C];
+#pragma unroll
+   for (int c = 0; c < C; ++c) acc[c] = 0.f;
+   for (int t = 0; t < T; ++t) {
+      const long long nb = neighbour(cell, cx, cy, cz, t);
+      if (nb < 0) continue;
+      const float v = __bfloat162float(x[nb]);
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[c] += w[t * C + c] * v;
+   }
+#pragma unroll
+   for (int c = 0; c < C; c += 2) {
+      __nv_bfloat162 o = __floats2bfloat162_rn(fmaxf(acc[c], 0.f), fmaxf(acc[c + 1], 0.f));
+      *reinterpret_cast<__nv_bfloat162 *>(y + cell * C + c) = o;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// layers 2, 3 (and their data gradients): 16 -> 16 on the tensor cores.
+// wt: [27][16 out][16 in] BF16.  mode 0: y = relu(acc); mode 1: y = acc *
+// (gate > 0) (ReLU backward with the forward activation as gate).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_conv_mid(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ wt,
+           __nv_bfloat16 *__restrict__ y, const __nv_bfloat16 *__restrict__ gate,
+           long long ncells, int mode)
+{
+   __shared__ __align__(16) __nv_bfloat16 w[T * C * C];
+   for (int i = threadIdx.x; i < T * C * C / 2; i += blockDim.x)
+      reinterpret_cast<uint32_t *>(w)[i] = reinterpret_cast<const uint32_t *>(wt)[i];
+   __syncthreads();
+   const int lane = threadIdx.x & 31;
+   const int g = lane >> 2, q = lane & 3;
+   const long long ntiles = (ncells + 15) / 16;
+   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+   for (long long tile = warp; tile < ntiles; tile += nwarps) {
+      const long long r0 = tile * 16 + g, r1 = r0 + 8;
+      int x0, y0, z0, x1, y1, z1;
+      cell_coords(r0, x0, y0, z0);
+      cell_coords(r1, x1, y1, z1);
+      const bool v0 = r0 < ncells, v1 = r1 < ncells;
+      float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+      for (int t = 0; t < T; ++t) {
+         const long long n0 = v0 ? neighbour(r0, x0, y0, z0, t) : -1;
+         const long long n1 = v1 ? neighbour(r1, x1, y1, z1, t) : -1;
+         uint32_t a[4];
+         a[0] = n0 >= 0 ? ld_pair(x, n0 * C + 2 * q) : 0u;
+         a[1] = n1 >= 0 ? ld_pair(x, n1 * C + 2 * q) : 0u;
+         a[2] = n0 >= 0 ? ld_pair(x, n0 * C + 2 * q + 8) : 0u;
+         a[3] = n1 >= 0 ? ld_pair(x, n1 * C + 2 * q + 8) : 0u;
+#pragma unroll
+         for (int j = 0; j < 2; ++j) {
+            const __nv_bfloat16 *wb = w + (t * C + 8 * j + g) * C + 2 * q;
+            const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wb);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wb + 8);
+            mma_bf16(acc[j], a, b0, b1);
+         }
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+         const int c = 8 * j + 2 * q;
+         float o0 = acc[j][0], o1 = acc[j][1], o2 = acc[j][2], o3 = acc[j][3];
+         if (mode == 0) {
+            o0 = fmaxf(o0, 0.f);
+            o1 = fmaxf(o1, 0.f);
+            o2 = fmaxf(o2, 0.f);
+            o3 = fmaxf(o3, 0.f);
+         } else {
+            if (v0) {
+               const __nv_bfloat162 gg = *reinterpret_cast<const __nv_bfloat162 *>(gate + r0 * C + c);
+               if (!(__bfloat162float(gg.x) > 0.f)) o0 = 0.f;
+               if (!(__bfloat162float(gg.y) > 0.f)) o1 = 0.f;
+            }
+            if (v1) {
+               const __nv_bfloat162 gg = *reinterpret_cast<const __nv_bfloat162 *>(gate + r1 * C + c);
+               if (!(__bfloat162float(gg.x) > 0.f)) o2 = 0.f;
+               if (!(__bfloat162float(gg.y) > 0.f)) o3 = 0.f;
+            }
+         }
+         if (v0) *reinterpret_cast<__nv_bfloat162 *>(y + r0 * C + c) = __floats2bfloat162_rn(o0, o1);
+         if (v1) *reinterpret_cast<__nv_bfloat162 *>(y + r1 * C + c) = __floats2bfloat162_rn(o2, o3);
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------
+// layer 4: 16 -> 1 (FP32 output)
+// ---------------------------------------------------------------------------
+__global__ void k_conv_out(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ w4,
+                           float *__restrict__ y, long long ncells)
+{
+   __shared__ float w[T * C];
+   for (int i = threadIdx.x; i < T * C; i += blockDim.x)
+      w[i] = __bfloat162float(__float2bfloat16_rn(w4[i]));
+   __syncthreads();
+   const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (cell >= ncells) return;
+   int cx, cy, cz;
+   cell_coords(cell, cx, cy, cz);
+   float acc = 0.f;
+   for (int t = 0; t < T; ++t) {
+      const long long nb = neighbour(cell, cx, cy, cz, t);
+      if (nb < 0) continue;
+#pragma unroll
+      for (int c = 0; c < C; c += 2) {
+         const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162 *>(x + nb * C + c);
+         acc += w[t * C + c] * __bfloat162float(v.x);
+         acc += w[t * C + c + 1] * __bfloat162float(v.y);
+      }
+   }
+   y[cell] = acc;
+}
+
+// masked MSE: dy = 2/m * mask * (y - target); loss += sum(mask*(y-target)^2)
+__global__ void k_loss_grad(const float *__restrict__ y, const float *__restrict__ target,
+                            const float *__restrict__ mask, float inv_m, float *__restrict__ dy,
+                            double *__restrict__ loss, long long ncells)
+{
+   const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   double l = 0.0;
+   if (cell < ncells) {
+      const float d = (y[cell] - target[cell]) * mask[cell];
+      dy[cell] = 2.f * inv_m * d;
+      l = (double)d * (double)d;
+   }
+   for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+   if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l);
+}
+
+// data gradient through layer 4, gated by layer 3's ReLU
+__global__ void k_bwd_out_data(const float *__restrict__ dy, const float *__restrict__ w4,
+                               const __nv_bfloat16 *__restrict__ a3,
+                               __nv_bfloat16 *__restrict__ d3, long long ncells)
+{
+   __shared__ float w[T * C];
+   for (int i = threadIdx.x; i < T * C; i += blockDim.x)
+      w[i] = __bfloat162float(__float2bfloat16_rn(w4[i]));
+   __syncthreads();
+   const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (cell >= ncells) return;
+   int cx, cy, cz;
+   cell_coords(cell, cx, cy, cz);
+   float acc[C];
+#pragma unroll
+   for (int c = 0; c < C; ++c) acc[c] = 0.f;
+   for (int t = 0; t < T; ++t) {
+      // dx[cell] += w[t] * dy[cell - off_t]: the neighbour at the reversed tap
+      const long long nb = neighbour(cell, cx, cy, cz, T - 1 - t);
+      if (nb < 0) continue;
+      const float g = dy[nb];
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[c] += w[t * C + c] * g;
+   }
+#pragma unroll
+   for (int c = 0; c < C; c += 2) {
+      const __nv_bfloat162 gg = *reinterpret_cast<const __nv_bfloat162 *>(a3 + cell * C + c);
+      const float o0 = __bfloat162float(gg.x) > 0.f ? acc[c] : 0.f;
+      const float o1 = __bfloat162float(gg.y) > 0.f ? acc[c + 1] : 0.f;
+      *reinterpret_cast<__nv_bfloat162 *>(d3 + cell * C + c) = __floats2bfloat162_rn(o0, o1);
+   }
+}
+
+// weight gradient of a 16 -> 16 layer: dw[t][ci][co] += sum_cells
+// x[cell + off_t][ci] * dy[cell][co].  27 warps per block, warp w = tap w,
+// each block reduces a run of `per_block` cells (a multiple of 16).
+__global__ void __launch_bounds__(T * 32)
+k_bwd_weight_mid(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ dy,
+                 float *__restrict__ dw, long long ncells, int per_block)
+{
+   const int t = threadIdx.x >> 5;
+   const int lane = threadIdx.x & 31;
+   const int g = lane >> 2, q = lane & 3;
+   const long long b0 = (long long)blockIdx.x * per_block;
+   const long long b1 = b0 + per_block < ncells ? b0 + per_block : ncells;
+   float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+   for (long long k0 = b0; k0 < b1; k0 += 16) {
+      // the four cells this thread touches: k0 + 2q, +1, +8, +9
+      long long cl[4] = {k0 + 2 * q, k0 + 2 * q + 1, k0 + 2 * q + 8, k0 + 2 * q + 9};
+      long long nb[4];
+      bool ok[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+         ok[i] = cl[i] < b1;
+         int cx, cy, cz;
+         cell_coords(cl[i], cx, cy, cz);
+         nb[i] = ok[i] ? neighbour(cl[i], cx, cy, cz, t) : -1;
+      }
+      // A[m=ci][k=cell] = x[cell + off_t][ci]
+      auto xa = [&](int i, int ci) -> __nv_bfloat16 {
+         return nb[i] >= 0 ? x[nb[i] * C + ci] : __float2bfloat16_rn(0.f);
+      };
+      uint32_t a[4];
+      {
+         __nv_bfloat162 p;
+         p = __halves2bfloat162(xa(0, g), xa(1, g));
+         a[0] = *reinterpret_cast<uint32_t *>(&p);
+         p = __halves2bfloat162(xa(0, g + 8), xa(1, g + 8));
+         a[1] = *reinterpret_cast<uint32_t *>(&p);
+         p = __halves2bfloat162(xa(2, g), xa(3, g));
+         a[2] = *reinterpret_cast<uint32_t *>(&p);
+         p = __halves2bfloat162(xa(2, g + 8), xa(3, g + 8));
+         a[3] = *reinterpret_cast<uint32_t *>(&p);
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+         const int co = 8 * j + g;
+         auto db = [&](int i) -> __nv_bfloat16 {
+            return ok[i] ? dy[cl[i] * C + co] : __float2bfloat16_rn(0.f);
+         };
+         __nv_bfloat162 p0 = __halves2bfloat162(db(0), db(1));
+         __nv_bfloat162 p1 = __halves2bfloat162(db(2), db(3));
+         mma_bf16(acc[j], a, *reinterpret_cast<uint32_t *>(&p0), *reinterpret_cast<uint32_t *>(&p1));
+      }
+   }
+#pragma unroll
+   for (int j = 0; j < 2; ++j) {
+      const int co = 8 * j + 2 * q;
+      atomicAdd(&dw[(t * C + g) * C + co], acc[j][0]);
+      atomicAdd(&dw[(t * C + g) * C + co + 1], acc[j][1]);
+      atomicAdd(&dw[(t * C + g + 8) * C + co], acc[j][2]);
+      atomicAdd(&dw[(t * C + g + 8) * C + co + 1], acc[j][3]);
+   }
+}
+
+// weight gradient of layer 1: dw1[t][co] += sum_cells x0[cell+off_t] * d1[cell][co]
+__global__ void k_bwd_weight_in(const __nv_bfloat16 *__restrict__ x0,
+                                const __nv_bfloat16 *__restrict__ d1, float *__restrict__ dw1,
+                                long long ncells, int per_block)
+{
+   const int t = threadIdx.x / C, co = threadIdx.x % C;  // 432 threads
+   const long long b0 = (long long)blockIdx.x * per_block;
+   const long long b1 = b0 + per_block < ncells ? b0 + per_block : ncells;
+   float acc = 0.f;
+   for (long long cell = b0; cell < b1; ++cell) {
+      int cx, cy, cz;
+      cell_coords(cell, cx, cy, cz);
+      const long long nb = neighbour(cell, cx, cy, cz, t);
+      if (nb < 0) continue;
+      acc += __bfloat162float(x0[nb]) * __bfloat162float(d1[cell * C + co]);
+   }
+   atomicAdd(&dw1[t * C + co], acc);
+}
+
+// weight gradient of layer 4: dw4[t][ci] += sum_cells a3[cell+off_t][ci] * dy[cell]
+__global__ void k_bwd_weight_out(const __nv_bfloat16 *__restrict__ a3,
+                                 const float *__restrict__ dy, float *__restrict__ dw4,
+                                 long long ncells, int per_block)
+{
+   const int t = threadIdx.x / C, ci = threadIdx.x % C;
+   const long long b0 = (long long)blockIdx.x * per_block;
+   const long long b1 = b0 + per_block < ncells ? b0 + per_block : ncells;
+   float acc = 0.f;
+   for (long long cell = b0; cell < b1; ++cell) {
+      int cx, cy, cz;
+      cell_coords(cell, cx, cy, cz);
+      const long long nb = neighbour(cell, cx, cy, cz, t);
+      if (nb < 0) continue;
+      acc += __bfloat162float(a3[nb * C + ci]) * dy[cell];
+   }
+   atomicAdd(&dw4[t * C + ci], acc);
+}
+
+// BF16 copies of the 16 -> 16 weights: forward [t][co][ci] and data-gradient
+// [t'][ci][co] with t' = 26 - t.
+__global__ void k_pack_mid(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wf,
+                           __nv_bfloat16 *__restrict__ wd)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= T * C * C) return;
+   const int t = i / (C * C), ci = (i / C) % C, co = i % C;
+   const __nv_bfloat16 v = __float2bfloat16_rn(w[i]);
+   wf[(t * C + co) * C + ci] = v;
+   wd[((T - 1 - t) * C + ci) * C + co] = v;
+}
+
+__global__ void k_round_bf16(const float *__restrict__ w, float *__restrict__ wr, int n)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i < n) wr[i] = __bfloat162float(__float2bfloat16_rn(w[i]));
+}
+
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= n) return;
+   const float gi = g[i];
+   const float mi = b1 * m[i] + (1.f - b1) * gi;
+   const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+   m[i] = mi;
+   v[i] = vi;
+   w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_to_bf16(const float *__restrict__ x, __nv_bfloat16 *__restrict__ y, long long n)
+{
+   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+}
+
+thread_local std::string t_cnn_error;
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// network object
+// ---------------------------------------------------------------------------
+
+struct fac_cnn {
+   int device = 0;
+   int max_batch = 0;
+   cudaStream_t stream = nullptr;
+   // FP32 masters, Adam moments and gradients: w1 [27*16], w2, w3 [27*16*16], w4 [27*16]
+   float *w[4] = {nullptr}, *gw[4] = {nullptr}, *m[4] = {nullptr}, *v[4] = {nullptr};
+   float *w1r = nullptr;                 // BF16-rounded w1 for the first layer
+   __nv_bfloat16 *wf[2] = {nullptr}, *wd[2] = {nullptr};  // layers 2, 3
+   __nv_bfloat16 *x0 = nullptr, *a[3] = {nullptr}, *d[3] = {nullptr};
+   float *y = nullptr, *dy = nullptr;
+   double *loss = nullptr;
+   int steps = 0;
+   std::vector<void *> allocs;
+};
+
+namespace {
+
+const int kSizes[4] = {T * C, T * C * C, T * C * C, T * C};
+
+#define CNN_CHECK(x)                                                                \
+   do {                                                                             \
+      cudaError_t _e = (x);                                                         \
+      if (_e != cudaSuccess) {                                                      \
+         t_cnn_error = std::string(#x) + ": " + cudaGetErrorString(_e);             \
+         return FAC_ERR_CUDA;                                                       \
+      }                                                                             \
+   } while (0)
+
+template <class P>
+int dalloc(fac_cnn *n, P **p, size_t bytes)
+{
+   cudaError_t e = cudaMalloc((void **)p, bytes);
+   if (e != cudaSuccess) {
+      t_cnn_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return FAC_ERR_NOMEM;
+   }
+   n->allocs.push_back((void *)*p);
+   return FAC_OK;
+}
+
+int pack(fac_cnn *n)
+{
+   for (int l = 0; l < 2; ++l) {
+      k_pack_mid<<<(T * C * C + 255) / 256, 256, 0, n->stream>>>(n->w[l + 1], n->wf[l], n->wd[l]);
+   }
+   k_round_bf16<<<(T * C + 127) / 128, 128, 0, n->stream>>>(n->w[0], n->w1r, T * C);
+   CNN_CHECK(cudaGetLastError());
+   return FAC_OK;
+}
+
+int forward_on(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st)
+{
+   const long long cells = nsamp * S3;
+   const int tb = 256;
+   const unsigned gb = (unsigned)((cells + tb - 1) / tb);
+   k_to_bf16<<<gb, tb, 0, st>>>(x, n->x0, cells);
+   k_conv_in<<<gb, tb, 0, st>>>(n->x0, n->w1r, n->a[0], cells);
+   const long long tiles = (cells + 15) / 16;
+   const unsigned mb = (unsigned)std::min<long long>((tiles + 7) / 8, 148 * 16);
+   k_conv_mid<<<mb, 256, 0, st>>>(n->a[0], n->wf[0], n->a[1], nullptr, cells, 0);
+   k_conv_mid<<<mb, 256, 0, st>>>(n->a[1], n->wf[1], n->a[2], nullptr, cells, 0);
+   k_conv_out<<<gb, tb, 0, st>>>(n->a[2], n->w[3], n->y, cells);
+   CNN_CHECK(cudaGetLastError());
+   return FAC_OK;
+}
+
+int forward(fac_cnn *n, const float *x, long long nsamp)
+{
+   return forward_on(n, x, nsamp, n->stream);
+}
+
+int backward(fac_cnn *n, const float *target, const float *mask, long long nsamp, float inv_m)
+{
+   const long long cells = nsamp * S3;
+   const int tb = 256;
+   const unsigned gb = (unsigned)((cells + tb - 1) / tb);
+   for (int l = 0; l < 4; ++l)
+      CNN_CHECK(cudaMemsetAsync(n->gw[l], 0, kSizes[l] * sizeof(float), n->stream));
+   CNN_CHECK(cudaMemsetAsync(n->loss, 0, sizeof(double), n->stream));
+   k_loss_grad<<<gb, tb, 0, n->stream>>>(n->y, target, mask, inv_m, n->dy, n->loss, cells);
+   const int per_block = 1024;
+   const unsigned wb = (unsigned)((cells + per_block - 1) / per_block);
+   k_bwd_weight_out<<<wb, T * C, 0, n->stream>>>(n->a[2], n->dy, n->gw[3], cells, per_block);
+   k_bwd_out_data<<<gb, tb, 0, n->stream>>>(n->dy, n->w[3], n->a[2], n->d[2], cells);
+   k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[1], n->d[2], n->gw[2], cells, per_block);
+   const long long tiles = (cells + 15) / 16;
+   const unsigned mb = (unsigned)std::min<long long>((tiles + 7) / 8, 148 * 16);
+   k_conv_mid<<<mb, 256, 0, n->stream>>>(n->d[2], n->wd[1], n->d[1], n->a[1], cells, 1);
+   k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[0], n->d[1], n->gw[1], cells, per_block);
+   k_conv_mid<<<mb, 256, 0, n->stream>>>(n->d[1], n->wd[0], n->d[0], n->a[0], cells, 1);
+   k_bwd_weight_in<<<wb, T * C, 0, n->stream>>>(n->x0, n->d[0], n->gw[0], cells, per_block);
+   CNN_CHECK(cudaGetLastError());
+   return FAC_OK;
+}
+
+int check_batch(fac_cnn *n, long long nsamp)
+{
+   if (!n) {
+      t_cnn_error = "null network";
+      return FAC_ERR_ARG;
+   }
+   if (nsamp < 1 || nsamp > n->max_batch) {
+      t_cnn_error = "batch size out of range";
+      return FAC_ERR_ARG;
+   }
+   return FAC_OK;
+}
+
+}  // namespace
+
+namespace samrai_b200 {
+// Forward pass on the caller's stream (used inside the FAC cycle); *y points
+// at the network's output buffer (nsamp * S^3 floats).
+int cnn_forward_on_stream(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st,
+                          const float **y)
+{
+   int rc = check_batch(n, nsamp);
+   if (rc) return rc;
+   rc = forward_on(n, x, nsamp, st);
+   if (y) *y = n->y;
+   return rc;
+}
+int cnn_max_batch(const fac_cnn *n) { return n ? n->max_batch : 0; }
+int cnn_device(const fac_cnn *n) { return n ? n->device : -1; }
+}  // namespace samrai_b200
+
+extern "C" {
+
+const char *fac_cnn_last_error(void) { return t_cnn_error.c_str(); }
+
+int fac_cnn_create(fac_cnn **out, int device, int max_batch, unsigned long long seed)
+{
+   if (!out || max_batch < 1) {
+      t_cnn_error = "bad arguments";
+      return FAC_ERR_ARG;
+   }
+   CNN_CHECK(cudaSetDevice(device));
+   fac_cnn *n = new fac_cnn();
+   n->device = device;
+   n->max_batch = max_batch;
+   int rc = FAC_OK;
+   auto fail = [&](int r) {
+      for (void *p : n->allocs) cudaFree(p);
+      delete n;
+      return r;
+   };
+   if (cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(FAC_ERR_CUDA);
+   const long long cells = (long long)max_batch * S3;
+   for (int l = 0; l < 4; ++l) {
+      if ((rc = dalloc(n, &n->w[l], kSizes[l] * sizeof(float))) ||
+          (rc = dalloc(n, &n->gw[l], kSizes[l] * sizeof(float))) ||
+          (rc = dalloc(n, &n->m[l], kSizes[l] * sizeof(float))) ||
+          (rc = dalloc(n, &n->v[l], kSizes[l] * sizeof(float))))
+         return fail(rc);
+   }
+   if ((rc = dalloc(n, &n->w1r, T * C * sizeof(float)))) return fail(rc);
+   for (int l = 0; l < 2; ++l)
+      if ((rc = dalloc(n, &n->wf[l], T * C * C * 2)) || (rc = dalloc(n, &n->wd[l], T * C * C * 2)))
+         return fail(rc);
+   if ((rc = dalloc(n, &n->x0, cells * 2))) return fail(rc);
+   for (int l = 0; l < 3; ++l)
+      if ((rc = dalloc(n, &n->a[l], cells * C * 2)) || (rc = dalloc(n, &n->d[l], cells * C * 2)))
+         return fail(rc);
+   if ((rc = dalloc(n, &n->y, cells * 4)) || (rc = dalloc(n, &n->dy, cells * 4)) ||
+       (rc = dalloc(n, &n->loss, sizeof(double))))
+      return fail(rc);
+   // He initialisation from a seeded host generator (splitmix64 + Box-Muller)
+   unsigned long long st = seed * 0x9E3779B97F4A7C15ull + 1;
+   auto next = [&]() {
+      st += 0x9E3779B97F4A7C15ull;
+      unsigned long long z = st;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      return ((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+   };
+   const int fan_in[4] = {T, T * C, T * C, T * C};
+   for (int l = 0; l < 4; ++l) {
+      std::vector<float> h(kSizes[l]);
+      const double sd = std::sqrt(2.0 / fan_in[l]);
+      for (auto &x : h) {
+         const double u1 = next() + 1e-300, u2 = next();
+         x = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
+      }
+      if (l == 3)
+         for (auto &x : h) x *= 0.1f;  // start close to a zero correction
+      CNN_CHECK(cudaMemcpyAsync(n->w[l], h.data(), kSizes[l] * 4, cudaMemcpyHostToDevice,
+                                n->stream));
+      CNN_CHECK(cudaMemsetAsync(n->m[l], 0, kSizes[l] * 4, n->stream));
+      CNN_CHECK(cudaMemsetAsync(n->v[l], 0, kSizes[l] * 4, n->stream));
+   }
+   if ((rc = pack(n))) return fail(rc);
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   *out = n;
+   return FAC_OK;
+}
+
+int fac_cnn_destroy(fac_cnn *n)
+{
+   if (!n) return FAC_OK;
+   cudaSetDevice(n->device);
+   cudaStreamSynchronize(n->stream);
+   for (void *p : n->allocs) cudaFree(p);
+   cudaStreamDestroy(n->stream);
+   delete n;
+   return FAC_OK;
+}
+
+int fac_cnn_set_weights(fac_cnn *n, const float *w1, const float *w2, const float *w3,
+                        const float *w4)
+{
+   if (!n || !w1 || !w2 || !w3 || !w4) {
+      t_cnn_error = "null argument";
+      return FAC_ERR_ARG;
+   }
+   const float *src[4] = {w1, w2, w3, w4};
+   for (int l = 0; l < 4; ++l)
+      CNN_CHECK(cudaMemcpyAsync(n->w[l], src[l], kSizes[l] * 4, cudaMemcpyHostToDevice,
+                                n->stream));
+   int rc = pack(n);
+   if (rc) return rc;
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   return FAC_OK;
+}
+
+int fac_cnn_get_weights(fac_cnn *n, float *w1, float *w2, float *w3, float *w4)
+{
+   if (!n || !w1 || !w2 || !w3 || !w4) {
+      t_cnn_error = "null argument";
+      return FAC_ERR_ARG;
+   }
+   float *dst[4] = {w1, w2, w3, w4};
+   for (int l = 0; l < 4; ++l)
+      CNN_CHECK(cudaMemcpyAsync(dst[l], n->w[l], kSizes[l] * 4, cudaMemcpyDeviceToHost,
+                                n->stream));
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   return FAC_OK;
+}
+
+int fac_cnn_forward(fac_cnn *n, const float *x, long long nsamp, float *y)
+{
+   int rc = check_batch(n, nsamp);
+   if (rc) return rc;
+   if (!x || !y) {
+      t_cnn_error = "null argument";
+      return FAC_ERR_ARG;
+   }
+   if ((rc = forward(n, x, nsamp))) return rc;
+   CNN_CHECK(cudaMemcpyAsync(y, n->y, nsamp * S3 * sizeof(float), cudaMemcpyDeviceToDevice,
+                             n->stream));
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   return FAC_OK;
+}
+
+int fac_cnn_gradients(fac_cnn *n, const float *x, const float *target, const float *mask,
+                      long long nsamp, double *loss, float *g1, float *g2, float *g3, float *g4)
+{
+   int rc = check_batch(n, nsamp);
+   if (rc) return rc;
+   if (!x || !target || !mask) {
+      t_cnn_error = "null argument";
+      return FAC_ERR_ARG;
+   }
+   std::vector<float> hm(nsamp * S3);
+   CNN_CHECK(cudaMemcpyAsync(hm.data(), mask, hm.size() * 4, cudaMemcpyDeviceToHost, n->stream));
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   double msum = 0;
+   for (float v : hm) msum += v;
+   if (msum <= 0) {
+      t_cnn_error = "empty mask";
+      return FAC_ERR_ARG;
+   }
+   if ((rc = forward(n, x, nsamp))) return rc;
+   if ((rc = backward(n, target, mask, nsamp, (float)(1.0 / msum)))) return rc;
+   double l = 0;
+   CNN_CHECK(cudaMemcpyAsync(&l, n->loss, sizeof(double), cudaMemcpyDeviceToHost, n->stream));
+   float *dst[4] = {g1, g2, g3, g4};
+   for (int k = 0; k < 4; ++k)
+      if (dst[k])
+         CNN_CHECK(cudaMemcpyAsync(dst[k], n->gw[k], kSizes[k] * 4, cudaMemcpyDeviceToHost,
+                                   n->stream));
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   if (loss) *loss = l / msum;
+   return FAC_OK;
+}
+
+int fac_cnn_train_step(fac_cnn *n, const float *x, const float *target, const float *mask,
+                       long long nsamp, double mask_sum, float lr, double *loss)
+{
+   int rc = check_batch(n, nsamp);
+   if (rc) return rc;
+   if (!x || !target || !mask || !(mask_sum > 0)) {
+      t_cnn_error = "bad arguments";
+      return FAC_ERR_ARG;
+   }
+   if ((rc = forward(n, x, nsamp))) return rc;
+   if ((rc = backward(n, target, mask, nsamp, (float)(1.0 / mask_sum)))) return rc;
+   n->steps += 1;
+   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+   const float c1 = 1.f - std::pow(b1, (float)n->steps), c2 = 1.f - std::pow(b2, (float)n->steps);
+   for (int l = 0; l < 4; ++l)
+      k_adam<<<(kSizes[l] + 255) / 256, 256, 0, n->stream>>>(n->w[l], n->gw[l], n->m[l], n->v[l],
+                                                              kSizes[l], lr, b1, b2, eps, c1, c2);
+   if ((rc = pack(n))) return rc;
+   if (loss) {
+      double l = 0;
+      CNN_CHECK(cudaMemcpyAsync(&l, n->loss, sizeof(double), cudaMemcpyDeviceToHost, n->stream));
+      CNN_CHECK(cudaStreamSynchronize(n->stream));
+      *loss = l / mask_sum;
+   }
+   return FAC_OK;
+}
+
+}  // extern "C"

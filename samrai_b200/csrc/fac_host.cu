@@ -20,6 +20,11 @@
 
 namespace samrai_b200 {
 
+int cnn_forward_on_stream(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st,
+                          const float **y);
+int cnn_max_batch(const fac_cnn *n);
+int cnn_device(const fac_cnn *n);
+
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
@@ -246,6 +251,10 @@ struct LevelState {
    // Ewing fluxes, coarse interpolation arrays)
    DevArray<float> e32, r32, d32, c32, cfflux32, tmp32;
    DevArray<unsigned char> cfmask;
+   // per face cell: index (ghost-1 buffer) of the same-level cell across the
+   // face, -1 physical boundary, -2 coarse-fine face (fused colour pass)
+   DevArray<long long> facemap;
+   bool fused_ok = false;
    DevArray<int> d_ratio;
 
    // work chunks
@@ -294,6 +303,17 @@ struct fac_ctx {
    int coarse_max_it = 500;
    int ewing = 1;
    int mixed = 0;            // 1: FP32 smoothing and error transfer
+   int use_graph = 1;        // capture one FAC cycle into a CUDA graph and replay it
+   int fused = 1;            // colour passes read across patch faces directly
+   bool capturing = false;   // inside stream capture: no host synchronisation
+   cudaGraphExec_t cycle_exec = nullptr;
+   // learned correction after every cycle (fac_set_learned)
+   fac_cnn *cnn = nullptr;
+   int learned_level = -1;
+   DevArray<float> cnn_in;
+   DevArray<double> cnn_scale, alpha;
+   DevArray<double2> dot_acc;
+   long long learned_applied = 0;
    std::vector<int> host_active;  // host copy of the active flags (instrumentation)
    int check_interval = 8;   // sweeps between host checks of convergence flags
 
@@ -321,6 +341,7 @@ struct fac_ctx {
 
    ~fac_ctx()
    {
+      if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
       for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
       if (t0) cudaEventDestroy(t0);
       if (t1) cudaEventDestroy(t1);
@@ -730,6 +751,70 @@ void build_cf_faces(fac_ctx *c, int ln)
    }
    L.cfmask.upload(mask, c->stream);
    L.d_cf.upload(L.cf, c->stream);
+}
+
+// Same-level neighbour of every face cell of every patch (fused colour
+// pass).  The fused pass reads a neighbour patch's cell during a colour
+// pass; that is exact only when the neighbour has the other colour, which
+// holds for the global 3-D colouring and, in 2-D, when every patch of the
+// level starts on the same parity of ifirst+jfirst (2d.f:140-147).
+void build_facemap(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   std::vector<long long> fmap(std::max<long long>(1, L.no), -3);
+   bool ok = true;
+   int parity = -1;
+   for (int ip = 0; ip < L.npatch && dim == 2; ++ip) {
+      const int q = ((L.box[ip].lo[0] + L.box[ip].lo[1]) % 2 + 2) % 2;
+      if (parity < 0) parity = q;
+      else if (q != parity) ok = false;
+   }
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      const PatchDesc &d = L.hp[ip];
+      const int p = d.prob;
+      const Box &b = L.box[ip];
+      const int pb = L.prob_patch_begin[p], pe = L.prob_patch_begin[p + 1];
+      for (int a = 0; a < dim; ++a)
+         for (int s = 0; s < 2; ++s) {
+            Box layer = b;
+            const int g = s == 0 ? b.lo[a] - 1 : b.hi[a] + 1;
+            layer.lo[a] = layer.hi[a] = g;
+            auto tlin = [&](int i, int j, int k) -> long long {
+               if (a == 0) return (j - b.lo[1]) + (long long)(b.hi[1] - b.lo[1] + 1) * (k - b.lo[2]);
+               if (a == 1) return (i - b.lo[0]) + (long long)(b.hi[0] - b.lo[0] + 1) * (k - b.lo[2]);
+               return (i - b.lo[0]) + (long long)(b.hi[0] - b.lo[0] + 1) * (j - b.lo[1]);
+            };
+            const bool outside = g < L.domain[p].lo[a] || g > L.domain[p].hi[a];
+            for (int k = layer.lo[2]; k <= layer.hi[2]; ++k)
+               for (int j = layer.lo[1]; j <= layer.hi[1]; ++j)
+                  for (int i = layer.lo[0]; i <= layer.hi[0]; ++i)
+                     fmap[d.offo[a][s] + tlin(i, j, k)] = outside ? -1 : -2;
+            if (outside) continue;
+            for (int iq = pb; iq < pe; ++iq) {
+               if (iq == ip) continue;
+               const Box ov = isect(layer, L.box[iq]);
+               if (ov.empty()) continue;
+               const Box qg = ghost_box(dim, L.box[iq], 1);
+               const long long qnx = qg.hi[0] - qg.lo[0] + 1, qny = qg.hi[1] - qg.lo[1] + 1;
+               for (int k = ov.lo[2]; k <= ov.hi[2]; ++k)
+                  for (int j = ov.lo[1]; j <= ov.hi[1]; ++j)
+                     for (int i = ov.lo[0]; i <= ov.hi[0]; ++i)
+                        fmap[d.offo[a][s] + tlin(i, j, k)] =
+                           L.hp[iq].off1 + (i - qg.lo[0]) + qnx * ((j - qg.lo[1]) + qny * (k - qg.lo[2]));
+            }
+         }
+   }
+   // -2 (not covered) must be exactly the coarse-fine faces
+   std::vector<unsigned char> mask(std::max<long long>(1, L.no), 0);
+   for (const CfFace &f : L.cf) mask[f.oidx] = 1;
+   for (long long t = 0; t < L.no; ++t) {
+      if (fmap[t] == -3) ok = false;
+      if ((fmap[t] == -2) != (mask[t] != 0))
+         throw FacError(FAC_ERR_NESTING, "face table disagrees with the coarse-fine boundary");
+   }
+   L.fused_ok = ok;
+   L.facemap.upload(fmap, c->stream);
 }
 
 void build_chunks(fac_ctx *c, int ln)
@@ -1218,6 +1303,7 @@ void initialize(fac_ctx *c)
    for (int ln = 0; ln < c->nlev; ++ln) {
       build_fill_tables(c, ln);
       build_cf_faces(c, ln);
+      build_facemap(c, ln);
       build_chunks(c, ln);
       build_dirichlet_index(c, ln);
       if (ln > 0) build_prolong_tables(c, ln);
@@ -1276,8 +1362,9 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
    ghost_fill(c, fid_e, ln, false, 1, c->run.p);
    if (ln > 0) ghost_fill(c, fid_e, ln, true, 1, c->run.p);
    std::vector<int> hrun(np);
+   const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
    for (int isweep = 0; isweep < nsweeps; ++isweep) {
-      if (tol >= 0.0 && isweep > 0 && isweep % c->check_interval == 0) {
+      if (tol >= 0.0 && isweep > 0 && isweep % c->check_interval == 0 && !c->capturing) {
          CUDA_CHECK(cudaMemcpyAsync(hrun.data(), c->run.p, np * sizeof(int),
                                     cudaMemcpyDeviceToHost, c->stream));
          CUDA_CHECK(cudaStreamSynchronize(c->stream));
@@ -1290,7 +1377,7 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
       CUDA_CHECK(cudaMemsetAsync(L.maxres_blk.p, 0, L.maxres_blk.n * sizeof(unsigned long long),
                                  c->stream));
       for (int color = 0; color < 2; ++color) {
-         ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+         if (!fmap) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
          if (ln > 0)
             launch_cf_flux(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, e, L.d.p,
                            c->spec.d_variable, c->spec.d_const, L.tranwt, L.longwt, L.cfflux.p,
@@ -1298,10 +1385,10 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
          const int pi = prof_begin(c, 0, c->profiling ? active_bytes(c, L.rb_bytes_prob) : 0.0);
          launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
                      L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
-                     color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p);
+                     color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p, fmap, c->bc);
          prof_end(c, pi);
       }
-      ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+      if (!fmap || isweep + 1 == nsweeps) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
       launch_sweep_check(c->stream, L.maxres_red.p, L.maxres_blk.p, L.last_patch.p, np, tol,
                          c->run.p, c->sweeps_call.p);
    }
@@ -1368,9 +1455,8 @@ void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
    CUDA_CHECK(cudaGetLastError());
 }
 
-void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
+void rms_norm_launch(fac_ctx *c, int fid)
 {
-   OpTimer ot(c, "rms_norm", 0);
    const int np = nprob(c);
    CUDA_CHECK(cudaMemsetAsync(c->norm_acc.p, 0, np * sizeof(double2), c->stream));
    const int g = field_ghost(fid);
@@ -1380,6 +1466,11 @@ void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
                   field_ptr(L, fid), g, L.w.p, L.norm_partial.p, L.d_prob_cell_chunk_begin.p, np,
                   c->norm_acc.p);
    }
+}
+
+void rms_norm_read(fac_ctx *c, std::vector<double> &out)
+{
+   const int np = nprob(c);
    std::vector<double2> acc(np);
    CUDA_CHECK(cudaMemcpyAsync(acc.data(), c->norm_acc.p, np * sizeof(double2),
                               cudaMemcpyDeviceToHost, c->stream));
@@ -1391,21 +1482,19 @@ void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
    }
 }
 
+void rms_norm(fac_ctx *c, int fid, std::vector<double> &out)
+{
+   OpTimer ot(c, "rms_norm", 0);
+   rms_norm_launch(c, fid);
+   rms_norm_read(c, out);
+}
+
 void solve_coarsest(fac_ctx *c)
 {
    OpTimer ot(c, "solve_coarsest", 0);
    smooth(c, FAC_E, FAC_R, 0, c->coarse_max_it, c->coarse_tol);
-   // accumulate the per-call sweep counts
-   const int np = nprob(c);
-   std::vector<long long> a(np), b(np);
-   CUDA_CHECK(cudaMemcpyAsync(a.data(), c->sweeps_call.p, np * sizeof(long long),
-                              cudaMemcpyDeviceToHost, c->stream));
-   CUDA_CHECK(cudaMemcpyAsync(b.data(), c->sweeps_coarse.p, np * sizeof(long long),
-                              cudaMemcpyDeviceToHost, c->stream));
-   CUDA_CHECK(cudaStreamSynchronize(c->stream));
-   for (int p = 0; p < np; ++p) b[p] += a[p];
-   CUDA_CHECK(cudaMemcpyAsync(c->sweeps_coarse.p, b.data(), np * sizeof(long long),
-                              cudaMemcpyHostToDevice, c->stream));
+   // accumulate the per-call sweep counts on the device
+   launch_accumulate(c->stream, c->sweeps_call.p, c->sweeps_coarse.p, nprob(c));
    ghost_fill(c, FAC_E, 0, false, 1, c->active.p);
 }
 
@@ -1425,7 +1514,7 @@ void fac_cycle_recursive(fac_ctx *c, int ln)
 }
 
 // FACPreconditioner::computeFullCompositeResidual (FACPreconditioner.C:775-814).
-void full_composite_residual(fac_ctx *c, std::vector<double> &norms)
+void full_composite_residual_launch(fac_ctx *c)
 {
    const int lmax = c->nlev - 1;
    comp_residual(c, FAC_R, FAC_U, FAC_F, lmax, 0);
@@ -1434,7 +1523,13 @@ void full_composite_residual(fac_ctx *c, std::vector<double> &norms)
       comp_residual(c, FAC_R, FAC_U, FAC_F, ln, 0);
       restrict_op(c, FAC_R, FAC_R, ln);
    }
-   rms_norm(c, FAC_R, norms);
+   rms_norm_launch(c, FAC_R);
+}
+
+void full_composite_residual(fac_ctx *c, std::vector<double> &norms)
+{
+   full_composite_residual_launch(c);
+   rms_norm_read(c, norms);
 }
 
 void zero_field(fac_ctx *c, int fid)
@@ -1485,9 +1580,10 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
    const int *run = c->active.p;
    ghost_fill32(c, ln, false, 1, run);
    if (ln > 0) ghost_fill32(c, ln, true, 1, run);
+   const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
    for (int isweep = 0; isweep < nsweeps; ++isweep) {
       for (int color = 0; color < 2; ++color) {
-         ghost_fill32(c, ln, false, 1, run);
+         if (!fmap) ghost_fill32(c, ln, false, 1, run);
          if (ln > 0)
             launch_cf_flux<float>(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, L.e32.p,
                                   L.d32.p, c->spec.d_variable, c->spec.d_const, L.tranwt,
@@ -1496,10 +1592,10 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
             prof_begin(c, 2, c->profiling ? 0.5 * active_bytes(c, L.rb_bytes_prob) : 0.0);
          launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
                             L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
-                            L.c32.p, L.cfflux32.p, L.cfmask.p, color, nullptr, run);
+                            L.c32.p, L.cfflux32.p, L.cfmask.p, color, nullptr, run, fmap, c->bc);
          prof_end(c, pi);
       }
-      ghost_fill32(c, ln, false, 1, run);
+      if (!fmap || isweep + 1 == nsweeps) ghost_fill32(c, ln, false, 1, run);
    }
    (void)np;
    CUDA_CHECK(cudaGetLastError());
@@ -1568,6 +1664,68 @@ void mixed_prepare(fac_ctx *c)
    }
 }
 
+// ---------------------------------------------------------------------------
+// learned correction (no reference counterpart).  After a cycle's composite
+// residual r: the network predicts the error on every patch of one level
+// from r on the patch and a one-cell halo; the prediction e is carried to
+// the coarser levels by restriction, d = A e is formed as r minus the
+// composite residual of the error equation, and u += alpha e, r -= alpha d
+// with alpha = <r,d>/<d,d> per problem (weighted inner products; alpha = 0
+// when it would not lower the residual).  The FAC residual therefore never
+// grows: plain FAC is the fallback and the judge.
+// ---------------------------------------------------------------------------
+
+void learned_gather(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int S = FAC_CNN_BOX;
+   CUDA_CHECK(cudaMemsetAsync(L.e.p, 0, L.e.n * sizeof(double), c->stream));
+   launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                   L.d_cell_chunks.p, L.r.p, L.e.p);
+   ghost_fill(c, FAC_E, ln, false, 1, nullptr);
+   launch_patch_rms(c->stream, c->dim, L.npatch, L.d_patches.p, L.r.p, c->cnn_scale.p);
+   launch_gather_samples(c->stream, c->dim, L.npatch, L.d_patches.p, L.e.p, c->cnn_scale.p,
+                         c->cnn_in.p, S);
+}
+
+void learned_step(fac_ctx *c)
+{
+   const int ln = c->learned_level;
+   LevelState &L = c->L[ln];
+   const int np = nprob(c);
+   learned_gather(c, ln);
+   const float *y = nullptr;
+   if (cnn_forward_on_stream(c->cnn, c->cnn_in.p, L.npatch, c->stream, &y) != FAC_OK)
+      throw FacError(FAC_ERR_CUDA, "learned correction: network forward failed");
+   zero_field(c, FAC_E);
+   launch_scatter_samples(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                          L.d_cell_chunks.p, y, c->cnn_scale.p, FAC_CNN_BOX, L.e.p);
+   // composite residual of the error equation with rhs r: TR = r - A e
+   const int lmax = c->nlev - 1;
+   for (int l = ln - 1; l >= 0; --l) {
+      restrict_op(c, FAC_E, FAC_E, l);
+   }
+   comp_residual(c, FAC_TR, FAC_E, FAC_R, lmax, 1);
+   for (int l = lmax - 1; l >= 0; --l) {
+      comp_residual(c, FAC_TR, FAC_E, FAC_R, l, 1);
+      restrict_op(c, FAC_TR, FAC_TR, l);
+   }
+   CUDA_CHECK(cudaMemsetAsync(c->dot_acc.p, 0, np * sizeof(double2), c->stream));
+   for (int l = 0; l < c->nlev; ++l) {
+      LevelState &Ll = c->L[l];
+      launch_dot_pair(c->stream, c->dim, (int)Ll.cell_chunks.size(), Ll.d_patches.p,
+                      Ll.d_cell_chunks.p, Ll.r.p, Ll.tr.p, Ll.w.p, Ll.norm_partial.p,
+                      Ll.d_prob_cell_chunk_begin.p, np, c->dot_acc.p);
+   }
+   launch_alpha(c->stream, c->dot_acc.p, c->active.p, np, c->alpha.p);
+   for (int l = 0; l < c->nlev; ++l) {
+      LevelState &Ll = c->L[l];
+      launch_apply_alpha(c->stream, c->dim, (int)Ll.cell_chunks.size(), Ll.d_patches.p,
+                         Ll.d_cell_chunks.p, c->alpha.p, Ll.u.p, Ll.e.p, Ll.r.p, Ll.tr.p);
+   }
+   CUDA_CHECK(cudaGetLastError());
+}
+
 // FACPreconditioner::solveSystem (FACPreconditioner.C:277-452) inside
 // CellPoissonFACSolver::solveSystem (CellPoissonFACSolver.C:310-352).
 void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
@@ -1596,7 +1754,8 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
    int it = 0;
    bool any = true;
    if (c->mixed) mixed_prepare(c);
-   while (any) {
+   // one FACPreconditioner cycle up to the norm kernels (no host sync)
+   auto cycle_body = [&]() {
       zero_field(c, FAC_E);
       if (c->mixed) {
          for (int ln = 0; ln < c->nlev; ++ln)
@@ -1618,8 +1777,43 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
                                         c->active.p);
       }
       for (int ln = c->nlev - 2; ln >= 0; --ln) restrict_solution(c, FAC_U, ln);
+      full_composite_residual_launch(c);
+      if (c->cnn) {
+         learned_step(c);
+         rms_norm_launch(c, FAC_R);
+      }
+   };
+   // The whole cycle is one CUDA graph, captured on first use and replayed:
+   // the launch sequence is fixed (converged problems are skipped on the
+   // device through the active flags), so only the norms come back per cycle.
+   const bool graph = c->use_graph && !c->profiling && !c->tracing;
+   if (graph && !c->cycle_exec) {
+      cudaGraph_t g = nullptr;
+      CUDA_CHECK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      c->capturing = true;
+      try {
+         cycle_body();
+      } catch (...) {
+         c->capturing = false;
+         cudaStreamEndCapture(c->stream, &g);
+         if (g) cudaGraphDestroy(g);
+         throw;
+      }
+      c->capturing = false;
+      CUDA_CHECK(cudaStreamEndCapture(c->stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&c->cycle_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+         c->cycle_exec = nullptr;
+         throw FacError(FAC_ERR_CUDA, std::string("cudaGraphInstantiate: ") +
+                                          cudaGetErrorString(e));
+      }
+   }
+   while (any) {
+      if (graph) CUDA_CHECK(cudaGraphLaunch(c->cycle_exec, c->stream));
+      else cycle_body();
       std::vector<double> nr;
-      full_composite_residual(c, nr);
+      rms_norm_read(c, nr);
       ++it;
       any = false;
       for (int p = 0; p < np; ++p) {
@@ -1821,6 +2015,87 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol, double rel
       ctx->coarse_tol = coarse_tol;
       ctx->coarse_max_it = coarse_max_it;
       ctx->ewing = ewing;
+   });
+}
+
+int fac_set_fused(fac_ctx *ctx, int on)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      ctx->fused = on != 0;
+      if (ctx->cycle_exec) {
+         cudaGraphExecDestroy(ctx->cycle_exec);
+         ctx->cycle_exec = nullptr;
+      }
+   });
+}
+
+int fac_set_graph(fac_ctx *ctx, int on)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      ctx->use_graph = on != 0;
+      if (ctx->cycle_exec) {
+         cudaGraphExecDestroy(ctx->cycle_exec);
+         ctx->cycle_exec = nullptr;
+      }
+   });
+}
+
+int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (ctx->cycle_exec) {
+         cudaGraphExecDestroy(ctx->cycle_exec);
+         ctx->cycle_exec = nullptr;
+      }
+      if (!net) {
+         ctx->cnn = nullptr;
+         ctx->learned_level = -1;
+         return;
+      }
+      if (level < 1 || level >= ctx->nlev) throw FacError(FAC_ERR_ARG, "bad learned level");
+      if (cnn_device(net) != ctx->device) throw FacError(FAC_ERR_ARG, "network on another device");
+      LevelState &L = ctx->L[level];
+      for (const Box &b : L.box)
+         for (int a = 0; a < ctx->dim; ++a)
+            if (b.hi[a] - b.lo[a] + 3 > FAC_CNN_BOX)
+               throw FacError(FAC_ERR_ARG, "patch too large for the network's sample box");
+      if (L.npatch > cnn_max_batch(net))
+         throw FacError(FAC_ERR_ARG, "network batch smaller than the level's patch count");
+      ctx->cnn = net;
+      ctx->learned_level = level;
+      ctx->cnn_in.alloc((size_t)L.npatch * FAC_CNN_BOX * FAC_CNN_BOX * FAC_CNN_BOX);
+      ctx->cnn_scale.alloc(std::max(1, L.npatch));
+      ctx->alpha.alloc(nprob(ctx));
+      ctx->dot_acc.alloc(nprob(ctx));
+   });
+}
+
+int fac_learned_samples(fac_ctx *ctx, int level, float *x, double *scale)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (level < 0 || level >= ctx->nlev) throw FacError(FAC_ERR_ARG, "bad level");
+      LevelState &L = ctx->L[level];
+      for (const Box &b : L.box)
+         for (int a = 0; a < ctx->dim; ++a)
+            if (b.hi[a] - b.lo[a] + 3 > FAC_CNN_BOX)
+               throw FacError(FAC_ERR_ARG, "patch too large for the network's sample box");
+      DevArray<double> sc;
+      sc.alloc(std::max(1, L.npatch));
+      CUDA_CHECK(cudaMemsetAsync(L.e.p, 0, L.e.n * sizeof(double), ctx->stream));
+      launch_g0_to_g1(ctx->stream, ctx->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                      L.d_cell_chunks.p, L.r.p, L.e.p);
+      ghost_fill(ctx, FAC_E, level, false, 1, nullptr);
+      launch_patch_rms(ctx->stream, ctx->dim, L.npatch, L.d_patches.p, L.r.p, sc.p);
+      launch_gather_samples(ctx->stream, ctx->dim, L.npatch, L.d_patches.p, L.e.p, sc.p, x,
+                            FAC_CNN_BOX);
+      if (scale)
+         CUDA_CHECK(cudaMemcpyAsync(scale, sc.p, L.npatch * sizeof(double),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
    });
 }
 

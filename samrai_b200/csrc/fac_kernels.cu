@@ -200,14 +200,21 @@ k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
 // (compflux* + rbgswithfluxmax*, 2d.f:10-364, 3d.f:10-484)
 // ---------------------------------------------------------------------------
 
-template <int DIM, bool DVAR, int CKIND, class T>
-__global__ void __launch_bounds__(kThreads)
+// FUSED: values across patch faces are read where they live instead of from
+// the patch's ghost cells -- the neighbour patch's interior cell (which has
+// the other colour, so it does not change during the pass), the Robin value
+// of the cell itself at a physical boundary (homogeneous, as the
+// smoother's fills are), or the precomputed Ewing flux at a coarse-fine
+// face -- so the three ghost fills around each colour pass are not needed.
+template <int DIM, bool DVAR, int CKIND, class T, bool FUSED>
+__global__ void __launch_bounds__(kThreads, 3)
 k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
        T *__restrict__ u, const T *__restrict__ f,
        const T *__restrict__ dside, const T *__restrict__ cfield,
        const T *__restrict__ cfflux, const unsigned char *__restrict__ cfmask,
        int offset, T dconst, T cconst,
-       unsigned long long *__restrict__ maxres_patch, const int *__restrict__ run)
+       unsigned long long *__restrict__ maxres_patch, const int *__restrict__ run,
+       const long long *__restrict__ facemap, BcCoefs bc)
 {
    const Chunk ch = chunks[blockIdx.x];
    const PatchDesc p = patches[ch.patch];
@@ -255,14 +262,40 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
       } else {
          dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
       }
-      T fxl = dxi * dx0 * (uc - u[c - sx]);
-      T fxh = dxi * dx1 * (u[c + sx] - uc);
-      T fyl = dyi * dy0 * (uc - u[c - sy]);
-      T fyh = dyi * dy1 * (u[c + sy] - uc);
+      T nxl, nxh, nyl, nyh, nzl = (T)0, nzh = (T)0;
+      if (FUSED) {
+         auto across = [&](int a, int sd, long long own) -> T {
+            const long long m = facemap[oidx(p, a, sd, i, j, k)];
+            if (m >= 0) return u[m];
+            if (m == -1) return robin<T>(uc, 2 * a + sd, (T)p.dx[a], 1, bc);
+            return u[own];
+         };
+         nxl = i == p.lo[0] ? across(0, 0, c - sx) : u[c - sx];
+         nxh = i == p.hi[0] ? across(0, 1, c + sx) : u[c + sx];
+         nyl = j == p.lo[1] ? across(1, 0, c - sy) : u[c - sy];
+         nyh = j == p.hi[1] ? across(1, 1, c + sy) : u[c + sy];
+         if (DIM == 3) {
+            nzl = k == p.lo[2] ? across(2, 0, c - sz) : u[c - sz];
+            nzh = k == p.hi[2] ? across(2, 1, c + sz) : u[c + sz];
+         }
+      } else {
+         nxl = u[c - sx];
+         nxh = u[c + sx];
+         nyl = u[c - sy];
+         nyh = u[c + sy];
+         if (DIM == 3) {
+            nzl = u[c - sz];
+            nzh = u[c + sz];
+         }
+      }
+      T fxl = dxi * dx0 * (uc - nxl);
+      T fxh = dxi * dx1 * (nxh - uc);
+      T fyl = dyi * dy0 * (uc - nyl);
+      T fyh = dyi * dy1 * (nyh - uc);
       T fzl = (T)0, fzh = (T)0;
       if (DIM == 3) {
-         fzl = dzi * dz0 * (uc - u[c - sz]);
-         fzh = dzi * dz1 * (u[c + sz] - uc);
+         fzl = dzi * dz0 * (uc - nzl);
+         fzh = dzi * dz1 * (nzh - uc);
       }
       if (has_cf) {
          if (i == p.lo[0]) {
@@ -740,6 +773,13 @@ __global__ void k_convert(const S *__restrict__ src, D *__restrict__ dst, long l
    if (t < n) dst[t] = (D)src[t];
 }
 
+__global__ void k_accumulate(const long long *__restrict__ src, long long *__restrict__ dst,
+                             int n)
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) dst[t] += src[t];
+}
+
 __global__ void k_gather(const long long *__restrict__ idx, long long n,
                          const double *__restrict__ src, double *__restrict__ dst)
 {
@@ -752,6 +792,175 @@ __global__ void k_scatter(const long long *__restrict__ idx, long long n,
 {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t < n) dst[idx[t]] = src[t];
+}
+
+// ---------------------------------------------------------------------------
+// learned correction: per-patch samples in and out of the CNN's S^3 boxes
+// ---------------------------------------------------------------------------
+
+// interior of a ghost-0 field copied into the interior of a ghost-1 field
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_g0_to_g1(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+           const double *__restrict__ src, double *__restrict__ dst)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int r = lin / nx;
+      const int j = p.lo[1] + r % ny;
+      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+      dst[cidx<DIM>(p, p.off1, 1, i, j, k)] = src[cidx<DIM>(p, p.off0, 0, i, j, k)];
+   }
+}
+
+// RMS of a ghost-0 field over each patch's interior (one block per patch)
+template <int DIM>
+__global__ void k_patch_rms(const PatchDesc *__restrict__ patches, const double *__restrict__ x,
+                            double *__restrict__ rms)
+{
+   const PatchDesc p = patches[blockIdx.x];
+   const long long n = (long long)(p.hi[0] - p.lo[0] + 1) * (p.hi[1] - p.lo[1] + 1) *
+                       (p.hi[2] - p.lo[2] + 1);
+   double sum = 0.0;
+   for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+      const double v = x[p.off0 + t];
+      sum += v * v;
+   }
+   __shared__ double red[kThreads];
+   red[threadIdx.x] = sum;
+   __syncthreads();
+   for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) rms[blockIdx.x] = n > 0 ? sqrt(red[0] / (double)n) : 0.0;
+}
+
+// sample p = ghosted box of patch p of a ghost-1 field, divided by scale[p],
+// at offset (0,0,0) of an S^3 box (the patch interior starts at 1), zeros
+// elsewhere; 2-D patches fill the middle z-plane
+template <int DIM>
+__global__ void k_gather_samples(const PatchDesc *__restrict__ patches,
+                                 const double *__restrict__ x, const double *__restrict__ scale,
+                                 float *__restrict__ out, int S)
+{
+   const int ip = blockIdx.y;
+   const PatchDesc p = patches[ip];
+   const long long S3 = (long long)S * S * S;
+   const double sc = scale[ip];
+   const double inv = sc > 0.0 ? 1.0 / sc : 0.0;
+   const int gx = p.hi[0] - p.lo[0] + 3, gy = p.hi[1] - p.lo[1] + 3;
+   const int gz = DIM == 3 ? p.hi[2] - p.lo[2] + 3 : 1;
+   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < S3;
+        c += (long long)gridDim.x * blockDim.x) {
+      const int sx = (int)(c % S), sy = (int)((c / S) % S), sz = (int)(c / ((long long)S * S));
+      const int zz = DIM == 3 ? sz : sz - S / 2;
+      float v = 0.f;
+      if (sx < gx && sy < gy && zz >= 0 && zz < gz) {
+         const long long idx = p.off1 + sx + (long long)gx * (sy + (long long)gy * zz);
+         v = (float)(x[idx] * inv);
+      }
+      out[(long long)ip * S3 + c] = v;
+   }
+}
+
+// interior cells of patch p of a ghost-1 field = y[p] * scale[p] * dx^2
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_scatter_samples(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+                  const float *__restrict__ y, const double *__restrict__ scale, int S,
+                  double *__restrict__ dst)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const long long S3 = (long long)S * S * S;
+   const double f = scale[ch.patch] * p.dx[0] * p.dx[0];
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int a = lin % nx;
+      const int r = lin / nx;
+      const int b = r % ny;
+      const int cz = DIM == 3 ? r / ny : 0;
+      const int sz = DIM == 3 ? cz + 1 : S / 2;
+      const long long sidx = (long long)ch.patch * S3 + (a + 1) + (long long)S * ((b + 1) + (long long)S * sz);
+      dst[cidx<DIM>(p, p.off1, 1, p.lo[0] + a, p.lo[1] + b, DIM == 3 ? p.lo[2] + cz : 0)] =
+         (double)y[sidx] * f;
+   }
+}
+
+// per chunk: sum w r d and sum w d d with d = r - r2 (ghost-0 fields)
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_dot_pair(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+           const double *__restrict__ r, const double *__restrict__ r2,
+           const double *__restrict__ w, double2 *__restrict__ partial)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   double a = 0.0, b = 0.0;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const long long c = p.off0 + ch.begin + t;
+      const double d = r[c] - r2[c];
+      a += w[c] * r[c] * d;
+      b += w[c] * d * d;
+   }
+   __shared__ double ra[kThreads], rb[kThreads];
+   ra[threadIdx.x] = a;
+   rb[threadIdx.x] = b;
+   __syncthreads();
+   for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) {
+         ra[threadIdx.x] += ra[threadIdx.x + o];
+         rb[threadIdx.x] += rb[threadIdx.x + o];
+      }
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(ra[0], rb[0]);
+}
+
+// minimal-residual step length per problem: alpha = <r, d> / <d, d>, kept
+// at 0 when it would not lower the residual
+__global__ void k_alpha(const double2 *__restrict__ acc, const int *__restrict__ active,
+                        int nprob, double *__restrict__ alpha)
+{
+   const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+   if (pr >= nprob) return;
+   const double a = acc[pr].x, b = acc[pr].y;
+   alpha[pr] = (active[pr] && b > 0.0 && a > 0.0) ? a / b : 0.0;
+}
+
+// u += alpha e (interior) and r = r - alpha (r - r2)
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_apply_alpha(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+              const double *__restrict__ alpha, double *__restrict__ u,
+              const double *__restrict__ e, double *__restrict__ r,
+              const double *__restrict__ r2)
+{
+   const Chunk ch = chunks[blockIdx.x];
+   const PatchDesc p = patches[ch.patch];
+   const double al = alpha[p.prob];
+   if (al == 0.0) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+      const int lin = ch.begin + t;
+      const int i = p.lo[0] + lin % nx;
+      const int rr = lin / nx;
+      const int j = p.lo[1] + rr % ny;
+      const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
+      const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
+      const long long c0 = p.off0 + lin;
+      u[c1] = u[c1] + al * e[c1];
+      r[c0] = r[c0] - al * (r[c0] - r2[c0]);
+   }
 }
 
 std::atomic<long long> g_launches{0};
@@ -796,11 +1005,17 @@ template <int DIM, bool DVAR, int CK, class T>
 static void rbgs_inst(cudaStream_t s, int nchunks, const PatchDesc *patches,
                       const Chunk *chunks, T *u, const T *f, const T *dside, const T *cfield,
                       const T *cfflux, const unsigned char *cfmask, int offset, double dconst,
-                      double cconst, unsigned long long *maxres, const int *run)
+                      double cconst, unsigned long long *maxres, const int *run,
+                      const long long *facemap, const BcCoefs &bc)
 {
-   k_rbgs<DIM, DVAR, CK, T><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, dside, cfield,
-                                                         cfflux, cfmask, offset, (T)dconst,
-                                                         (T)cconst, maxres, run);
+   if (facemap)
+      k_rbgs<DIM, DVAR, CK, T, true><<<nchunks, kThreads, 0, s>>>(
+         patches, chunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
+         maxres, run, facemap, bc);
+   else
+      k_rbgs<DIM, DVAR, CK, T, false><<<nchunks, kThreads, 0, s>>>(
+         patches, chunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
+         maxres, run, facemap, bc);
 }
 
 template <class T>
@@ -808,13 +1023,13 @@ void launch_rbgs(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                  const PatchDesc *patches, const Chunk *chunks, T *u, const T *f,
                  const T *dside, const T *cfield, const T *cfflux,
                  const unsigned char *cfmask, int offset, unsigned long long *maxres,
-                 const int *run)
+                 const int *run, const long long *facemap, const BcCoefs &bc)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
 #define RB(D, V, C)                                                                        \
    rbgs_inst<D, V, C, T>(s, nchunks, patches, chunks, u, f, dside, cfield, cfflux, cfmask, \
-                         offset, spec.d_const, spec.c_const, maxres, run)
+                         offset, spec.d_const, spec.c_const, maxres, run, facemap, bc)
    if (dim == 2) {
       if (spec.d_variable) {
          if (spec.c_kind == 2) RB(2, true, 2);
@@ -977,6 +1192,86 @@ void launch_sweep_check(cudaStream_t s, const unsigned long long *red,
    k_sweep_check<<<nb, 128, 0, s>>>(red, blk, last_patch, nprob, tol, run, sweeps);
 }
 
+void launch_accumulate(cudaStream_t s, const long long *src, long long *dst, int n)
+{
+   if (n <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_accumulate<<<(n + 127) / 128, 128, 0, s>>>(src, dst, n);
+}
+
+void launch_g0_to_g1(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const double *src, double *dst)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2) k_g0_to_g1<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, src, dst);
+   else k_g0_to_g1<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, src, dst);
+}
+
+void launch_patch_rms(cudaStream_t s, int dim, int npatch, const PatchDesc *patches,
+                      const double *x, double *rms)
+{
+   if (npatch <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2) k_patch_rms<2><<<npatch, kThreads, 0, s>>>(patches, x, rms);
+   else k_patch_rms<3><<<npatch, kThreads, 0, s>>>(patches, x, rms);
+}
+
+void launch_gather_samples(cudaStream_t s, int dim, int npatch, const PatchDesc *patches,
+                           const double *x, const double *scale, float *out, int S)
+{
+   if (npatch <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   const long long S3 = (long long)S * S * S;
+   dim3 grid((unsigned)((S3 + kThreads - 1) / kThreads), (unsigned)npatch);
+   if (dim == 2) k_gather_samples<2><<<grid, kThreads, 0, s>>>(patches, x, scale, out, S);
+   else k_gather_samples<3><<<grid, kThreads, 0, s>>>(patches, x, scale, out, S);
+}
+
+void launch_scatter_samples(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                            const Chunk *chunks, const float *y, const double *scale, int S,
+                            double *dst)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_scatter_samples<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, y, scale, S, dst);
+   else
+      k_scatter_samples<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, y, scale, S, dst);
+}
+
+void launch_dot_pair(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const double *r, const double *r2, const double *w,
+                     double2 *partial, const int *prob_chunk_begin, int nprob, double2 *acc)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(2, std::memory_order_relaxed);
+   if (dim == 2)
+      k_dot_pair<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, r, r2, w, partial);
+   else
+      k_dot_pair<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, r, r2, w, partial);
+   k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
+}
+
+void launch_alpha(cudaStream_t s, const double2 *acc, const int *active, int nprob,
+                  double *alpha)
+{
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_alpha<<<(nprob + 127) / 128, 128, 0, s>>>(acc, active, nprob, alpha);
+}
+
+void launch_apply_alpha(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                        const Chunk *chunks, const double *alpha, double *u, const double *e,
+                        double *r, const double *r2)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_apply_alpha<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, alpha, u, e, r, r2);
+   else
+      k_apply_alpha<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, alpha, u, e, r, r2);
+}
+
 void launch_gather(cudaStream_t s, const long long *idx, long long n, const double *src,
                    double *dst)
 {
@@ -1004,7 +1299,8 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
    template void launch_rbgs<T>(cudaStream_t, int, const PoissonSpec &, int,                \
                                 const PatchDesc *, const Chunk *, T *, const T *, const T *, \
                                 const T *, const T *, const unsigned char *, int,           \
-                                unsigned long long *, const int *);                         \
+                                unsigned long long *, const int *, const long long *,       \
+                                const BcCoefs &);                                           \
    template void launch_flux<T>(cudaStream_t, int, const PoissonSpec &, int,                \
                                 const PatchDesc *, const Chunk *, const T *, const double *, \
                                 const unsigned char *, const double *, const double *,      \

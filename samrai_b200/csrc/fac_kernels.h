@@ -20,12 +20,13 @@ void launch_cf_flux(cudaStream_t s, const CfFace *faces, int nfaces, const Patch
                     const T *u, const T *dside, int dvar, double dconst, const double *tranwt,
                     const double *longwt, T *cfflux, const int *run);
 
+// facemap != NULL: fused colour pass (no ghost cells read, see fac_kernels.cu)
 template <class T>
 void launch_rbgs(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                  const PatchDesc *patches, const Chunk *chunks, T *u, const T *f,
                  const T *dside, const T *cfield, const T *cfflux,
                  const unsigned char *cfmask, int offset, unsigned long long *maxres,
-                 const int *run);
+                 const int *run, const long long *facemap, const BcCoefs &bc);
 
 // Fluxes and residual are always FP64; the unknown may be FP32 (mixed).
 template <class TU>
@@ -68,6 +69,26 @@ void launch_sweep_check(cudaStream_t s, const unsigned long long *red,
                         const unsigned long long *blk, const int *last_patch, int nprob,
                         double tol, int *run, long long *sweeps);
 
+void launch_accumulate(cudaStream_t s, const long long *src, long long *dst, int n);
+
+// learned correction
+void launch_g0_to_g1(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const double *src, double *dst);
+void launch_patch_rms(cudaStream_t s, int dim, int npatch, const PatchDesc *patches,
+                      const double *x, double *rms);
+void launch_gather_samples(cudaStream_t s, int dim, int npatch, const PatchDesc *patches,
+                           const double *x, const double *scale, float *out, int S);
+void launch_scatter_samples(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                            const Chunk *chunks, const float *y, const double *scale, int S,
+                            double *dst);
+void launch_dot_pair(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const double *r, const double *r2, const double *w,
+                     double2 *partial, const int *prob_chunk_begin, int nprob, double2 *acc);
+void launch_alpha(cudaStream_t s, const double2 *acc, const int *active, int nprob,
+                  double *alpha);
+void launch_apply_alpha(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                        const Chunk *chunks, const double *alpha, double *u, const double *e,
+                        double *r, const double *r2);
 void launch_gather(cudaStream_t s, const long long *idx, long long n, const double *src,
                    double *dst);
 void launch_scatter(cudaStream_t s, const long long *idx, long long n, const double *src,

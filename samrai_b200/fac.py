@@ -51,6 +51,7 @@ def load_library(build_if_missing=True):
     L = ctypes.CDLL(path)
     vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
     szp = ctypes.POINTER(ctypes.c_size_t)
+    fp = ctypes.POINTER(ctypes.c_float)
     sig = {
         "fac_last_error": (ctypes.c_char_p, []),
         "fac_ctx_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int]),
@@ -64,6 +65,8 @@ def load_library(build_if_missing=True):
                                           ctypes.c_int, ctypes.c_int]),
         "fac_initialize": (ctypes.c_int, [vp]),
         "fac_set_precision": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_fused": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
         "fac_side_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
         "fac_oside_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
@@ -101,6 +104,17 @@ def load_library(build_if_missing=True):
         "fac_timer": (ctypes.c_int, [vp, ctypes.c_int, dp]),
         "fac_trace_enable": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_trace_read": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int, ip]),
+        "fac_cnn_last_error": (ctypes.c_char_p, []),
+        "fac_cnn_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_ulonglong]),
+        "fac_cnn_destroy": (ctypes.c_int, [vp]),
+        "fac_cnn_set_weights": (ctypes.c_int, [vp, fp, fp, fp, fp]),
+        "fac_cnn_get_weights": (ctypes.c_int, [vp, fp, fp, fp, fp]),
+        "fac_cnn_forward": (ctypes.c_int, [vp, vp, ctypes.c_longlong, vp]),
+        "fac_cnn_gradients": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_longlong, dp, fp, fp,
+                                             fp, fp]),
+        "fac_cnn_train_step": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_longlong,
+                                              ctypes.c_double, ctypes.c_float, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -315,6 +329,12 @@ class FacContext:
     def synchronize(self):
         _check(load_library().fac_synchronize(self.h))
 
+    def set_fused(self, on=True):
+        _check(load_library().fac_set_fused(self.h, int(on)))
+
+    def set_graph(self, on=True):
+        _check(load_library().fac_set_graph(self.h, int(on)))
+
     def zero(self, fid):
         _check(load_library().fac_zero_field(self.h, fid))
 
@@ -481,3 +501,64 @@ class CellPoissonFACSolver:
         net = hist[-1] / (hist[0] + 1e-20)
         avg = net ** (1.0 / (len(hist) - 1))
         return avg, hist[-1] / hist[-2]
+
+
+CNN_BOX = 18
+CNN_SHAPES = [(27, 16), (27, 16, 16), (27, 16, 16), (27, 16)]
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _cnn_check(rc):
+    if rc != 0:
+        raise FacError(rc, load_library().fac_cnn_last_error().decode())
+
+
+class CNN:
+    """The learned coarse-correction network (fac_cnn_* in the C ABI).
+    Inputs and outputs are device pointers (e.g. torch CUDA tensors'
+    data_ptr()) holding nsamp * 18^3 FP32 values."""
+
+    def __init__(self, max_batch, device=0, seed=0):
+        self.h = ctypes.c_void_p()
+        _cnn_check(load_library().fac_cnn_create(ctypes.byref(self.h), device, max_batch, seed))
+        self.max_batch = max_batch
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().fac_cnn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_weights(self, ws):
+        ws = [np.ascontiguousarray(w, dtype=np.float32).reshape(s) for w, s in zip(ws, CNN_SHAPES)]
+        _cnn_check(load_library().fac_cnn_set_weights(self.h, *[_fp(w) for w in ws]))
+
+    def get_weights(self):
+        ws = [np.zeros(s, dtype=np.float32) for s in CNN_SHAPES]
+        _cnn_check(load_library().fac_cnn_get_weights(self.h, *[_fp(w) for w in ws]))
+        return ws
+
+    def forward(self, x_ptr, nsamp, y_ptr):
+        _cnn_check(load_library().fac_cnn_forward(self.h, x_ptr, nsamp, y_ptr))
+
+    def gradients(self, x_ptr, t_ptr, m_ptr, nsamp):
+        gs = [np.zeros(s, dtype=np.float32) for s in CNN_SHAPES]
+        loss = ctypes.c_double(0.0)
+        _cnn_check(load_library().fac_cnn_gradients(self.h, x_ptr, t_ptr, m_ptr, nsamp,
+                                                    ctypes.byref(loss), *[_fp(g) for g in gs]))
+        return loss.value, gs
+
+    def train_step(self, x_ptr, t_ptr, m_ptr, nsamp, mask_sum, lr):
+        loss = ctypes.c_double(0.0)
+        _cnn_check(load_library().fac_cnn_train_step(self.h, x_ptr, t_ptr, m_ptr, nsamp,
+                                                     float(mask_sum), float(lr),
+                                                     ctypes.byref(loss)))
+        return loss.value

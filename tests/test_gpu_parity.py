@@ -207,3 +207,22 @@ def test_mg_extended_hierarchy_matches_oracle(require_gpu):
         num += float(np.sum((a - b) ** 2))
         den += float(np.sum(b ** 2))
     assert (num / den) ** 0.5 <= 1e-9
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_matches_eager(precision, require_gpu):
+    """fac_solve replays one captured CUDA graph per cycle; the eager launch
+    sequence must give bit-identical results."""
+    probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (31, 32)]
+    prm = dict(coarse_tol=1e-300, coarse_max_it=20)
+    out = []
+    for graph in (True, False):
+        g = fac.FacContext(probs, params=prm, precision=precision)
+        g.set_graph(graph)
+        conv, its, res = g.solve()
+        out.append((its.copy(), [g.download(U, i, ln) for i in range(2)
+                                 for ln in range(probs[0].nlev)]))
+        g.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        assert np.array_equal(a, b)
