@@ -286,6 +286,35 @@ int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level);
  * FAC_E of that level as scratch. */
 int fac_learned_samples(fac_ctx *ctx, int level, float *x, double *scale);
 
+/* ---- allocation-free norm.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory when they need a norm:
+ * codes that hand all device memory to a pool allocator up front (as
+ * SAMRAI does with Umpire pools), so a cudaMalloc would fail or take memory
+ * the pool was promised, and codes whose time step may not call cudaMalloc
+ * because it synchronises the device and stalls their other streams.
+ *
+ * Weighted RMS norm per segment: norms[s] = sqrt(sum w x^2) / sqrt(sum w)
+ * over elements seg_offsets[s] .. seg_offsets[s+1]-1 of the device arrays
+ * x and w (the reduction of fac_rms_norm).  x, w and norms are device
+ * pointers owned by the caller; seg_offsets is a host array of nseg+1
+ * ascending offsets; stream is a cudaStream_t (NULL: legacy default
+ * stream) and the call returns without waiting for the result.
+ *
+ * Partial sums live in a static device array of FAC_NOALLOC_MAX_SEGMENTS x
+ * 64 double2 (256 KiB) that every GPU loading this library holds until the
+ * process exits; nothing is allocated or freed per call.  nseg above
+ * FAC_NOALLOC_MAX_SEGMENTS returns FAC_ERR_ARG.  The first call on each
+ * device looks up that device's address of the array (cudaGetSymbolAddress,
+ * with the device current); make that first call before any stream capture.
+ * All calls share the array: calls whose work can overlap on the GPU (two
+ * streams, or two host threads) race and must be serialised by the caller.
+ * Every partial sum a call reads it first writes, so no clearing is needed. */
+#define FAC_NOALLOC_MAX_SEGMENTS 256
+int fac_rms_norm_noalloc(const double *x, const double *w,
+                         const long long *seg_offsets, int nseg, double *norms,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif
