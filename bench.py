@@ -202,6 +202,9 @@ def main():
                     help="precision of the headline (multigrid-extended) variant")
     ap.add_argument("--smoother-only", type=int, default=0, metavar="SWEEPS",
                     help="only run SWEEPS red-black sweeps on the largest level (for ncu)")
+    ap.add_argument("--cycles", type=int, default=0, metavar="N",
+                    help="only run one solve of the headline variant stopped after N cycles "
+                         "(a short, fixed launch sequence for kernel captures)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -243,6 +246,18 @@ def main():
         ms = ctx.timer_stop()
         print(json.dumps({"smoother_only": args.smoother_only, "level": ln, "cells": sizes[ln],
                           "ms": ms}), flush=True)
+        ctx.close()
+        return 0
+
+    if args.cycles:
+        ctx.close()
+        ctx = fac.FacContext(mg, params=dict(PARAMS_MG, max_cycles=args.cycles),
+                             device=local_rank, precision=args.precision)
+        ctx.timer_start()
+        conv, its, res = ctx.solve()
+        ms = ctx.timer_stop()
+        print(json.dumps({"cycles": args.cycles, "problems": len(mg), "cells": cells,
+                          "ms": ms, "launches": fac.kernel_launches()}), flush=True)
         ctx.close()
         return 0
 

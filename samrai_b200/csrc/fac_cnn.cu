@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/samrai_fac_b200.h"
+#include "fac_kernels.h"
 
 namespace {
 
@@ -437,6 +438,7 @@ int pack(fac_cnn *n)
       k_pack_mid<<<(T * C * C + 255) / 256, 256, 0, n->stream>>>(n->w[l + 1], n->wf[l], n->wd[l]);
    }
    k_round_bf16<<<(T * C + 127) / 128, 128, 0, n->stream>>>(n->w[0], n->w1r, T * C);
+   samrai_b200::add_kernel_launches(3);
    CNN_CHECK(cudaGetLastError());
    return FAC_OK;
 }
@@ -453,6 +455,7 @@ int forward_on(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st)
    k_conv_mid<<<mb, 256, 0, st>>>(n->a[0], n->wf[0], n->a[1], nullptr, cells, 0);
    k_conv_mid<<<mb, 256, 0, st>>>(n->a[1], n->wf[1], n->a[2], nullptr, cells, 0);
    k_conv_out<<<gb, tb, 0, st>>>(n->a[2], n->w[3], n->y, cells);
+   samrai_b200::add_kernel_launches(5);
    CNN_CHECK(cudaGetLastError());
    return FAC_OK;
 }
@@ -482,6 +485,7 @@ int backward(fac_cnn *n, const float *target, const float *mask, long long nsamp
    k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[0], n->d[1], n->gw[1], cells, per_block);
    k_conv_mid<<<mb, 256, 0, n->stream>>>(n->d[1], n->wd[0], n->d[0], n->a[0], cells, 1);
    k_bwd_weight_in<<<wb, T * C, 0, n->stream>>>(n->x0, n->d[0], n->gw[0], cells, per_block);
+   samrai_b200::add_kernel_launches(8);
    CNN_CHECK(cudaGetLastError());
    return FAC_OK;
 }
@@ -694,6 +698,7 @@ int fac_cnn_train_step(fac_cnn *n, const float *x, const float *target, const fl
    for (int l = 0; l < 4; ++l)
       k_adam<<<(kSizes[l] + 255) / 256, 256, 0, n->stream>>>(n->w[l], n->gw[l], n->m[l], n->v[l],
                                                               kSizes[l], lr, b1, b2, eps, c1, c2);
+   samrai_b200::add_kernel_launches(4);
    if ((rc = pack(n))) return rc;
    if (loss) {
       double l = 0;

@@ -185,12 +185,20 @@ struct DevArray {
    DevArray &operator=(const DevArray &) = delete;
 };
 
+// The full chunk list and per-problem chunk ranges behind a work list that
+// the device compacts to the active problems (k_compact).
+struct WorkSrc {
+   DevArray<Chunk> all;
+   DevArray<int> pcb;
+};
+
 template <class I>
 struct ItemList {
    std::vector<I> items;
    std::vector<Chunk> chunks;
    DevArray<I> d_items;
    DevArray<Chunk> d_chunks;
+   WorkSrc ws;
    void add(const I &it, long long ncells, int aux = 0)
    {
       const int id = (int)items.size();
@@ -216,6 +224,8 @@ struct ItemList {
       chunks.clear();
       d_items.free();
       d_chunks.free();
+      ws.all.free();
+      ws.pcb.free();
    }
 };
 
@@ -260,6 +270,7 @@ struct LevelState {
    // work chunks
    std::vector<Chunk> cell_chunks, slot_chunks, flux_chunks;
    DevArray<Chunk> d_cell_chunks, d_slot_chunks, d_flux_chunks;
+   WorkSrc ws_cell, ws_slot, ws_flux;
    std::vector<int> prob_cell_chunk_begin;
    DevArray<int> d_prob_cell_chunk_begin;
    DevArray<double2> norm_partial;
@@ -322,8 +333,22 @@ struct fac_ctx {
       int kind;
       cudaEvent_t a, b;
       double bytes;
+      // records inside the captured cycle: bytes of the problems active in
+      // each replay = scale x sum of per_prob over the active problems
+      const std::vector<double> *per_prob;
+      double scale;
    };
    bool profiling = false;
+   // the captured cycle: its event records, how many of our kernels it
+   // launches, and whether it was captured with profiling on
+   std::vector<ProfRec> graph_prof;
+   long long graph_launches = 0;
+   bool graph_profiled = false;
+   struct KindAcc {
+      long long n = 0;
+      double ms = 0, bytes = 0;
+   };
+   KindAcc graph_acc[4];
    // per-operation wall time with a stream synchronisation on both sides
    // (tbox::Timer::barrierAndStart semantics, tbox/Timer.C:174)
    bool tracing = false;
@@ -335,13 +360,28 @@ struct fac_ctx {
 
    LevelState L[kMaxLevels];
    DevArray<int> active, run;
+   // every work list of the context, compacted after each change of active
+   std::vector<WorkReg> work_regs;
+   DevArray<WorkReg> d_work_regs;
    DevArray<long long> sweeps_call, sweeps_coarse;
    DevArray<double2> norm_acc;
    std::vector<std::vector<double>> hist;  // per problem residual history
 
-   ~fac_ctx()
+   void drop_graph()
    {
       if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+      cycle_exec = nullptr;
+      for (const ProfRec &r : graph_prof) {
+         cudaEventDestroy(r.a);
+         cudaEventDestroy(r.b);
+      }
+      graph_prof.clear();
+      graph_launches = 0;
+   }
+
+   ~fac_ctx()
+   {
+      drop_graph();
       for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
       if (t0) cudaEventDestroy(t0);
       if (t1) cudaEventDestroy(t1);
@@ -393,13 +433,25 @@ double active_bytes(const fac_ctx *c, const std::vector<double> &per_prob)
    return b;
 }
 
-// Record the start of a profiled launch; returns its index or -1.
-int prof_begin(fac_ctx *c, int kind, double bytes)
+// Record the start of a profiled launch; returns its index or -1.  During
+// stream capture the two events become event-record nodes of the cycle graph
+// (external records), read back after every replay (harvest_graph_profile).
+int prof_begin(fac_ctx *c, int kind, const std::vector<double> &per_prob, double scale)
 {
    if (!c->profiling) return -1;
    fac_ctx::ProfRec r;
    r.kind = kind;
-   r.bytes = bytes;
+   r.per_prob = &per_prob;
+   r.scale = scale;
+   if (c->capturing) {
+      r.bytes = 0;
+      CUDA_CHECK(cudaEventCreate(&r.a));
+      CUDA_CHECK(cudaEventCreate(&r.b));
+      CUDA_CHECK(cudaEventRecordWithFlags(r.a, c->stream, cudaEventRecordExternal));
+      c->graph_prof.push_back(r);
+      return (int)c->graph_prof.size() - 1;
+   }
+   r.bytes = scale * active_bytes(c, per_prob);
    r.a = next_event(c);
    r.b = next_event(c);
    CUDA_CHECK(cudaEventRecord(r.a, c->stream));
@@ -410,7 +462,25 @@ int prof_begin(fac_ctx *c, int kind, double bytes)
 void prof_end(fac_ctx *c, int idx)
 {
    if (idx < 0) return;
-   CUDA_CHECK(cudaEventRecord(c->prof[idx].b, c->stream));
+   if (c->capturing)
+      CUDA_CHECK(cudaEventRecordWithFlags(c->graph_prof[idx].b, c->stream,
+                                          cudaEventRecordExternal));
+   else
+      CUDA_CHECK(cudaEventRecord(c->prof[idx].b, c->stream));
+}
+
+// After a replay of the cycle graph has completed: add its launch times and
+// the bytes of the problems that were active in it.
+void harvest_graph_profile(fac_ctx *c)
+{
+   for (const fac_ctx::ProfRec &r : c->graph_prof) {
+      float e = 0.f;
+      CUDA_CHECK(cudaEventElapsedTime(&e, r.a, r.b));
+      fac_ctx::KindAcc &acc = c->graph_acc[r.kind];
+      acc.n += 1;
+      acc.ms += e;
+      acc.bytes += r.scale * active_bytes(c, *r.per_prob);
+   }
 }
 
 double *field_ptr(LevelState &L, int fid)
@@ -810,6 +880,7 @@ void build_facemap(fac_ctx *c, int ln)
    for (const CfFace &f : L.cf) mask[f.oidx] = 1;
    for (long long t = 0; t < L.no; ++t) {
       if (fmap[t] == -3) ok = false;
+      if (fmap[t] >= L.n1) throw FacError(FAC_ERR_ARG, "face table index out of range");
       if ((fmap[t] == -2) != (mask[t] != 0))
          throw FacError(FAC_ERR_NESTING, "face table disagrees with the coarse-fine boundary");
    }
@@ -834,8 +905,10 @@ void build_chunks(fac_ctx *c, int ln)
          L.prob_cell_chunk_begin[cur_prob] = (int)L.cell_chunks.size();
       }
       const long long n = b.size();
+      // aux: the chunk's own index (slot of its partial sums)
       for (long long s = 0; s < n; s += kChunk)
-         L.cell_chunks.push_back({ip, (int)s, (int)std::min<long long>(kChunk, n - s), 0});
+         L.cell_chunks.push_back({ip, (int)s, (int)std::min<long long>(kChunk, n - s),
+                                  (int)L.cell_chunks.size()});
       const long long nx = b.hi[0] - b.lo[0] + 1;
       const long long slots = ((nx + 1) / 2) * (n / nx);
       for (long long s = 0; s < slots; s += kChunk)
@@ -1250,6 +1323,67 @@ void validate_tables(fac_ctx *c)
    }
 }
 
+// Record one work list for device-side compaction; its chunks must be in
+// problem order.
+template <class ProbOf>
+void register_work(fac_ctx *c, WorkSrc &ws, const std::vector<Chunk> &chunks, Chunk *list,
+                   ProbOf prob_of)
+{
+   const int np = nprob(c);
+   std::vector<int> pcb(np + 1, 0);
+   int prev = 0;
+   for (const Chunk &ch : chunks) {
+      const int p = prob_of(ch);
+      if (p < prev || p >= np) throw FacError(FAC_ERR_ARG, "work list not in problem order");
+      prev = p;
+      pcb[p + 1] += 1;
+   }
+   for (int p = 0; p < np; ++p) pcb[p + 1] += pcb[p];
+   if (!chunks.empty() && !list && !g_dry)
+      throw FacError(FAC_ERR_STATE, "work list registered before its upload");
+   ws.all.upload(chunks, c->stream);
+   ws.pcb.upload(pcb, c->stream);
+   if (!chunks.empty()) c->work_regs.push_back({ws.all.p, list, ws.pcb.p, (int)chunks.size(), 0});
+}
+
+template <class I>
+void register_items(fac_ctx *c, ItemList<I> &it)
+{
+   register_work(c, it.ws, it.chunks, it.d_chunks.p,
+                 [&](const Chunk &ch) { return it.items[ch.patch].prob; });
+}
+
+void register_work_lists(fac_ctx *c)
+{
+   c->work_regs.clear();
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      auto pp = [&](const Chunk &ch) { return L.hp[ch.patch].prob; };
+      register_work(c, L.ws_cell, L.cell_chunks, L.d_cell_chunks.p, pp);
+      register_work(c, L.ws_slot, L.slot_chunks, L.d_slot_chunks.p, pp);
+      register_work(c, L.ws_flux, L.flux_chunks, L.d_flux_chunks.p, pp);
+      register_items(c, L.fill_nc);
+      register_items(c, L.fill_wc);
+      register_items(c, L.restrict_g1);
+      register_items(c, L.restrict_g0);
+      register_items(c, L.fcoarsen);
+      register_items(c, L.tmp_fill);
+      register_items(c, L.prolong);
+   }
+   c->d_work_regs.upload(c->work_regs, c->stream);
+}
+
+// New active flags: upload them and compact every work list to the chunks of
+// the active problems (stream ordered, so graph replays see the new lists).
+void set_active(fac_ctx *c, const std::vector<int> &act)
+{
+   const int np = nprob(c);
+   CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int), cudaMemcpyHostToDevice,
+                              c->stream));
+   launch_compact(c->stream, c->d_work_regs.p, (int)c->work_regs.size(), c->active.p, np);
+   CUDA_CHECK(cudaGetLastError());
+}
+
 void initialize(fac_ctx *c)
 {
    if (c->probs.empty()) throw FacError(FAC_ERR_STATE, "no problems added");
@@ -1316,6 +1450,7 @@ void initialize(fac_ctx *c)
       L.fill_nc.upload(c->stream);
       L.fill_wc.upload(c->stream);
    }
+   register_work_lists(c);
    std::vector<int> ones(np, 1);
    c->active.upload(ones, c->stream);
    c->run.upload(ones, c->stream);
@@ -1342,7 +1477,7 @@ void ghost_fill(fac_ctx *c, int fid, int ln, bool with_coarse, int homogeneous, 
    double *dst = field_ptr(L, fid);
    const double *coarse = ln > 0 ? field_ptr(c->L[ln - 1], fid) : nullptr;
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
-   const int pi = prof_begin(c, 1, c->profiling ? active_bytes(c, L.fill_bytes_prob) : 0.0);
+   const int pi = prof_begin(c, 1, L.fill_bytes_prob, 1.0);
    launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), dst, dst, coarse,
                homogeneous, c->bc, mask);
    prof_end(c, pi);
@@ -1382,16 +1517,21 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
             launch_cf_flux(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, e, L.d.p,
                            c->spec.d_variable, c->spec.d_const, L.tranwt, L.longwt, L.cfflux.p,
                            c->run.p);
-         const int pi = prof_begin(c, 0, c->profiling ? active_bytes(c, L.rb_bytes_prob) : 0.0);
+         const int pi = prof_begin(c, 0, L.rb_bytes_prob, 1.0);
          launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
                      L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
                      color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p, fmap, c->bc);
          prof_end(c, pi);
       }
-      if (!fmap || isweep + 1 == nsweeps) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+      if (!fmap) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
       launch_sweep_check(c->stream, L.maxres_red.p, L.maxres_blk.p, L.last_patch.p, np, tol,
                          c->run.p, c->sweeps_call.p);
    }
+   // Fused passes leave the same-level ghosts stale; one fill of every active
+   // problem gives the ghost values the per-sweep fills would have left (a
+   // fill depends only on the interior, which a stopped problem no longer
+   // changes).
+   if (fmap && nsweeps > 0) ghost_fill(c, fid_e, ln, false, 1, c->active.p);
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1566,7 +1706,7 @@ void ghost_fill32(fac_ctx *c, int ln, bool with_coarse, int homogeneous, const i
    const float *coarse = ln > 0 ? c->L[ln - 1].e32.p : nullptr;
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
    const int pi =
-      prof_begin(c, 3, c->profiling ? 0.5 * active_bytes(c, L.fill_bytes_prob) : 0.0);
+      prof_begin(c, 3, L.fill_bytes_prob, 0.5);
    launch_fill<float>(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), L.e32.p, L.e32.p,
                       coarse, homogeneous, c->bc, mask);
    prof_end(c, pi);
@@ -1589,14 +1729,15 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
                                   L.d32.p, c->spec.d_variable, c->spec.d_const, L.tranwt,
                                   L.longwt, L.cfflux32.p, run);
          const int pi =
-            prof_begin(c, 2, c->profiling ? 0.5 * active_bytes(c, L.rb_bytes_prob) : 0.0);
+            prof_begin(c, 2, L.rb_bytes_prob, 0.5);
          launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
                             L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
                             L.c32.p, L.cfflux32.p, L.cfmask.p, color, nullptr, run, fmap, c->bc);
          prof_end(c, pi);
       }
-      if (!fmap || isweep + 1 == nsweeps) ghost_fill32(c, ln, false, 1, run);
+      if (!fmap) ghost_fill32(c, ln, false, 1, run);
    }
+   if (fmap && nsweeps > 0) ghost_fill32(c, ln, false, 1, run);
    (void)np;
    CUDA_CHECK(cudaGetLastError());
 }
@@ -1733,8 +1874,7 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
    const int np = nprob(c);
    std::vector<int> act(np, 1);
    c->host_active = act;
-   CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int), cudaMemcpyHostToDevice,
-                              c->stream));
+   set_active(c, act);
    dirichlet(c, false);
    zero_field(c, FAC_E);
    zero_field(c, FAC_R);
@@ -1786,9 +1926,13 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
    // The whole cycle is one CUDA graph, captured on first use and replayed:
    // the launch sequence is fixed (converged problems are skipped on the
    // device through the active flags), so only the norms come back per cycle.
-   const bool graph = c->use_graph && !c->profiling && !c->tracing;
+   // With profiling on, the cycle is captured with event-record nodes around
+   // the profiled launches, so their times carry no host launch gaps.
+   const bool graph = c->use_graph && !c->tracing;
+   if (graph && c->cycle_exec && c->graph_profiled != c->profiling) c->drop_graph();
    if (graph && !c->cycle_exec) {
       cudaGraph_t g = nullptr;
+      const long long n0 = kernel_launch_count();
       CUDA_CHECK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       c->capturing = true;
       try {
@@ -1797,23 +1941,33 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
          c->capturing = false;
          cudaStreamEndCapture(c->stream, &g);
          if (g) cudaGraphDestroy(g);
+         c->drop_graph();
          throw;
       }
       c->capturing = false;
       CUDA_CHECK(cudaStreamEndCapture(c->stream, &g));
+      c->graph_launches = kernel_launch_count() - n0;
+      add_kernel_launches(-c->graph_launches);  // captured, not launched
+      c->graph_profiled = c->profiling;
       cudaError_t e = cudaGraphInstantiate(&c->cycle_exec, g, 0);
       cudaGraphDestroy(g);
       if (e != cudaSuccess) {
          c->cycle_exec = nullptr;
+         c->drop_graph();
          throw FacError(FAC_ERR_CUDA, std::string("cudaGraphInstantiate: ") +
                                           cudaGetErrorString(e));
       }
    }
    while (any) {
-      if (graph) CUDA_CHECK(cudaGraphLaunch(c->cycle_exec, c->stream));
-      else cycle_body();
+      if (graph) {
+         CUDA_CHECK(cudaGraphLaunch(c->cycle_exec, c->stream));
+         add_kernel_launches(c->graph_launches);
+      } else {
+         cycle_body();
+      }
       std::vector<double> nr;
       rms_norm_read(c, nr);
+      if (graph && c->profiling) harvest_graph_profile(c);
       ++it;
       any = false;
       for (int p = 0; p < np; ++p) {
@@ -1824,14 +1978,11 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
          if (!(nr[p] > eff[p] && it < c->max_cycles)) act[p] = 0;
          any = any || act[p];
       }
-      CUDA_CHECK(cudaMemcpyAsync(c->active.p, act.data(), np * sizeof(int),
-                                 cudaMemcpyHostToDevice, c->stream));
+      if (act != c->host_active) set_active(c, act);
       c->host_active = act;
    }
    c->host_active.assign(np, 1);
-   std::vector<int> ones(np, 1);
-   CUDA_CHECK(cudaMemcpyAsync(c->active.p, ones.data(), np * sizeof(int), cudaMemcpyHostToDevice,
-                              c->stream));
+   set_active(c, c->host_active);
    dirichlet(c, true);
    CUDA_CHECK(cudaStreamSynchronize(c->stream));
    for (int p = 0; p < np; ++p) {
@@ -2015,6 +2166,7 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol, double rel
       ctx->coarse_tol = coarse_tol;
       ctx->coarse_max_it = coarse_max_it;
       ctx->ewing = ewing;
+      ctx->drop_graph();  // sweep counts are part of the captured cycle
    });
 }
 
@@ -2023,10 +2175,7 @@ int fac_set_fused(fac_ctx *ctx, int on)
    return guarded([&] {
       if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
       ctx->fused = on != 0;
-      if (ctx->cycle_exec) {
-         cudaGraphExecDestroy(ctx->cycle_exec);
-         ctx->cycle_exec = nullptr;
-      }
+      ctx->drop_graph();
    });
 }
 
@@ -2035,10 +2184,7 @@ int fac_set_graph(fac_ctx *ctx, int on)
    return guarded([&] {
       if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
       ctx->use_graph = on != 0;
-      if (ctx->cycle_exec) {
-         cudaGraphExecDestroy(ctx->cycle_exec);
-         ctx->cycle_exec = nullptr;
-      }
+      ctx->drop_graph();
    });
 }
 
@@ -2046,10 +2192,7 @@ int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level)
 {
    return guarded([&] {
       check_ops(ctx);
-      if (ctx->cycle_exec) {
-         cudaGraphExecDestroy(ctx->cycle_exec);
-         ctx->cycle_exec = nullptr;
-      }
+      ctx->drop_graph();
       if (!net) {
          ctx->cnn = nullptr;
          ctx->learned_level = -1;
@@ -2484,6 +2627,7 @@ int fac_profile_enable(fac_ctx *ctx, int on)
       ctx->profiling = on != 0;
       ctx->prof.clear();
       ctx->ev_next = 0;
+      for (auto &a : ctx->graph_acc) a = fac_ctx::KindAcc();
    });
 }
 
@@ -2492,8 +2636,9 @@ int fac_profile_read(fac_ctx *ctx, int kind, long long *launches, double *ms, do
    return guarded([&] {
       check_ops(ctx);
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-      long long n = 0;
-      double t = 0, b = 0;
+      if (kind < 0 || kind > 3) throw FacError(FAC_ERR_ARG, "profile kind out of range");
+      long long n = ctx->graph_acc[kind].n;
+      double t = ctx->graph_acc[kind].ms, b = ctx->graph_acc[kind].bytes;
       for (const auto &r : ctx->prof) {
          if (r.kind != kind) continue;
          float e = 0.f;
@@ -2515,6 +2660,7 @@ int fac_profile_reset(fac_ctx *ctx)
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
       ctx->prof.clear();
       ctx->ev_next = 0;
+      for (auto &a : ctx->graph_acc) a = fac_ctx::KindAcc();
    });
 }
 

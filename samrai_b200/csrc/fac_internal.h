@@ -37,6 +37,17 @@ struct Chunk {
    int aux;
 };
 
+// A work list that is compacted on the device: `all` holds the full list
+// (chunks in problem order, problem p owning [pcb[p], pcb[p+1])), `list` the
+// chunks of the active problems followed by end markers (patch = -1).
+struct WorkReg {
+   const Chunk *all;
+   Chunk *list;
+   const int *pcb;
+   int n;
+   int pad;
+};
+
 // Array descriptor: element (i,j,k) of the box lo..lo+n-1 lives at
 // base + (i-lo0) + n0*((j-lo1) + n1*(k-lo2)).
 struct ArrDesc {

@@ -21,6 +21,20 @@ namespace samrai_b200 {
 namespace {
 
 constexpr int kThreads = 256;
+// Blocks of a chunk kernel: enough to fill the GPU; each block walks the
+// work list with a grid stride.
+constexpr int kGridCap = 148 * 8;
+
+inline int work_grid(int nchunks) { return nchunks < kGridCap ? nchunks : kGridCap; }
+
+// Grid-stride walk over a work list of nwork entries.  The list is compacted
+// on the device whenever the set of iterating problems changes: the chunks of
+// those problems come first and a chunk with patch < 0 ends the list.
+#define WORK_LOOP(ch)                                      \
+   for (int w_ = blockIdx.x; w_ < nwork; w_ += gridDim.x) \
+      if (const Chunk ch = chunks[w_]; ch.patch < 0)       \
+         break;                                            \
+      else
 
 __device__ __forceinline__ long long aidx(const ArrDesc &A, int i, int j, int k)
 {
@@ -88,64 +102,65 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, doub
 
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks,
+k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
        T *__restrict__ dst, const T *__restrict__ src_same,
        const T *__restrict__ src_coarse, int homogeneous, BcCoefs bc,
        const int *__restrict__ active)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const FillItem &it = items[ch.patch];
-   if (active && !active[it.prob]) return;
-   const T *src = it.src_is_coarse ? src_coarse : src_same;
-   const int nx = it.hi[0] - it.lo[0] + 1;
-   const int ny = it.hi[1] - it.lo[1] + 1;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = it.lo[0] + lin % nx;
-      const int r = lin / nx;
-      const int j = it.lo[1] + r % ny;
-      const int k = it.lo[2] + r / ny;
-      T v;
-      if (it.kind == kFillCopy) {
-         v = src[aidx(it.src, i, j, k)];
-      } else if (it.kind == kFillCoarse) {
-         v = src[aidx(it.src, coarsen_index(i, it.ratio[0]),
-                      coarsen_index(j, it.ratio[1]),
-                      coarsen_index(k, it.ratio[2]))];
-      } else {
-         // Every ghost value of codimension m depends only on the interior
-         // cell reached by moving inward along all m outside axes
-         // (settype1/2/3cells{2,3}d applied in codimension order).
-         const T uin =
-            src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
-         T f[3];
-         int m = 0;
-         for (int a = 0; a < 3; ++a) {
-            if (it.side[a]) {
-               f[a] = robin<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc);
-               ++m;
+   WORK_LOOP(ch) {
+      const FillItem &it = items[ch.patch];
+      if (active && !active[it.prob]) continue;
+      const T *src = it.src_is_coarse ? src_coarse : src_same;
+      const int nx = it.hi[0] - it.lo[0] + 1;
+      const int ny = it.hi[1] - it.lo[1] + 1;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = it.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = it.lo[1] + r % ny;
+         const int k = it.lo[2] + r / ny;
+         T v;
+         if (it.kind == kFillCopy) {
+            v = src[aidx(it.src, i, j, k)];
+         } else if (it.kind == kFillCoarse) {
+            v = src[aidx(it.src, coarsen_index(i, it.ratio[0]),
+                         coarsen_index(j, it.ratio[1]),
+                         coarsen_index(k, it.ratio[2]))];
+         } else {
+            // Every ghost value of codimension m depends only on the interior
+            // cell reached by moving inward along all m outside axes
+            // (settype1/2/3cells{2,3}d applied in codimension order).
+            const T uin =
+               src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
+            T f[3];
+            int m = 0;
+            for (int a = 0; a < 3; ++a) {
+               if (it.side[a]) {
+                  f[a] = robin<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc);
+                  ++m;
+               } else {
+                  f[a] = (T)0;
+               }
+            }
+            if (m == 1) {
+               v = it.side[0] ? f[0] : (it.side[1] ? f[1] : f[2]);
+            } else if (m == 2) {
+               T s0 = (T)0, s1 = (T)0;
+               int n = 0;
+               for (int a = 0; a < 3; ++a)
+                  if (it.side[a]) {
+                     if (n == 0) s0 = f[a];
+                     else s1 = f[a];
+                     ++n;
+                  }
+               v = -uin + (s1 + s0);
             } else {
-               f[a] = (T)0;
+               const T two3 = (T)(2.0f / 3.0f);
+               v = -uin + two3 * ((f[0] + f[1]) + f[2]);
             }
          }
-         if (m == 1) {
-            v = it.side[0] ? f[0] : (it.side[1] ? f[1] : f[2]);
-         } else if (m == 2) {
-            T s0 = (T)0, s1 = (T)0;
-            int n = 0;
-            for (int a = 0; a < 3; ++a)
-               if (it.side[a]) {
-                  if (n == 0) s0 = f[a];
-                  else s1 = f[a];
-                  ++n;
-               }
-            v = -uin + (s1 + s0);
-         } else {
-            const T two3 = (T)(2.0f / 3.0f);
-            v = -uin + two3 * ((f[0] + f[1]) + f[2]);
-         }
+         dst[aidx(it.dst, i, j, k)] = v;
       }
-      dst[aidx(it.dst, i, j, k)] = v;
    }
 }
 
@@ -208,7 +223,7 @@ k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
 // face -- so the three ghost fills around each colour pass are not needed.
 template <int DIM, bool DVAR, int CKIND, class T, bool FUSED>
 __global__ void __launch_bounds__(kThreads, 3)
-k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
        T *__restrict__ u, const T *__restrict__ f,
        const T *__restrict__ dside, const T *__restrict__ cfield,
        const T *__restrict__ cfflux, const unsigned char *__restrict__ cfmask,
@@ -216,146 +231,148 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
        unsigned long long *__restrict__ maxres_patch, const int *__restrict__ run,
        const long long *__restrict__ facemap, BcCoefs bc)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   if (run && !run[p.prob]) return;
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   const int hx = (nx + 1) >> 1;
-   const T one = (T)1;
-   const T dxi = one / (T)p.dx[0], dyi = one / (T)p.dx[1];
-   const T dzi = DIM == 3 ? one / (T)p.dx[2] : (T)0;
-   const bool has_cf = (p.flags & 1) != 0;
-   const T rcoef = one;
-   double maxres = 0.0;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int s = ch.begin + t;
-      const int row = s / hx;
-      const int mm = s - row * hx;
-      const int j = p.lo[1] + row % ny;
-      const int k = DIM == 3 ? p.lo[2] + row / ny : 0;
-      int ioffset;
-      if (DIM == 2) {
-         const int q = p.lo[1] + j;
-         ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
-      } else {
-         const int q = p.lo[0] + j + k;
-         ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
-      }
-      const int i = p.lo[0] + ioffset + 2 * mm;
-      if (i > p.hi[0]) continue;
-      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
-      const long long sx = 1;
-      const long long sy = nx + 2;
-      const long long sz = (long long)(nx + 2) * (ny + 2);
-      const T uc = u[c];
-      T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
-      if (DVAR) {
-         dx0 = dside[sidx(p, 0, i, j, k)];
-         dx1 = dside[sidx(p, 0, i + 1, j, k)];
-         dy0 = dside[sidx(p, 1, i, j, k)];
-         dy1 = dside[sidx(p, 1, i, j + 1, k)];
-         if (DIM == 3) {
-            dz0 = dside[sidx(p, 2, i, j, k)];
-            dz1 = dside[sidx(p, 2, i, j, k + 1)];
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      if (run && !run[p.prob]) continue;
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const int hx = (nx + 1) >> 1;
+      const T one = (T)1;
+      const T dxi = one / (T)p.dx[0], dyi = one / (T)p.dx[1];
+      const T dzi = DIM == 3 ? one / (T)p.dx[2] : (T)0;
+      const bool has_cf = (p.flags & 1) != 0;
+      const T rcoef = one;
+      double maxres = 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int s = ch.begin + t;
+         const int row = s / hx;
+         const int mm = s - row * hx;
+         const int j = p.lo[1] + row % ny;
+         const int k = DIM == 3 ? p.lo[2] + row / ny : 0;
+         int ioffset;
+         if (DIM == 2) {
+            const int q = p.lo[1] + j;
+            ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
+         } else {
+            const int q = p.lo[0] + j + k;
+            ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
          }
-      } else {
-         dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
-      }
-      T nxl, nxh, nyl, nyh, nzl = (T)0, nzh = (T)0;
-      if (FUSED) {
-         auto across = [&](int a, int sd, long long own) -> T {
-            const long long m = facemap[oidx(p, a, sd, i, j, k)];
-            if (m >= 0) return u[m];
-            if (m == -1) return robin<T>(uc, 2 * a + sd, (T)p.dx[a], 1, bc);
-            return u[own];
-         };
-         nxl = i == p.lo[0] ? across(0, 0, c - sx) : u[c - sx];
-         nxh = i == p.hi[0] ? across(0, 1, c + sx) : u[c + sx];
-         nyl = j == p.lo[1] ? across(1, 0, c - sy) : u[c - sy];
-         nyh = j == p.hi[1] ? across(1, 1, c + sy) : u[c + sy];
-         if (DIM == 3) {
-            nzl = k == p.lo[2] ? across(2, 0, c - sz) : u[c - sz];
-            nzh = k == p.hi[2] ? across(2, 1, c + sz) : u[c + sz];
-         }
-      } else {
-         nxl = u[c - sx];
-         nxh = u[c + sx];
-         nyl = u[c - sy];
-         nyh = u[c + sy];
-         if (DIM == 3) {
-            nzl = u[c - sz];
-            nzh = u[c + sz];
-         }
-      }
-      T fxl = dxi * dx0 * (uc - nxl);
-      T fxh = dxi * dx1 * (nxh - uc);
-      T fyl = dyi * dy0 * (uc - nyl);
-      T fyh = dyi * dy1 * (nyh - uc);
-      T fzl = (T)0, fzh = (T)0;
-      if (DIM == 3) {
-         fzl = dzi * dz0 * (uc - nzl);
-         fzh = dzi * dz1 * (nzh - uc);
-      }
-      if (has_cf) {
-         if (i == p.lo[0]) {
-            const long long o = oidx(p, 0, 0, i, j, k);
-            if (cfmask[o]) fxl = cfflux[o];
-         }
-         if (i == p.hi[0]) {
-            const long long o = oidx(p, 0, 1, i, j, k);
-            if (cfmask[o]) fxh = cfflux[o];
-         }
-         if (j == p.lo[1]) {
-            const long long o = oidx(p, 1, 0, i, j, k);
-            if (cfmask[o]) fyl = cfflux[o];
-         }
-         if (j == p.hi[1]) {
-            const long long o = oidx(p, 1, 1, i, j, k);
-            if (cfmask[o]) fyh = cfflux[o];
-         }
-         if (DIM == 3) {
-            if (k == p.lo[2]) {
-               const long long o = oidx(p, 2, 0, i, j, k);
-               if (cfmask[o]) fzl = cfflux[o];
+         const int i = p.lo[0] + ioffset + 2 * mm;
+         if (i > p.hi[0]) continue;
+         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+         const long long sx = 1;
+         const long long sy = nx + 2;
+         const long long sz = (long long)(nx + 2) * (ny + 2);
+         const T uc = u[c];
+         T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
+         if (DVAR) {
+            dx0 = dside[sidx(p, 0, i, j, k)];
+            dx1 = dside[sidx(p, 0, i + 1, j, k)];
+            dy0 = dside[sidx(p, 1, i, j, k)];
+            dy1 = dside[sidx(p, 1, i, j + 1, k)];
+            if (DIM == 3) {
+               dz0 = dside[sidx(p, 2, i, j, k)];
+               dz1 = dside[sidx(p, 2, i, j, k + 1)];
             }
-            if (k == p.hi[2]) {
-               const long long o = oidx(p, 2, 1, i, j, k);
-               if (cfmask[o]) fzh = cfflux[o];
+         } else {
+            dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
+         }
+         T nxl, nxh, nyl, nyh, nzl = (T)0, nzh = (T)0;
+         if (FUSED) {
+            auto across = [&](int a, int sd, long long own) -> T {
+               const long long m = facemap[oidx(p, a, sd, i, j, k)];
+               if (m >= 0) return u[m];
+               if (m == -1) return robin<T>(uc, 2 * a + sd, (T)p.dx[a], 1, bc);
+               return u[own];
+            };
+            nxl = i == p.lo[0] ? across(0, 0, c - sx) : u[c - sx];
+            nxh = i == p.hi[0] ? across(0, 1, c + sx) : u[c + sx];
+            nyl = j == p.lo[1] ? across(1, 0, c - sy) : u[c - sy];
+            nyh = j == p.hi[1] ? across(1, 1, c + sy) : u[c + sy];
+            if (DIM == 3) {
+               nzl = k == p.lo[2] ? across(2, 0, c - sz) : u[c - sz];
+               nzh = k == p.hi[2] ? across(2, 1, c + sz) : u[c + sz];
+            }
+         } else {
+            nxl = u[c - sx];
+            nxh = u[c + sx];
+            nyl = u[c - sy];
+            nyh = u[c + sy];
+            if (DIM == 3) {
+               nzl = u[c - sz];
+               nzh = u[c + sz];
             }
          }
+         T fxl = dxi * dx0 * (uc - nxl);
+         T fxh = dxi * dx1 * (nxh - uc);
+         T fyl = dyi * dy0 * (uc - nyl);
+         T fyh = dyi * dy1 * (nyh - uc);
+         T fzl = (T)0, fzh = (T)0;
+         if (DIM == 3) {
+            fzl = dzi * dz0 * (uc - nzl);
+            fzh = dzi * dz1 * (nzh - uc);
+         }
+         if (has_cf) {
+            if (i == p.lo[0]) {
+               const long long o = oidx(p, 0, 0, i, j, k);
+               if (cfmask[o]) fxl = cfflux[o];
+            }
+            if (i == p.hi[0]) {
+               const long long o = oidx(p, 0, 1, i, j, k);
+               if (cfmask[o]) fxh = cfflux[o];
+            }
+            if (j == p.lo[1]) {
+               const long long o = oidx(p, 1, 0, i, j, k);
+               if (cfmask[o]) fyl = cfflux[o];
+            }
+            if (j == p.hi[1]) {
+               const long long o = oidx(p, 1, 1, i, j, k);
+               if (cfmask[o]) fyh = cfflux[o];
+            }
+            if (DIM == 3) {
+               if (k == p.lo[2]) {
+                  const long long o = oidx(p, 2, 0, i, j, k);
+                  if (cfmask[o]) fzl = cfflux[o];
+               }
+               if (k == p.hi[2]) {
+                  const long long o = oidx(p, 2, 1, i, j, k);
+                  if (cfmask[o]) fzh = cfflux[o];
+               }
+            }
+         }
+         const T sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
+                                 : (CKIND == 1 ? cconst : (T)0);
+         const T fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
+         T residual, dudr;
+         if (DIM == 2) {
+            residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
+            dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
+         } else {
+            const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
+            residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
+                       sf * uc;
+            dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
+                          sf);
+         }
+         const T du = -residual * dudr;
+         u[c] = uc + du * rcoef;
+         const double ar = fabs((double)residual);
+         if (maxres < ar) maxres = ar;
       }
-      const T sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
-                              : (CKIND == 1 ? cconst : (T)0);
-      const T fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
-      T residual, dudr;
-      if (DIM == 2) {
-         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
-         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
-      } else {
-         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
-         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
-                    sf * uc;
-         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
-                       sf);
+      // block max, then one atomic per block
+      __shared__ double red[kThreads / 32];
+      for (int o = 16; o > 0; o >>= 1) {
+         const double other = __shfl_down_sync(0xffffffffu, maxres, o);
+         maxres = other > maxres ? other : maxres;
       }
-      const T du = -residual * dudr;
-      u[c] = uc + du * rcoef;
-      const double ar = fabs((double)residual);
-      if (maxres < ar) maxres = ar;
-   }
-   // block max, then one atomic per block
-   __shared__ double red[kThreads / 32];
-   for (int o = 16; o > 0; o >>= 1) {
-      const double other = __shfl_down_sync(0xffffffffu, maxres, o);
-      maxres = other > maxres ? other : maxres;
-   }
-   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxres;
-   __syncthreads();
-   if (threadIdx.x == 0) {
-      double m = red[0];
-      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
-      if (maxres_patch) atomic_max_nonneg(&maxres_patch[ch.patch], m);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxres;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+         double m = red[0];
+         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
+         if (maxres_patch) atomic_max_nonneg(&maxres_patch[ch.patch], m);
+      }
+      __syncthreads();  // shared memory is reused by the next chunk
    }
 }
 
@@ -366,58 +383,59 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
 
 template <int DIM, bool DVAR, class TU>
 __global__ void __launch_bounds__(kThreads)
-k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
        const TU *__restrict__ u, const double *__restrict__ dside,
        double dconst, const unsigned char *__restrict__ cfmask, EwingWeights w,
        const int *ratio_to_coarser, double *__restrict__ flux,
        const int *__restrict__ run)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   if (run && !run[p.prob]) return;
-   const int a = ch.aux;
-   const int nx = p.hi[0] - p.lo[0] + 1 + (a == 0);
-   const int ny = p.hi[1] - p.lo[1] + 1 + (a == 1);
-   const double dai = 1. / p.dx[a];
-   const bool has_cf = (p.flags & 1) != 0;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int r = lin / nx;
-      const int j = p.lo[1] + r % ny;
-      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-      int cm[3] = {i, j, k};
-      cm[a] -= 1;
-      const long long cp = cidx<DIM>(p, p.off1, 1, i, j, k);
-      const long long cq = cidx<DIM>(p, p.off1, 1, cm[0], cm[1], cm[2]);
-      const long long si = sidx(p, a, i, j, k);
-      const double d = DVAR ? dside[si] : dconst;
-      double fl = dai * d * ((double)u[cp] - (double)u[cq]);
-      if (has_cf) {
-         const int fc[3] = {i, j, k};
-         int s = -1;
-         if (fc[a] == p.lo[a]) s = 0;
-         else if (fc[a] == p.hi[a] + 1) s = 1;
-         if (s >= 0) {
-            int cc[3] = {i, j, k};
-            if (s == 1) cc[a] -= 1;
-            const long long o = oidx(p, a, s, cc[0], cc[1], cc[2]);
-            if (cfmask[o]) {
-               int mq[3] = {cc[0], cc[1], cc[2]};
-               for (int tt = 0; tt < DIM; ++tt) {
-                  if (tt == a) continue;
-                  const int rr = ratio_to_coarser[tt];
-                  const int base = coarsen_index(cc[tt], rr) * rr;
-                  mq[tt] = base + (rr - (cc[tt] - base) - 1);
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      if (run && !run[p.prob]) continue;
+      const int a = ch.aux;
+      const int nx = p.hi[0] - p.lo[0] + 1 + (a == 0);
+      const int ny = p.hi[1] - p.lo[1] + 1 + (a == 1);
+      const double dai = 1. / p.dx[a];
+      const bool has_cf = (p.flags & 1) != 0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         int cm[3] = {i, j, k};
+         cm[a] -= 1;
+         const long long cp = cidx<DIM>(p, p.off1, 1, i, j, k);
+         const long long cq = cidx<DIM>(p, p.off1, 1, cm[0], cm[1], cm[2]);
+         const long long si = sidx(p, a, i, j, k);
+         const double d = DVAR ? dside[si] : dconst;
+         double fl = dai * d * ((double)u[cp] - (double)u[cq]);
+         if (has_cf) {
+            const int fc[3] = {i, j, k};
+            int s = -1;
+            if (fc[a] == p.lo[a]) s = 0;
+            else if (fc[a] == p.hi[a] + 1) s = 1;
+            if (s >= 0) {
+               int cc[3] = {i, j, k};
+               if (s == 1) cc[a] -= 1;
+               const long long o = oidx(p, a, s, cc[0], cc[1], cc[2]);
+               if (cfmask[o]) {
+                  int mq[3] = {cc[0], cc[1], cc[2]};
+                  for (int tt = 0; tt < DIM; ++tt) {
+                     if (tt == a) continue;
+                     const int rr = ratio_to_coarser[tt];
+                     const int base = coarsen_index(cc[tt], rr) * rr;
+                     mq[tt] = base + (rr - (cc[tt] - base) - 1);
+                  }
+                  const double uc = (double)u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
+                  const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
+                  if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
+                  else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
                }
-               const double uc = (double)u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
-               const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
-               if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
-               else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
             }
          }
+         flux[si] = fl;
       }
-      flux[si] = fl;
    }
 }
 
@@ -427,46 +445,47 @@ k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
 
 template <int DIM, int CKIND, class TU>
 __global__ void __launch_bounds__(kThreads)
-k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
            const TU *__restrict__ u, const double *__restrict__ f,
            const double *__restrict__ flux, const double *__restrict__ cfield,
            double cconst, double *__restrict__ res, double *__restrict__ oflux,
            const int *__restrict__ run)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   if (run && !run[p.prob]) return;
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
-   const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int r = lin / nx;
-      const int j = p.lo[1] + r % ny;
-      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-      const double fxl = flux[sidx(p, 0, i, j, k)], fxh = flux[sidx(p, 0, i + 1, j, k)];
-      const double fyl = flux[sidx(p, 1, i, j, k)], fyh = flux[sidx(p, 1, i, j + 1, k)];
-      const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
-      const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
-      const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
-      double rv;
-      if (DIM == 2) {
-         rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
-      } else {
-         const double fzl = flux[sidx(p, 2, i, j, k)], fzh = flux[sidx(p, 2, i, j, k + 1)];
-         rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - sf * uc;
-      }
-      res[c0] = rv;
-      if (oflux) {
-         if (i == p.lo[0]) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
-         if (i == p.hi[0]) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
-         if (j == p.lo[1]) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
-         if (j == p.hi[1]) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
-         if (DIM == 3) {
-            if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = flux[sidx(p, 2, i, j, k)];
-            if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = flux[sidx(p, 2, i, j, k + 1)];
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      if (run && !run[p.prob]) continue;
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
+      const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         const double fxl = flux[sidx(p, 0, i, j, k)], fxh = flux[sidx(p, 0, i + 1, j, k)];
+         const double fyl = flux[sidx(p, 1, i, j, k)], fyh = flux[sidx(p, 1, i, j + 1, k)];
+         const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
+         const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
+         const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
+         double rv;
+         if (DIM == 2) {
+            rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
+         } else {
+            const double fzl = flux[sidx(p, 2, i, j, k)], fzh = flux[sidx(p, 2, i, j, k + 1)];
+            rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - sf * uc;
+         }
+         res[c0] = rv;
+         if (oflux) {
+            if (i == p.lo[0]) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
+            if (i == p.hi[0]) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
+            if (j == p.lo[1]) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
+            if (j == p.hi[1]) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
+            if (DIM == 3) {
+               if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = flux[sidx(p, 2, i, j, k)];
+               if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = flux[sidx(p, 2, i, j, k + 1)];
+            }
          }
       }
    }
@@ -477,61 +496,62 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(kThreads)
-k_flux_coarsen(const FluxCoarsenItem *__restrict__ items, const Chunk *__restrict__ chunks,
+k_flux_coarsen(const FluxCoarsenItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
                const PatchDesc *__restrict__ fine, const PatchDesc *__restrict__ coarse,
                const double *__restrict__ oflux_fine, double *__restrict__ flux_coarse,
                const int *__restrict__ run)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const FluxCoarsenItem it = items[ch.patch];
-   if (run && !run[it.prob]) return;
-   const PatchDesc fp = fine[it.fine_patch];
-   const PatchDesc cp = coarse[it.coarse_patch];
-   const int a = it.axis;
-   const int nx = it.hi[0] - it.lo[0] + 1;
-   const int ny = it.hi[1] - it.lo[1] + 1;
-   // refinement ratios along the tangential axes come in the chunk's aux word
-   double wf, wc;
-   if (it.t1 < 0) {
-      wf = fp.dx[it.t0];
-      wc = cp.dx[it.t0];
-   } else {
-      wf = fp.dx[it.t0] * fp.dx[it.t1];
-      wc = cp.dx[it.t0] * cp.dx[it.t1];
-   }
-   const int r0 = ch.aux & 0xff;
-   const int r1 = (ch.aux >> 8) & 0xff;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      int c[3];
-      c[0] = it.lo[0] + lin % nx;
-      const int rr = lin / nx;
-      c[1] = it.lo[1] + rr % ny;
-      c[2] = it.lo[2] + rr / ny;
-      double acc = 0.0;
+   WORK_LOOP(ch) {
+      const FluxCoarsenItem it = items[ch.patch];
+      if (run && !run[it.prob]) continue;
+      const PatchDesc fp = fine[it.fine_patch];
+      const PatchDesc cp = coarse[it.coarse_patch];
+      const int a = it.axis;
+      const int nx = it.hi[0] - it.lo[0] + 1;
+      const int ny = it.hi[1] - it.lo[1] + 1;
+      // refinement ratios along the tangential axes come in the chunk's aux word
+      double wf, wc;
       if (it.t1 < 0) {
-         for (int ir = 0; ir < r0; ++ir) {
-            int fc[3] = {0, 0, 0};
-            fc[a] = it.fface;
-            fc[it.t0] = c[it.t0] * r0 + ir;
-            int cc[3] = {fc[0], fc[1], fc[2]};
-            if (it.side == 1) cc[a] -= 1;
-            acc = acc + oflux_fine[oidx(fp, a, it.side, cc[0], cc[1], cc[2])] * wf;
-         }
+         wf = fp.dx[it.t0];
+         wc = cp.dx[it.t0];
       } else {
-         for (int ro = 0; ro < r1; ++ro)
-            for (int ri = 0; ri < r0; ++ri) {
-               int fc[3];
+         wf = fp.dx[it.t0] * fp.dx[it.t1];
+         wc = cp.dx[it.t0] * cp.dx[it.t1];
+      }
+      const int r0 = ch.aux & 0xff;
+      const int r1 = (ch.aux >> 8) & 0xff;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         int c[3];
+         c[0] = it.lo[0] + lin % nx;
+         const int rr = lin / nx;
+         c[1] = it.lo[1] + rr % ny;
+         c[2] = it.lo[2] + rr / ny;
+         double acc = 0.0;
+         if (it.t1 < 0) {
+            for (int ir = 0; ir < r0; ++ir) {
+               int fc[3] = {0, 0, 0};
                fc[a] = it.fface;
-               fc[it.t0] = c[it.t0] * r0 + ri;
-               fc[it.t1] = c[it.t1] * r1 + ro;
+               fc[it.t0] = c[it.t0] * r0 + ir;
                int cc[3] = {fc[0], fc[1], fc[2]};
                if (it.side == 1) cc[a] -= 1;
                acc = acc + oflux_fine[oidx(fp, a, it.side, cc[0], cc[1], cc[2])] * wf;
             }
+         } else {
+            for (int ro = 0; ro < r1; ++ro)
+               for (int ri = 0; ri < r0; ++ri) {
+                  int fc[3];
+                  fc[a] = it.fface;
+                  fc[it.t0] = c[it.t0] * r0 + ri;
+                  fc[it.t1] = c[it.t1] * r1 + ro;
+                  int cc[3] = {fc[0], fc[1], fc[2]};
+                  if (it.side == 1) cc[a] -= 1;
+                  acc = acc + oflux_fine[oidx(fp, a, it.side, cc[0], cc[1], cc[2])] * wf;
+               }
+         }
+         acc = acc / wc;
+         flux_coarse[sidx(cp, a, c[0], c[1], c[2])] = acc;
       }
-      acc = acc / wc;
-      flux_coarse[sidx(cp, a, c[0], c[1], c[2])] = acc;
    }
 }
 
@@ -541,45 +561,46 @@ k_flux_coarsen(const FluxCoarsenItem *__restrict__ items, const Chunk *__restric
 
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
-k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chunks,
+k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
            const PatchDesc *__restrict__ fine, const PatchDesc *__restrict__ coarse,
            const double *__restrict__ src, int src_g, double *__restrict__ dst,
            int dst_g, const int *__restrict__ run)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const RestrictItem it = items[ch.patch];
-   if (run && !run[it.prob]) return;
-   const PatchDesc fp = fine[it.fine_patch];
-   const PatchDesc cp = coarse[it.coarse_patch];
-   const int nx = it.hi[0] - it.lo[0] + 1;
-   const int ny = it.hi[1] - it.lo[1] + 1;
-   const int r0 = ch.aux & 0xff, r1 = (ch.aux >> 8) & 0xff, r2 = (ch.aux >> 16) & 0xff;
-   double dVf, dVc;
-   if (DIM == 2) {
-      dVf = fp.dx[0] * fp.dx[1];
-      dVc = cp.dx[0] * cp.dx[1];
-   } else {
-      dVf = fp.dx[0] * fp.dx[1] * fp.dx[2];
-      dVc = cp.dx[0] * cp.dx[1] * cp.dx[2];
-   }
-   const long long soff = src_g ? fp.off1 : fp.off0;
-   const long long doff = dst_g ? cp.off1 : cp.off0;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = it.lo[0] + lin % nx;
-      const int rr = lin / nx;
-      const int j = it.lo[1] + rr % ny;
-      const int k = it.lo[2] + rr / ny;
-      double acc = 0.0;
-      const int nr2 = DIM == 3 ? r2 : 1;
-      for (int i2 = 0; i2 < nr2; ++i2)
-         for (int i1 = 0; i1 < r1; ++i1)
-            for (int i0 = 0; i0 < r0; ++i0) {
-               const int fk = DIM == 3 ? k * r2 + i2 : 0;
-               acc = acc + src[cidx<DIM>(fp, soff, src_g, i * r0 + i0, j * r1 + i1, fk)] * dVf;
-            }
-      acc = acc / dVc;
-      dst[cidx<DIM>(cp, doff, dst_g, i, j, k)] = acc;
+   WORK_LOOP(ch) {
+      const RestrictItem it = items[ch.patch];
+      if (run && !run[it.prob]) continue;
+      const PatchDesc fp = fine[it.fine_patch];
+      const PatchDesc cp = coarse[it.coarse_patch];
+      const int nx = it.hi[0] - it.lo[0] + 1;
+      const int ny = it.hi[1] - it.lo[1] + 1;
+      const int r0 = ch.aux & 0xff, r1 = (ch.aux >> 8) & 0xff, r2 = (ch.aux >> 16) & 0xff;
+      double dVf, dVc;
+      if (DIM == 2) {
+         dVf = fp.dx[0] * fp.dx[1];
+         dVc = cp.dx[0] * cp.dx[1];
+      } else {
+         dVf = fp.dx[0] * fp.dx[1] * fp.dx[2];
+         dVc = cp.dx[0] * cp.dx[1] * cp.dx[2];
+      }
+      const long long soff = src_g ? fp.off1 : fp.off0;
+      const long long doff = dst_g ? cp.off1 : cp.off0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = it.lo[0] + lin % nx;
+         const int rr = lin / nx;
+         const int j = it.lo[1] + rr % ny;
+         const int k = it.lo[2] + rr / ny;
+         double acc = 0.0;
+         const int nr2 = DIM == 3 ? r2 : 1;
+         for (int i2 = 0; i2 < nr2; ++i2)
+            for (int i1 = 0; i1 < r1; ++i1)
+               for (int i0 = 0; i0 < r0; ++i0) {
+                  const int fk = DIM == 3 ? k * r2 + i2 : 0;
+                  acc = acc + src[cidx<DIM>(fp, soff, src_g, i * r0 + i0, j * r1 + i1, fk)] * dVf;
+               }
+         acc = acc / dVc;
+         dst[cidx<DIM>(cp, doff, dst_g, i, j, k)] = acc;
+      }
    }
 }
 
@@ -590,63 +611,64 @@ k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chu
 
 template <int DIM, class T>
 __global__ void __launch_bounds__(kThreads)
-k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ chunks,
+k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
               const PatchDesc *__restrict__ fine, const T *__restrict__ tmp,
               const double *__restrict__ dxc_prob, int ratio0, int ratio1, int ratio2,
               T *__restrict__ e, const int *__restrict__ run)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const ProlongItem it = items[ch.patch];
-   if (run && !run[it.prob]) return;
-   const PatchDesc p = fine[it.fine_patch];
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   const T half = (T)0.5, one = (T)1;
-   const double *dxc = dxc_prob + 3 * it.prob;
-   const int r[3] = {ratio0, ratio1, ratio2};
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int rr = lin / nx;
-      const int j = p.lo[1] + rr % ny;
-      const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
-      const int fi[3] = {i, j, k};
-      int ic[3];
-      T x[3];
-      for (int a = 0; a < DIM; ++a) {
-         ic[a] = coarsen_index(fi[a], r[a]);
-         const int ir = fi[a] - ic[a] * r[a];
-         const T deltax = ((T)ir + half) * (T)p.dx[a] - (T)dxc[a] * half;
-         x[a] = deltax / (T)dxc[a];
-         if (x[a] < 0.0) {
-            ic[a] = ic[a] - 1;
-            x[a] = x[a] + one;
+   WORK_LOOP(ch) {
+      const ProlongItem it = items[ch.patch];
+      if (run && !run[it.prob]) continue;
+      const PatchDesc p = fine[it.fine_patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const T half = (T)0.5, one = (T)1;
+      const double *dxc = dxc_prob + 3 * it.prob;
+      const int r[3] = {ratio0, ratio1, ratio2};
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int rr = lin / nx;
+         const int j = p.lo[1] + rr % ny;
+         const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
+         const int fi[3] = {i, j, k};
+         int ic[3];
+         T x[3];
+         for (int a = 0; a < DIM; ++a) {
+            ic[a] = coarsen_index(fi[a], r[a]);
+            const int ir = fi[a] - ic[a] * r[a];
+            const T deltax = ((T)ir + half) * (T)p.dx[a] - (T)dxc[a] * half;
+            x[a] = deltax / (T)dxc[a];
+            if (x[a] < 0.0) {
+               ic[a] = ic[a] - 1;
+               x[a] = x[a] + one;
+            }
          }
+         T v;
+         const ArrDesc &A = it.tmp;
+         if (DIM == 2) {
+            const T c00 = tmp[aidx(A, ic[0], ic[1], 0)];
+            const T c10 = tmp[aidx(A, ic[0] + 1, ic[1], 0)];
+            const T c01 = tmp[aidx(A, ic[0], ic[1] + 1, 0)];
+            const T c11 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, 0)];
+            v = (c00 + (c10 - c00) * x[0]) * (one - x[1]) + (c01 + (c11 - c01) * x[0]) * x[1];
+         } else {
+            const T c000 = tmp[aidx(A, ic[0], ic[1], ic[2])];
+            const T c100 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2])];
+            const T c010 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2])];
+            const T c110 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2])];
+            const T c001 = tmp[aidx(A, ic[0], ic[1], ic[2] + 1)];
+            const T c101 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2] + 1)];
+            const T c011 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2] + 1)];
+            const T c111 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2] + 1)];
+            const T y = x[1], z = x[2], xx = x[0];
+            v = ((c000 + (c100 - c000) * xx) * (one - y) + (c010 + (c110 - c010) * xx) * y) *
+                   (one - z) +
+                ((c001 + (c101 - c001) * xx) * (one - y) + (c011 + (c111 - c011) * xx) * y) * z;
+         }
+         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+         e[c] = e[c] + v;
       }
-      T v;
-      const ArrDesc &A = it.tmp;
-      if (DIM == 2) {
-         const T c00 = tmp[aidx(A, ic[0], ic[1], 0)];
-         const T c10 = tmp[aidx(A, ic[0] + 1, ic[1], 0)];
-         const T c01 = tmp[aidx(A, ic[0], ic[1] + 1, 0)];
-         const T c11 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, 0)];
-         v = (c00 + (c10 - c00) * x[0]) * (one - x[1]) + (c01 + (c11 - c01) * x[0]) * x[1];
-      } else {
-         const T c000 = tmp[aidx(A, ic[0], ic[1], ic[2])];
-         const T c100 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2])];
-         const T c010 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2])];
-         const T c110 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2])];
-         const T c001 = tmp[aidx(A, ic[0], ic[1], ic[2] + 1)];
-         const T c101 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2] + 1)];
-         const T c011 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2] + 1)];
-         const T c111 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2] + 1)];
-         const T y = x[1], z = x[2], xx = x[0];
-         v = ((c000 + (c100 - c000) * xx) * (one - y) + (c010 + (c110 - c010) * xx) * y) *
-                (one - z) +
-             ((c001 + (c101 - c001) * xx) * (one - y) + (c011 + (c111 - c011) * xx) * y) * z;
-      }
-      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
-      e[c] = e[c] + v;
    }
 }
 
@@ -656,62 +678,65 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
 
 template <int DIM, class T>
 __global__ void __launch_bounds__(kThreads)
-k_add_interior(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_add_interior(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
                double *__restrict__ u, const T *__restrict__ e,
                const int *__restrict__ run)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   if (run && !run[p.prob]) return;
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int r = lin / nx;
-      const int j = p.lo[1] + r % ny;
-      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
-      u[c] = u[c] + (double)e[c];
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      if (run && !run[p.prob]) continue;
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+         u[c] = u[c] + (double)e[c];
+      }
    }
 }
 
 // Weighted sums sum(w x^2), sum(w) per chunk.
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
-k_norm_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_norm_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
                const double *__restrict__ x, int xg, const double *__restrict__ w,
                double2 *__restrict__ partial)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   const long long xoff = xg ? p.off1 : p.off0;
-   double sd = 0.0, sv = 0.0;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int r = lin / nx;
-      const int j = p.lo[1] + r % ny;
-      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-      const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
-      const double wv = w[cidx<DIM>(p, p.off0, 0, i, j, k)];
-      sd += xv * xv * wv;
-      sv += wv;
-   }
-   __shared__ double rs[kThreads], rv[kThreads];
-   rs[threadIdx.x] = sd;
-   rv[threadIdx.x] = sv;
-   __syncthreads();
-   for (int o = kThreads / 2; o > 0; o >>= 1) {
-      if ((int)threadIdx.x < o) {
-         rs[threadIdx.x] += rs[threadIdx.x + o];
-         rv[threadIdx.x] += rv[threadIdx.x + o];
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const long long xoff = xg ? p.off1 : p.off0;
+      double sd = 0.0, sv = 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
+         const double wv = w[cidx<DIM>(p, p.off0, 0, i, j, k)];
+         sd += xv * xv * wv;
+         sv += wv;
       }
+      __shared__ double rs[kThreads], rv[kThreads];
+      rs[threadIdx.x] = sd;
+      rv[threadIdx.x] = sv;
       __syncthreads();
+      for (int o = kThreads / 2; o > 0; o >>= 1) {
+         if ((int)threadIdx.x < o) {
+            rs[threadIdx.x] += rs[threadIdx.x + o];
+            rv[threadIdx.x] += rv[threadIdx.x + o];
+         }
+         __syncthreads();
+      }
+      if (threadIdx.x == 0) partial[ch.aux] = make_double2(rs[0], rv[0]);
+      __syncthreads();  // shared memory is reused by the next chunk
    }
-   if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(rs[0], rv[0]);
 }
 
 // Per problem: sum the partials of its chunks (in chunk order) and add them
@@ -801,20 +826,21 @@ __global__ void k_scatter(const long long *__restrict__ idx, long long n,
 // interior of a ghost-0 field copied into the interior of a ghost-1 field
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
-k_g0_to_g1(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_g0_to_g1(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
            const double *__restrict__ src, double *__restrict__ dst)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int r = lin / nx;
-      const int j = p.lo[1] + r % ny;
-      const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-      dst[cidx<DIM>(p, p.off1, 1, i, j, k)] = src[cidx<DIM>(p, p.off0, 0, i, j, k)];
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         dst[cidx<DIM>(p, p.off1, 1, i, j, k)] = src[cidx<DIM>(p, p.off0, 0, i, j, k)];
+      }
    }
 }
 
@@ -872,57 +898,60 @@ __global__ void k_gather_samples(const PatchDesc *__restrict__ patches,
 // interior cells of patch p of a ghost-1 field = y[p] * scale[p] * dx^2
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
-k_scatter_samples(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_scatter_samples(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
                   const float *__restrict__ y, const double *__restrict__ scale, int S,
                   double *__restrict__ dst)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   const long long S3 = (long long)S * S * S;
-   const double f = scale[ch.patch] * p.dx[0] * p.dx[0];
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int a = lin % nx;
-      const int r = lin / nx;
-      const int b = r % ny;
-      const int cz = DIM == 3 ? r / ny : 0;
-      const int sz = DIM == 3 ? cz + 1 : S / 2;
-      const long long sidx = (long long)ch.patch * S3 + (a + 1) + (long long)S * ((b + 1) + (long long)S * sz);
-      dst[cidx<DIM>(p, p.off1, 1, p.lo[0] + a, p.lo[1] + b, DIM == 3 ? p.lo[2] + cz : 0)] =
-         (double)y[sidx] * f;
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const long long S3 = (long long)S * S * S;
+      const double f = scale[ch.patch] * p.dx[0] * p.dx[0];
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int a = lin % nx;
+         const int r = lin / nx;
+         const int b = r % ny;
+         const int cz = DIM == 3 ? r / ny : 0;
+         const int sz = DIM == 3 ? cz + 1 : S / 2;
+         const long long sidx = (long long)ch.patch * S3 + (a + 1) + (long long)S * ((b + 1) + (long long)S * sz);
+         dst[cidx<DIM>(p, p.off1, 1, p.lo[0] + a, p.lo[1] + b, DIM == 3 ? p.lo[2] + cz : 0)] =
+            (double)y[sidx] * f;
+      }
    }
 }
 
 // per chunk: sum w r d and sum w d d with d = r - r2 (ghost-0 fields)
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
-k_dot_pair(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_dot_pair(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
            const double *__restrict__ r, const double *__restrict__ r2,
            const double *__restrict__ w, double2 *__restrict__ partial)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   double a = 0.0, b = 0.0;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const long long c = p.off0 + ch.begin + t;
-      const double d = r[c] - r2[c];
-      a += w[c] * r[c] * d;
-      b += w[c] * d * d;
-   }
-   __shared__ double ra[kThreads], rb[kThreads];
-   ra[threadIdx.x] = a;
-   rb[threadIdx.x] = b;
-   __syncthreads();
-   for (int o = kThreads / 2; o > 0; o >>= 1) {
-      if ((int)threadIdx.x < o) {
-         ra[threadIdx.x] += ra[threadIdx.x + o];
-         rb[threadIdx.x] += rb[threadIdx.x + o];
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      double a = 0.0, b = 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const long long c = p.off0 + ch.begin + t;
+         const double d = r[c] - r2[c];
+         a += w[c] * r[c] * d;
+         b += w[c] * d * d;
       }
+      __shared__ double ra[kThreads], rb[kThreads];
+      ra[threadIdx.x] = a;
+      rb[threadIdx.x] = b;
       __syncthreads();
+      for (int o = kThreads / 2; o > 0; o >>= 1) {
+         if ((int)threadIdx.x < o) {
+            ra[threadIdx.x] += ra[threadIdx.x + o];
+            rb[threadIdx.x] += rb[threadIdx.x + o];
+         }
+         __syncthreads();
+      }
+      if (threadIdx.x == 0) partial[ch.aux] = make_double2(ra[0], rb[0]);
+      __syncthreads();  // shared memory is reused by the next chunk
    }
-   if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(ra[0], rb[0]);
 }
 
 // minimal-residual step length per problem: alpha = <r, d> / <d, d>, kept
@@ -939,27 +968,55 @@ __global__ void k_alpha(const double2 *__restrict__ acc, const int *__restrict__
 // u += alpha e (interior) and r = r - alpha (r - r2)
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
-k_apply_alpha(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+k_apply_alpha(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
               const double *__restrict__ alpha, double *__restrict__ u,
               const double *__restrict__ e, double *__restrict__ r,
               const double *__restrict__ r2)
 {
-   const Chunk ch = chunks[blockIdx.x];
-   const PatchDesc p = patches[ch.patch];
-   const double al = alpha[p.prob];
-   if (al == 0.0) return;
-   const int nx = p.hi[0] - p.lo[0] + 1;
-   const int ny = p.hi[1] - p.lo[1] + 1;
-   for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-      const int lin = ch.begin + t;
-      const int i = p.lo[0] + lin % nx;
-      const int rr = lin / nx;
-      const int j = p.lo[1] + rr % ny;
-      const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
-      const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
-      const long long c0 = p.off0 + lin;
-      u[c1] = u[c1] + al * e[c1];
-      r[c0] = r[c0] - al * (r[c0] - r2[c0]);
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      const double al = alpha[p.prob];
+      if (al == 0.0) continue;
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int rr = lin / nx;
+         const int j = p.lo[1] + rr % ny;
+         const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
+         const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
+         const long long c0 = p.off0 + lin;
+         u[c1] = u[c1] + al * e[c1];
+         r[c0] = r[c0] - al * (r[c0] - r2[c0]);
+      }
+   }
+}
+
+// Block (list, problem): copy the problem's chunks of one work list to their
+// place in the compacted list when the problem is active; the block of the
+// last problem also writes the end markers.
+__global__ void __launch_bounds__(kThreads)
+k_compact(const WorkReg *__restrict__ regs, const int *__restrict__ active, int nprob)
+{
+   const WorkReg r = regs[blockIdx.x];
+   const int p = blockIdx.y;
+   int before = 0;
+   for (int q = threadIdx.x; q < p; q += blockDim.x)
+      if (active[q]) before += r.pcb[q + 1] - r.pcb[q];
+   __shared__ int part[kThreads / 32];
+   for (int o = 16; o > 0; o >>= 1) before += __shfl_down_sync(0xffffffffu, before, o);
+   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = before;
+   __syncthreads();
+   int pos = 0;
+   for (int w = 0; w < kThreads / 32; ++w) pos += part[w];
+   const int b = r.pcb[p], n = r.pcb[p + 1] - b;
+   const bool on = active[p] != 0;
+   if (on)
+      for (int t = threadIdx.x; t < n; t += blockDim.x) r.list[pos + t] = r.all[b + t];
+   if (p == nprob - 1) {
+      const int total = pos + (on ? n : 0);
+      for (int t = total + threadIdx.x; t < r.n; t += blockDim.x) r.list[t] = Chunk{-1, 0, 0, 0};
    }
 }
 
@@ -968,6 +1025,15 @@ std::atomic<long long> g_launches{0};
 }  // namespace
 
 long long kernel_launch_count() { return g_launches.load(); }
+
+void add_kernel_launches(long long n) { g_launches += n; }
+
+void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *active, int nprob)
+{
+   if (nregs <= 0 || nprob <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_compact<<<dim3(nregs, nprob), kThreads, 0, s>>>(regs, active, nprob);
+}
 
 // ---------------------------------------------------------------------------
 // launchers
@@ -980,7 +1046,7 @@ void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_fill<T><<<nchunks, kThreads, 0, s>>>(items, chunks, dst, src_same, src_coarse,
+   k_fill<T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, dst, src_same, src_coarse,
                                           homogeneous, bc, active);
 }
 
@@ -1009,12 +1075,12 @@ static void rbgs_inst(cudaStream_t s, int nchunks, const PatchDesc *patches,
                       const long long *facemap, const BcCoefs &bc)
 {
    if (facemap)
-      k_rbgs<DIM, DVAR, CK, T, true><<<nchunks, kThreads, 0, s>>>(
-         patches, chunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
+      k_rbgs<DIM, DVAR, CK, T, true><<<work_grid(nchunks), kThreads, 0, s>>>(
+         patches, chunks, nchunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
          maxres, run, facemap, bc);
    else
-      k_rbgs<DIM, DVAR, CK, T, false><<<nchunks, kThreads, 0, s>>>(
-         patches, chunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
+      k_rbgs<DIM, DVAR, CK, T, false><<<work_grid(nchunks), kThreads, 0, s>>>(
+         patches, chunks, nchunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
          maxres, run, facemap, bc);
 }
 
@@ -1069,20 +1135,20 @@ void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
    }
    if (dim == 2) {
       if (spec.d_variable)
-         k_flux<2, true, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+         k_flux<2, true, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                           spec.d_const, cfmask, w, ratio_dev,
                                                           flux, run);
       else
-         k_flux<2, false, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+         k_flux<2, false, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                            spec.d_const, cfmask, w,
                                                            ratio_dev, flux, run);
    } else {
       if (spec.d_variable)
-         k_flux<3, true, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+         k_flux<3, true, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                           spec.d_const, cfmask, w, ratio_dev,
                                                           flux, run);
       else
-         k_flux<3, false, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, dside,
+         k_flux<3, false, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                            spec.d_const, cfmask, w,
                                                            ratio_dev, flux, run);
    }
@@ -1097,7 +1163,7 @@ void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchun
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
 #define RS(D, C)                                                                         \
-   k_residual<D, C, TU><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, f, flux, cfield, \
+   k_residual<D, C, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, f, flux, cfield, \
                                                      spec.c_const, res, oflux, run)
    if (dim == 2) {
       if (spec.c_kind == 2) RS(2, 2);
@@ -1117,7 +1183,7 @@ void launch_flux_coarsen(cudaStream_t s, const FluxCoarsenItem *items, const Chu
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_flux_coarsen<<<nchunks, kThreads, 0, s>>>(items, chunks, fine, coarse, oflux_fine,
+   k_flux_coarsen<<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, coarse, oflux_fine,
                                                flux_coarse, run);
 }
 
@@ -1128,10 +1194,10 @@ void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const C
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_restrict<2><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, coarse, src, src_g, dst,
+      k_restrict<2><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, coarse, src, src_g, dst,
                                                  dst_g, run);
    else
-      k_restrict<3><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, coarse, src, src_g, dst,
+      k_restrict<3><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, coarse, src, src_g, dst,
                                                  dst_g, run);
 }
 
@@ -1143,10 +1209,10 @@ void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_prolong_add<2, T><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
+      k_prolong_add<2, T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, tmp, dxc_prob,
                                                        ratio[0], ratio[1], ratio[2], e, run);
    else
-      k_prolong_add<3, T><<<nchunks, kThreads, 0, s>>>(items, chunks, fine, tmp, dxc_prob,
+      k_prolong_add<3, T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, tmp, dxc_prob,
                                                        ratio[0], ratio[1], ratio[2], e, run);
 }
 
@@ -1157,9 +1223,9 @@ void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_add_interior<2, T><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+      k_add_interior<2, T><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, e, run);
    else
-      k_add_interior<3, T><<<nchunks, kThreads, 0, s>>>(patches, chunks, u, e, run);
+      k_add_interior<3, T><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, e, run);
 }
 
 template <class S, class D>
@@ -1177,9 +1243,9 @@ void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
    if (nchunks <= 0) return;
    g_launches.fetch_add(2, std::memory_order_relaxed);
    if (dim == 2)
-      k_norm_partial<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, x, xg, w, partial);
+      k_norm_partial<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
    else
-      k_norm_partial<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, x, xg, w, partial);
+      k_norm_partial<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
    k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
 }
 
@@ -1204,8 +1270,8 @@ void launch_g0_to_g1(cudaStream_t s, int dim, int nchunks, const PatchDesc *patc
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   if (dim == 2) k_g0_to_g1<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, src, dst);
-   else k_g0_to_g1<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, src, dst);
+   if (dim == 2) k_g0_to_g1<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+   else k_g0_to_g1<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
 }
 
 void launch_patch_rms(cudaStream_t s, int dim, int npatch, const PatchDesc *patches,
@@ -1235,9 +1301,9 @@ void launch_scatter_samples(cudaStream_t s, int dim, int nchunks, const PatchDes
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_scatter_samples<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, y, scale, S, dst);
+      k_scatter_samples<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, y, scale, S, dst);
    else
-      k_scatter_samples<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, y, scale, S, dst);
+      k_scatter_samples<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, y, scale, S, dst);
 }
 
 void launch_dot_pair(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
@@ -1247,9 +1313,9 @@ void launch_dot_pair(cudaStream_t s, int dim, int nchunks, const PatchDesc *patc
    if (nchunks <= 0) return;
    g_launches.fetch_add(2, std::memory_order_relaxed);
    if (dim == 2)
-      k_dot_pair<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, r, r2, w, partial);
+      k_dot_pair<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, r, r2, w, partial);
    else
-      k_dot_pair<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, r, r2, w, partial);
+      k_dot_pair<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, r, r2, w, partial);
    k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
 }
 
@@ -1267,9 +1333,9 @@ void launch_apply_alpha(cudaStream_t s, int dim, int nchunks, const PatchDesc *p
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_apply_alpha<2><<<nchunks, kThreads, 0, s>>>(patches, chunks, alpha, u, e, r, r2);
+      k_apply_alpha<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, alpha, u, e, r, r2);
    else
-      k_apply_alpha<3><<<nchunks, kThreads, 0, s>>>(patches, chunks, alpha, u, e, r, r2);
+      k_apply_alpha<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, alpha, u, e, r, r2);
 }
 
 void launch_gather(cudaStream_t s, const long long *idx, long long n, const double *src,

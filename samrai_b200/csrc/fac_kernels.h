@@ -9,6 +9,12 @@ namespace samrai_b200 {
 
 // Kernels launched by this process so far (all contexts).
 long long kernel_launch_count();
+// Adjust the count: kernels of other files, kernels captured into a CUDA
+// graph (removed at capture, added per replay).
+void add_kernel_launches(long long n);
+
+// Rebuild every registered work list for the current active flags.
+void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *active, int nprob);
 
 template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,

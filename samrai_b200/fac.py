@@ -338,6 +338,15 @@ class FacContext:
     def zero(self, fid):
         _check(load_library().fac_zero_field(self.h, fid))
 
+    def set_params(self, **changes):
+        """Change solver parameters (same keys as the constructor's params)."""
+        self.params.update(changes)
+        prm = self.params
+        _check(load_library().fac_set_params(
+            self.h, prm["max_cycles"], prm["residual_tol"], prm["relative_residual_tol"],
+            prm["pre_sweeps"], prm["post_sweeps"], prm["coarse_tol"], prm["coarse_max_it"],
+            prm["ewing"]))
+
     def profile(self, on=True):
         _check(load_library().fac_profile_enable(self.h, int(on)))
 

@@ -226,3 +226,46 @@ def test_graph_replay_matches_eager(precision, require_gpu):
     assert np.array_equal(out[0][0], out[1][0])
     for a, b in zip(out[0][1], out[1][1]):
         assert np.array_equal(a, b)
+
+
+def _fused_levels_2d(probs):
+    """Levels whose patches all start on the same parity of lo0+lo1 (the
+    condition under which the fused colour pass runs in 2-D)."""
+    out = []
+    for ln in range(probs[0].nlev):
+        par = {int(b[0] + b[1]) % 2 for p in probs for b in p.levels[ln].boxes}
+        if len(par) == 1:
+            out.append(ln)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["config1", "small_3d_mg", "config2"])
+def test_fused_colour_pass_matches_filled(case, precision, require_gpu):
+    """Colour passes that read across patch faces directly must give the same
+    bits as passes that read ghost cells filled before each pass, including
+    the ghost values left after the solve."""
+    if case == "config1":
+        probs = [configs.config1()]
+        assert len(_fused_levels_2d(probs)) >= 1
+    elif case == "config2":
+        probs = [configs.config2()]
+        assert _fused_levels_2d(probs) == list(range(probs[0].nlev))
+    else:
+        probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (41, 42)]
+    prm = dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=2 if case == "config2" else 6)
+    out = []
+    for fused in (True, False):
+        g = fac.FacContext(probs, params=prm, precision=precision)
+        g.set_fused(fused)
+        conv, its, res = g.solve()
+        fields = [g.download(U, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
+        g.smooth(E, R, probs[0].nlev - 1, 3)
+        fields += [g.download(E, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
+        out.append((its.copy(), res.copy(), fields))
+        g.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    for a, b in zip(out[0][2], out[1][2]):
+        assert np.array_equal(a, b)
