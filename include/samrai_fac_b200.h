@@ -111,6 +111,29 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol,
  * patches (always in 3-D). */
 int fac_set_fused(fac_ctx *ctx, int on);
 
+/* 1 (default): on levels where the fused pass is used, sweeps with a fixed
+ * count (every sweep except the coarsest-level solve to a tolerance) run on
+ * shared-memory staged units: TMA bulk copies bring a run of slices of one
+ * patch into shared memory, the colour pass runs there and a bulk store
+ * writes the slices back.  Results are bit-identical to 0. */
+int fac_set_staged(fac_ctx *ctx, int on);
+
+/* 1: the composite residual forms the face fluxes while it sums
+ * them (computeFluxOnPatch and the residual loop of
+ * CellPoissonFACOps.C:1792-1956 in one kernel), taking the coarsened finer
+ * fluxes where the flux coarsening stored them.  Bit-identical to 0.
+ * fac_comp_residual itself always stores the face fluxes (fac_download_flux);
+ * the setting applies to the residuals inside fac_solve / fac_fac_cycle.
+ * Default 0: on B200 the two bandwidth-bound kernels beat the one
+ * index-heavy kernel. */
+int fac_set_fused_residual(fac_ctx *ctx, int on);
+
+/* Shared-memory bytes of one stage (one work unit) of the staged pass,
+ * 4096 .. 77,482 (default 24,576): patches are cut into units of as many
+ * slices as fit.  Rebuilds the unit tables when the context is
+ * initialised.  fac_autotune picks it by timing. */
+int fac_set_stage_budget(fac_ctx *ctx, int bytes);
+
 /* 1 (default): fac_solve captures one FAC cycle (V-cycle, correction,
  * restriction, composite residual, norm kernels) into a CUDA graph on first
  * use and replays it every cycle; converged problems are skipped on the

@@ -1,0 +1,84 @@
+// Device-side helpers shared by the FAC kernel files: index maps of the
+// level buffers, the work-list loop and the Robin boundary formula.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fac_internal.h"
+
+namespace samrai_b200 {
+namespace dev {
+
+constexpr int kThreads = 256;
+// Blocks of a chunk kernel: enough to fill the GPU; each block walks the
+// work list with a grid stride.
+constexpr int kGridCap = 148 * 8;
+
+inline int work_grid(int nchunks) { return nchunks < kGridCap ? nchunks : kGridCap; }
+
+// Grid-stride walk over a work list of nwork entries.  The list is compacted
+// on the device whenever the set of iterating problems changes: the chunks of
+// those problems come first and a chunk with patch < 0 ends the list.
+#define WORK_LOOP(ch)                                      \
+   for (int w_ = blockIdx.x; w_ < nwork; w_ += gridDim.x) \
+      if (const Chunk ch = chunks[w_]; ch.patch < 0)       \
+         break;                                            \
+      else
+
+__device__ __forceinline__ long long aidx(const ArrDesc &A, int i, int j, int k)
+{
+   return A.base + (long long)(i - A.lo[0]) +
+          (long long)A.n[0] * ((long long)(j - A.lo[1]) +
+                               (long long)A.n[1] * (long long)(k - A.lo[2]));
+}
+
+// Index of cell (i,j,k) in a patch's array with ghost width g.
+template <int DIM>
+__device__ __forceinline__ long long cidx(const PatchDesc &p, long long off,
+                                          int g, int i, int j, int k)
+{
+   const int gz = DIM == 3 ? g : 0;
+   const long long nx = p.hi[0] - p.lo[0] + 1 + 2 * g;
+   const long long ny = p.hi[1] - p.lo[1] + 1 + 2 * g;
+   return off + (i - p.lo[0] + g) + nx * ((j - p.lo[1] + g) + ny * (k - p.lo[2] + gz));
+}
+
+// Index of face (i,j,k) of axis a in a patch's side array (ghost 0).
+__device__ __forceinline__ long long sidx(const PatchDesc &p, int a, int i, int j,
+                                          int k)
+{
+   const long long nx = p.hi[0] - p.lo[0] + 1 + (a == 0);
+   const long long ny = p.hi[1] - p.lo[1] + 1 + (a == 1);
+   return p.offs[a] + (i - p.lo[0]) + nx * ((j - p.lo[1]) + ny * (k - p.lo[2]));
+}
+
+// Index of the tangential position of cell (i,j,k) in a face array of axis a.
+__device__ __forceinline__ long long oidx(const PatchDesc &p, int a, int s, int i,
+                                          int j, int k)
+{
+   const long long nx = p.hi[0] - p.lo[0] + 1;
+   const long long ny = p.hi[1] - p.lo[1] + 1;
+   long long t;
+   if (a == 0) t = (j - p.lo[1]) + ny * (k - p.lo[2]);
+   else if (a == 1) t = (i - p.lo[0]) + nx * (k - p.lo[2]);
+   else t = (i - p.lo[0]) + nx * (j - p.lo[1]);
+   return p.offo[a][s] + t;
+}
+
+__device__ __forceinline__ int coarsen_index(int i, int r)
+{
+   return i < 0 ? (i + 1) / r - 1 : i / r;
+}
+
+// settype1cells{2,3}d (robinbchelper2d.f:10-72): ghost value from the
+// interior value next to the boundary.
+template <class T>
+__device__ __forceinline__ T robin(T uin, int loc, T h, int hom, const BcCoefs &bc)
+{
+   const T a = (T)bc.a[loc], b = (T)bc.b[loc], half = (T)0.5;
+   if (hom) return (uin * (b - half * h * a)) / (b + half * h * a);
+   return (h * (T)bc.g[loc] + uin * (b - half * h * a)) / (b + half * h * a);
+}
+
+}  // namespace dev
+}  // namespace samrai_b200

@@ -160,7 +160,8 @@ struct DevArray {
       n = count;
       if (g_dry) return;
       if (count) {
-         cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+         // 64 spare bytes: bulk copies round their ends out to 16 bytes
+         cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T) + 64);
          if (e != cudaSuccess) {
             p = nullptr;
             throw FacError(FAC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
@@ -264,7 +265,18 @@ struct LevelState {
    // per face cell: index (ghost-1 buffer) of the same-level cell across the
    // face, -1 physical boundary, -2 coarse-fine face (fused colour pass)
    DevArray<long long> facemap;
+   DevArray<int> pushmap;
+   // side-array faces that carry a coarsened finer-level flux
+   DevArray<unsigned char> fcmask;
    bool fused_ok = false;
+   // staged colour pass: units (runs of slices of one patch) for FP64 [0]
+   // and FP32 [1] data, and the largest shared memory of a unit
+   std::vector<Chunk> units[2];  // {patch, first copy, copies, header}
+   DevArray<Chunk> d_units[2];
+   DevArray<UnitCopy> d_copies[2];
+   DevArray<unsigned char> d_hdrs[2];
+   WorkSrc ws_units[2];
+   int unit_smem[2] = {0, 0};
    DevArray<int> d_ratio;
 
    // work chunks
@@ -316,6 +328,10 @@ struct fac_ctx {
    int mixed = 0;            // 1: FP32 smoothing and error transfer
    int use_graph = 1;        // capture one FAC cycle into a CUDA graph and replay it
    int fused = 1;            // colour passes read across patch faces directly
+   int staged = 1;           // fused passes on shared-memory staged units
+   int fused_residual = 0;   // residual kernels form the fluxes on the fly
+   int stage_budget = 24 * 1024;  // shared memory of one stage (unit) of the staged pass
+   DevArray<int> kerr;       // set by kernels whose bounded waits ran out
    bool capturing = false;   // inside stream capture: no host synchronisation
    cudaGraphExec_t cycle_exec = nullptr;
    // learned correction after every cycle (fac_set_learned)
@@ -823,6 +839,161 @@ void build_cf_faces(fac_ctx *c, int ln)
    L.d_cf.upload(L.cf, c->stream);
 }
 
+// Units of the staged colour pass: each patch is cut along its slowest axis
+// into runs of slices whose shared-memory plan fits the budget (one slice at
+// least; a level whose single slice does not fit is not staged).  For every
+// unit the host writes its header and its list of bulk copies (byte ranges
+// of the level arrays, rounded out to 16 bytes, and where they land in the
+// stage), so the producer warp only streams them.
+void build_stage_units(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   const bool dvar = c->spec.d_variable != 0, cvar = c->spec.c_kind == 2;
+   struct HdrRec {
+      UnitHdr h;
+      char pad[kStageHeader - sizeof(UnitHdr)];
+   };
+   static_assert(sizeof(HdrRec) == kStageHeader, "header record size");
+   for (int t = 0; t < 2; ++t) {
+      const int ts = t == 0 ? 8 : 4;
+      std::vector<Chunk> &U = L.units[t];
+      std::vector<UnitCopy> copies;
+      std::vector<HdrRec> hdrs;
+      U.clear();
+      int maxb = 0;
+      bool decode_ok = true;
+      for (int ip = 0; ip < L.npatch; ++ip) {
+         const Box &b = L.box[ip];
+         const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+         const int nslow = dim == 3 ? b.hi[2] - b.lo[2] + 1 : ny;
+         const PatchDesc &d = L.hp[ip];
+         const bool cf = (d.flags & 1) != 0;
+         // plan of a unit of ns slices; sizing takes both slow-axis faces
+         auto bytes = [&](int ns) {
+            return stage_plan(dim, nx, ny, ns, ts, dvar, cvar, true, true, cf).bytes;
+         };
+         // the slot decode wants fewer than 2^14 active cells per unit
+         const long long row_slots = (long long)((nx + 1) / 2) * (dim == 3 ? ny : 1);
+         int nsmax = 1;
+         while (nsmax < nslow && bytes(nsmax + 1) <= c->stage_budget &&
+                row_slots * (nsmax + 1) < (1 << 14))
+            ++nsmax;
+         const int nunit = (nslow + nsmax - 1) / nsmax;
+         const int base = nslow / nunit, rem = nslow % nunit;
+         int s0 = 0;
+         const long long g1 = dim == 3 ? (long long)(nx + 2) * (ny + 2) : nx + 2;
+         const long long g0 = dim == 3 ? (long long)nx * ny : nx;
+         for (int u = 0; u < nunit; ++u) {
+            const int ns = base + (u < rem ? 1 : 0);
+            const bool slo = s0 == 0, shi = s0 + ns == nslow;
+            const StagePlan sp = stage_plan(dim, nx, ny, ns, ts, dvar, cvar, slo, shi, cf);
+            maxb = std::max(maxb, sp.bytes);
+            HdrRec rec;
+            std::memset(&rec, 0, sizeof(rec));
+            UnitHdr &h = rec.h;
+            for (int a = 0; a < 3; ++a) {
+               h.lo[a] = d.lo[a];
+               h.hi[a] = d.hi[a];
+               h.dx[a] = d.dx[a];
+               // the reciprocals the kernels would form: IEEE divisions in
+               // the working precision
+               h.dxi_d[a] = 1.0 / d.dx[a];
+               h.dxi_f[a] = 1.0f / (float)d.dx[a];
+            }
+            h.flags = d.flags;
+            h.off1 = d.off1;
+            h.s0 = s0;
+            h.ns = ns;
+            h.hx = (nx + 1) / 2;
+            h.mhx = (unsigned)(((1ull << 32) + h.hx - 1) / h.hx);
+            h.mny = (unsigned)(((1ull << 32) + ny - 1) / ny);
+            if (h.nslots >= (1 << 14) || nx > 2048 || ny > 1024) decode_ok = false;
+            h.nslots = h.hx * (dim == 3 ? ny * ns : ns);
+            h.fmask = 0;
+            for (int k = 0; k < 6; ++k) h.off_push[k] = h.off_cff[k] = -1;
+            const int first = (int)copies.size();
+            copies.push_back({(long long)hdrs.size() * kStageHeader, kSrcHdr, kStageHeader, 0, 0});
+            long long total = kStageHeader;
+            for (int r = 0; r < sp.nreg; ++r) {
+               int src;
+               long long e0;  // first element
+               long long limit;  // end of the source array (elements)
+               if (r == 0) {
+                  src = kSrcU;
+                  e0 = d.off1 + (long long)s0 * g1;
+                  limit = std::min<long long>(L.n1, d.off1 + cell_count(dim, b, 1));
+               } else if (r == 1) {
+                  src = kSrcF;
+                  e0 = d.off0 + (long long)s0 * g0;
+                  limit = std::min<long long>(L.n0, d.off0 + b.size());
+               } else if (r < sp.nbase) {
+                  const int a = r - 2;
+                  if (dvar && a < dim) {
+                     const long long per =
+                        dim == 3 ? (a == 0 ? (long long)(nx + 1) * ny
+                                           : (a == 1 ? (long long)nx * (ny + 1) : g0))
+                                 : (a == 0 ? nx + 1 : nx);
+                     src = kSrcD;
+                     e0 = d.offs[a] + (long long)s0 * per;
+                     limit = std::min<long long>(L.ns, d.offs[a] + side_box(b, a).size());
+                  } else {
+                     src = kSrcC;
+                     e0 = d.off0 + (long long)s0 * g0;
+                     limit = std::min<long long>(L.n0, d.off0 + b.size());
+                  }
+               } else {
+                  const bool flux = r >= sp.cff0;
+                  const int fid = sp.face[flux ? r - sp.cff0 : r - sp.face0];
+                  const int a = fid >> 1, sd = fid & 1;
+                  long long st;
+                  if (a == dim - 1) st = 0;  // slow-axis face: the whole face
+                  else if (dim == 3) st = (long long)s0 * (a == 0 ? ny : nx);
+                  else st = s0;
+                  src = flux ? kSrcFlux : kSrcPush;
+                  e0 = d.offo[a][sd] + st;
+                  const long long fsize = dim == 3 ? (a == 0 ? (long long)ny * (b.hi[2] - b.lo[2] + 1)
+                                                   : (a == 1 ? (long long)nx * (b.hi[2] - b.lo[2] + 1)
+                                                             : (long long)nx * ny))
+                                             : (a == 0 ? ny : nx);
+                  limit = std::min<long long>(L.no, d.offo[a][sd] + fsize);
+               }
+               if (e0 < 0 || e0 + sp.count[r] > limit)
+                  throw FacError(FAC_ERR_ARG, "staged unit outside its patch arrays");
+               const long long b0 = e0 * sp.esize[r], b1 = b0 + sp.count[r] * sp.esize[r];
+               const long long a0 = b0 & ~15ll, a1 = (b1 + 15) & ~15ll;
+               const int off = sp.off[r] + (int)(b0 - a0);
+               if (r == 0) h.off_u = off;
+               else if (r == 1) h.off_f = off;
+               else if (r < sp.nbase) {
+                  if (dvar && r - 2 < dim) h.off_d[r - 2] = off;
+                  else h.off_c = off;
+               } else if (r >= sp.cff0) {
+                  h.off_cff[sp.face[r - sp.cff0]] = off;
+               } else {
+                  h.off_push[sp.face[r - sp.face0]] = off;
+                  h.fmask |= 1 << sp.face[r - sp.face0];
+               }
+               copies.push_back({a0, src, (int)(a1 - a0), sp.off[r], 0});
+               total += a1 - a0;
+            }
+            copies[first].total = (int)total;
+            U.push_back({ip, first, (int)copies.size() - first, (int)hdrs.size()});
+            hdrs.push_back(rec);
+            s0 += ns;
+         }
+         if (s0 != nslow) throw FacError(FAC_ERR_ARG, "staged units do not tile the patch");
+      }
+      // three stages per CTA after 128 bytes of barriers and copy sources
+      L.unit_smem[t] = decode_ok && 128 + 3 * (long long)maxb <= kStageSmemMax ? maxb : 0;
+      L.d_units[t].upload(U, c->stream);
+      L.d_copies[t].upload(copies, c->stream);
+      std::vector<unsigned char> raw(hdrs.size() * kStageHeader);
+      if (!hdrs.empty()) std::memcpy(raw.data(), hdrs.data(), raw.size());
+      L.d_hdrs[t].upload(raw, c->stream);
+   }
+}
+
 // Same-level neighbour of every face cell of every patch (fused colour
 // pass).  The fused pass reads a neighbour patch's cell during a colour
 // pass; that is exact only when the neighbour has the other colour, which
@@ -833,7 +1004,10 @@ void build_facemap(fac_ctx *c, int ln)
    LevelState &L = c->L[ln];
    const int dim = c->dim;
    std::vector<long long> fmap(std::max<long long>(1, L.no), -3);
-   bool ok = true;
+   // push targets: where a face cell's value goes in the neighbour's ghost
+   // cells (staged pass), same -1 / -2 codes
+   std::vector<int> pmap(std::max<long long>(1, L.no), -3);
+   bool ok = L.n1 < (1ll << 31);
    int parity = -1;
    for (int ip = 0; ip < L.npatch && dim == 2; ++ip) {
       const int q = ((L.box[ip].lo[0] + L.box[ip].lo[1]) % 2 + 2) % 2;
@@ -859,7 +1033,8 @@ void build_facemap(fac_ctx *c, int ln)
             for (int k = layer.lo[2]; k <= layer.hi[2]; ++k)
                for (int j = layer.lo[1]; j <= layer.hi[1]; ++j)
                   for (int i = layer.lo[0]; i <= layer.hi[0]; ++i)
-                     fmap[d.offo[a][s] + tlin(i, j, k)] = outside ? -1 : -2;
+                     fmap[d.offo[a][s] + tlin(i, j, k)] = pmap[d.offo[a][s] + tlin(i, j, k)] =
+                        outside ? -1 : -2;
             if (outside) continue;
             for (int iq = pb; iq < pe; ++iq) {
                if (iq == ip) continue;
@@ -869,9 +1044,16 @@ void build_facemap(fac_ctx *c, int ln)
                const long long qnx = qg.hi[0] - qg.lo[0] + 1, qny = qg.hi[1] - qg.lo[1] + 1;
                for (int k = ov.lo[2]; k <= ov.hi[2]; ++k)
                   for (int j = ov.lo[1]; j <= ov.hi[1]; ++j)
-                     for (int i = ov.lo[0]; i <= ov.hi[0]; ++i)
+                     for (int i = ov.lo[0]; i <= ov.hi[0]; ++i) {
                         fmap[d.offo[a][s] + tlin(i, j, k)] =
                            L.hp[iq].off1 + (i - qg.lo[0]) + qnx * ((j - qg.lo[1]) + qny * (k - qg.lo[2]));
+                        // the face cell itself, one step back into patch ip
+                        int x[3] = {i, j, k};
+                        x[a] += s == 0 ? 1 : -1;
+                        pmap[d.offo[a][s] + tlin(i, j, k)] = (int)(
+                           L.hp[iq].off1 + (x[0] - qg.lo[0]) +
+                           qnx * ((x[1] - qg.lo[1]) + qny * (x[2] - qg.lo[2])));
+                     }
             }
          }
    }
@@ -880,12 +1062,16 @@ void build_facemap(fac_ctx *c, int ln)
    for (const CfFace &f : L.cf) mask[f.oidx] = 1;
    for (long long t = 0; t < L.no; ++t) {
       if (fmap[t] == -3) ok = false;
-      if (fmap[t] >= L.n1) throw FacError(FAC_ERR_ARG, "face table index out of range");
+      if (fmap[t] >= L.n1 || pmap[t] >= L.n1 || (pmap[t] < 0) != (fmap[t] < 0) ||
+          (fmap[t] < 0 && pmap[t] != fmap[t]))
+         throw FacError(FAC_ERR_ARG, "face table index out of range");
       if ((fmap[t] == -2) != (mask[t] != 0))
          throw FacError(FAC_ERR_NESTING, "face table disagrees with the coarse-fine boundary");
    }
    L.fused_ok = ok;
    L.facemap.upload(fmap, c->stream);
+   L.pushmap.upload(pmap, c->stream);
+   build_stage_units(c, ln);
 }
 
 void build_chunks(fac_ctx *c, int ln)
@@ -1032,6 +1218,23 @@ void build_coarsen_tables(fac_ctx *c, int ln)
    C.restrict_g1.upload(c->stream);
    C.restrict_g0.upload(c->stream);
    C.fcoarsen.upload(c->stream);
+   // faces of level ln written by the flux coarsening
+   std::vector<unsigned char> fm(std::max<long long>(1, C.ns), 0);
+   for (const FluxCoarsenItem &it : C.fcoarsen.items) {
+      const PatchDesc &cp = C.hp[it.coarse_patch];
+      const int a = it.axis;
+      const long long nxa = cp.hi[0] - cp.lo[0] + 1 + (a == 0);
+      const long long nya = cp.hi[1] - cp.lo[1] + 1 + (a == 1);
+      for (int k = it.lo[2]; k <= it.hi[2]; ++k)
+         for (int j = it.lo[1]; j <= it.hi[1]; ++j)
+            for (int i = it.lo[0]; i <= it.hi[0]; ++i) {
+               const long long si = cp.offs[a] + (i - cp.lo[0]) +
+                                    nxa * ((j - cp.lo[1]) + nya * (k - cp.lo[2]));
+               if (si < 0 || si >= C.ns) throw FacError(FAC_ERR_ARG, "flux coarsening face");
+               fm[si] = 1;
+            }
+   }
+   C.fcmask.upload(fm, c->stream);
 }
 
 // Coarse interpolation arrays for prolongation into level ln
@@ -1369,6 +1572,8 @@ void register_work_lists(fac_ctx *c)
       register_items(c, L.fcoarsen);
       register_items(c, L.tmp_fill);
       register_items(c, L.prolong);
+      for (int t = 0; t < 2; ++t)
+         register_work(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
    }
    c->d_work_regs.upload(c->work_regs, c->stream);
 }
@@ -1451,6 +1656,8 @@ void initialize(fac_ctx *c)
       L.fill_wc.upload(c->stream);
    }
    register_work_lists(c);
+   c->kerr.alloc(1);
+   if (!g_dry) CUDA_CHECK(cudaMemsetAsync(c->kerr.p, 0, sizeof(int), c->stream));
    std::vector<int> ones(np, 1);
    c->active.upload(ones, c->stream);
    c->run.upload(ones, c->stream);
@@ -1494,10 +1701,15 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
    CUDA_CHECK(cudaMemcpyAsync(c->run.p, c->active.p, np * sizeof(int), cudaMemcpyDeviceToDevice,
                               c->stream));
    CUDA_CHECK(cudaMemsetAsync(c->sweeps_call.p, 0, np * sizeof(long long), c->stream));
-   ghost_fill(c, fid_e, ln, false, 1, c->run.p);
-   if (ln > 0) ghost_fill(c, fid_e, ln, true, 1, c->run.p);
-   std::vector<int> hrun(np);
    const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
+   // the staged pass computes no residual maxima: fixed sweep counts only
+   const bool staged = fmap && c->staged && tol < 0.0 && L.unit_smem[0] > 0;
+   // The fill with the coarser level is a full fill.  Pulling fused passes
+   // read only its coarse-fine ghosts; staged passes read face ghost cells,
+   // which their pushes keep current after this fill.
+   if (ln > 0) ghost_fill(c, fid_e, ln, true, 1, c->run.p);
+   else if (!fmap || staged) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
+   std::vector<int> hrun(np);
    for (int isweep = 0; isweep < nsweeps; ++isweep) {
       if (tol >= 0.0 && isweep > 0 && isweep % c->check_interval == 0 && !c->capturing) {
          CUDA_CHECK(cudaMemcpyAsync(hrun.data(), c->run.p, np * sizeof(int),
@@ -1518,9 +1730,15 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
                            c->spec.d_variable, c->spec.d_const, L.tranwt, L.longwt, L.cfflux.p,
                            c->run.p);
          const int pi = prof_begin(c, 0, L.rb_bytes_prob, 1.0);
-         launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
-                     L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
-                     color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p, fmap, c->bc);
+         if (staged)
+            launch_rb_staged<double>(c->stream, c->dim, c->spec, (int)L.units[0].size(),
+                                     L.unit_smem[0], L.d_units[0].p, L.d_copies[0].p,
+                                     L.d_hdrs[0].p, e, r, L.d.p, L.c.p, L.cfflux.p, color,
+                                     L.pushmap.p, c->bc, c->kerr.p);
+         else
+            launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
+                        L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
+                        color == 0 ? L.maxres_red.p : L.maxres_blk.p, c->run.p, fmap, c->bc);
          prof_end(c, pi);
       }
       if (!fmap) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
@@ -1543,18 +1761,27 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
    const int *run = c->active.p;
    ghost_fill(c, fid_u, ln, ln > 0, error_eq, run);
    const double *u = field_ptr(L, fid_u);
-   launch_flux(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
-               L.d_flux_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt, L.d_ratio.p,
-               L.flux.p, run);
-   if (ln < c->nlev - 1) {
+   const bool finer = ln < c->nlev - 1;
+   if (!c->fused_residual)
+      launch_flux(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
+                  L.d_flux_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt, L.d_ratio.p,
+                  L.flux.p, run);
+   if (finer) {
       LevelState &Fl = c->L[ln + 1];
       launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
                           L.fcoarsen.nchunks(), Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
-   launch_residual(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
-                   L.d_cell_chunks.p, u, field_ptr(L, fid_f), L.flux.p, L.c.p,
-                   field_ptr(L, fid_r), ln > 0 ? L.oflux.p : nullptr, run);
+   if (c->fused_residual)
+      launch_residual_fused(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
+                            L.d_patches.p, L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt,
+                            L.longwt, L.d_ratio.p, finer ? L.fcmask.p : nullptr, L.flux.p,
+                            field_ptr(L, fid_f), L.c.p, field_ptr(L, fid_r),
+                            ln > 0 ? L.oflux.p : nullptr, run);
+   else
+      launch_residual(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
+                      L.d_cell_chunks.p, u, field_ptr(L, fid_f), L.flux.p, L.c.p,
+                      field_ptr(L, fid_r), ln > 0 ? L.oflux.p : nullptr, run);
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1614,7 +1841,10 @@ void rms_norm_read(fac_ctx *c, std::vector<double> &out)
    std::vector<double2> acc(np);
    CUDA_CHECK(cudaMemcpyAsync(acc.data(), c->norm_acc.p, np * sizeof(double2),
                               cudaMemcpyDeviceToHost, c->stream));
+   int kerr = 0;
+   CUDA_CHECK(cudaMemcpyAsync(&kerr, c->kerr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
    CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   if (kerr) throw FacError(FAC_ERR_CUDA, "a staged colour pass lost its shared-memory copies");
    out.resize(np);
    for (int p = 0; p < np; ++p) {
       const double num = std::sqrt(acc[p].x);
@@ -1718,9 +1948,10 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
    LevelState &L = c->L[ln];
    const int np = nprob(c);
    const int *run = c->active.p;
-   ghost_fill32(c, ln, false, 1, run);
-   if (ln > 0) ghost_fill32(c, ln, true, 1, run);
    const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
+   const bool staged = fmap && c->staged && L.unit_smem[1] > 0;
+   if (ln > 0) ghost_fill32(c, ln, true, 1, run);
+   else if (!fmap || staged) ghost_fill32(c, ln, false, 1, run);
    for (int isweep = 0; isweep < nsweeps; ++isweep) {
       for (int color = 0; color < 2; ++color) {
          if (!fmap) ghost_fill32(c, ln, false, 1, run);
@@ -1730,14 +1961,23 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
                                   L.longwt, L.cfflux32.p, run);
          const int pi =
             prof_begin(c, 2, L.rb_bytes_prob, 0.5);
-         launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
-                            L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
-                            L.c32.p, L.cfflux32.p, L.cfmask.p, color, nullptr, run, fmap, c->bc);
+         if (staged)
+            launch_rb_staged<float>(c->stream, c->dim, c->spec, (int)L.units[1].size(),
+                                    L.unit_smem[1], L.d_units[1].p, L.d_copies[1].p,
+                                    L.d_hdrs[1].p, L.e32.p, L.r32.p, L.d32.p, L.c32.p,
+                                    L.cfflux32.p, color, L.pushmap.p, c->bc, c->kerr.p);
+         else
+            launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
+                               L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
+                               L.c32.p, L.cfflux32.p, L.cfmask.p, color, nullptr, run, fmap,
+                               c->bc);
          prof_end(c, pi);
       }
       if (!fmap) ghost_fill32(c, ln, false, 1, run);
    }
-   if (fmap && nsweeps > 0) ghost_fill32(c, ln, false, 1, run);
+   // after fused passes the same-level ghosts of e32 are left stale: every
+   // reader in the mixed cycle fills them first (comp_residual_mixed) or
+   // reads interiors only (prolongation sources, u += e)
    (void)np;
    CUDA_CHECK(cudaGetLastError());
 }
@@ -1748,18 +1988,27 @@ void comp_residual_mixed(fac_ctx *c, int ln)
    LevelState &L = c->L[ln];
    const int *run = c->active.p;
    ghost_fill32(c, ln, ln > 0, 1, run);
-   launch_flux<float>(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
-                      L.d_flux_chunks.p, L.e32.p, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
-                      L.d_ratio.p, L.flux.p, run);
-   if (ln < c->nlev - 1) {
+   const bool finer = ln < c->nlev - 1;
+   if (!c->fused_residual)
+      launch_flux<float>(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
+                         L.d_flux_chunks.p, L.e32.p, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
+                         L.d_ratio.p, L.flux.p, run);
+   if (finer) {
       LevelState &Fl = c->L[ln + 1];
       launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
                           L.fcoarsen.nchunks(), Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
-   launch_residual<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
-                          L.d_cell_chunks.p, L.e32.p, L.r.p, L.flux.p, L.c.p, L.tr.p,
-                          ln > 0 ? L.oflux.p : nullptr, run);
+   if (c->fused_residual)
+      launch_residual_fused<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
+                                   L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
+                                   L.tranwt, L.longwt, L.d_ratio.p,
+                                   finer ? L.fcmask.p : nullptr, L.flux.p, L.r.p, L.c.p, L.tr.p,
+                                   ln > 0 ? L.oflux.p : nullptr, run);
+   else
+      launch_residual<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
+                             L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.r.p, L.flux.p, L.c.p,
+                             L.tr.p, ln > 0 ? L.oflux.p : nullptr, run);
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -2170,6 +2419,44 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol, double rel
    });
 }
 
+int fac_set_stage_budget(fac_ctx *ctx, int bytes)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      if (bytes < 4096 || bytes > kStageSmemMax / 3)
+         throw FacError(FAC_ERR_ARG, "stage budget out of range");
+      ctx->stage_budget = bytes;
+      if (ctx->initialized && ctx->device >= 0) {
+         CUDA_CHECK(cudaSetDevice(ctx->device));
+         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+         ctx->drop_graph();
+         for (int ln = 0; ln < ctx->nlev; ++ln) build_stage_units(ctx, ln);
+         register_work_lists(ctx);
+         launch_compact(ctx->stream, ctx->d_work_regs.p, (int)ctx->work_regs.size(),
+                        ctx->active.p, nprob(ctx));
+         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      }
+   });
+}
+
+int fac_set_fused_residual(fac_ctx *ctx, int on)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      ctx->fused_residual = on != 0;
+      ctx->drop_graph();
+   });
+}
+
+int fac_set_staged(fac_ctx *ctx, int on)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      ctx->staged = on != 0;
+      ctx->drop_graph();
+   });
+}
+
 int fac_set_fused(fac_ctx *ctx, int on)
 {
    return guarded([&] {
@@ -2413,6 +2700,14 @@ int fac_comp_residual(fac_ctx *ctx, int fid_r, int fid_u, int fid_f, int ln, int
       check_pl(ctx, 0, ln);
       if (field_ghost(fid_u) != 1 || field_ghost(fid_r) != 0 || field_ghost(fid_f) != 0)
          throw FacError(FAC_ERR_ARG, "bad field kinds for the residual");
+      // this entry point leaves the face fluxes in the flux side data, as
+      // the reference operator does; solves use the fused kernel
+      struct Restore {
+         fac_ctx *c;
+         int v;
+         ~Restore() { c->fused_residual = v; }
+      } restore{ctx, ctx->fused_residual};
+      ctx->fused_residual = 0;
       comp_residual(ctx, fid_r, fid_u, fid_f, ln, error_equation ? 1 : 0);
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
    });

@@ -122,6 +122,154 @@ struct BcCoefs {
    double a[6], b[6], g[6];
 };
 
+#ifdef __CUDACC__
+#define FAC_HD __host__ __device__
+#else
+#define FAC_HD
+#endif
+
+// Largest dynamic shared memory of one CTA of the staged colour pass.
+constexpr int kStageSmemMax = 227 * 1024;
+
+// Shared-memory plan of one unit of the staged colour pass: a run of ns
+// slices (planes in 3-D, rows in 2-D) along the slowest axis of an nx x ny
+// (x nz) patch.  A stage holds a 256-byte unit header and the regions
+//   0 u over the slices and one slice either side (ghosted rows), 1 f,
+//   2..1+dim the side arrays of D, then C when variable,
+//   then per patch face of the unit (x lo/hi, y lo/hi (3-D), slow-axis
+//   lo/hi where the unit reaches the patch's end) the push targets (int32),
+//   then, for a patch with coarse-fine faces, the Ewing fluxes of the same
+//   faces.
+// Each region is sized for its elements plus a 16-byte alignment shift;
+// off[r] is its start from the stage start (16-byte multiples).
+constexpr int kStageHeader = 256;
+constexpr int kStageMaxRegions = 18;
+
+struct StagePlan {
+   int nreg;
+   int nbase;        // u, f, D, C regions
+   int face0;        // first push-target region
+   int cff0;         // first Ewing-flux region (== nreg when none)
+   int off[kStageMaxRegions];
+   long long count[kStageMaxRegions];  // elements
+   int esize[kStageMaxRegions];        // element bytes
+   int face[6];      // face id (2*axis + side) of the k-th face region
+   int nface;
+   int bytes;
+};
+
+FAC_HD inline StagePlan stage_plan(int dim, int nx, int ny, int ns, int tsize, bool dvar,
+                                   bool cvar, bool slo, bool shi, bool cf)
+{
+   StagePlan sp;
+   const long long g1 = dim == 3 ? (long long)(nx + 2) * (ny + 2) : nx + 2;
+   const long long g0 = dim == 3 ? (long long)nx * ny : nx;
+   int r = 0;
+   sp.count[r] = (ns + 2) * g1;
+   sp.esize[r++] = tsize;
+   sp.count[r] = ns * g0;
+   sp.esize[r++] = tsize;
+   if (dvar) {
+      for (int a = 0; a < dim; ++a) {
+         long long n;
+         if (dim == 3) {
+            n = a == 0 ? (long long)ns * (nx + 1) * ny
+                       : (a == 1 ? (long long)ns * nx * (ny + 1) : (long long)(ns + 1) * nx * ny);
+         } else {
+            n = a == 0 ? (long long)ns * (nx + 1) : (long long)(ns + 1) * nx;
+         }
+         sp.count[r] = n;
+         sp.esize[r++] = tsize;
+      }
+   }
+   if (cvar) {
+      sp.count[r] = ns * g0;
+      sp.esize[r++] = tsize;
+   }
+   sp.nbase = r;
+   // faces of the unit
+   sp.nface = 0;
+   const long long lat0 = dim == 3 ? (long long)ny * ns : ns;  // x faces
+   const long long lat1 = (long long)nx * ns;                   // y faces (3-D)
+   const long long slow = dim == 3 ? (long long)nx * ny : nx;   // slow-axis faces
+   long long fcount[6];
+   for (int s = 0; s < 2; ++s) {
+      sp.face[sp.nface] = s;
+      fcount[sp.nface++] = lat0;
+   }
+   if (dim == 3)
+      for (int s = 0; s < 2; ++s) {
+         sp.face[sp.nface] = 2 + s;
+         fcount[sp.nface++] = lat1;
+      }
+   if (slo) {
+      sp.face[sp.nface] = 2 * (dim - 1);
+      fcount[sp.nface++] = slow;
+   }
+   if (shi) {
+      sp.face[sp.nface] = 2 * (dim - 1) + 1;
+      fcount[sp.nface++] = slow;
+   }
+   sp.face0 = r;
+   for (int k = 0; k < sp.nface; ++k) {
+      sp.count[r] = fcount[k];
+      sp.esize[r++] = 4;
+   }
+   sp.cff0 = r;
+   if (cf)
+      for (int k = 0; k < sp.nface; ++k) {
+         sp.count[r] = fcount[k];
+         sp.esize[r++] = tsize;
+      }
+   sp.nreg = r;
+   long long o = kStageHeader;
+   for (int k = 0; k < r; ++k) {
+      sp.off[k] = (int)o;
+      o += ((sp.count[k] * sp.esize[k] + 15) / 16) * 16 + 16;
+   }
+   for (int k = r; k < kStageMaxRegions; ++k) {
+      sp.off[k] = (int)o;
+      sp.count[k] = 0;
+      sp.esize[k] = 0;
+   }
+   sp.bytes = o > 0x3fffffff ? 0x3fffffff : (int)o;
+   return sp;
+}
+
+// Header of one staged unit (built on the host, copied into the stage
+// ahead of the unit's data): the patch geometry the consumers need, values
+// computed once per unit (reciprocals in both precisions, slot counts) and
+// the stage offsets (bytes from the stage start to element 0) of the regions.
+struct UnitHdr {
+   int lo[3], hi[3];
+   int flags, s0, ns, hx;  // hx: active cells per row, (nx + 1) / 2
+   long long off1;         // patch start in ghost-1 cell buffers
+   double dx[3];
+   double dxi_d[3];        // 1 / dx in FP64
+   float dxi_f[3];         // 1 / dx rounded from FP32 dx, in FP32
+   unsigned mhx, mny;      // ceil(2^32 / hx), ceil(2^32 / ny): q / d = umulhi(q, m)
+                           // for the slot decode (q < 2^14, d <= 1024)
+   int nslots;             // hx * rows
+   int fmask;              // bit 2*axis+side: the unit has that patch face
+   int off_u, off_f, off_d[3], off_c;
+   int off_push[6];        // per face id 2*axis+side: push targets, -1 if none
+   int off_cff[6];         // Ewing fluxes of the same faces, -1 if none
+};
+
+// One bulk copy of a staged unit: nbytes (a multiple of 16) from byte
+// src_off (16-byte aligned) of source array src into the stage at dst_off.
+// The first copy of a unit carries the unit's total in total.
+enum StageSrc : int {
+   kSrcU = 0, kSrcF, kSrcD, kSrcC, kSrcPush, kSrcFlux, kSrcHdr, kSrcCount
+};
+struct UnitCopy {
+   long long src_off;
+   int src;
+   int nbytes;
+   int dst_off;
+   int total;
+};
+
 struct PoissonSpec {
    int d_variable;
    int c_kind;        // 0 zero, 1 constant, 2 variable

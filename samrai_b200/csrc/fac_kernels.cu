@@ -13,6 +13,7 @@
 #include <atomic>
 #include <cstdint>
 
+#include "fac_device.h"
 #include "fac_internal.h"
 #include "fac_kernels.h"
 
@@ -20,76 +21,7 @@ namespace samrai_b200 {
 
 namespace {
 
-constexpr int kThreads = 256;
-// Blocks of a chunk kernel: enough to fill the GPU; each block walks the
-// work list with a grid stride.
-constexpr int kGridCap = 148 * 8;
-
-inline int work_grid(int nchunks) { return nchunks < kGridCap ? nchunks : kGridCap; }
-
-// Grid-stride walk over a work list of nwork entries.  The list is compacted
-// on the device whenever the set of iterating problems changes: the chunks of
-// those problems come first and a chunk with patch < 0 ends the list.
-#define WORK_LOOP(ch)                                      \
-   for (int w_ = blockIdx.x; w_ < nwork; w_ += gridDim.x) \
-      if (const Chunk ch = chunks[w_]; ch.patch < 0)       \
-         break;                                            \
-      else
-
-__device__ __forceinline__ long long aidx(const ArrDesc &A, int i, int j, int k)
-{
-   return A.base + (long long)(i - A.lo[0]) +
-          (long long)A.n[0] * ((long long)(j - A.lo[1]) +
-                               (long long)A.n[1] * (long long)(k - A.lo[2]));
-}
-
-// Index of cell (i,j,k) in a patch's array with ghost width g.
-template <int DIM>
-__device__ __forceinline__ long long cidx(const PatchDesc &p, long long off,
-                                          int g, int i, int j, int k)
-{
-   const int gz = DIM == 3 ? g : 0;
-   const long long nx = p.hi[0] - p.lo[0] + 1 + 2 * g;
-   const long long ny = p.hi[1] - p.lo[1] + 1 + 2 * g;
-   return off + (i - p.lo[0] + g) + nx * ((j - p.lo[1] + g) + ny * (k - p.lo[2] + gz));
-}
-
-// Index of face (i,j,k) of axis a in a patch's side array (ghost 0).
-__device__ __forceinline__ long long sidx(const PatchDesc &p, int a, int i, int j,
-                                          int k)
-{
-   const long long nx = p.hi[0] - p.lo[0] + 1 + (a == 0);
-   const long long ny = p.hi[1] - p.lo[1] + 1 + (a == 1);
-   return p.offs[a] + (i - p.lo[0]) + nx * ((j - p.lo[1]) + ny * (k - p.lo[2]));
-}
-
-// Index of the tangential position of cell (i,j,k) in a face array of axis a.
-__device__ __forceinline__ long long oidx(const PatchDesc &p, int a, int s, int i,
-                                          int j, int k)
-{
-   const long long nx = p.hi[0] - p.lo[0] + 1;
-   const long long ny = p.hi[1] - p.lo[1] + 1;
-   long long t;
-   if (a == 0) t = (j - p.lo[1]) + ny * (k - p.lo[2]);
-   else if (a == 1) t = (i - p.lo[0]) + nx * (k - p.lo[2]);
-   else t = (i - p.lo[0]) + nx * (j - p.lo[1]);
-   return p.offo[a][s] + t;
-}
-
-__device__ __forceinline__ int coarsen_index(int i, int r)
-{
-   return i < 0 ? (i + 1) / r - 1 : i / r;
-}
-
-// settype1cells{2,3}d (robinbchelper2d.f:10-72): ghost value from the
-// interior value next to the boundary.
-template <class T>
-__device__ __forceinline__ T robin(T uin, int loc, T h, int hom, const BcCoefs &bc)
-{
-   const T a = (T)bc.a[loc], b = (T)bc.b[loc], half = (T)0.5;
-   if (hom) return (uin * (b - half * h * a)) / (b + half * h * a);
-   return (h * (T)bc.g[loc] + uin * (b - half * h * a)) / (b + half * h * a);
-}
+using namespace dev;
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v)
 {
@@ -485,6 +417,102 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
             if (DIM == 3) {
                if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = flux[sidx(p, 2, i, j, k)];
                if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = flux[sidx(p, 2, i, j, k + 1)];
+            }
+         }
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------
+// composite residual with the fluxes formed on the fly: the arithmetic of
+// k_flux (Ewing fix on coarse-fine faces) and k_residual in one pass, so the
+// side-array fluxes are neither written nor read back.  Faces that carry a
+// coarsened finer-level flux (fcmask) take it from fcflux, where
+// k_flux_coarsen put it, as the two-kernel sequence does.
+// ---------------------------------------------------------------------------
+
+template <int DIM, bool DVAR, int CKIND, class TU>
+__global__ void __launch_bounds__(kThreads)
+k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+                 int nwork, const TU *__restrict__ u, const double *__restrict__ dside,
+                 double dconst, const unsigned char *__restrict__ cfmask, EwingWeights w,
+                 const int *ratio_to_coarser, const unsigned char *__restrict__ fcmask,
+                 const double *__restrict__ fcflux, const double *__restrict__ f,
+                 const double *__restrict__ cfield, double cconst, double *__restrict__ res,
+                 double *__restrict__ oflux, const int *__restrict__ run)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      if (run && !run[p.prob]) continue;
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const bool has_cf = (p.flags & 1) != 0;
+      const long long gx = nx + 2, gxy = (long long)(nx + 2) * (ny + 2);
+      // flux on the face of axis a whose upper cell is (fi, fj, fk)
+      auto face_flux = [&](int a, int fi, int fj, int fk) -> double {
+         const long long si = sidx(p, a, fi, fj, fk);
+         if (fcmask && fcmask[si]) return fcflux[si];
+         const double dai = 1. / p.dx[a];
+         const double d = DVAR ? dside[si] : dconst;
+         const long long cp = cidx<DIM>(p, p.off1, 1, fi, fj, fk);
+         const long long cq = cp - (a == 0 ? 1 : (a == 1 ? gx : gxy));
+         double fl = dai * d * ((double)u[cp] - (double)u[cq]);
+         if (has_cf) {
+            const int fc[3] = {fi, fj, fk};
+            int s = -1;
+            if (fc[a] == p.lo[a]) s = 0;
+            else if (fc[a] == p.hi[a] + 1) s = 1;
+            if (s >= 0) {
+               int cc[3] = {fi, fj, fk};
+               if (s == 1) cc[a] -= 1;
+               const long long o = oidx(p, a, s, cc[0], cc[1], cc[2]);
+               if (cfmask[o]) {
+                  int mq[3] = {cc[0], cc[1], cc[2]};
+                  for (int tt = 0; tt < DIM; ++tt) {
+                     if (tt == a) continue;
+                     const int rr = ratio_to_coarser[tt];
+                     const int base = coarsen_index(cc[tt], rr) * rr;
+                     mq[tt] = base + (rr - (cc[tt] - base) - 1);
+                  }
+                  const double uc = (double)u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
+                  const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
+                  if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
+                  else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
+               }
+            }
+         }
+         return fl;
+      };
+      const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
+      const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         const double fxl = face_flux(0, i, j, k), fxh = face_flux(0, i + 1, j, k);
+         const double fyl = face_flux(1, i, j, k), fyh = face_flux(1, i, j + 1, k);
+         const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
+         const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
+         const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
+         double rv, fzl = 0.0, fzh = 0.0;
+         if (DIM == 2) {
+            rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
+         } else {
+            fzl = face_flux(2, i, j, k);
+            fzh = face_flux(2, i, j, k + 1);
+            rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - sf * uc;
+         }
+         res[c0] = rv;
+         if (oflux) {
+            if (i == p.lo[0]) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
+            if (i == p.hi[0]) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
+            if (j == p.lo[1]) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
+            if (j == p.hi[1]) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
+            if (DIM == 3) {
+               if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = fzl;
+               if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = fzh;
             }
          }
       }
@@ -1155,6 +1183,49 @@ void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
 }
 
 template <class TU>
+void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                           const PatchDesc *patches, const Chunk *chunks, const TU *u,
+                           const double *dside, const unsigned char *cfmask,
+                           const double *tranwt, const double *longwt, const int *ratio_dev,
+                           const unsigned char *fcmask, const double *fcflux, const double *f,
+                           const double *cfield, double *res, double *oflux, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   EwingWeights w;
+   for (int a = 0; a < 3; ++a) {
+      w.tranwt[a] = tranwt[a];
+      w.longwt[a] = longwt[a];
+   }
+#define RF(D, V, C)                                                                         \
+   k_residual_fused<D, V, C, TU><<<work_grid(nchunks), kThreads, 0, s>>>(                   \
+      patches, chunks, nchunks, u, dside, spec.d_const, cfmask, w, ratio_dev, fcmask, fcflux, \
+      f, cfield, spec.c_const, res, oflux, run)
+   if (dim == 2) {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RF(2, true, 2);
+         else if (spec.c_kind == 1) RF(2, true, 1);
+         else RF(2, true, 0);
+      } else {
+         if (spec.c_kind == 2) RF(2, false, 2);
+         else if (spec.c_kind == 1) RF(2, false, 1);
+         else RF(2, false, 0);
+      }
+   } else {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RF(3, true, 2);
+         else if (spec.c_kind == 1) RF(3, true, 1);
+         else RF(3, true, 0);
+      } else {
+         if (spec.c_kind == 2) RF(3, false, 2);
+         else if (spec.c_kind == 1) RF(3, false, 1);
+         else RF(3, false, 0);
+      }
+   }
+#undef RF
+}
+
+template <class TU>
 void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                      const PatchDesc *patches, const Chunk *chunks, const TU *u,
                      const double *f, const double *flux, const double *cfield,
@@ -1375,6 +1446,11 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
                                     const PatchDesc *, const Chunk *, const T *,            \
                                     const double *, const double *, const double *,         \
                                     double *, double *, const int *);                       \
+   template void launch_residual_fused<T>(                                                  \
+      cudaStream_t, int, const PoissonSpec &, int, const PatchDesc *, const Chunk *, const T *, \
+      const double *, const unsigned char *, const double *, const double *, const int *,   \
+      const unsigned char *, const double *, const double *, const double *, double *,      \
+      double *, const int *);                                                               \
    template void launch_prolong_add<T>(cudaStream_t, int, const ProlongItem *,              \
                                        const Chunk *, int, const PatchDesc *, const T *,    \
                                        const double *, const int *, T *, const int *);      \

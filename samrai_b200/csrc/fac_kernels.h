@@ -13,6 +13,20 @@ long long kernel_launch_count();
 // graph (removed at capture, added per replay).
 void add_kernel_launches(long long n);
 
+// Staged colour pass (fac_stage.cu): units {patch, first copy, copies,
+// header} of the compacted list (active problems only) with their copy
+// lists and headers; stage_bytes is the largest StagePlan::bytes of the
+// units; pushmap gives per face cell where its new value goes (>= 0 a
+// neighbour's ghost cell, -1 physical boundary, -2 coarse-fine face); err is
+// set to 1 when a bounded wait runs out.  The field's face ghost cells must
+// be filled before the first pass.
+template <class T>
+void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nunits,
+                      int stage_bytes, const Chunk *units, const UnitCopy *copies,
+                      const unsigned char *headers, T *u, const T *f, const T *dside,
+                      const T *cfield, const T *cfflux, int offset, const int *pushmap,
+                      const BcCoefs &bc, int *err);
+
 // Rebuild every registered work list for the current active flags.
 void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *active, int nprob);
 
@@ -46,6 +60,17 @@ void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchun
                      const PatchDesc *patches, const Chunk *chunks, const TU *u,
                      const double *f, const double *flux, const double *cfield,
                      double *res, double *oflux, const int *run);
+
+// Fluxes on the fly + residual (+ outer-side fluxes): k_flux and k_residual
+// in one pass; fcmask marks faces whose flux is the coarsened finer-level
+// flux already stored in fcflux (NULL when the level has no finer level).
+template <class TU>
+void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                           const PatchDesc *patches, const Chunk *chunks, const TU *u,
+                           const double *dside, const unsigned char *cfmask,
+                           const double *tranwt, const double *longwt, const int *ratio_dev,
+                           const unsigned char *fcmask, const double *fcflux, const double *f,
+                           const double *cfield, double *res, double *oflux, const int *run);
 
 void launch_flux_coarsen(cudaStream_t s, const FluxCoarsenItem *items, const Chunk *chunks,
                          int nchunks, const PatchDesc *fine, const PatchDesc *coarse,

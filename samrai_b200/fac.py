@@ -67,6 +67,9 @@ def load_library(build_if_missing=True):
         "fac_set_precision": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_fused": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_staged": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_fused_residual": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_stage_budget": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
         "fac_side_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
         "fac_oside_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
@@ -328,6 +331,15 @@ class FacContext:
 
     def synchronize(self):
         _check(load_library().fac_synchronize(self.h))
+
+    def set_stage_budget(self, nbytes):
+        _check(load_library().fac_set_stage_budget(self.h, int(nbytes)))
+
+    def set_fused_residual(self, on=True):
+        _check(load_library().fac_set_fused_residual(self.h, int(on)))
+
+    def set_staged(self, on=True):
+        _check(load_library().fac_set_staged(self.h, int(on)))
 
     def set_fused(self, on=True):
         _check(load_library().fac_set_fused(self.h, int(on)))

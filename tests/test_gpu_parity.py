@@ -242,7 +242,7 @@ def _fused_levels_2d(probs):
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("case", ["config1", "small_3d_mg", "config2"])
-def test_fused_colour_pass_matches_filled(case, precision, require_gpu):
+def test_fused_and_staged_colour_passes_match_filled(case, precision, require_gpu):
     """Colour passes that read across patch faces directly must give the same
     bits as passes that read ghost cells filled before each pass, including
     the ghost values left after the solve."""
@@ -256,14 +256,45 @@ def test_fused_colour_pass_matches_filled(case, precision, require_gpu):
         probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (41, 42)]
     prm = dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=2 if case == "config2" else 6)
     out = []
-    for fused in (True, False):
+    # fused passes on staged shared-memory units, fused passes reading HBM,
+    # and passes between ghost fills
+    for fused, staged in ((True, True), (True, False), (False, False)):
         g = fac.FacContext(probs, params=prm, precision=precision)
         g.set_fused(fused)
+        g.set_staged(staged)
         conv, its, res = g.solve()
         fields = [g.download(U, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
         g.smooth(E, R, probs[0].nlev - 1, 3)
         fields += [g.download(E, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
         out.append((its.copy(), res.copy(), fields))
+        g.close()
+    for other in out[1:]:
+        assert np.array_equal(out[0][0], other[0])
+        assert np.array_equal(out[0][1], other[1])
+        for a, b in zip(out[0][2], other[2]):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["config1", "small_3d_mg", "config3"])
+def test_fused_residual_matches_flux_arrays(case, precision, require_gpu):
+    """Residuals that form the face fluxes on the fly must give the same bits
+    as the flux-array kernels (flux, coarsening, residual) in a full solve."""
+    if case == "config1":
+        probs = [configs.config1()]
+    elif case == "config3":
+        probs = [configs.config3()]
+    else:
+        probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (51, 52)]
+    prm = dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=5)
+    out = []
+    for fused in (True, False):
+        g = fac.FacContext(probs, params=prm, precision=precision)
+        g.set_fused_residual(fused)
+        conv, its, res = g.solve()
+        out.append((its.copy(), res.copy(),
+                    [g.download(U, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]))
         g.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
