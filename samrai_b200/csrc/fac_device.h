@@ -25,6 +25,27 @@ inline int work_grid(int nchunks) { return nchunks < kGridCap ? nchunks : kGridC
          break;                                            \
       else
 
+// Item and cell (within the item) of element t of a transaction-list chunk:
+// a chunk of one item covers its cells [begin, begin + count); a packed
+// chunk covers its aux items back to back (prefix: first cell of each item).
+__device__ __forceinline__ int chunk_item(const Chunk &ch, const int *__restrict__ prefix, int t,
+                                          int &lin)
+{
+   if (ch.aux <= 1) {
+      lin = ch.begin + t;
+      return ch.patch;
+   }
+   const int g = prefix[ch.patch] + t;
+   int lo = ch.patch, hi = ch.patch + ch.aux - 1;
+   while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= g) lo = mid;
+      else hi = mid - 1;
+   }
+   lin = g - prefix[lo];
+   return lo;
+}
+
 __device__ __forceinline__ long long aidx(const ArrDesc &A, int i, int j, int k)
 {
    return A.base + (long long)(i - A.lo[0]) +

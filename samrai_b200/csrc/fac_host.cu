@@ -196,35 +196,67 @@ struct WorkSrc {
 template <class I>
 struct ItemList {
    std::vector<I> items;
+   std::vector<long long> cells;  // per item
    std::vector<Chunk> chunks;
+   std::vector<int> prefix;       // first cell of each item (list order)
    DevArray<I> d_items;
    DevArray<Chunk> d_chunks;
+   DevArray<int> d_prefix;
    WorkSrc ws;
-   void add(const I &it, long long ncells, int aux = 0)
+   void add(const I &it, long long ncells)
    {
-      const int id = (int)items.size();
       items.push_back(it);
-      for (long long b = 0; b < ncells; b += kChunk) {
-         Chunk c;
-         c.patch = id;
-         c.begin = (int)b;
-         c.count = (int)std::min<long long>(kChunk, ncells - b);
-         c.aux = aux;
-         chunks.push_back(c);
+      cells.push_back(ncells);
+   }
+   // Chunks: an item larger than kChunk cells gets chunks of its own; runs
+   // of smaller items of one problem share a chunk of up to kChunk cells.
+   void pack()
+   {
+      chunks.clear();
+      prefix.assign(items.size() + 1, 0);
+      long long run = 0;
+      for (size_t i = 0; i < items.size(); ++i) {
+         if (run + cells[i] >= (1ll << 31)) throw FacError(FAC_ERR_ARG, "transaction list too long");
+         prefix[i] = (int)run;
+         run += cells[i];
+      }
+      prefix[items.size()] = (int)run;
+      size_t i = 0;
+      while (i < items.size()) {
+         if (cells[i] > kChunk) {
+            for (long long b = 0; b < cells[i]; b += kChunk)
+               chunks.push_back({(int)i, (int)b, (int)std::min<long long>(kChunk, cells[i] - b), 1});
+            ++i;
+            continue;
+         }
+         size_t j = i;
+         long long n = 0;
+         while (j < items.size() && cells[j] <= kChunk && n + cells[j] <= kChunk &&
+                items[j].prob == items[i].prob) {
+            n += cells[j];
+            ++j;
+         }
+         if (n > 0) chunks.push_back({(int)i, 0, (int)n, (int)(j - i)});
+         i = j;
       }
    }
    void upload(cudaStream_t s)
    {
+      pack();
       d_items.upload(items, s);
       d_chunks.upload(chunks, s);
+      d_prefix.upload(prefix, s);
    }
    int nchunks() const { return (int)chunks.size(); }
    void clear()
    {
       items.clear();
+      cells.clear();
       chunks.clear();
+      prefix.clear();
       d_items.free();
       d_chunks.free();
+      d_prefix.free();
       ws.all.free();
       ws.pcb.free();
    }
@@ -1178,7 +1210,8 @@ void build_coarsen_tables(fac_ctx *c, int ln)
                   it.lo[a] = ov.lo[a];
                   it.hi[a] = ov.hi[a];
                }
-               (g ? C.restrict_g1 : C.restrict_g0).add(it, ov.size(), raux);
+               it.ratio = raux;
+               (g ? C.restrict_g1 : C.restrict_g0).add(it, ov.size());
             }
          }
          for (int a = 0; a < dim; ++a) {
@@ -1209,7 +1242,8 @@ void build_coarsen_tables(fac_ctx *c, int ln)
                   it.t0 = t0;
                   it.t1 = t1;
                   const int aux = r[t0] | ((t1 >= 0 ? r[t1] : 1) << 8);
-                  C.fcoarsen.add(it, ov.size(), aux);
+                  it.ratio = aux;
+                  C.fcoarsen.add(it, ov.size());
                }
             }
          }
@@ -1421,7 +1455,25 @@ Box item_box(const int *lo, const int *hi)
    return b;
 }
 
-void validate_fill(const ItemList<FillItem> &L, long long dstlen, long long samelen,
+// Packed chunk ranges of a transaction list (see ItemList::pack).
+template <class I>
+void validate_chunks(ItemList<I> &L, const char *what)
+{
+   L.pack();
+   for (const Chunk &ch : L.chunks) {
+      vcheck(ch.patch >= 0 && ch.aux >= 1 && ch.patch + ch.aux <= (int)L.items.size(), what);
+      if (ch.aux == 1)
+         vcheck(ch.begin >= 0 && ch.count > 0 && ch.begin + ch.count <= L.cells[ch.patch], what);
+      else
+         vcheck(ch.begin == 0 && ch.count == L.prefix[ch.patch + ch.aux] - L.prefix[ch.patch] &&
+                   ch.count <= kChunk,
+                what);
+      for (int j = ch.patch; j < ch.patch + ch.aux; ++j)
+         vcheck(L.items[j].prob == L.items[ch.patch].prob, what);
+   }
+}
+
+void validate_fill(ItemList<FillItem> &L, long long dstlen, long long samelen,
                    long long coarselen)
 {
    for (const FillItem &it : L.items) {
@@ -1443,13 +1495,9 @@ void validate_fill(const ItemList<FillItem> &L, long long dstlen, long long same
       }
       vcheck(desc_contains(it.src, sb, it.src_is_coarse ? coarselen : samelen), "fill source");
    }
-   for (const Chunk &ch : L.chunks) {
-      vcheck(ch.patch >= 0 && ch.patch < (int)L.items.size(), "fill chunk item");
-      const FillItem &it = L.items[ch.patch];
-      vcheck(ch.begin >= 0 && ch.count > 0 &&
-                ch.begin + ch.count <= item_box(it.lo, it.hi).size(),
-             "fill chunk range");
-   }
+   for (size_t i = 0; i < L.items.size(); ++i)
+      vcheck(L.cells[i] == item_box(L.items[i].lo, L.items[i].hi).size(), "fill item cells");
+   validate_chunks(L, "fill chunk range");
 }
 
 void validate_tables(fac_ctx *c)
@@ -1523,6 +1571,14 @@ void validate_tables(fac_ctx *c)
                    "flux coarsen source");
          }
       }
+   }
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      validate_chunks(L.restrict_g1, "restrict chunk range");
+      validate_chunks(L.restrict_g0, "restrict chunk range");
+      validate_chunks(L.fcoarsen, "flux coarsening chunk range");
+      validate_chunks(L.tmp_fill, "coarse interpolation chunk range");
+      validate_chunks(L.prolong, "prolongation chunk range");
    }
 }
 
@@ -1685,7 +1741,7 @@ void ghost_fill(fac_ctx *c, int fid, int ln, bool with_coarse, int homogeneous, 
    const double *coarse = ln > 0 ? field_ptr(c->L[ln - 1], fid) : nullptr;
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
    const int pi = prof_begin(c, 1, L.fill_bytes_prob, 1.0);
-   launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), dst, dst, coarse,
+   launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, dst, dst, coarse,
                homogeneous, c->bc, mask);
    prof_end(c, pi);
 }
@@ -1763,13 +1819,13 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
    const double *u = field_ptr(L, fid_u);
    const bool finer = ln < c->nlev - 1;
    if (!c->fused_residual)
-      launch_flux(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
-                  L.d_flux_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt, L.d_ratio.p,
-                  L.flux.p, run);
+      launch_flux_cells(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
+                        L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
+                        L.d_ratio.p, L.flux.p, run);
    if (finer) {
       LevelState &Fl = c->L[ln + 1];
       launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
-                          L.fcoarsen.nchunks(), Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
+                          L.fcoarsen.nchunks(), L.fcoarsen.d_prefix.p, Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
    if (c->fused_residual)
@@ -1792,7 +1848,7 @@ void restrict_op(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
    LevelState &Fl = c->L[dest_ln + 1];
    const int sg = field_ghost(fid_src), dg = field_ghost(fid_dst);
    ItemList<RestrictItem> &it = dg ? C.restrict_g1 : C.restrict_g0;
-   launch_restrict(c->stream, c->dim, it.d_items.p, it.d_chunks.p, it.nchunks(), Fl.d_patches.p,
+   launch_restrict(c->stream, c->dim, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, Fl.d_patches.p,
                    C.d_patches.p, field_ptr(Fl, fid_src), sg, field_ptr(C, fid_dst), dg,
                    c->active.p);
    CUDA_CHECK(cudaGetLastError());
@@ -1814,10 +1870,10 @@ void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
    if (field_ghost(fid_src) != 1 || field_ghost(fid_dst) != 1)
       throw FacError(FAC_ERR_ARG, "prolongation needs ghosted cell fields");
    launch_fill<double>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
-                       Fl.tmp_fill.nchunks(), Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1, c->bc,
+                       Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1, c->bc,
                        c->active.p);
    launch_prolong_add(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
-                      Fl.prolong.nchunks(), Fl.d_patches.p, Fl.tmp.p, Fl.dxc_prob.p, Fl.ratio,
+                      Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp.p, Fl.dxc_prob.p, Fl.ratio,
                       field_ptr(Fl, fid_dst), c->active.p);
    CUDA_CHECK(cudaGetLastError());
 }
@@ -1937,7 +1993,7 @@ void ghost_fill32(fac_ctx *c, int ln, bool with_coarse, int homogeneous, const i
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
    const int pi =
       prof_begin(c, 3, L.fill_bytes_prob, 0.5);
-   launch_fill<float>(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), L.e32.p, L.e32.p,
+   launch_fill<float>(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, L.e32.p, L.e32.p,
                       coarse, homogeneous, c->bc, mask);
    prof_end(c, pi);
 }
@@ -1990,13 +2046,13 @@ void comp_residual_mixed(fac_ctx *c, int ln)
    ghost_fill32(c, ln, ln > 0, 1, run);
    const bool finer = ln < c->nlev - 1;
    if (!c->fused_residual)
-      launch_flux<float>(c->stream, c->dim, c->spec, (int)L.flux_chunks.size(), L.d_patches.p,
-                         L.d_flux_chunks.p, L.e32.p, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
-                         L.d_ratio.p, L.flux.p, run);
+      launch_flux_cells<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
+                               L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
+                               L.tranwt, L.longwt, L.d_ratio.p, L.flux.p, run);
    if (finer) {
       LevelState &Fl = c->L[ln + 1];
       launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
-                          L.fcoarsen.nchunks(), Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
+                          L.fcoarsen.nchunks(), L.fcoarsen.d_prefix.p, Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
    if (c->fused_residual)
@@ -2018,10 +2074,10 @@ void prolong32(fac_ctx *c, int dest_ln)
    LevelState &Fl = c->L[dest_ln];
    LevelState &C = c->L[dest_ln - 1];
    launch_fill<float>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
-                      Fl.tmp_fill.nchunks(), Fl.tmp32.p, nullptr, C.e32.p, 1, c->bc,
+                      Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp32.p, nullptr, C.e32.p, 1, c->bc,
                       c->active.p);
    launch_prolong_add<float>(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
-                             Fl.prolong.nchunks(), Fl.d_patches.p, Fl.tmp32.p, Fl.dxc_prob.p,
+                             Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp32.p, Fl.dxc_prob.p,
                              Fl.ratio, Fl.e32.p, c->active.p);
    CUDA_CHECK(cudaGetLastError());
 }

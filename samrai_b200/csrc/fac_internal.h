@@ -29,7 +29,11 @@ struct PatchDesc {
 };
 
 // Chunk of work over one patch: cells [begin, begin+count) of a
-// linearisation chosen by the kernel that consumes it.
+// linearisation chosen by the kernel that consumes it.  Transaction lists
+// (fills, restriction, flux coarsening, prolongation) pack small items of
+// one problem into one chunk: then patch is the first item, aux > 1 the
+// number of items and the chunk covers their cells back to back (a list's
+// item prefix sums give each item's first cell).
 struct Chunk {
    int patch;
    int begin;
@@ -100,6 +104,7 @@ struct FluxCoarsenItem {
    int lo[3], hi[3];   // coarse face cells (index space of the side box)
    int fface;          // fine face index along the axis
    int t0, t1;         // tangential axes (t1 = -1 in 2-D); t1 is outer
+   int ratio;          // refinement ratios along t0 (bits 0-7) and t1 (bits 8-15)
 };
 
 // Restriction: coarse cells of one destination patch covered by one fine
@@ -109,6 +114,7 @@ struct RestrictItem {
    int fine_patch;
    int coarse_patch;
    int lo[3], hi[3];   // coarse cells
+   int ratio;          // refinement ratios, 8 bits per axis
 };
 
 // Prolongation: one fine patch with its coarse interpolation array.

@@ -35,18 +35,18 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, doub
 template <class T>
 __global__ void __launch_bounds__(kThreads)
 k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
-       T *__restrict__ dst, const T *__restrict__ src_same,
+       const int *__restrict__ prefix, T *__restrict__ dst, const T *__restrict__ src_same,
        const T *__restrict__ src_coarse, int homogeneous, BcCoefs bc,
        const int *__restrict__ active)
 {
    WORK_LOOP(ch) {
-      const FillItem &it = items[ch.patch];
-      if (active && !active[it.prob]) continue;
-      const T *src = it.src_is_coarse ? src_coarse : src_same;
-      const int nx = it.hi[0] - it.lo[0] + 1;
-      const int ny = it.hi[1] - it.lo[1] + 1;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const int lin = ch.begin + t;
+         int lin;
+         const FillItem &it = items[chunk_item(ch, prefix, t, lin)];
+         if (active && !active[it.prob]) continue;
+         const T *src = it.src_is_coarse ? src_coarse : src_same;
+         const int nx = it.hi[0] - it.lo[0] + 1;
+         const int ny = it.hi[1] - it.lo[1] + 1;
          const int i = it.lo[0] + lin % nx;
          const int r = lin / nx;
          const int j = it.lo[1] + r % ny;
@@ -371,6 +371,67 @@ k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, 
    }
 }
 
+// Fluxes of every face of the level, one thread per cell: the lower face of
+// each axis, and the upper one as well for the last cell of a row -- the
+// arithmetic of k_flux with one cell decode for all axes.
+template <int DIM, bool DVAR, class TU>
+__global__ void __launch_bounds__(kThreads)
+k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
+             const TU *__restrict__ u, const double *__restrict__ dside, double dconst,
+             const unsigned char *__restrict__ cfmask, EwingWeights w,
+             const int *ratio_to_coarser, double *__restrict__ flux,
+             const int *__restrict__ run)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      if (run && !run[p.prob]) continue;
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const bool has_cf = (p.flags & 1) != 0;
+      const long long st[3] = {1, nx + 2, (long long)(nx + 2) * (ny + 2)};
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         const int cc[3] = {i, j, k};
+         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+#pragma unroll
+         for (int a = 0; a < DIM; ++a) {
+            const double dai = 1. / p.dx[a];
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+               if (s == 1 && cc[a] != p.hi[a]) break;
+               int fc[3] = {i, j, k};
+               fc[a] += s;
+               const long long si = sidx(p, a, fc[0], fc[1], fc[2]);
+               const double d = DVAR ? dside[si] : dconst;
+               const long long cp = s ? c + st[a] : c;
+               double fl = dai * d * ((double)u[cp] - (double)u[cp - st[a]]);
+               if (has_cf && (s == 1 || cc[a] == p.lo[a])) {
+                  const long long o = oidx(p, a, s, i, j, k);
+                  if (cfmask[o]) {
+                     int mq[3] = {i, j, k};
+                     for (int tt = 0; tt < DIM; ++tt) {
+                        if (tt == a) continue;
+                        const int rr = ratio_to_coarser[tt];
+                        const int base = coarsen_index(cc[tt], rr) * rr;
+                        mq[tt] = base + (rr - (cc[tt] - base) - 1);
+                     }
+                     const double uc = (double)u[c];
+                     const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
+                     if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
+                     else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
+                  }
+               }
+               flux[si] = fl;
+            }
+         }
+      }
+   }
+}
+
 // ---------------------------------------------------------------------------
 // residual from side fluxes (compres{var,con}sca{2,3}d) and outer-side save
 // ---------------------------------------------------------------------------
@@ -525,31 +586,31 @@ k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict_
 
 __global__ void __launch_bounds__(kThreads)
 k_flux_coarsen(const FluxCoarsenItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
-               const PatchDesc *__restrict__ fine, const PatchDesc *__restrict__ coarse,
-               const double *__restrict__ oflux_fine, double *__restrict__ flux_coarse,
-               const int *__restrict__ run)
+               const int *__restrict__ prefix, const PatchDesc *__restrict__ fine,
+               const PatchDesc *__restrict__ coarse, const double *__restrict__ oflux_fine,
+               double *__restrict__ flux_coarse, const int *__restrict__ run)
 {
    WORK_LOOP(ch) {
-      const FluxCoarsenItem it = items[ch.patch];
-      if (run && !run[it.prob]) continue;
-      const PatchDesc fp = fine[it.fine_patch];
-      const PatchDesc cp = coarse[it.coarse_patch];
-      const int a = it.axis;
-      const int nx = it.hi[0] - it.lo[0] + 1;
-      const int ny = it.hi[1] - it.lo[1] + 1;
-      // refinement ratios along the tangential axes come in the chunk's aux word
-      double wf, wc;
-      if (it.t1 < 0) {
-         wf = fp.dx[it.t0];
-         wc = cp.dx[it.t0];
-      } else {
-         wf = fp.dx[it.t0] * fp.dx[it.t1];
-         wc = cp.dx[it.t0] * cp.dx[it.t1];
-      }
-      const int r0 = ch.aux & 0xff;
-      const int r1 = (ch.aux >> 8) & 0xff;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const int lin = ch.begin + t;
+         int lin;
+         const FluxCoarsenItem &it = items[chunk_item(ch, prefix, t, lin)];
+         if (run && !run[it.prob]) continue;
+         const PatchDesc &fp = fine[it.fine_patch];
+         const PatchDesc &cp = coarse[it.coarse_patch];
+         const int a = it.axis;
+         const int nx = it.hi[0] - it.lo[0] + 1;
+         const int ny = it.hi[1] - it.lo[1] + 1;
+         double wf, wc;
+         if (it.t1 < 0) {
+            wf = fp.dx[it.t0];
+            wc = cp.dx[it.t0];
+         } else {
+            wf = fp.dx[it.t0] * fp.dx[it.t1];
+            wc = cp.dx[it.t0] * cp.dx[it.t1];
+         }
+         // refinement ratios along the tangential axes
+         const int r0 = it.ratio & 0xff;
+         const int r1 = (it.ratio >> 8) & 0xff;
          int c[3];
          c[0] = it.lo[0] + lin % nx;
          const int rr = lin / nx;
@@ -590,30 +651,31 @@ k_flux_coarsen(const FluxCoarsenItem *__restrict__ items, const Chunk *__restric
 template <int DIM>
 __global__ void __launch_bounds__(kThreads)
 k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
-           const PatchDesc *__restrict__ fine, const PatchDesc *__restrict__ coarse,
-           const double *__restrict__ src, int src_g, double *__restrict__ dst,
-           int dst_g, const int *__restrict__ run)
+           const int *__restrict__ prefix, const PatchDesc *__restrict__ fine,
+           const PatchDesc *__restrict__ coarse, const double *__restrict__ src, int src_g,
+           double *__restrict__ dst, int dst_g, const int *__restrict__ run)
 {
    WORK_LOOP(ch) {
-      const RestrictItem it = items[ch.patch];
-      if (run && !run[it.prob]) continue;
-      const PatchDesc fp = fine[it.fine_patch];
-      const PatchDesc cp = coarse[it.coarse_patch];
-      const int nx = it.hi[0] - it.lo[0] + 1;
-      const int ny = it.hi[1] - it.lo[1] + 1;
-      const int r0 = ch.aux & 0xff, r1 = (ch.aux >> 8) & 0xff, r2 = (ch.aux >> 16) & 0xff;
-      double dVf, dVc;
-      if (DIM == 2) {
-         dVf = fp.dx[0] * fp.dx[1];
-         dVc = cp.dx[0] * cp.dx[1];
-      } else {
-         dVf = fp.dx[0] * fp.dx[1] * fp.dx[2];
-         dVc = cp.dx[0] * cp.dx[1] * cp.dx[2];
-      }
-      const long long soff = src_g ? fp.off1 : fp.off0;
-      const long long doff = dst_g ? cp.off1 : cp.off0;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const int lin = ch.begin + t;
+         int lin;
+         const RestrictItem &it = items[chunk_item(ch, prefix, t, lin)];
+         if (run && !run[it.prob]) continue;
+         const PatchDesc &fp = fine[it.fine_patch];
+         const PatchDesc &cp = coarse[it.coarse_patch];
+         const int nx = it.hi[0] - it.lo[0] + 1;
+         const int ny = it.hi[1] - it.lo[1] + 1;
+         const int r0 = it.ratio & 0xff, r1 = (it.ratio >> 8) & 0xff,
+                   r2 = (it.ratio >> 16) & 0xff;
+         double dVf, dVc;
+         if (DIM == 2) {
+            dVf = fp.dx[0] * fp.dx[1];
+            dVc = cp.dx[0] * cp.dx[1];
+         } else {
+            dVf = fp.dx[0] * fp.dx[1] * fp.dx[2];
+            dVc = cp.dx[0] * cp.dx[1] * cp.dx[2];
+         }
+         const long long soff = src_g ? fp.off1 : fp.off0;
+         const long long doff = dst_g ? cp.off1 : cp.off0;
          const int i = it.lo[0] + lin % nx;
          const int rr = lin / nx;
          const int j = it.lo[1] + rr % ny;
@@ -640,21 +702,21 @@ k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chu
 template <int DIM, class T>
 __global__ void __launch_bounds__(kThreads)
 k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
-              const PatchDesc *__restrict__ fine, const T *__restrict__ tmp,
-              const double *__restrict__ dxc_prob, int ratio0, int ratio1, int ratio2,
-              T *__restrict__ e, const int *__restrict__ run)
+              const int *__restrict__ prefix, const PatchDesc *__restrict__ fine,
+              const T *__restrict__ tmp, const double *__restrict__ dxc_prob, int ratio0,
+              int ratio1, int ratio2, T *__restrict__ e, const int *__restrict__ run)
 {
+   const T half = (T)0.5, one = (T)1;
+   const int r[3] = {ratio0, ratio1, ratio2};
    WORK_LOOP(ch) {
-      const ProlongItem it = items[ch.patch];
-      if (run && !run[it.prob]) continue;
-      const PatchDesc p = fine[it.fine_patch];
-      const int nx = p.hi[0] - p.lo[0] + 1;
-      const int ny = p.hi[1] - p.lo[1] + 1;
-      const T half = (T)0.5, one = (T)1;
-      const double *dxc = dxc_prob + 3 * it.prob;
-      const int r[3] = {ratio0, ratio1, ratio2};
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const int lin = ch.begin + t;
+         int lin;
+         const ProlongItem &it = items[chunk_item(ch, prefix, t, lin)];
+         if (run && !run[it.prob]) continue;
+         const PatchDesc &p = fine[it.fine_patch];
+         const int nx = p.hi[0] - p.lo[0] + 1;
+         const int ny = p.hi[1] - p.lo[1] + 1;
+         const double *dxc = dxc_prob + 3 * it.prob;
          const int i = p.lo[0] + lin % nx;
          const int rr = lin / nx;
          const int j = p.lo[1] + rr % ny;
@@ -1069,12 +1131,12 @@ void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *a
 
 template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
-                 T *dst, const T *src_same, const T *src_coarse, int homogeneous,
-                 const BcCoefs &bc, const int *active)
+                 const int *prefix, T *dst, const T *src_same, const T *src_coarse,
+                 int homogeneous, const BcCoefs &bc, const int *active)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_fill<T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, dst, src_same, src_coarse,
+   k_fill<T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, dst, src_same, src_coarse,
                                           homogeneous, bc, active);
 }
 
@@ -1183,6 +1245,32 @@ void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
 }
 
 template <class TU>
+void launch_flux_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                       const PatchDesc *patches, const Chunk *cell_chunks, const TU *u,
+                       const double *dside, const unsigned char *cfmask, const double *tranwt,
+                       const double *longwt, const int *ratio_dev, double *flux, const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   EwingWeights w;
+   for (int a = 0; a < 3; ++a) {
+      w.tranwt[a] = tranwt[a];
+      w.longwt[a] = longwt[a];
+   }
+#define FC(D, V)                                                                            \
+   k_flux_cells<D, V, TU><<<work_grid(nchunks), kThreads, 0, s>>>(                          \
+      patches, cell_chunks, nchunks, u, dside, spec.d_const, cfmask, w, ratio_dev, flux, run)
+   if (dim == 2) {
+      if (spec.d_variable) FC(2, true);
+      else FC(2, false);
+   } else {
+      if (spec.d_variable) FC(3, true);
+      else FC(3, false);
+   }
+#undef FC
+}
+
+template <class TU>
 void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                            const PatchDesc *patches, const Chunk *chunks, const TU *u,
                            const double *dside, const unsigned char *cfmask,
@@ -1249,42 +1337,44 @@ void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchun
 }
 
 void launch_flux_coarsen(cudaStream_t s, const FluxCoarsenItem *items, const Chunk *chunks,
-                         int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
-                         const double *oflux_fine, double *flux_coarse, const int *run)
+                         int nchunks, const int *prefix, const PatchDesc *fine,
+                         const PatchDesc *coarse, const double *oflux_fine, double *flux_coarse,
+                         const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_flux_coarsen<<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, coarse, oflux_fine,
-                                               flux_coarse, run);
+   k_flux_coarsen<<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
+                                                          coarse, oflux_fine, flux_coarse, run);
 }
 
 void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const Chunk *chunks,
-                     int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
-                     const double *src, int src_g, double *dst, int dst_g, const int *run)
+                     int nchunks, const int *prefix, const PatchDesc *fine,
+                     const PatchDesc *coarse, const double *src, int src_g, double *dst,
+                     int dst_g, const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_restrict<2><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, coarse, src, src_g, dst,
-                                                 dst_g, run);
+      k_restrict<2><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
+                                                            coarse, src, src_g, dst, dst_g, run);
    else
-      k_restrict<3><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, coarse, src, src_g, dst,
-                                                 dst_g, run);
+      k_restrict<3><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
+                                                            coarse, src, src_g, dst, dst_g, run);
 }
 
 template <class T>
 void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const Chunk *chunks,
-                        int nchunks, const PatchDesc *fine, const T *tmp,
+                        int nchunks, const int *prefix, const PatchDesc *fine, const T *tmp,
                         const double *dxc_prob, const int *ratio, T *e, const int *run)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_prolong_add<2, T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, tmp, dxc_prob,
-                                                       ratio[0], ratio[1], ratio[2], e, run);
+      k_prolong_add<2, T><<<work_grid(nchunks), kThreads, 0, s>>>(
+         items, chunks, nchunks, prefix, fine, tmp, dxc_prob, ratio[0], ratio[1], ratio[2], e, run);
    else
-      k_prolong_add<3, T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, fine, tmp, dxc_prob,
-                                                       ratio[0], ratio[1], ratio[2], e, run);
+      k_prolong_add<3, T><<<work_grid(nchunks), kThreads, 0, s>>>(
+         items, chunks, nchunks, prefix, fine, tmp, dxc_prob, ratio[0], ratio[1], ratio[2], e, run);
 }
 
 template <class T>
@@ -1428,7 +1518,7 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
 // explicit instantiations: FP64 (reference arithmetic) and FP32 (mixed
 // precision smoothing and transfer of the error)
 #define INST_T(T)                                                                          \
-   template void launch_fill<T>(cudaStream_t, const FillItem *, const Chunk *, int, T *,    \
+   template void launch_fill<T>(cudaStream_t, const FillItem *, const Chunk *, int, const int *, T *,    \
                                 const T *, const T *, int, const BcCoefs &, const int *);   \
    template void launch_cf_flux<T>(cudaStream_t, const CfFace *, int, const PatchDesc *,    \
                                    const T *, const T *, int, double, const double *,       \
@@ -1446,13 +1536,18 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
                                     const PatchDesc *, const Chunk *, const T *,            \
                                     const double *, const double *, const double *,         \
                                     double *, double *, const int *);                       \
+   template void launch_flux_cells<T>(cudaStream_t, int, const PoissonSpec &, int,          \
+                                      const PatchDesc *, const Chunk *, const T *,          \
+                                      const double *, const unsigned char *,                \
+                                      const double *, const double *, const int *, double *, \
+                                      const int *);                                          \
    template void launch_residual_fused<T>(                                                  \
       cudaStream_t, int, const PoissonSpec &, int, const PatchDesc *, const Chunk *, const T *, \
       const double *, const unsigned char *, const double *, const double *, const int *,   \
       const unsigned char *, const double *, const double *, const double *, double *,      \
       double *, const int *);                                                               \
    template void launch_prolong_add<T>(cudaStream_t, int, const ProlongItem *,              \
-                                       const Chunk *, int, const PatchDesc *, const T *,    \
+                                       const Chunk *, int, const int *, const PatchDesc *, const T *, \
                                        const double *, const int *, T *, const int *);      \
    template void launch_add_interior<T>(cudaStream_t, int, int, const PatchDesc *,          \
                                         const Chunk *, double *, const T *, const int *);

@@ -32,7 +32,7 @@ void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *a
 
 template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
-                 T *dst, const T *src_same, const T *src_coarse, int homogeneous,
+                 const int *prefix, T *dst, const T *src_same, const T *src_coarse, int homogeneous,
                  const BcCoefs &bc, const int *active);
 
 template <class T>
@@ -61,6 +61,13 @@ void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchun
                      const double *f, const double *flux, const double *cfield,
                      double *res, double *oflux, const int *run);
 
+// All face fluxes of a level from its cell chunks (one decode per cell).
+template <class TU>
+void launch_flux_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
+                       const PatchDesc *patches, const Chunk *cell_chunks, const TU *u,
+                       const double *dside, const unsigned char *cfmask, const double *tranwt,
+                       const double *longwt, const int *ratio_dev, double *flux, const int *run);
+
 // Fluxes on the fly + residual (+ outer-side fluxes): k_flux and k_residual
 // in one pass; fcmask marks faces whose flux is the coarsened finer-level
 // flux already stored in fcflux (NULL when the level has no finer level).
@@ -72,17 +79,21 @@ void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int
                            const unsigned char *fcmask, const double *fcflux, const double *f,
                            const double *cfield, double *res, double *oflux, const int *run);
 
+// Transaction-list launchers take the list's item prefix sums (packed
+// chunks, see Chunk).
 void launch_flux_coarsen(cudaStream_t s, const FluxCoarsenItem *items, const Chunk *chunks,
-                         int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
-                         const double *oflux_fine, double *flux_coarse, const int *run);
+                         int nchunks, const int *prefix, const PatchDesc *fine,
+                         const PatchDesc *coarse, const double *oflux_fine, double *flux_coarse,
+                         const int *run);
 
 void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const Chunk *chunks,
-                     int nchunks, const PatchDesc *fine, const PatchDesc *coarse,
-                     const double *src, int src_g, double *dst, int dst_g, const int *run);
+                     int nchunks, const int *prefix, const PatchDesc *fine,
+                     const PatchDesc *coarse, const double *src, int src_g, double *dst,
+                     int dst_g, const int *run);
 
 template <class T>
 void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const Chunk *chunks,
-                        int nchunks, const PatchDesc *fine, const T *tmp,
+                        int nchunks, const int *prefix, const PatchDesc *fine, const T *tmp,
                         const double *dxc_prob, const int *ratio, T *e, const int *run);
 
 template <class T>

@@ -68,6 +68,8 @@ def load_library(build_if_missing=True):
         "fac_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_fused": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_staged": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_learned": (ctypes.c_int, [vp, vp, ctypes.c_int]),
+        "fac_learned_samples": (ctypes.c_int, [vp, ctypes.c_int, vp, dp]),
         "fac_set_fused_residual": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_stage_budget": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
@@ -337,6 +339,20 @@ class FacContext:
 
     def set_fused_residual(self, on=True):
         _check(load_library().fac_set_fused_residual(self.h, int(on)))
+
+    def set_learned(self, net, level):
+        """Apply the learned correction of `net` (a CNN, or None) on `level`
+        after every cycle of solve()."""
+        _check(load_library().fac_set_learned(self.h, net.h if net is not None else None,
+                                              int(level)))
+        self._net = net  # keep the network alive while the context uses it
+
+    def learned_samples(self, level, x_ptr, npatch):
+        """Network inputs for the current residual of `level` into the device
+        array at x_ptr (npatch * CNN_BOX^3 FP32); returns the patch scales."""
+        scale = np.zeros(max(1, npatch))
+        _check(load_library().fac_learned_samples(self.h, int(level), x_ptr, _dp(scale)))
+        return scale[:npatch]
 
     def set_staged(self, on=True):
         _check(load_library().fac_set_staged(self.h, int(on)))
