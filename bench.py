@@ -277,6 +277,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # autotuner: stage size of the staged smoother, timed on this workload
+    tuned, tune_ms = ctx.autotune()
     for _ in range(args.warmup):
         conv, its, res = step(ctx)
     barrier()
@@ -330,6 +332,7 @@ def main():
     k = MG_LEVELS[args.config]
     if args.precision == "mixed":
         c64 = fac.FacContext(mg, params=PARAMS_MG, device=local_rank, precision="fp64")
+        c64.autotune()
         step(c64)
         c64.profile(True)
         c64.timer_start()
@@ -405,6 +408,8 @@ def main():
                         "2/2 red-black sweeps, Ewing, linear refine",
             "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": f"problem shards x{world}",
+            "autotuned_stage_bytes": int(tuned),
+            "autotune_sweep_ms": [round(float(x), 3) for x in tune_ms],
         },
         "converged": int(np.sum(conv)),
         "cycles_max": int(np.max(its)),
@@ -413,9 +418,9 @@ def main():
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "roofline": {
-            "kernel": ("k_rbgs<float> (red-black colour pass, fused flux, FP32)"
-                       if args.precision == "mixed" else
-                       "k_rbgs<double> (red-black colour pass, fused flux)"),
+            "kernel": ("k_rb_staged<3,D var,float> (red-black colour pass on TMA-staged "
+                       "units, FP32)" if args.precision == "mixed" else
+                       "k_rb_staged<3,D var,double> (red-black colour pass on TMA-staged units)"),
             "bound": "hbm",
             "achieved": round(achieved, 1),
             "peak": peak,

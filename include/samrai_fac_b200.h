@@ -134,6 +134,12 @@ int fac_set_fused_residual(fac_ctx *ctx, int on);
  * initialised.  fac_autotune picks it by timing. */
 int fac_set_stage_budget(fac_ctx *ctx, int bytes);
 
+/* Autotuner: times one red-black sweep of every smoothed level for stage
+ * sizes of 12, 16, 24, 32 and 48 KiB (best of three, CUDA events) and keeps
+ * the fastest; chosen and ms_per_candidate (5 entries) may be NULL.  Uses
+ * the smoothing fields as scratch: call it before fac_solve. */
+int fac_autotune(fac_ctx *ctx, int *chosen, double *ms_per_candidate);
+
 /* 1 (default): fac_solve captures one FAC cycle (V-cycle, correction,
  * restriction, composite residual, norm kernels) into a CUDA graph on first
  * use and replays it every cycle; converged problems are skipped on the

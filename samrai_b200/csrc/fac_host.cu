@@ -2504,6 +2504,62 @@ int fac_set_fused_residual(fac_ctx *ctx, int on)
    });
 }
 
+// Autotuner of the staged pass: rebuild the units for each candidate stage
+// size, time a red-black sweep of every staged level (CUDA events, best of
+// three), keep the fastest.  Uses the smoothing fields (E, R or their FP32
+// copies) as scratch, so it belongs before a solve.
+int fac_autotune(fac_ctx *ctx, int *chosen, double *ms_per_candidate)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (ctx->device < 0) throw FacError(FAC_ERR_STATE, "host-only context");
+      static const int cand[] = {12 * 1024, 16 * 1024, 24 * 1024, 32 * 1024, 48 * 1024};
+      const int nc = (int)(sizeof(cand) / sizeof(cand[0]));
+      cudaEvent_t e0, e1;
+      CUDA_CHECK(cudaEventCreate(&e0));
+      CUDA_CHECK(cudaEventCreate(&e1));
+      struct Ev {
+         cudaEvent_t a, b;
+         ~Ev()
+         {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+         }
+      } ev{e0, e1};
+      const bool was_tracing = ctx->tracing, was_prof = ctx->profiling;
+      ctx->tracing = ctx->profiling = false;
+      int best = ctx->stage_budget;
+      float best_ms = 1e30f;
+      for (int k = 0; k < nc; ++k) {
+         if (fac_set_stage_budget(ctx, cand[k]) != FAC_OK)
+            throw FacError(FAC_ERR_CUDA, g_last_error);
+         float t = 1e30f;
+         for (int rep = 0; rep < 3; ++rep) {
+            CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+            for (int ln = 1; ln < ctx->nlev; ++ln) {
+               if (ctx->mixed) smooth32(ctx, ln, 1);
+               else smooth(ctx, FAC_E, FAC_R, ln, 1, -1.0);
+            }
+            CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+            CUDA_CHECK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+            t = std::min(t, ms);
+         }
+         if (ms_per_candidate) ms_per_candidate[k] = t;
+         if (t < best_ms) {
+            best_ms = t;
+            best = cand[k];
+         }
+      }
+      ctx->tracing = was_tracing;
+      ctx->profiling = was_prof;
+      if (fac_set_stage_budget(ctx, best) != FAC_OK)
+         throw FacError(FAC_ERR_CUDA, g_last_error);
+      if (chosen) *chosen = best;
+   });
+}
+
 int fac_set_staged(fac_ctx *ctx, int on)
 {
    return guarded([&] {

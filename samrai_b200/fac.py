@@ -72,6 +72,7 @@ def load_library(build_if_missing=True):
         "fac_learned_samples": (ctypes.c_int, [vp, ctypes.c_int, vp, dp]),
         "fac_set_fused_residual": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_stage_budget": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), dp]),
         "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
         "fac_side_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
         "fac_oside_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
@@ -333,6 +334,14 @@ class FacContext:
 
     def synchronize(self):
         _check(load_library().fac_synchronize(self.h))
+
+    def autotune(self):
+        """Pick the staged pass's stage size by timing (before a solve);
+        returns (chosen bytes, ms per candidate)."""
+        chosen = ctypes.c_int(0)
+        ms = np.zeros(5)
+        _check(load_library().fac_autotune(self.h, ctypes.byref(chosen), _dp(ms)))
+        return chosen.value, ms
 
     def set_stage_budget(self, nbytes):
         _check(load_library().fac_set_stage_budget(self.h, int(nbytes)))

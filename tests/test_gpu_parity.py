@@ -300,3 +300,26 @@ def test_fused_residual_matches_flux_arrays(case, precision, require_gpu):
     assert np.array_equal(out[0][1], out[1][1])
     for a, b in zip(out[0][2], out[1][2]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_results(require_gpu):
+    """The autotuner only changes how patches are cut into staged units:
+    the solve after it gives the same bits as with the default units."""
+    probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (61, 62)]
+    prm = dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=6)
+    out = []
+    for tune in (True, False):
+        g = fac.FacContext(probs, params=prm, precision="mixed")
+        if tune:
+            chosen, ms = g.autotune()
+            assert chosen in (12288, 16384, 24576, 32768, 49152)
+            assert np.all(ms > 0)
+        g.zero(U)
+        conv, its, res = g.solve()
+        out.append((its.copy(), res.copy(), [g.download(U, i, ln) for i in range(2)
+                                             for ln in range(probs[0].nlev)]))
+        g.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for a, b in zip(out[0][2], out[1][2]):
+        assert np.array_equal(a, b)
