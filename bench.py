@@ -49,6 +49,8 @@ PARAMS = dict(max_cycles=100, residual_tol=1e-300, relative_residual_tol=1e-10,
 # sweeps on the coarsest extension level.
 PARAMS_MG = dict(PARAMS, coarse_max_it=20)
 MG_LEVELS = {"c5": 3, "c2": 4, "c1": 3, "c3": 3}
+# headline: FGMRES(KRYLOV) with one FAC cycle as the flexible preconditioner
+KRYLOV = 20
 
 
 def make_workload(name, nprob, rank):
@@ -202,6 +204,8 @@ def main():
                     help="precision of the headline (multigrid-extended) variant")
     ap.add_argument("--smoother-only", type=int, default=0, metavar="SWEEPS",
                     help="only run SWEEPS red-black sweeps on the largest level (for ncu)")
+    ap.add_argument("--krylov", type=int, default=KRYLOV,
+                    help="FGMRES restart length of the headline solve (0: stationary FAC)")
     ap.add_argument("--cycles", type=int, default=0, metavar="N",
                     help="only run one solve of the headline variant stopped after N cycles "
                          "(a short, fixed launch sequence for kernel captures)")
@@ -228,6 +232,7 @@ def main():
     probs, desc = make_workload(args.config, args.nprob, rank)
     mg = [configs.extend_hierarchy(p, k=MG_LEVELS[args.config]) for p in probs]
     ctx = fac.FacContext(mg, params=PARAMS_MG, device=local_rank, precision=args.precision)
+    ctx.set_krylov(args.krylov)
     cells = sum(p.num_cells() for p in probs)
     npatch = sum(p.num_patches() for p in probs)
     if args.smoother_only:
@@ -327,11 +332,24 @@ def main():
     barrier()
     e2e_ms = max_over_ranks((time.perf_counter() - t) * 1e3 / e2e_steps)
 
+    # the same context without the Krylov acceleration (stationary FAC cycles)
+    fac_only = None
+    if args.krylov > 0:
+        ctx.set_krylov(0)
+        step(ctx)
+        ctx.timer_start()
+        conv_s, its_s, _ = step(ctx)
+        ms_s = ctx.timer_stop()
+        ctx.set_krylov(args.krylov)
+        fac_only = {"ms": round(max_over_ranks(ms_s), 1), "converged": int(np.sum(conv_s)),
+                    "cycles_max": int(np.max(its_s)), "cycles_mean": float(np.mean(its_s))}
+
     # the same multigrid-extended FAC all in FP64 (one timed solve)
     fp64_mg = None
     k = MG_LEVELS[args.config]
     if args.precision == "mixed":
         c64 = fac.FacContext(mg, params=PARAMS_MG, device=local_rank, precision="fp64")
+        c64.set_krylov(args.krylov)
         c64.autotune()
         step(c64)
         c64.profile(True)
@@ -399,8 +417,9 @@ def main():
         "data": "synthetic",
         "config": {
             "workload": desc,
-            "variant": (f"{args.precision} FAC on the hierarchy extended by {k} fully covered "
-                        f"coarser levels (multigrid coarsest solve)"),
+            "variant": ((f"FGMRES({args.krylov}) preconditioned by one " if args.krylov else "")
+                        + f"{args.precision} FAC cycle on the hierarchy extended by {k} fully "
+                        f"covered coarser levels (multigrid coarsest solve)"),
             "problems_per_gpu": len(probs),
             "cells_per_gpu": cells,
             "patches_per_gpu": npatch,
@@ -436,6 +455,7 @@ def main():
                        "gbs": round(fl_bytes / max(fl_ms, 1e-9) / 1e6, 1),
                        "share_of_step": round(fl_ms / max(prof_ms, 1e-9), 4)},
         "fp64_multigrid": fp64_mg,
+        "stationary_fac": fac_only,
         "plain_fp64": plain,
         "clocks": clocks,
     }

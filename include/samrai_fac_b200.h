@@ -140,6 +140,20 @@ int fac_set_stage_budget(fac_ctx *ctx, int bytes);
  * the smoothing fields as scratch: call it before fac_solve. */
 int fac_autotune(fac_ctx *ctx, int *chosen, double *ms_per_candidate);
 
+/* FGMRES(restart) with one FAC cycle (FP32 in the mixed precision) as the
+ * flexible right preconditioner, every problem with its own Krylov space.
+ * Inner products are the weighted sums of fac_rms_norm, the stopping rule
+ * that of fac_solve (weighted RMS composite residual <= max(residual_tol,
+ * relative_residual_tol * ||f||)); max_cycles bounds the preconditioner
+ * applications, which iterations reports.  Same outputs as fac_solve.
+ * Holds 2*restart+1 composite vectors per context.  No counterpart in the
+ * reference (FACPreconditioner is the stationary iteration). */
+int fac_solve_fgmres(fac_ctx *ctx, int restart, int *converged, int *iterations,
+                     double *residual);
+/* restart > 0: fac_solve and fac_solve_host run fac_solve_fgmres(restart);
+ * 0 (default): the reference's stationary FAC iteration. */
+int fac_set_krylov(fac_ctx *ctx, int restart);
+
 /* 1 (default): fac_solve captures one FAC cycle (V-cycle, correction,
  * restriction, composite residual, norm kernels) into a CUDA graph on first
  * use and replays it every cycle; converged problems are skipped on the

@@ -274,6 +274,9 @@ struct HostProblem {
    std::vector<Box> boxes[kMaxLevels];
 };
 
+// internal field id: the all-zero ghost-0 field
+constexpr int kFieldZero = 100;
+
 struct LevelState {
    int npatch = 0;
    std::vector<PatchDesc> hp;
@@ -290,6 +293,10 @@ struct LevelState {
 
    DevArray<PatchDesc> d_patches;
    DevArray<double> u, e, f, r, tr, w, c, d, flux, oflux, cfflux;
+   DevArray<double> zero;  // all-zero ghost-0 field (right-hand side of A x)
+   // Krylov workspace (fac_solve_fgmres): V_0..V_m then Z_0..Z_{m-1}, n0
+   // apart, and per-chunk partial sums of the multi-dot products
+   DevArray<double> kry, kry_partial;
    // FP32 copies for the mixed-precision cycle (error, smoother rhs, D, C,
    // Ewing fluxes, coarse interpolation arrays)
    DevArray<float> e32, r32, d32, c32, cfflux32, tmp32;
@@ -366,6 +373,13 @@ struct fac_ctx {
    DevArray<int> kerr;       // set by kernels whose bounded waits ran out
    bool capturing = false;   // inside stream capture: no host synchronisation
    cudaGraphExec_t cycle_exec = nullptr;
+   // captured FGMRES pieces: FAC cycle on R into E (the preconditioner) and
+   // the composite operator on E into TR; our kernels in each graph
+   cudaGraphExec_t prec_exec = nullptr, apply_exec = nullptr;
+   long long prec_launches = 0, apply_launches = 0;
+   int kry_m = 0;
+   DevArray<double> kry_dots, kry_coef, kry_a;
+   int krylov = 0;  // > 0: fac_solve runs FGMRES(krylov) around the FAC cycle
    // learned correction after every cycle (fac_set_learned)
    fac_cnn *cnn = nullptr;
    int learned_level = -1;
@@ -419,6 +433,10 @@ struct fac_ctx {
    {
       if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
       cycle_exec = nullptr;
+      if (prec_exec) cudaGraphExecDestroy(prec_exec);
+      if (apply_exec) cudaGraphExecDestroy(apply_exec);
+      prec_exec = apply_exec = nullptr;
+      prec_launches = apply_launches = 0;
       for (const ProfRec &r : graph_prof) {
          cudaEventDestroy(r.a);
          cudaEventDestroy(r.b);
@@ -534,6 +552,7 @@ void harvest_graph_profile(fac_ctx *c)
 double *field_ptr(LevelState &L, int fid)
 {
    switch (fid) {
+      case kFieldZero: return L.zero.p;
       case FAC_U: return L.u.p;
       case FAC_F: return L.f.p;
       case FAC_E: return L.e.p;
@@ -547,6 +566,7 @@ double *field_ptr(LevelState &L, int fid)
 
 int field_ghost(int fid)
 {
+   if (fid == kFieldZero) return 0;
    if (fid < 0 || fid > FAC_C) throw FacError(FAC_ERR_ARG, "bad field id");
    return (fid == FAC_U || fid == FAC_E) ? 1 : 0;
 }
@@ -1678,6 +1698,8 @@ void initialize(fac_ctx *c)
       L.flux.alloc(std::max<long long>(1, L.ns));
       L.oflux.alloc(std::max<long long>(1, L.no));
       L.cfflux.alloc(std::max<long long>(1, L.no));
+      L.zero.alloc(n0);
+      if (!g_dry) CUDA_CHECK(cudaMemsetAsync(L.zero.p, 0, n0 * sizeof(double), c->stream));
       if (!g_dry)
          for (auto *b : {&L.u, &L.e, &L.f, &L.r, &L.tr, &L.w, &L.c, &L.d, &L.flux, &L.oflux,
                          &L.cfflux})
@@ -2174,8 +2196,14 @@ void learned_step(fac_ctx *c)
 
 // FACPreconditioner::solveSystem (FACPreconditioner.C:277-452) inside
 // CellPoissonFACSolver::solveSystem (CellPoissonFACSolver.C:310-352).
+void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *residual);
+
 void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
 {
+   if (c->krylov > 0) {
+      fgmres_solve(c, c->krylov, converged, iterations, residual);
+      return;
+   }
    const int np = nprob(c);
    std::vector<int> act(np, 1);
    c->host_active = act;
@@ -2285,6 +2313,352 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
       }
       if (act != c->host_active) set_active(c, act);
       c->host_active = act;
+   }
+   c->host_active.assign(np, 1);
+   set_active(c, c->host_active);
+   dirichlet(c, true);
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   for (int p = 0; p < np; ++p) {
+      if (converged) converged[p] = res[p] < eff[p];
+      if (iterations) iterations[p] = its[p];
+      if (residual) residual[p] = res[p];
+   }
+}
+
+// ---------------------------------------------------------------------------
+// FGMRES(m) with one FAC cycle as the (flexible) right preconditioner, for
+// every problem of the context at once: each problem has its own Krylov
+// basis, Hessenberg matrix and Givens rotations; the level operations run
+// on all problems that are still iterating.  Inner products are the
+// control-volume-weighted sums of the RMS norm (weights 0 under finer
+// levels), so the stopping test is FACPreconditioner's: weighted RMS
+// residual <= max(residual_tol, relative_residual_tol * ||f||).  The
+// preconditioner (a FAC cycle, FP32 in the mixed precision) changes from
+// one application to the next only through its arithmetic, which the
+// flexible variant allows for.  The composite operator is the residual of
+// the error equation with a zero right-hand side (fills with the coarser
+// level, Ewing fluxes, flux coarsening, restriction of finer values).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+double *kry_vec(fac_ctx *c, int ln, int slot)
+{
+   return c->L[ln].kry.p + (size_t)slot * (size_t)std::max<long long>(1, c->L[ln].n0);
+}
+
+void kry_alloc(fac_ctx *c, int m)
+{
+   if (c->kry_m == m) return;
+   const int np = nprob(c);
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      L.kry.alloc((size_t)(2 * m + 1) * (size_t)std::max<long long>(1, L.n0));
+      L.kry_partial.alloc((size_t)std::max<size_t>(1, L.cell_chunks.size()) * (m + 1));
+      // finite contents: slots a problem did not reach enter x += Z y with y = 0
+      CUDA_CHECK(cudaMemsetAsync(L.kry.p, 0, L.kry.n * sizeof(double), c->stream));
+   }
+   c->kry_dots.alloc((size_t)np * (m + 1));
+   c->kry_coef.alloc((size_t)np * (m + 1));
+   c->kry_a.alloc(np);
+   c->kry_m = m;
+}
+
+// out[p*K + i] = <x, V_i> (weighted) over all levels, for i < K
+void kry_dots(fac_ctx *c, int xslot, int vslot, int K, std::vector<double> &out)
+{
+   const int np = nprob(c);
+   CUDA_CHECK(cudaMemsetAsync(c->kry_dots.p, 0, (size_t)np * K * sizeof(double), c->stream));
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      launch_multidot(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                      L.d_cell_chunks.p, L.w.p, kry_vec(c, ln, xslot), kry_vec(c, ln, vslot),
+                      std::max<long long>(1, L.n0), K, L.kry_partial.p,
+                      L.d_prob_cell_chunk_begin.p, np, c->active.p, c->kry_dots.p);
+   }
+   out.resize((size_t)np * K);
+   CUDA_CHECK(cudaMemcpyAsync(out.data(), c->kry_dots.p, (size_t)np * K * sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+}
+
+// V_x = a[p] V_x + sum_i coef[p*K+i] V_{vslot+i}
+void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot, int K,
+                 const std::vector<double> &coef)
+{
+   const int np = nprob(c);
+   CUDA_CHECK(cudaMemcpyAsync(c->kry_a.p, a.data(), np * sizeof(double), cudaMemcpyHostToDevice,
+                              c->stream));
+   if (K > 0)
+      CUDA_CHECK(cudaMemcpyAsync(c->kry_coef.p, coef.data(), (size_t)np * K * sizeof(double),
+                                 cudaMemcpyHostToDevice, c->stream));
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      launch_combine(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                     L.d_cell_chunks.p, kry_vec(c, ln, xslot), c->kry_a.p,
+                     K > 0 ? kry_vec(c, ln, vslot) : nullptr, std::max<long long>(1, L.n0), K,
+                     c->kry_coef.p);
+   }
+}
+
+// Run body() through a CUDA graph captured on first use (eager when graphs
+// are off or the context traces / profiles).
+template <class Body>
+void run_graph(fac_ctx *c, cudaGraphExec_t &exec, long long &launches, Body body)
+{
+   if (!c->use_graph || c->tracing || c->profiling) {
+      body();
+      return;
+   }
+   if (!exec) {
+      cudaGraph_t g = nullptr;
+      const long long n0 = kernel_launch_count();
+      CUDA_CHECK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      c->capturing = true;
+      try {
+         body();
+      } catch (...) {
+         c->capturing = false;
+         cudaStreamEndCapture(c->stream, &g);
+         if (g) cudaGraphDestroy(g);
+         throw;
+      }
+      c->capturing = false;
+      CUDA_CHECK(cudaStreamEndCapture(c->stream, &g));
+      launches = kernel_launch_count() - n0;
+      add_kernel_launches(-launches);
+      cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+         exec = nullptr;
+         throw FacError(FAC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      }
+   }
+   CUDA_CHECK(cudaGraphLaunch(exec, c->stream));
+   add_kernel_launches(launches);
+}
+
+}  // namespace
+
+void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *residual)
+{
+   const int np = nprob(c);
+   if (m < 1 || m > 64) throw FacError(FAC_ERR_ARG, "restart length must be 1..64");
+   kry_alloc(c, m);
+   const int zslot0 = m + 1;
+   std::vector<int> act(np, 1);
+   c->host_active = act;
+   set_active(c, act);
+   dirichlet(c, false);
+   zero_field(c, FAC_E);
+   zero_field(c, FAC_R);
+   std::vector<double> res, fnorm, wsum(np, 0.0);
+   full_composite_residual(c, res);
+   rms_norm(c, FAC_F, fnorm);
+   {
+      // sum of the weights per problem (the RMS norm's denominator)
+      std::vector<double2> acc(np);
+      CUDA_CHECK(cudaMemcpyAsync(acc.data(), c->norm_acc.p, np * sizeof(double2),
+                                 cudaMemcpyDeviceToHost, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      for (int p = 0; p < np; ++p) wsum[p] = acc[p].y;
+   }
+   std::vector<double> eff(np);
+   for (int p = 0; p < np; ++p) {
+      eff[p] = c->residual_tol;
+      if (c->rel_residual_tol >= 0) eff[p] = std::max(eff[p], fnorm[p] * c->rel_residual_tol);
+      c->hist[p].assign(1, res[p]);
+   }
+   if (c->mixed) mixed_prepare(c);
+   std::vector<int> its(np, 0), done(np, 0);
+   for (int p = 0; p < np; ++p)
+      if (!(res[p] > eff[p])) done[p] = 1;
+   auto prec_body = [&]() {
+      zero_field(c, FAC_E);
+      if (c->mixed) {
+         for (int ln = 0; ln < c->nlev; ++ln)
+            CUDA_CHECK(cudaMemsetAsync(c->L[ln].e32.p, 0, c->L[ln].e32.n * sizeof(float),
+                                       c->stream));
+         fac_cycle_mixed(c, c->nlev - 1);
+      } else {
+         fac_cycle_recursive(c, c->nlev - 1);
+      }
+   };
+   auto apply_body = [&]() {
+      // as for u in the solve: finer values restricted onto covered cells
+      // first, then the composite residual level by level
+      const int lmax = c->nlev - 1;
+      for (int ln = lmax - 1; ln >= 0; --ln) restrict_solution(c, FAC_E, ln);
+      comp_residual(c, FAC_TR, FAC_E, kFieldZero, lmax, 1);
+      for (int ln = lmax - 1; ln >= 0; --ln) {
+         restrict_solution(c, FAC_E, ln);
+         comp_residual(c, FAC_TR, FAC_E, kFieldZero, ln, 1);
+         restrict_op(c, FAC_TR, FAC_TR, ln);
+      }
+   };
+   const int H = m + 1;  // Hessenberg rows
+   std::vector<double> h((size_t)np * H * m), cs((size_t)np * m), sn((size_t)np * m),
+      g((size_t)np * H);
+   std::vector<int> kp(np);
+   std::vector<double> dots, coef, a(np);
+   while (true) {
+      for (int p = 0; p < np; ++p) act[p] = !done[p] && its[p] < c->max_cycles;
+      bool any = false;
+      for (int v : act) any = any || v;
+      if (!any) break;
+      set_active(c, act);
+      c->host_active = act;
+      // V_0 = r / beta
+      std::vector<int> cyc = act;
+      for (int ln = 0; ln < c->nlev; ++ln) {
+         LevelState &L = c->L[ln];
+         CUDA_CHECK(cudaMemcpyAsync(kry_vec(c, ln, 0), L.r.p,
+                                    std::max<long long>(1, L.n0) * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+      }
+      std::fill(g.begin(), g.end(), 0.0);
+      std::fill(h.begin(), h.end(), 0.0);
+      for (int p = 0; p < np; ++p) {
+         const double beta = res[p] * std::sqrt(wsum[p]);
+         g[(size_t)p * H] = beta;
+         a[p] = cyc[p] && beta > 0 ? 1.0 / beta : 0.0;
+         kp[p] = 0;
+      }
+      kry_combine(c, 0, a, 0, 0, coef);
+      for (int j = 0; j < m; ++j) {
+         bool live = false;
+         for (int v : act) live = live || v;
+         if (!live) break;
+         // Z_j = M^-1 V_j: one FAC cycle on the residual V_j
+         for (int ln = 0; ln < c->nlev; ++ln) {
+            LevelState &L = c->L[ln];
+            CUDA_CHECK(cudaMemcpyAsync(L.r.p, kry_vec(c, ln, j),
+                                       std::max<long long>(1, L.n0) * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, c->stream));
+         }
+         run_graph(c, c->prec_exec, c->prec_launches, prec_body);
+         for (int ln = 0; ln < c->nlev; ++ln) {
+            LevelState &L = c->L[ln];
+            if (c->mixed)
+               launch_g1_to_g0<float>(c->stream, c->dim, (int)L.cell_chunks.size(),
+                                      L.d_patches.p, L.d_cell_chunks.p, L.e32.p,
+                                      kry_vec(c, ln, zslot0 + j));
+            else
+               launch_g1_to_g0<double>(c->stream, c->dim, (int)L.cell_chunks.size(),
+                                       L.d_patches.p, L.d_cell_chunks.p, L.e.p,
+                                       kry_vec(c, ln, zslot0 + j));
+         }
+         // W = A Z_j = -(0 - A Z_j)
+         zero_field(c, FAC_E);
+         for (int ln = 0; ln < c->nlev; ++ln) {
+            LevelState &L = c->L[ln];
+            launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                            L.d_cell_chunks.p, kry_vec(c, ln, zslot0 + j), L.e.p);
+         }
+         run_graph(c, c->apply_exec, c->apply_launches, apply_body);
+         for (int ln = 0; ln < c->nlev; ++ln) {
+            LevelState &L = c->L[ln];
+            CUDA_CHECK(cudaMemcpyAsync(kry_vec(c, ln, j + 1), L.tr.p,
+                                       std::max<long long>(1, L.n0) * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, c->stream));
+         }
+         // classical Gram-Schmidt twice: W = -TR - sum h_i V_i
+         const int K = j + 1;
+         kry_dots(c, j + 1, 0, K, dots);  // <TR, V_i>
+         coef.assign((size_t)np * K, 0.0);
+         for (int p = 0; p < np; ++p) {
+            a[p] = -1.0;
+            for (int i = 0; i < K; ++i) {
+               const double hi = act[p] ? -dots[(size_t)p * K + i] : 0.0;
+               h[((size_t)p * H + i) * m + j] = hi;
+               coef[(size_t)p * K + i] = -hi;
+            }
+         }
+         kry_combine(c, j + 1, a, 0, K, coef);
+         kry_dots(c, j + 1, 0, K, dots);
+         for (int p = 0; p < np; ++p) {
+            a[p] = 1.0;
+            for (int i = 0; i < K; ++i) {
+               const double d = act[p] ? dots[(size_t)p * K + i] : 0.0;
+               h[((size_t)p * H + i) * m + j] += d;
+               coef[(size_t)p * K + i] = -d;
+            }
+         }
+         kry_combine(c, j + 1, a, 0, K, coef);
+         kry_dots(c, j + 1, j + 1, 1, dots);  // ||W||^2
+         for (int p = 0; p < np; ++p) {
+            if (!act[p]) {
+               a[p] = 0.0;
+               continue;
+            }
+            double *hp = &h[(size_t)p * H * m];
+            const double hn = std::sqrt(std::max(0.0, dots[p]));
+            hp[(size_t)(j + 1) * m + j] = hn;
+            a[p] = hn > 0 ? 1.0 / hn : 0.0;
+            // Givens rotations on column j
+            for (int i = 0; i < j; ++i) {
+               const double x = hp[(size_t)i * m + j], y = hp[(size_t)(i + 1) * m + j];
+               hp[(size_t)i * m + j] = cs[(size_t)p * m + i] * x + sn[(size_t)p * m + i] * y;
+               hp[(size_t)(i + 1) * m + j] = -sn[(size_t)p * m + i] * x + cs[(size_t)p * m + i] * y;
+            }
+            const double x = hp[(size_t)j * m + j], y = hp[(size_t)(j + 1) * m + j];
+            const double r = std::hypot(x, y);
+            const double cj = r > 0 ? x / r : 1.0, sj = r > 0 ? y / r : 0.0;
+            cs[(size_t)p * m + j] = cj;
+            sn[(size_t)p * m + j] = sj;
+            hp[(size_t)j * m + j] = r;
+            hp[(size_t)(j + 1) * m + j] = 0.0;
+            double *gp = &g[(size_t)p * H];
+            gp[j + 1] = -sj * gp[j];
+            gp[j] = cj * gp[j];
+            its[p] += 1;
+            kp[p] = j + 1;
+            const double est = std::fabs(gp[j + 1]) / std::sqrt(std::max(wsum[p], 1e-300));
+            c->hist[p].push_back(est);
+            if (!(est > eff[p]) || its[p] >= c->max_cycles || !(hn > 0)) act[p] = 0;
+         }
+         kry_combine(c, j + 1, a, 0, 0, coef);  // V_{j+1} = W / ||W||
+         set_active(c, act);
+         c->host_active = act;
+      }
+      // x += Z y for every problem of this restart cycle
+      std::vector<double> y((size_t)np * m, 0.0);
+      for (int p = 0; p < np; ++p) {
+         if (!cyc[p]) continue;
+         const double *hp = &h[(size_t)p * H * m];
+         const double *gp = &g[(size_t)p * H];
+         for (int i = kp[p] - 1; i >= 0; --i) {
+            double sum = gp[i];
+            for (int q = i + 1; q < kp[p]; ++q) sum -= hp[(size_t)i * m + q] * y[(size_t)p * m + q];
+            y[(size_t)p * m + i] = hp[(size_t)i * m + i] != 0 ? sum / hp[(size_t)i * m + i] : 0.0;
+         }
+      }
+      set_active(c, cyc);
+      c->host_active = cyc;
+      int kmax = 0;
+      for (int p = 0; p < np; ++p)
+         if (cyc[p]) kmax = std::max(kmax, kp[p]);
+      std::vector<double> yk((size_t)np * std::max(1, kmax), 0.0);
+      for (int p = 0; p < np; ++p)
+         for (int i = 0; i < kmax; ++i) yk[(size_t)p * kmax + i] = y[(size_t)p * m + i];
+      if (kmax > 0)
+         CUDA_CHECK(cudaMemcpyAsync(c->kry_coef.p, yk.data(), (size_t)np * kmax * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
+      for (int ln = 0; ln < c->nlev; ++ln) {
+         LevelState &L = c->L[ln];
+         launch_add_combination(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                                L.d_cell_chunks.p, L.u.p, kry_vec(c, ln, zslot0),
+                                std::max<long long>(1, L.n0), kmax, c->kry_coef.p);
+      }
+      for (int ln = c->nlev - 2; ln >= 0; --ln) restrict_solution(c, FAC_U, ln);
+      std::vector<double> nr;
+      full_composite_residual(c, nr);
+      for (int p = 0; p < np; ++p) {
+         if (!cyc[p]) continue;
+         res[p] = nr[p];
+         if (!c->hist[p].empty()) c->hist[p].back() = nr[p];
+         if (!(nr[p] > eff[p])) done[p] = 1;
+      }
    }
    c->host_active.assign(np, 1);
    set_active(c, c->host_active);
@@ -2908,6 +3282,23 @@ int fac_solve(fac_ctx *ctx, int *converged, int *iterations, double *residual)
    return guarded([&] {
       check_ops(ctx);
       solve(ctx, converged, iterations, residual);
+   });
+}
+
+int fac_set_krylov(fac_ctx *ctx, int restart)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      if (restart < 0 || restart > 64) throw FacError(FAC_ERR_ARG, "restart length must be 0..64");
+      ctx->krylov = restart;
+   });
+}
+
+int fac_solve_fgmres(fac_ctx *ctx, int restart, int *converged, int *iterations, double *residual)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      fgmres_solve(ctx, restart, converged, iterations, residual);
    });
 }
 

@@ -1110,6 +1110,131 @@ k_compact(const WorkReg *__restrict__ regs, const int *__restrict__ active, int 
    }
 }
 
+// ---------------------------------------------------------------------------
+// Krylov vector operations on composite vectors (ghost-0 cell arrays of a
+// level, one vector every vstride elements), per problem, deterministic
+// ---------------------------------------------------------------------------
+
+// partial[chunk * K + i] = sum over the chunk of w x V_i
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_multidot(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
+           const double *__restrict__ w, const double *__restrict__ x,
+           const double *__restrict__ V, long long vstride, int K,
+           double *__restrict__ partial)
+{
+   __shared__ double red[kThreads / 32];
+   WORK_LOOP(ch) {
+      const PatchDesc &p = patches[ch.patch];
+      for (int i = 0; i < K; ++i) {
+         const double *vi = V + (long long)i * vstride;
+         double sum = 0.0;
+         for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+            const long long c = p.off0 + ch.begin + t;
+            sum += w[c] * x[c] * vi[c];
+         }
+         for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+         __syncthreads();
+         if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) b += red[q];
+            partial[(long long)ch.aux * K + i] = b;
+         }
+         __syncthreads();
+      }
+   }
+}
+
+// out[p * K + i] += sum of the problem's chunk partials, in chunk order
+__global__ void k_multidot_reduce(const double *__restrict__ partial,
+                                  const int *__restrict__ prob_chunk_begin, int K,
+                                  const int *__restrict__ active, double *__restrict__ out)
+{
+   const int p = blockIdx.x, i = blockIdx.y;
+   if (active && !active[p]) return;
+   const int b = prob_chunk_begin[p], e = prob_chunk_begin[p + 1];
+   __shared__ double red[kThreads];
+   double sum = 0.0;
+   for (int c = b + threadIdx.x; c < e; c += blockDim.x) sum += partial[(long long)c * K + i];
+   red[threadIdx.x] = sum;
+   __syncthreads();
+   for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) out[(long long)p * K + i] += red[0];
+}
+
+// x = a[p] x + sum_i coef[p * K + i] V_i
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_combine(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
+          double *__restrict__ x, const double *__restrict__ a,
+          const double *__restrict__ V, long long vstride, int K,
+          const double *__restrict__ coef)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc &p = patches[ch.patch];
+      const double ap = a[p.prob];
+      const double *cp = coef + (long long)p.prob * K;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const long long c = p.off0 + ch.begin + t;
+         double v = ap * x[c];
+         for (int i = 0; i < K; ++i) v = v + cp[i] * V[(long long)i * vstride + c];
+         x[c] = v;
+      }
+   }
+}
+
+// dst (ghost-0, FP64) = src interior (ghost-1)
+template <int DIM, class TS>
+__global__ void __launch_bounds__(kThreads)
+k_g1_to_g0(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
+           const TS *__restrict__ src, double *__restrict__ dst)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc &p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         dst[p.off0 + lin] = (double)src[cidx<DIM>(p, p.off1, 1, i, j, k)];
+      }
+   }
+}
+
+// u interior (ghost-1) += sum_i y[p * K + i] Z_i (ghost-0)
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_add_combination(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
+                  int nwork, double *__restrict__ u, const double *__restrict__ Z,
+                  long long zstride, int K, const double *__restrict__ y)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc &p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const double *yp = y + (long long)p.prob * K;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         const int i = p.lo[0] + lin % nx;
+         const int r = lin / nx;
+         const int j = p.lo[1] + r % ny;
+         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         const long long c0 = p.off0 + lin;
+         double s = 0.0;
+         for (int q = 0; q < K; ++q) s = s + yp[q] * Z[(long long)q * zstride + c0];
+         const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
+         u[c1] = u[c1] + s;
+      }
+   }
+}
+
 std::atomic<long long> g_launches{0};
 
 }  // namespace
@@ -1117,6 +1242,70 @@ std::atomic<long long> g_launches{0};
 long long kernel_launch_count() { return g_launches.load(); }
 
 void add_kernel_launches(long long n) { g_launches += n; }
+
+void launch_multidot(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const double *w, const double *x, const double *V,
+                     long long vstride, int K, double *partial, const int *prob_chunk_begin,
+                     int nprob, const int *active, double *out)
+{
+   if (K <= 0) return;
+   if (nchunks > 0) {
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      if (dim == 2)
+         k_multidot<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, w, x, V,
+                                                                vstride, K, partial);
+      else
+         k_multidot<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, w, x, V,
+                                                                vstride, K, partial);
+   }
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_multidot_reduce<<<dim3(nprob, K), kThreads, 0, s>>>(partial, prob_chunk_begin, K, active,
+                                                         out);
+}
+
+void launch_combine(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                    const Chunk *chunks, double *x, const double *a, const double *V,
+                    long long vstride, int K, const double *coef)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_combine<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, a, V,
+                                                            vstride, K, coef);
+   else
+      k_combine<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, a, V,
+                                                            vstride, K, coef);
+}
+
+template <class TS>
+void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const TS *src, double *dst)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_g1_to_g0<2, TS><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+   else
+      k_g1_to_g0<3, TS><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+}
+template void launch_g1_to_g0<double>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
+                                      const double *, double *);
+template void launch_g1_to_g0<float>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
+                                     const float *, double *);
+
+void launch_add_combination(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                            const Chunk *chunks, double *u, const double *Z, long long zstride,
+                            int K, const double *y)
+{
+   if (nchunks <= 0 || K <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_add_combination<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, Z,
+                                                                    zstride, K, y);
+   else
+      k_add_combination<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, Z,
+                                                                    zstride, K, y);
+}
 
 void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *active, int nprob)
 {

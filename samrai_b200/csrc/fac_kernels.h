@@ -27,6 +27,27 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
                       const T *cfield, const T *cfflux, int offset, const int *pushmap,
                       const BcCoefs &bc, int *err);
 
+// Krylov vector operations on composite vectors: ghost-0 level arrays, one
+// vector every vstride elements; per-problem coefficients; cell chunks with
+// aux = chunk index (partial is nchunks x K).
+// out[p*K+i] += sum_w x V_i over problem p's chunks of this level.
+void launch_multidot(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const double *w, const double *x, const double *V,
+                     long long vstride, int K, double *partial, const int *prob_chunk_begin,
+                     int nprob, const int *active, double *out);
+// x = a[p] x + sum_i coef[p*K+i] V_i
+void launch_combine(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                    const Chunk *chunks, double *x, const double *a, const double *V,
+                    long long vstride, int K, const double *coef);
+// dst (ghost-0) = interior of src (ghost-1), converted to FP64
+template <class TS>
+void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                     const Chunk *chunks, const TS *src, double *dst);
+// u interior += sum_i y[p*K+i] Z_i
+void launch_add_combination(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                            const Chunk *chunks, double *u, const double *Z, long long zstride,
+                            int K, const double *y);
+
 // Rebuild every registered work list for the current active flags.
 void launch_compact(cudaStream_t s, const WorkReg *regs, int nregs, const int *active, int nprob);
 

@@ -68,6 +68,8 @@ def load_library(build_if_missing=True):
         "fac_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_fused": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_staged": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_solve_fgmres": (ctypes.c_int, [vp, ctypes.c_int, ip, ip, dp]),
+        "fac_set_krylov": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_learned": (ctypes.c_int, [vp, vp, ctypes.c_int]),
         "fac_learned_samples": (ctypes.c_int, [vp, ctypes.c_int, vp, dp]),
         "fac_set_fused_residual": (ctypes.c_int, [vp, ctypes.c_int]),
@@ -362,6 +364,21 @@ class FacContext:
         scale = np.zeros(max(1, npatch))
         _check(load_library().fac_learned_samples(self.h, int(level), x_ptr, _dp(scale)))
         return scale[:npatch]
+
+    def set_krylov(self, restart):
+        """restart > 0: solve() / solve_host() run FGMRES(restart) around the
+        FAC cycle; 0: the stationary FAC iteration."""
+        _check(load_library().fac_set_krylov(self.h, int(restart)))
+
+    def solve_fgmres(self, restart=20):
+        """FGMRES(restart) with the FAC cycle as preconditioner; same
+        outputs as solve()."""
+        conv = np.zeros(self.nprob, dtype=np.int32)
+        its = np.zeros(self.nprob, dtype=np.int32)
+        res = np.zeros(self.nprob)
+        _check(load_library().fac_solve_fgmres(self.h, int(restart), _ip(conv), _ip(its),
+                                               _dp(res)))
+        return conv.astype(bool), its, res
 
     def set_staged(self, on=True):
         _check(load_library().fac_set_staged(self.h, int(on)))

@@ -323,3 +323,35 @@ def test_autotune_keeps_results(require_gpu):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     for a, b in zip(out[0][2], out[1][2]):
         assert np.array_equal(a, b)
+
+
+def _rel_l2(a_list, b_list):
+    num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(a_list, b_list))
+    den = sum(float(np.sum(b ** 2)) for b in b_list)
+    return (num / max(den, 1e-300)) ** 0.5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["config1", "small_3d_mg", "config3"])
+def test_fgmres_matches_fac_solution(case, precision, require_gpu):
+    """FGMRES with the FAC cycle as preconditioner reaches the same 1e-10
+    relative residual with no more preconditioner applications than FAC
+    needs cycles, and the same solution to 1e-9 relative L2."""
+    if case == "config1":
+        probs = [configs.extend_hierarchy(configs.config1(), k=3)]
+    elif case == "config3":
+        probs = [configs.extend_hierarchy(configs.config3(), k=3)]
+    else:
+        probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (71, 72)]
+    prm = dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=100)
+    g = fac.FacContext(probs, params=prm, precision=precision)
+    conv_f, its_f, res_f = g.solve()
+    uf = [g.download(U, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
+    g.zero(U)
+    conv_k, its_k, res_k = g.solve_fgmres(20)
+    uk = [g.download(U, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
+    g.close()
+    assert conv_f.all() and conv_k.all(), (its_f, res_f, its_k, res_k)
+    assert (its_k <= its_f).all(), (its_k, its_f)
+    assert _rel_l2(uk, uf) <= 1e-9
