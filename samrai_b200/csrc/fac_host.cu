@@ -2562,30 +2562,40 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                                        std::max<long long>(1, L.n0) * sizeof(double),
                                        cudaMemcpyDeviceToDevice, c->stream));
          }
-         // classical Gram-Schmidt twice: W = -TR - sum h_i V_i
+         // classical Gram-Schmidt, W = -TR - sum h_i V_i, repeated once for
+         // the problems whose W lost more than half its norm (cancellation)
          const int K = j + 1;
-         kry_dots(c, j + 1, 0, K, dots);  // <TR, V_i>
+         kry_dots(c, j + 1, 0, K + 1, dots);  // <TR, V_i>, i <= j, and <TR, TR>
+         std::vector<double> before(np, 0.0);
          coef.assign((size_t)np * K, 0.0);
          for (int p = 0; p < np; ++p) {
             a[p] = -1.0;
+            before[p] = dots[(size_t)p * (K + 1) + K];
             for (int i = 0; i < K; ++i) {
-               const double hi = act[p] ? -dots[(size_t)p * K + i] : 0.0;
+               const double hi = act[p] ? -dots[(size_t)p * (K + 1) + i] : 0.0;
                h[((size_t)p * H + i) * m + j] = hi;
                coef[(size_t)p * K + i] = -hi;
             }
          }
          kry_combine(c, j + 1, a, 0, K, coef);
-         kry_dots(c, j + 1, 0, K, dots);
-         for (int p = 0; p < np; ++p) {
-            a[p] = 1.0;
-            for (int i = 0; i < K; ++i) {
-               const double d = act[p] ? dots[(size_t)p * K + i] : 0.0;
-               h[((size_t)p * H + i) * m + j] += d;
-               coef[(size_t)p * K + i] = -d;
-            }
-         }
-         kry_combine(c, j + 1, a, 0, K, coef);
          kry_dots(c, j + 1, j + 1, 1, dots);  // ||W||^2
+         bool again = false;
+         std::vector<int> reo(np, 0);
+         for (int p = 0; p < np; ++p)
+            if (act[p] && dots[p] < 0.25 * before[p]) reo[p] = again = true;
+         if (again) {
+            kry_dots(c, j + 1, 0, K, dots);
+            for (int p = 0; p < np; ++p) {
+               a[p] = 1.0;
+               for (int i = 0; i < K; ++i) {
+                  const double d = reo[p] ? dots[(size_t)p * K + i] : 0.0;
+                  h[((size_t)p * H + i) * m + j] += d;
+                  coef[(size_t)p * K + i] = -d;
+               }
+            }
+            kry_combine(c, j + 1, a, 0, K, coef);
+            kry_dots(c, j + 1, j + 1, 1, dots);
+         }
          for (int p = 0; p < np; ++p) {
             if (!act[p]) {
                a[p] = 0.0;

@@ -371,11 +371,33 @@ k_flux(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, 
    }
 }
 
+// Ewing fix of the flux on face (a, s) of cell (i, j, k) of patch p
+// (ewingfixflux*, 2d.f:460-686, 3d.f:604-1012); out of line: only
+// coarse-fine faces take it.
+template <int DIM, class TU>
+__device__ __noinline__ double ewing_face(const PatchDesc &p, const TU *__restrict__ u, int a,
+                                          int s, int i, int j, int k, double fl, double d,
+                                          const EwingWeights &w, const int *ratio_to_coarser)
+{
+   const int cc[3] = {i, j, k};
+   int mq[3] = {i, j, k};
+   for (int tt = 0; tt < DIM; ++tt) {
+      if (tt == a) continue;
+      const int rr = ratio_to_coarser[tt];
+      const int base = coarsen_index(cc[tt], rr) * rr;
+      mq[tt] = base + (rr - (cc[tt] - base) - 1);
+   }
+   const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
+   const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
+   if (s == 0) return w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
+   return w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
+}
+
 // Fluxes of every face of the level, one thread per cell: the lower face of
 // each axis, and the upper one as well for the last cell of a row -- the
-// arithmetic of k_flux with one cell decode for all axes.
+// arithmetic of computeFluxOnPatch with one cell decode for all axes.
 template <int DIM, bool DVAR, class TU>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
              const TU *__restrict__ u, const double *__restrict__ dside, double dconst,
              const unsigned char *__restrict__ cfmask, EwingWeights w,
@@ -383,47 +405,47 @@ k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ ch
              const int *__restrict__ run)
 {
    WORK_LOOP(ch) {
-      const PatchDesc p = patches[ch.patch];
+      const PatchDesc &p = patches[ch.patch];
       if (run && !run[p.prob]) continue;
       const int nx = p.hi[0] - p.lo[0] + 1;
       const int ny = p.hi[1] - p.lo[1] + 1;
+      const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
       const bool has_cf = (p.flags & 1) != 0;
-      const long long st[3] = {1, nx + 2, (long long)(nx + 2) * (ny + 2)};
+      const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
+      const TU *up = u + p.off1;
+      const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
+         const int li = lin % nx;
          const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-         const int cc[3] = {i, j, k};
-         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+         const int lj = r % ny;
+         const int lk = DIM == 3 ? r / ny : 0;
+         const int c = (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0);
+         const double uc = (double)up[c];
+         // side-array positions of the cell's lower faces
+         const int sx = li + (nx + 1) * (lj + ny * lk);
+         const int sy = li + nx * (lj + (ny + 1) * lk);
+         const int sz = li + nx * (lj + ny * lk);
 #pragma unroll
          for (int a = 0; a < DIM; ++a) {
-            const double dai = 1. / p.dx[a];
+            const int la = a == 0 ? li : (a == 1 ? lj : lk);
+            const int na = a == 0 ? nx : (a == 1 ? ny : nz);
+            const int st = a == 0 ? 1 : (a == 1 ? gx : gxy);
+            const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
+            const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
-               if (s == 1 && cc[a] != p.hi[a]) break;
-               int fc[3] = {i, j, k};
-               fc[a] += s;
-               const long long si = sidx(p, a, fc[0], fc[1], fc[2]);
+               if (s == 1 && la != na - 1) break;
+               const long long si = sbase + (s ? sup : 0);
                const double d = DVAR ? dside[si] : dconst;
-               const long long cp = s ? c + st[a] : c;
-               double fl = dai * d * ((double)u[cp] - (double)u[cp - st[a]]);
-               if (has_cf && (s == 1 || cc[a] == p.lo[a])) {
-                  const long long o = oidx(p, a, s, i, j, k);
-                  if (cfmask[o]) {
-                     int mq[3] = {i, j, k};
-                     for (int tt = 0; tt < DIM; ++tt) {
-                        if (tt == a) continue;
-                        const int rr = ratio_to_coarser[tt];
-                        const int base = coarsen_index(cc[tt], rr) * rr;
-                        mq[tt] = base + (rr - (cc[tt] - base) - 1);
-                     }
-                     const double uc = (double)u[c];
-                     const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
-                     if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
-                     else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
-                  }
+               const double ulo = s ? uc : (double)up[c - st];
+               const double uhi = s ? (double)up[c + st] : uc;
+               double fl = dai[a] * d * (uhi - ulo);
+               if (has_cf && (s == 1 || la == 0)) {
+                  const int i = p.lo[0] + li, j = p.lo[1] + lj;
+                  const int k = DIM == 3 ? p.lo[2] + lk : 0;
+                  if (cfmask[oidx(p, a, s, i, j, k)])
+                     fl = ewing_face<DIM, TU>(p, u, a, s, i, j, k, fl, d, w, ratio_to_coarser);
                }
                flux[si] = fl;
             }
@@ -437,7 +459,7 @@ k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ ch
 // ---------------------------------------------------------------------------
 
 template <int DIM, int CKIND, class TU>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
            const TU *__restrict__ u, const double *__restrict__ f,
            const double *__restrict__ flux, const double *__restrict__ cfield,
@@ -445,39 +467,49 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
            const int *__restrict__ run)
 {
    WORK_LOOP(ch) {
-      const PatchDesc p = patches[ch.patch];
+      const PatchDesc &p = patches[ch.patch];
       if (run && !run[p.prob]) continue;
       const int nx = p.hi[0] - p.lo[0] + 1;
       const int ny = p.hi[1] - p.lo[1] + 1;
+      const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
+      const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
       const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
       const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+      const double *fx = flux + p.offs[0], *fy = flux + p.offs[1];
+      const double *fz = DIM == 3 ? flux + p.offs[2] : nullptr;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
+         const int li = lin % nx;
          const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-         const double fxl = flux[sidx(p, 0, i, j, k)], fxh = flux[sidx(p, 0, i + 1, j, k)];
-         const double fyl = flux[sidx(p, 1, i, j, k)], fyh = flux[sidx(p, 1, i, j + 1, k)];
-         const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
-         const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
+         const int lj = r % ny;
+         const int lk = DIM == 3 ? r / ny : 0;
+         const int sx = li + (nx + 1) * (lj + ny * lk);
+         const int sy = li + nx * (lj + (ny + 1) * lk);
+         const double fxl = fx[sx], fxh = fx[sx + 1];
+         const double fyl = fy[sy], fyh = fy[sy + nx];
+         const long long c0 = p.off0 + lin;
+         const double uc =
+            (double)u[p.off1 + (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0)];
          const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
-         double rv;
+         double rv, fzl = 0.0, fzh = 0.0;
          if (DIM == 2) {
             rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
          } else {
-            const double fzl = flux[sidx(p, 2, i, j, k)], fzh = flux[sidx(p, 2, i, j, k + 1)];
+            const int sz = li + nx * (lj + ny * lk);
+            fzl = fz[sz];
+            fzh = fz[sz + nx * ny];
             rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - sf * uc;
          }
          res[c0] = rv;
          if (oflux) {
-            if (i == p.lo[0]) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
-            if (i == p.hi[0]) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
-            if (j == p.lo[1]) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
-            if (j == p.hi[1]) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
+            const int i = p.lo[0] + li, j = p.lo[1] + lj, k = DIM == 3 ? p.lo[2] + lk : 0;
+            if (li == 0) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
+            if (li == nx - 1) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
+            if (lj == 0) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
+            if (lj == ny - 1) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
             if (DIM == 3) {
-               if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = flux[sidx(p, 2, i, j, k)];
-               if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = flux[sidx(p, 2, i, j, k + 1)];
+               if (lk == 0) oflux[oidx(p, 2, 0, i, j, k)] = fzl;
+               if (lk == nz - 1) oflux[oidx(p, 2, 1, i, j, k)] = fzh;
             }
          }
       }
