@@ -525,7 +525,7 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
 // ---------------------------------------------------------------------------
 
 template <int DIM, bool DVAR, int CKIND, class TU>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
                  int nwork, const TU *__restrict__ u, const double *__restrict__ dside,
                  double dconst, const unsigned char *__restrict__ cfmask, EwingWeights w,
@@ -535,77 +535,74 @@ k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict_
                  double *__restrict__ oflux, const int *__restrict__ run)
 {
    WORK_LOOP(ch) {
-      const PatchDesc p = patches[ch.patch];
+      const PatchDesc &p = patches[ch.patch];
       if (run && !run[p.prob]) continue;
       const int nx = p.hi[0] - p.lo[0] + 1;
       const int ny = p.hi[1] - p.lo[1] + 1;
+      const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
       const bool has_cf = (p.flags & 1) != 0;
-      const long long gx = nx + 2, gxy = (long long)(nx + 2) * (ny + 2);
-      // flux on the face of axis a whose upper cell is (fi, fj, fk)
-      auto face_flux = [&](int a, int fi, int fj, int fk) -> double {
-         const long long si = sidx(p, a, fi, fj, fk);
-         if (fcmask && fcmask[si]) return fcflux[si];
-         const double dai = 1. / p.dx[a];
-         const double d = DVAR ? dside[si] : dconst;
-         const long long cp = cidx<DIM>(p, p.off1, 1, fi, fj, fk);
-         const long long cq = cp - (a == 0 ? 1 : (a == 1 ? gx : gxy));
-         double fl = dai * d * ((double)u[cp] - (double)u[cq]);
-         if (has_cf) {
-            const int fc[3] = {fi, fj, fk};
-            int s = -1;
-            if (fc[a] == p.lo[a]) s = 0;
-            else if (fc[a] == p.hi[a] + 1) s = 1;
-            if (s >= 0) {
-               int cc[3] = {fi, fj, fk};
-               if (s == 1) cc[a] -= 1;
-               const long long o = oidx(p, a, s, cc[0], cc[1], cc[2]);
-               if (cfmask[o]) {
-                  int mq[3] = {cc[0], cc[1], cc[2]};
-                  for (int tt = 0; tt < DIM; ++tt) {
-                     if (tt == a) continue;
-                     const int rr = ratio_to_coarser[tt];
-                     const int base = coarsen_index(cc[tt], rr) * rr;
-                     mq[tt] = base + (rr - (cc[tt] - base) - 1);
-                  }
-                  const double uc = (double)u[cidx<DIM>(p, p.off1, 1, cc[0], cc[1], cc[2])];
-                  const double um = (double)u[cidx<DIM>(p, p.off1, 1, mq[0], mq[1], mq[2])];
-                  if (s == 0) fl = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
-                  else fl = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
-               }
-            }
-         }
-         return fl;
-      };
-      const double dxi = 1. / p.dx[0], dyi = 1. / p.dx[1];
-      const double dzi = DIM == 3 ? 1. / p.dx[2] : 0.0;
+      const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
+      const TU *up = u + p.off1;
+      const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
+         const int li = lin % nx;
          const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-         const double fxl = face_flux(0, i, j, k), fxh = face_flux(0, i + 1, j, k);
-         const double fyl = face_flux(1, i, j, k), fyh = face_flux(1, i, j + 1, k);
-         const long long c0 = cidx<DIM>(p, p.off0, 0, i, j, k);
-         const double uc = (double)u[cidx<DIM>(p, p.off1, 1, i, j, k)];
-         const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
-         double rv, fzl = 0.0, fzh = 0.0;
-         if (DIM == 2) {
-            rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
-         } else {
-            fzl = face_flux(2, i, j, k);
-            fzh = face_flux(2, i, j, k + 1);
-            rv = f[c0] - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - sf * uc;
+         const int lj = r % ny;
+         const int lk = DIM == 3 ? r / ny : 0;
+         const int c = (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0);
+         const double uc = (double)up[c];
+         const int sx = li + (nx + 1) * (lj + ny * lk);
+         const int sy = li + nx * (lj + (ny + 1) * lk);
+         const int sz = li + nx * (lj + ny * lk);
+         double fl[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+         for (int a = 0; a < DIM; ++a) {
+            const int la = a == 0 ? li : (a == 1 ? lj : lk);
+            const int na = a == 0 ? nx : (a == 1 ? ny : nz);
+            const int st = a == 0 ? 1 : (a == 1 ? gx : gxy);
+            const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
+            const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+               const long long si = sbase + (s ? sup : 0);
+               if (fcmask && fcmask[si]) {
+                  fl[a][s] = fcflux[si];
+                  continue;
+               }
+               const double d = DVAR ? dside[si] : dconst;
+               const double ulo = s ? uc : (double)up[c - st];
+               const double uhi = s ? (double)up[c + st] : uc;
+               double v = dai[a] * d * (uhi - ulo);
+               if (has_cf && (s ? la == na - 1 : la == 0)) {
+                  const int i = p.lo[0] + li, j = p.lo[1] + lj;
+                  const int k = DIM == 3 ? p.lo[2] + lk : 0;
+                  if (cfmask[oidx(p, a, s, i, j, k)])
+                     v = ewing_face<DIM, TU>(p, u, a, s, i, j, k, v, d, w, ratio_to_coarser);
+               }
+               fl[a][s] = v;
+            }
          }
+         const long long c0 = p.off0 + lin;
+         const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
+         double rv;
+         if (DIM == 2)
+            rv = f[c0] - (dai[0] * (fl[0][1] - fl[0][0]) + dai[1] * (fl[1][1] - fl[1][0])) -
+                 sf * uc;
+         else
+            rv = f[c0] - (dai[0] * (fl[0][1] - fl[0][0]) + dai[1] * (fl[1][1] - fl[1][0]) +
+                          dai[2] * (fl[2][1] - fl[2][0])) -
+                 sf * uc;
          res[c0] = rv;
          if (oflux) {
-            if (i == p.lo[0]) oflux[oidx(p, 0, 0, i, j, k)] = fxl;
-            if (i == p.hi[0]) oflux[oidx(p, 0, 1, i, j, k)] = fxh;
-            if (j == p.lo[1]) oflux[oidx(p, 1, 0, i, j, k)] = fyl;
-            if (j == p.hi[1]) oflux[oidx(p, 1, 1, i, j, k)] = fyh;
+            const int i = p.lo[0] + li, j = p.lo[1] + lj, k = DIM == 3 ? p.lo[2] + lk : 0;
+            if (li == 0) oflux[oidx(p, 0, 0, i, j, k)] = fl[0][0];
+            if (li == nx - 1) oflux[oidx(p, 0, 1, i, j, k)] = fl[0][1];
+            if (lj == 0) oflux[oidx(p, 1, 0, i, j, k)] = fl[1][0];
+            if (lj == ny - 1) oflux[oidx(p, 1, 1, i, j, k)] = fl[1][1];
             if (DIM == 3) {
-               if (k == p.lo[2]) oflux[oidx(p, 2, 0, i, j, k)] = fzl;
-               if (k == p.hi[2]) oflux[oidx(p, 2, 1, i, j, k)] = fzh;
+               if (lk == 0) oflux[oidx(p, 2, 0, i, j, k)] = fl[2][0];
+               if (lk == nz - 1) oflux[oidx(p, 2, 1, i, j, k)] = fl[2][1];
             }
          }
       }
