@@ -51,6 +51,11 @@ PARAMS_MG = dict(PARAMS, coarse_max_it=20)
 MG_LEVELS = {"c5": 3, "c2": 4, "c1": 3, "c3": 3}
 # headline: FGMRES(KRYLOV) with one FAC cycle as the flexible preconditioner
 KRYLOV = 20
+# DRAM bytes per algorithmic byte of the FP32 staged colour pass, from one ncu
+# capture (profiles/k_rb_staged_f32_config5x8_finest-level.md: 69.6 MB read +
+# write for 54.6 MB algorithmic on 2.48 M cells); traffic per launch is this
+# times the launch's algorithmic bytes (scaling by cells processed)
+STAGED_F32_TRAFFIC_RATIO = 69.6 / 54.6
 
 
 def make_workload(name, nprob, rank):
@@ -446,7 +451,9 @@ def main():
             "peak_kind": peak_kind,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
-            "traffic": None,
+            "traffic": (round(STAGED_F32_TRAFFIC_RATIO * rb_bytes / max(rb_n, 1) / 1e6, 2)
+                        if args.precision == "mixed" else None),
+            "traffic_unit": "MB per launch",
             "launches": int(rb_n),
             "avg_launch_us": round(rb_ms * 1e3 / max(rb_n, 1), 2),
             "share_of_step": round(rb_ms / max(prof_ms, 1e-9), 4),
