@@ -1840,10 +1840,15 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
    ghost_fill(c, fid_u, ln, ln > 0, error_eq, run);
    const double *u = field_ptr(L, fid_u);
    const bool finer = ln < c->nlev - 1;
-   if (!c->fused_residual)
+   if (!c->fused_residual) {
       launch_flux_cells(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
                         L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
                         L.d_ratio.p, L.flux.p, run);
+      if (ln > 0)
+         launch_ewing_fix(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, u, L.d.p,
+                          c->spec.d_variable, c->spec.d_const, L.tranwt, L.longwt, L.flux.p,
+                          run);
+   }
    if (finer) {
       LevelState &Fl = c->L[ln + 1];
       launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,
@@ -2067,10 +2072,15 @@ void comp_residual_mixed(fac_ctx *c, int ln)
    const int *run = c->active.p;
    ghost_fill32(c, ln, ln > 0, 1, run);
    const bool finer = ln < c->nlev - 1;
-   if (!c->fused_residual)
+   if (!c->fused_residual) {
       launch_flux_cells<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                                L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
                                L.tranwt, L.longwt, L.d_ratio.p, L.flux.p, run);
+      if (ln > 0)
+         launch_ewing_fix<float>(c->stream, L.d_cf.p, (int)L.cf.size(), L.d_patches.p, L.e32.p,
+                                 L.d.p, c->spec.d_variable, c->spec.d_const, L.tranwt,
+                                 L.longwt, L.flux.p, run);
+   }
    if (finer) {
       LevelState &Fl = c->L[ln + 1];
       launch_flux_coarsen(c->stream, L.fcoarsen.d_items.p, L.fcoarsen.d_chunks.p,

@@ -395,7 +395,8 @@ __device__ __noinline__ double ewing_face(const PatchDesc &p, const TU *__restri
 
 // Fluxes of every face of the level, one thread per cell: the lower face of
 // each axis, and the upper one as well for the last cell of a row -- the
-// arithmetic of computeFluxOnPatch with one cell decode for all axes.
+// arithmetic of computeFluxOnPatch with one cell decode for all axes.  The
+// Ewing fix of the coarse-fine faces follows in k_ewing_fix.
 template <int DIM, bool DVAR, class TU>
 __global__ void __launch_bounds__(kThreads, 4)
 k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
@@ -410,7 +411,6 @@ k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ ch
       const int nx = p.hi[0] - p.lo[0] + 1;
       const int ny = p.hi[1] - p.lo[1] + 1;
       const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
-      const bool has_cf = (p.flags & 1) != 0;
       const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
       const TU *up = u + p.off1;
       const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
@@ -440,18 +440,34 @@ k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ ch
                const double d = DVAR ? dside[si] : dconst;
                const double ulo = s ? uc : (double)up[c - st];
                const double uhi = s ? (double)up[c + st] : uc;
-               double fl = dai[a] * d * (uhi - ulo);
-               if (has_cf && (s == 1 || la == 0)) {
-                  const int i = p.lo[0] + li, j = p.lo[1] + lj;
-                  const int k = DIM == 3 ? p.lo[2] + lk : 0;
-                  if (cfmask[oidx(p, a, s, i, j, k)])
-                     fl = ewing_face<DIM, TU>(p, u, a, s, i, j, k, fl, d, w, ratio_to_coarser);
-               }
-               flux[si] = fl;
+               flux[si] = dai[a] * d * (uhi - ulo);
             }
          }
       }
    }
+}
+
+// Ewing fix of the stored flux on every coarse-fine face of the level
+// (ewingfixflux*, 2d.f:460-686, 3d.f:604-1012): flux = longwt*flux
+// +/- tranwt*D*(u(mirror) - u(cell))/h, after k_flux_cells.
+template <class TU>
+__global__ void __launch_bounds__(kThreads)
+k_ewing_fix(const CfFace *__restrict__ faces, int nfaces, const PatchDesc *__restrict__ patches,
+            const TU *__restrict__ u, const double *__restrict__ dside, int dvar,
+            double dconst, EwingWeights w, double *__restrict__ flux,
+            const int *__restrict__ run)
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= nfaces) return;
+   const CfFace cf = faces[t];
+   const PatchDesc &p = patches[cf.patch];
+   if (run && !run[p.prob]) return;
+   const int a = cf.axis;
+   const double d = dvar ? dside[cf.sidx] : dconst;
+   const double fl = flux[cf.sidx];
+   const double uc = (double)u[cf.cell], um = (double)u[cf.mirror];
+   if (cf.side == 0) flux[cf.sidx] = w.longwt[a] * fl + w.tranwt[a] * d * (um - uc) / p.dx[a];
+   else flux[cf.sidx] = w.longwt[a] * fl - w.tranwt[a] * d * (um - uc) / p.dx[a];
 }
 
 // ---------------------------------------------------------------------------
@@ -1489,6 +1505,22 @@ void launch_flux_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int nch
 }
 
 template <class TU>
+void launch_ewing_fix(cudaStream_t s, const CfFace *faces, int nfaces, const PatchDesc *patches,
+                      const TU *u, const double *dside, int dvar, double dconst,
+                      const double *tranwt, const double *longwt, double *flux, const int *run)
+{
+   if (nfaces <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   EwingWeights w;
+   for (int a = 0; a < 3; ++a) {
+      w.tranwt[a] = tranwt[a];
+      w.longwt[a] = longwt[a];
+   }
+   k_ewing_fix<TU><<<(nfaces + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+      faces, nfaces, patches, u, dside, dvar, dconst, w, flux, run);
+}
+
+template <class TU>
 void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                            const PatchDesc *patches, const Chunk *chunks, const TU *u,
                            const double *dside, const unsigned char *cfmask,
@@ -1754,6 +1786,9 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
                                     const PatchDesc *, const Chunk *, const T *,            \
                                     const double *, const double *, const double *,         \
                                     double *, double *, const int *);                       \
+   template void launch_ewing_fix<T>(cudaStream_t, const CfFace *, int, const PatchDesc *,   \
+                                     const T *, const double *, int, double, const double *, \
+                                     const double *, double *, const int *);                \
    template void launch_flux_cells<T>(cudaStream_t, int, const PoissonSpec &, int,          \
                                       const PatchDesc *, const Chunk *, const T *,          \
                                       const double *, const unsigned char *,                \

@@ -82,7 +82,14 @@ void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchun
                      const double *f, const double *flux, const double *cfield,
                      double *res, double *oflux, const int *run);
 
-// All face fluxes of a level from its cell chunks (one decode per cell).
+// Ewing fix of the stored fluxes on the level's coarse-fine faces.
+template <class TU>
+void launch_ewing_fix(cudaStream_t s, const CfFace *faces, int nfaces, const PatchDesc *patches,
+                      const TU *u, const double *dside, int dvar, double dconst,
+                      const double *tranwt, const double *longwt, double *flux, const int *run);
+
+// All face fluxes of a level from its cell chunks (one decode per cell);
+// the coarse-fine faces need launch_ewing_fix afterwards.
 template <class TU>
 void launch_flux_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                        const PatchDesc *patches, const Chunk *cell_chunks, const TU *u,
