@@ -726,13 +726,29 @@ k_restrict(const RestrictItem *__restrict__ items, const Chunk *__restrict__ chu
          const int j = it.lo[1] + rr % ny;
          const int k = it.lo[2] + rr / ny;
          double acc = 0.0;
-         const int nr2 = DIM == 3 ? r2 : 1;
-         for (int i2 = 0; i2 < nr2; ++i2)
-            for (int i1 = 0; i1 < r1; ++i1)
-               for (int i0 = 0; i0 < r0; ++i0) {
-                  const int fk = DIM == 3 ? k * r2 + i2 : 0;
-                  acc = acc + src[cidx<DIM>(fp, soff, src_g, i * r0 + i0, j * r1 + i1, fk)] * dVf;
-               }
+         if (r0 == 2 && r1 == 2 && (DIM == 2 || r2 == 2)) {
+            // ratio 2: all fine values loaded first, summed in the loop order
+            // below (i2 outer, i1, i0 inner)
+            constexpr int NF = DIM == 3 ? 8 : 4;
+            const long long b = cidx<DIM>(fp, soff, src_g, 2 * i, 2 * j, DIM == 3 ? 2 * k : 0);
+            const long long sy = fp.hi[0] - fp.lo[0] + 1 + 2 * src_g;
+            const long long sz = sy * (fp.hi[1] - fp.lo[1] + 1 + 2 * src_g);
+            double v[NF];
+#pragma unroll
+            for (int q = 0; q < NF; ++q)
+               v[q] = src[b + (q & 1) + ((q >> 1) & 1) * sy + (q >> 2) * sz];
+#pragma unroll
+            for (int q = 0; q < NF; ++q) acc = acc + v[q] * dVf;
+         } else {
+            const int nr2 = DIM == 3 ? r2 : 1;
+            for (int i2 = 0; i2 < nr2; ++i2)
+               for (int i1 = 0; i1 < r1; ++i1)
+                  for (int i0 = 0; i0 < r0; ++i0) {
+                     const int fk = DIM == 3 ? k * r2 + i2 : 0;
+                     acc = acc +
+                           src[cidx<DIM>(fp, soff, src_g, i * r0 + i0, j * r1 + i1, fk)] * dVf;
+                  }
+         }
          acc = acc / dVc;
          dst[cidx<DIM>(cp, doff, dst_g, i, j, k)] = acc;
       }
@@ -847,16 +863,27 @@ k_norm_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ 
       const int ny = p.hi[1] - p.lo[1] + 1;
       const long long xoff = xg ? p.off1 : p.off0;
       double sd = 0.0, sv = 0.0;
-      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
-         const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
-         const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
-         const double wv = w[cidx<DIM>(p, p.off0, 0, i, j, k)];
-         sd += xv * xv * wv;
-         sv += wv;
+      if (!xg) {
+         // ghost-0 field: the same linear index as the weights
+         for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+            const long long c = p.off0 + ch.begin + t;
+            const double xv = x[c];
+            const double wv = w[c];
+            sd += xv * xv * wv;
+            sv += wv;
+         }
+      } else {
+         for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+            const int lin = ch.begin + t;
+            const int i = p.lo[0] + lin % nx;
+            const int r = lin / nx;
+            const int j = p.lo[1] + r % ny;
+            const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+            const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
+            const double wv = w[p.off0 + lin];
+            sd += xv * xv * wv;
+            sv += wv;
+         }
       }
       __shared__ double rs[kThreads], rv[kThreads];
       rs[threadIdx.x] = sd;
