@@ -433,6 +433,7 @@ def main():
             "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": f"problem shards x{world}",
             "autotuned_stage_bytes": int(tuned),
+            "autotuned_stage_depth": int(ctx.stage_depth),
             "autotune_sweep_ms": [round(float(x), 3) for x in tune_ms],
         },
         "converged": int(np.sum(conv)),

@@ -129,16 +129,23 @@ int fac_set_staged(fac_ctx *ctx, int on);
 int fac_set_fused_residual(fac_ctx *ctx, int on);
 
 /* Shared-memory bytes of one stage (one work unit) of the staged pass,
- * 4096 .. 77,482 (default 24,576): patches are cut into units of as many
+ * 4096 .. 116,160 (default 32,768): patches are cut into units of as many
  * slices as fit.  Rebuilds the unit tables when the context is
- * initialised.  fac_autotune picks it by timing. */
+ * initialised; a level whose largest unit does not fit depth stages in
+ * 227 KiB of shared memory runs the unstaged pass.  fac_autotune picks it
+ * by timing. */
 int fac_set_stage_budget(fac_ctx *ctx, int bytes);
+/* Stages a CTA of the staged pass cycles through, 2 .. 4 (default 2): more
+ * stages keep more copies in flight per CTA, fewer leave room for more
+ * CTAs per SM.  Rebuilds the unit tables like fac_set_stage_budget. */
+int fac_set_stage_depth(fac_ctx *ctx, int depth);
 
 /* Autotuner: times one red-black sweep of every smoothed level for stage
- * sizes of 12, 16, 24, 32 and 48 KiB (best of three, CUDA events) and keeps
- * the fastest; chosen and ms_per_candidate (5 entries) may be NULL.  Uses
+ * sizes of 12, 16, 24, 32 and 48 KiB at depths 2 and 3 (best of three, CUDA
+ * events) and keeps the fastest; ms_per_candidate (10 entries, depth 2
+ * then depth 3, sizes ascending) and the chosen outputs may be NULL.  Uses
  * the smoothing fields as scratch: call it before fac_solve. */
-int fac_autotune(fac_ctx *ctx, int *chosen, double *ms_per_candidate);
+int fac_autotune(fac_ctx *ctx, int *chosen_bytes, int *chosen_depth, double *ms_per_candidate);
 
 /* FGMRES(restart) with one FAC cycle (FP32 in the mixed precision) as the
  * flexible right preconditioner, every problem with its own Krylov space.

@@ -305,6 +305,7 @@ struct LevelState {
    // face, -1 physical boundary, -2 coarse-fine face (fused colour pass)
    DevArray<long long> facemap;
    DevArray<int> pushmap;
+   std::vector<int> pushmap_h;  // host copy (face masks of the staged units)
    // side-array faces that carry a coarsened finer-level flux
    DevArray<unsigned char> fcmask;
    bool fused_ok = false;
@@ -369,7 +370,8 @@ struct fac_ctx {
    int fused = 1;            // colour passes read across patch faces directly
    int staged = 1;           // fused passes on shared-memory staged units
    int fused_residual = 0;   // residual kernels form the fluxes on the fly
-   int stage_budget = 24 * 1024;  // shared memory of one stage (unit) of the staged pass
+   int stage_budget = 32 * 1024;  // shared memory of one stage (unit) of the staged pass
+   int stage_depth = 2;           // stages per CTA of the staged pass
    DevArray<int> kerr;       // set by kernels whose bounded waits ran out
    bool capturing = false;   // inside stream capture: no host synchronisation
    cudaGraphExec_t cycle_exec = nullptr;
@@ -960,9 +962,15 @@ void build_stage_units(fac_ctx *c, int ln)
             h.hx = (nx + 1) / 2;
             h.mhx = (unsigned)(((1ull << 32) + h.hx - 1) / h.hx);
             h.mny = (unsigned)(((1ull << 32) + ny - 1) / ny);
-            if (h.nslots >= (1 << 14) || nx > 2048 || ny > 1024) decode_ok = false;
+            h.mnx = (unsigned)(((1ull << 32) + nx - 1) / nx);
             h.nslots = h.hx * (dim == 3 ? ny * ns : ns);
-            h.fmask = 0;
+            // exact magic divisions: quotient q by divisor d with q d < 2^32
+            // (slots by hx, rows by ny, face entries by ny or nx)
+            const long long lim = 1ll << 32;
+            if ((long long)h.nslots * h.hx >= lim || (long long)ny * ns * ny >= lim ||
+                (long long)nx * ns * nx >= lim || (long long)nx * ny * nx >= lim)
+               decode_ok = false;
+            h.fmask = h.cfmask = h.pmask = 0;
             for (int k = 0; k < 6; ++k) h.off_push[k] = h.off_cff[k] = -1;
             const int first = (int)copies.size();
             copies.push_back({(long long)hdrs.size() * kStageHeader, kSrcHdr, kStageHeader, 0, 0});
@@ -1023,8 +1031,13 @@ void build_stage_units(fac_ctx *c, int ln)
                } else if (r >= sp.cff0) {
                   h.off_cff[sp.face[r - sp.cff0]] = off;
                } else {
-                  h.off_push[sp.face[r - sp.face0]] = off;
-                  h.fmask |= 1 << sp.face[r - sp.face0];
+                  const int fid = sp.face[r - sp.face0];
+                  h.off_push[fid] = off;
+                  h.fmask |= 1 << fid;
+                  for (long long q = e0; q < e0 + sp.count[r]; ++q) {
+                     if (L.pushmap_h[q] == -2) h.cfmask |= 1 << fid;
+                     else h.pmask |= 1 << fid;
+                  }
                }
                copies.push_back({a0, src, (int)(a1 - a0), sp.off[r], 0});
                total += a1 - a0;
@@ -1036,8 +1049,12 @@ void build_stage_units(fac_ctx *c, int ln)
          }
          if (s0 != nslow) throw FacError(FAC_ERR_ARG, "staged units do not tile the patch");
       }
-      // three stages per CTA after 128 bytes of barriers and copy sources
-      L.unit_smem[t] = decode_ok && 128 + 3 * (long long)maxb <= kStageSmemMax ? maxb : 0;
+      // stage_depth stages per CTA after the barriers and copy sources; a
+      // level whose units do not fit runs the unstaged pass
+      L.unit_smem[t] =
+         decode_ok && kStageBarrierBytes + (long long)c->stage_depth * maxb <= kStageSmemMax
+            ? maxb
+            : 0;
       L.d_units[t].upload(U, c->stream);
       L.d_copies[t].upload(copies, c->stream);
       std::vector<unsigned char> raw(hdrs.size() * kStageHeader);
@@ -1123,6 +1140,7 @@ void build_facemap(fac_ctx *c, int ln)
    L.fused_ok = ok;
    L.facemap.upload(fmap, c->stream);
    L.pushmap.upload(pmap, c->stream);
+   L.pushmap_h = std::move(pmap);
    build_stage_units(c, ln);
 }
 
@@ -1810,9 +1828,9 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
          const int pi = prof_begin(c, 0, L.rb_bytes_prob, 1.0);
          if (staged)
             launch_rb_staged<double>(c->stream, c->dim, c->spec, (int)L.units[0].size(),
-                                     L.unit_smem[0], L.d_units[0].p, L.d_copies[0].p,
-                                     L.d_hdrs[0].p, e, r, L.d.p, L.c.p, L.cfflux.p, color,
-                                     L.pushmap.p, c->bc, c->kerr.p);
+                                     L.unit_smem[0], c->stage_depth, L.d_units[0].p,
+                                     L.d_copies[0].p, L.d_hdrs[0].p, e, r, L.d.p, L.c.p,
+                                     L.cfflux.p, color, L.pushmap.p, c->bc, c->kerr.p);
          else
             launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
                         L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
@@ -2046,9 +2064,10 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
             prof_begin(c, 2, L.rb_bytes_prob, 0.5);
          if (staged)
             launch_rb_staged<float>(c->stream, c->dim, c->spec, (int)L.units[1].size(),
-                                    L.unit_smem[1], L.d_units[1].p, L.d_copies[1].p,
-                                    L.d_hdrs[1].p, L.e32.p, L.r32.p, L.d32.p, L.c32.p,
-                                    L.cfflux32.p, color, L.pushmap.p, c->bc, c->kerr.p);
+                                    L.unit_smem[1], c->stage_depth, L.d_units[1].p,
+                                    L.d_copies[1].p, L.d_hdrs[1].p, L.e32.p, L.r32.p,
+                                    L.d32.p, L.c32.p, L.cfflux32.p, color, L.pushmap.p,
+                                    c->bc, c->kerr.p);
          else
             launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
                                L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
@@ -2869,23 +2888,40 @@ int fac_set_params(fac_ctx *ctx, int max_cycles, double residual_tol, double rel
    });
 }
 
+// Stage size and depth of the staged pass; rebuilds the unit tables of an
+// initialised context.
+void set_stage_shape(fac_ctx *ctx, int bytes, int depth)
+{
+   if (bytes < 4096 || bytes > (kStageSmemMax - kStageBarrierBytes) / 2)
+      throw FacError(FAC_ERR_ARG, "stage budget out of range");
+   if (depth < 2 || depth > kStageDepthMax) throw FacError(FAC_ERR_ARG, "stage depth out of range");
+   ctx->stage_budget = bytes;
+   ctx->stage_depth = depth;
+   if (ctx->initialized && ctx->device >= 0) {
+      CUDA_CHECK(cudaSetDevice(ctx->device));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      ctx->drop_graph();
+      for (int ln = 0; ln < ctx->nlev; ++ln) build_stage_units(ctx, ln);
+      register_work_lists(ctx);
+      launch_compact(ctx->stream, ctx->d_work_regs.p, (int)ctx->work_regs.size(),
+                     ctx->active.p, nprob(ctx));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   }
+}
+
 int fac_set_stage_budget(fac_ctx *ctx, int bytes)
 {
    return guarded([&] {
       if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
-      if (bytes < 4096 || bytes > kStageSmemMax / 3)
-         throw FacError(FAC_ERR_ARG, "stage budget out of range");
-      ctx->stage_budget = bytes;
-      if (ctx->initialized && ctx->device >= 0) {
-         CUDA_CHECK(cudaSetDevice(ctx->device));
-         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-         ctx->drop_graph();
-         for (int ln = 0; ln < ctx->nlev; ++ln) build_stage_units(ctx, ln);
-         register_work_lists(ctx);
-         launch_compact(ctx->stream, ctx->d_work_regs.p, (int)ctx->work_regs.size(),
-                        ctx->active.p, nprob(ctx));
-         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-      }
+      set_stage_shape(ctx, bytes, ctx->stage_depth);
+   });
+}
+
+int fac_set_stage_depth(fac_ctx *ctx, int depth)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      set_stage_shape(ctx, ctx->stage_budget, depth);
    });
 }
 
@@ -2899,16 +2935,17 @@ int fac_set_fused_residual(fac_ctx *ctx, int on)
 }
 
 // Autotuner of the staged pass: rebuild the units for each candidate stage
-// size, time a red-black sweep of every staged level (CUDA events, best of
-// three), keep the fastest.  Uses the smoothing fields (E, R or their FP32
-// copies) as scratch, so it belongs before a solve.
-int fac_autotune(fac_ctx *ctx, int *chosen, double *ms_per_candidate)
+// size and depth, time a red-black sweep of every staged level (CUDA
+// events, best of three), keep the fastest.  Uses the smoothing fields (E,
+// R or their FP32 copies) as scratch, so it belongs before a solve.
+int fac_autotune(fac_ctx *ctx, int *chosen_bytes, int *chosen_depth, double *ms_per_candidate)
 {
    return guarded([&] {
       check_ops(ctx);
       if (ctx->device < 0) throw FacError(FAC_ERR_STATE, "host-only context");
       static const int cand[] = {12 * 1024, 16 * 1024, 24 * 1024, 32 * 1024, 48 * 1024};
       const int nc = (int)(sizeof(cand) / sizeof(cand[0]));
+      static const int depths[] = {2, 3};
       cudaEvent_t e0, e1;
       CUDA_CHECK(cudaEventCreate(&e0));
       CUDA_CHECK(cudaEventCreate(&e1));
@@ -2922,35 +2959,36 @@ int fac_autotune(fac_ctx *ctx, int *chosen, double *ms_per_candidate)
       } ev{e0, e1};
       const bool was_tracing = ctx->tracing, was_prof = ctx->profiling;
       ctx->tracing = ctx->profiling = false;
-      int best = ctx->stage_budget;
+      int best = ctx->stage_budget, best_depth = ctx->stage_depth;
       float best_ms = 1e30f;
-      for (int k = 0; k < nc; ++k) {
-         if (fac_set_stage_budget(ctx, cand[k]) != FAC_OK)
-            throw FacError(FAC_ERR_CUDA, g_last_error);
-         float t = 1e30f;
-         for (int rep = 0; rep < 3; ++rep) {
-            CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
-            for (int ln = 1; ln < ctx->nlev; ++ln) {
-               if (ctx->mixed) smooth32(ctx, ln, 1);
-               else smooth(ctx, FAC_E, FAC_R, ln, 1, -1.0);
+      for (int kd = 0; kd < 2; ++kd)
+         for (int k = 0; k < nc; ++k) {
+            set_stage_shape(ctx, cand[k], depths[kd]);
+            float t = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+               CUDA_CHECK(cudaEventRecord(e0, ctx->stream));
+               for (int ln = 1; ln < ctx->nlev; ++ln) {
+                  if (ctx->mixed) smooth32(ctx, ln, 1);
+                  else smooth(ctx, FAC_E, FAC_R, ln, 1, -1.0);
+               }
+               CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
+               CUDA_CHECK(cudaEventSynchronize(e1));
+               float ms = 0.f;
+               CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+               t = std::min(t, ms);
             }
-            CUDA_CHECK(cudaEventRecord(e1, ctx->stream));
-            CUDA_CHECK(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-            t = std::min(t, ms);
+            if (ms_per_candidate) ms_per_candidate[kd * nc + k] = t;
+            if (t < best_ms) {
+               best_ms = t;
+               best = cand[k];
+               best_depth = depths[kd];
+            }
          }
-         if (ms_per_candidate) ms_per_candidate[k] = t;
-         if (t < best_ms) {
-            best_ms = t;
-            best = cand[k];
-         }
-      }
       ctx->tracing = was_tracing;
       ctx->profiling = was_prof;
-      if (fac_set_stage_budget(ctx, best) != FAC_OK)
-         throw FacError(FAC_ERR_CUDA, g_last_error);
-      if (chosen) *chosen = best;
+      set_stage_shape(ctx, best, best_depth);
+      if (chosen_bytes) *chosen_bytes = best;
+      if (chosen_depth) *chosen_depth = best_depth;
    });
 }
 

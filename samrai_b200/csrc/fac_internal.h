@@ -136,6 +136,10 @@ struct BcCoefs {
 
 // Largest dynamic shared memory of one CTA of the staged colour pass.
 constexpr int kStageSmemMax = 227 * 1024;
+// staged pass: mbarriers and copy sources ahead of the stages, and the
+// largest ring of stages a CTA holds
+constexpr int kStageBarrierBytes = 128;
+constexpr int kStageDepthMax = 4;
 
 // Shared-memory plan of one unit of the staged colour pass: a run of ns
 // slices (planes in 3-D, rows in 2-D) along the slowest axis of an nx x ny
@@ -253,10 +257,12 @@ struct UnitHdr {
    double dx[3];
    double dxi_d[3];        // 1 / dx in FP64
    float dxi_f[3];         // 1 / dx rounded from FP32 dx, in FP32
-   unsigned mhx, mny;      // ceil(2^32 / hx), ceil(2^32 / ny): q / d = umulhi(q, m)
-                           // for the slot decode (q < 2^14, d <= 1024)
+   unsigned mhx, mny, mnx; // ceil(2^32 / d) for d = hx, ny, nx: q / d = umulhi(q, m)
+                           // for the slot and face decodes (exact for q d < 2^32)
    int nslots;             // hx * rows
    int fmask;              // bit 2*axis+side: the unit has that patch face
+   int cfmask;             // faces of fmask with coarse-fine entries (-2)
+   int pmask;              // faces of fmask with push targets (>= -1)
    int off_u, off_f, off_d[3], off_c;
    int off_push[6];        // per face id 2*axis+side: push targets, -1 if none
    int off_cff[6];         // Ewing fluxes of the same faces, -1 if none

@@ -16,13 +16,14 @@ void add_kernel_launches(long long n);
 // Staged colour pass (fac_stage.cu): units {patch, first copy, copies,
 // header} of the compacted list (active problems only) with their copy
 // lists and headers; stage_bytes is the largest StagePlan::bytes of the
-// units; pushmap gives per face cell where its new value goes (>= 0 a
+// units and depth (2 .. kStageDepthMax) the stages a CTA cycles through;
+// pushmap gives per face cell where its new value goes (>= 0 a
 // neighbour's ghost cell, -1 physical boundary, -2 coarse-fine face); err is
 // set to 1 when a bounded wait runs out.  The field's face ghost cells must
 // be filled before the first pass.
 template <class T>
 void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nunits,
-                      int stage_bytes, const Chunk *units, const UnitCopy *copies,
+                      int stage_bytes, int depth, const Chunk *units, const UnitCopy *copies,
                       const unsigned char *headers, T *u, const T *f, const T *dside,
                       const T *cfield, const T *cfflux, int offset, const int *pushmap,
                       const BcCoefs &bc, int *err);

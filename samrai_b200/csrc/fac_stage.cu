@@ -2,25 +2,29 @@
 //
 // A CTA walks its share of the level's work units -- runs of slices of one
 // patch along the patch's slowest axis -- through a ring of shared-memory
-// stages.  One producer warp copies each unit's data from HBM into a stage
-// with TMA bulk copies (cp.async.bulk, completion counted on the stage's
-// "full" mbarrier): u over the unit's slices and one slice either side,
-// ghost cells included, f, the side arrays of D, C, and for the unit's patch
-// faces the push targets and Ewing fluxes.  Eight consumer warps update the
-// cells of the active colour from the staged values with the arithmetic of
-// compflux + rbgswithfluxmax (2d.f:10-364, 3d.f:10-484; --fmad=false), store
-// each new value to HBM, and push new face values where the ghost fill would
-// have put them: into the neighbour patch's ghost cell, or the homogeneous
-// Robin value into the patch's own ghost cell at a physical boundary.  Each
-// consumer warp releases the stage on its "empty" mbarrier.
+// stages (2 to 4, a launch parameter).  One producer warp copies each unit's
+// data from HBM into a stage with TMA bulk copies (cp.async.bulk, completion
+// counted on the stage's "full" mbarrier): u over the unit's slices and one
+// slice either side, ghost cells included, f, the side arrays of D, C, and
+// for the unit's patch faces the push targets and Ewing fluxes.  Eight
+// consumer warps then treat the unit in two phases.  Update: the cells of
+// the active colour get their new values from the staged values with the
+// arithmetic of compflux + rbgswithfluxmax (2d.f:10-364, 3d.f:10-484;
+// --fmad=false), stored to HBM and over the staged old value.  Push: after
+// a named barrier of the consumers, the new values of the active face cells
+// go where the ghost fill would have put them -- into the neighbour patch's
+// ghost cell, or the homogeneous Robin value into the patch's own ghost
+// cell at a physical boundary.  Each consumer warp then releases the stage
+// on its "empty" mbarrier.
 //
 // Race freedom within a pass: a unit reads cells of the other colour only
 // (its own slices, the neighbouring slices and the ghost cells that hold the
-// other colour's pushed values), and writes cells of the active colour and
-// ghost cells next to cells of the other colour, which no unit reads in
-// this pass.  The ghost cells must be filled before the first pass of a
-// smoothing call; they are then kept current by the pushes except the
-// edge and corner ghost cells, which the 7-point stencil never reads.
+// other colour's pushed values) besides each active cell's own old value,
+// and writes cells of the active colour and ghost cells next to cells of
+// the other colour, which no unit reads in this pass.  The ghost cells must
+// be filled before the first pass of a smoothing call; they are then kept
+// current by the pushes except the edge and corner ghost cells, which the
+// 7-point stencil never reads.
 #include <cuda_runtime.h>
 
 #include "fac_device.h"
@@ -80,13 +84,13 @@ __device__ __forceinline__ void bulk_load(void *sdst, const void *gsrc, unsigned
 constexpr int kConsumerWarps = 8;
 constexpr int kConsumers = kConsumerWarps * 32;
 constexpr int kStageBlock = kConsumers + 32;  // + one producer warp
-constexpr int kStages = 3;
-// full[3], empty[3] mbarriers and the copy sources (StageBases)
-constexpr int kBarrierBytes = 128;
+// full[depth], empty[depth] mbarriers and the copy sources (StageBases)
+constexpr int kBarrierBytes = kStageBarrierBytes;
 
-// q / d for 0 <= q < 2^14 and 1 <= d <= 2^10 with m = ceil(2^32 / d):
-// q m / 2^32 exceeds q / d by less than 2^-18 < 1 / d, so the high word
-// of the product is the quotient (integer pipe, no conversions).
+// q / d with m = ceil(2^32 / d) = (2^32 + r) / d, 0 <= r < d: q m / 2^32 =
+// q / d + q r / (d 2^32), and the excess stays below 1 / d (so the high word
+// of the product is the quotient) whenever q d < 2^32.  The host checks
+// that bound for every decode of a unit (integer pipe, no conversions).
 __device__ __forceinline__ int udiv(int q, unsigned m)
 {
    return (int)__umulhi((unsigned)q, m);
@@ -112,29 +116,282 @@ __device__ __forceinline__ bool wait_phase(unsigned long long *bar, unsigned par
    return true;
 }
 
+// OR of a predicate over the consumer warps: named barrier 1, which the
+// producer warp never takes.  Orders the consumers' shared-memory accesses
+// before it against those after it.
+__device__ __forceinline__ bool consumers_any(bool p)
+{
+   unsigned r;
+   asm volatile(
+      "{\n"
+      " .reg .pred pi, po;\n"
+      " setp.ne.u32 pi, %1, 0;\n"
+      " bar.red.or.pred po, 1, %2, pi;\n"
+      " selp.u32 %0, 1, 0, po;\n"
+      "}\n"
+      : "=r"(r)
+      : "r"((unsigned)p), "n"(kConsumers)
+      : "memory");
+   return r != 0;
+}
+
 // Source arrays of the bulk copies, indexed by StageSrc.
 struct StageBases {
    const char *p[kSrcCount];
 };
 
-static_assert(3 * 2 * 8 + sizeof(StageBases) <= kBarrierBytes, "barrier area");
+static_assert(2 * kStageDepthMax * 8 + sizeof(StageBases) <= kBarrierBytes, "barrier area");
+
+// Red-black parity of a row of a unit: the first active cell of the row is
+// at li = ioffset (2d.f:141-147, 3d.f:201-207 with their integer modulo).
+__device__ __forceinline__ int row_ioffset(int q, int offset)
+{
+   return (q - (q / 2) * 2) != offset ? 1 : 0;
+}
+
+// Phase 1 of a unit: the new values of the active colour, stored to HBM and
+// over the staged old values (which no other cell of this pass reads).
+template <int DIM, bool DVAR, int CKIND, class T>
+__device__ __forceinline__ void stage_update(unsigned char *stage, int tid, T *__restrict__ u,
+                                             int offset, T dconst, T cconst)
+{
+   const UnitHdr *h = reinterpret_cast<const UnitHdr *>(stage);
+   const int s0 = h->s0;
+   const int lo0 = h->lo[0], lo1 = h->lo[1], lo2 = DIM == 3 ? h->lo[2] : 0;
+   const int nx = h->hi[0] - lo0 + 1;
+   const int ny = h->hi[1] - lo1 + 1;
+   const int gx = nx + 2, gy = ny + 2;
+   const int sy = gx, sz = gx * gy;
+   T *su = reinterpret_cast<T *>(stage + h->off_u);
+   const T *sf = reinterpret_cast<const T *>(stage + h->off_f);
+   const T *sdx = reinterpret_cast<const T *>(stage + h->off_d[0]);
+   const T *sdy = reinterpret_cast<const T *>(stage + h->off_d[1]);
+   const T *sdz = reinterpret_cast<const T *>(stage + h->off_d[2]);
+   const T *sc = reinterpret_cast<const T *>(stage + h->off_c);
+   // faces of the unit with coarse-fine entries, whose fluxes are the
+   // staged Ewing fluxes
+   const int cfm = h->cfmask;
+   const int ns = h->ns;
+   // global element of staged u element 0 (the slice before the unit)
+   T *gu = u + h->off1 + (long long)s0 * (DIM == 3 ? (long long)sz : (long long)gx);
+   const int hx = h->hx;
+   const int nslots = h->nslots;
+   const unsigned mhx = h->mhx, mny = h->mny;
+   const T one = (T)1;
+   const bool f64 = sizeof(T) == 8;
+   const T dxi = f64 ? (T)h->dxi_d[0] : (T)h->dxi_f[0];
+   const T dyi = f64 ? (T)h->dxi_d[1] : (T)h->dxi_f[1];
+   const T dzi = DIM == 3 ? (f64 ? (T)h->dxi_d[2] : (T)h->dxi_f[2]) : (T)0;
+   const T rcoef = one;
+   // parity of the first cell of each row: lo1 + j (2-D), lo0 + j + k (3-D)
+   const int qbase = DIM == 3 ? lo0 + lo1 + lo2 + s0 : 2 * lo1 + s0;
+   for (int t = tid; t < nslots; t += kConsumers) {
+      const int row = udiv(t, mhx);
+      const int mm = t - row * hx;
+      int lj, ls;
+      if (DIM == 3) {
+         ls = udiv(row, mny);
+         lj = row - ls * ny;
+      } else {
+         lj = s0 + row;
+         ls = row;
+      }
+      const int li = row_ioffset(DIM == 3 ? qbase + lj + ls : qbase + row, offset) + 2 * mm;
+      if (li >= nx) continue;
+      const int c = DIM == 3 ? (li + 1) + gx * ((lj + 1) + gy * (ls + 1))
+                             : (li + 1) + gx * (ls + 1);
+      const T uc = su[c];
+      T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
+      if (DVAR) {
+         if (DIM == 3) {
+            const int bx = li + (nx + 1) * (lj + ny * ls);
+            dx0 = sdx[bx];
+            dx1 = sdx[bx + 1];
+            const int by = li + nx * (lj + (ny + 1) * ls);
+            dy0 = sdy[by];
+            dy1 = sdy[by + nx];
+            const int bz = li + nx * (lj + ny * ls);
+            dz0 = sdz[bz];
+            dz1 = sdz[bz + nx * ny];
+         } else {
+            const int bx = li + (nx + 1) * ls;
+            dx0 = sdx[bx];
+            dx1 = sdx[bx + 1];
+            const int by = li + nx * ls;
+            dy0 = sdy[by];
+            dy1 = sdy[by + nx];
+         }
+      } else {
+         dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
+      }
+      const T nxl = su[c - 1], nxh = su[c + 1];
+      const T nyl = su[c - sy], nyh = su[c + sy];
+      T nzl = (T)0, nzh = (T)0;
+      if (DIM == 3) {
+         nzl = su[c - sz];
+         nzh = su[c + sz];
+      }
+      T fxl = dxi * dx0 * (uc - nxl);
+      T fxh = dxi * dx1 * (nxh - uc);
+      T fyl = dyi * dy0 * (uc - nyl);
+      T fyh = dyi * dy1 * (nyh - uc);
+      T fzl = (T)0, fzh = (T)0;
+      if (DIM == 3) {
+         fzl = dzi * dz0 * (uc - nzl);
+         fzh = dzi * dz1 * (nzh - uc);
+      }
+      if (cfm) {
+         // coarse-fine faces this cell lies on (bit 2*axis+side)
+         int on = 0;
+         on |= li == 0 ? 1 : 0;
+         on |= li == nx - 1 ? 2 : 0;
+         on |= lj == 0 ? 4 : 0;
+         on |= lj == ny - 1 ? 8 : 0;
+         if (DIM == 3) {
+            on |= ls == 0 ? 16 : 0;
+            on |= ls == ns - 1 ? 32 : 0;
+         }
+         on &= cfm;
+         if (on) {
+#pragma unroll
+            for (int fid = 0; fid < 2 * DIM; ++fid) {
+               if (!(on & (1 << fid))) continue;
+               const int a = fid >> 1;
+               // index of the cell in the face region of axis a
+               const int e = a == 0 ? (DIM == 3 ? lj + ny * ls : ls)
+                                    : (a == DIM - 1 ? (DIM == 3 ? li + nx * lj : li)
+                                                    : li + nx * ls);
+               if (reinterpret_cast<const int *>(stage + h->off_push[fid])[e] != -2) continue;
+               const T fl = reinterpret_cast<const T *>(stage + h->off_cff[fid])[e];
+               switch (fid) {
+                  case 0: fxl = fl; break;
+                  case 1: fxh = fl; break;
+                  case 2: fyl = fl; break;
+                  case 3: fyh = fl; break;
+                  case 4: fzl = fl; break;
+                  default: fzh = fl; break;
+               }
+            }
+         }
+      }
+      const int l0 = DIM == 3 ? li + nx * (lj + ny * ls) : li + nx * ls;
+      const T scv = CKIND == 2 ? sc[l0] : (CKIND == 1 ? cconst : (T)0);
+      const T fv = sf[l0];
+      T residual, dudr;
+      if (DIM == 2) {
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - scv * uc;
+         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - scv);
+      } else {
+         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - scv * uc;
+         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) - scv);
+      }
+      const T du = -residual * dudr;
+      const T v = uc + du * rcoef;
+      gu[c] = v;
+      su[c] = v;
+   }
+}
+
+// Phase 2 of a unit: the new values of the active cells on the unit's patch
+// faces go where the ghost fill would put them -- the neighbour patch's
+// ghost cell, or the homogeneous Robin value into the patch's own ghost cell
+// at a physical boundary.  One flat loop over the entries of the faces
+// with push targets (pmask), so that no thread walks six face tests.
+template <int DIM, class T>
+__device__ __forceinline__ void stage_push(const unsigned char *stage, int tid,
+                                           T *__restrict__ u, int offset, const BcCoefs &bc)
+{
+   const UnitHdr *h = reinterpret_cast<const UnitHdr *>(stage);
+   const int pm = h->pmask;
+   if (!pm) return;
+   const int s0 = h->s0, ns = h->ns;
+   const int lo0 = h->lo[0], lo1 = h->lo[1], lo2 = DIM == 3 ? h->lo[2] : 0;
+   const int nx = h->hi[0] - lo0 + 1;
+   const int ny = h->hi[1] - lo1 + 1;
+   const int gx = nx + 2, gy = ny + 2;
+   const int sz = gx * gy;
+   const T *su = reinterpret_cast<const T *>(stage + h->off_u);
+   T *gu = u + h->off1 + (long long)s0 * (DIM == 3 ? (long long)sz : (long long)gx);
+   const unsigned mnx = h->mnx, mny = h->mny;
+   const int qbase = DIM == 3 ? lo0 + lo1 + lo2 + s0 : 2 * lo1 + s0;
+   // entries of each face region (0 for faces without push targets)
+   int cnt[2 * DIM];
+   int total = 0;
+#pragma unroll
+   for (int f = 0; f < 2 * DIM; ++f) {
+      const int a = f >> 1;
+      const int n = a == 0 ? (DIM == 3 ? ny * ns : ns) : (a == DIM - 1 ? (DIM == 3 ? nx * ny : nx)
+                                                                       : nx * ns);
+      cnt[f] = (pm >> f) & 1 ? n : 0;
+      total += cnt[f];
+   }
+   for (int t = tid; t < total; t += kConsumers) {
+      int f = 0, e = t;
+#pragma unroll
+      for (int q = 0; q < 2 * DIM - 1; ++q)
+         if (f == q && e >= cnt[q]) {
+            e -= cnt[q];
+            f = q + 1;
+         }
+      const int a = f >> 1, side = f & 1;
+      int li, lj, ls;
+      if (DIM == 3) {
+         if (a == 0) {
+            ls = udiv(e, mny);
+            lj = e - ls * ny;
+            li = side ? nx - 1 : 0;
+         } else if (a == 1) {
+            ls = udiv(e, mnx);
+            li = e - ls * nx;
+            lj = side ? ny - 1 : 0;
+         } else {
+            lj = udiv(e, mnx);
+            li = e - lj * nx;
+            ls = side ? ns - 1 : 0;
+         }
+      } else {
+         if (a == 0) {
+            ls = e;
+            li = side ? nx - 1 : 0;
+         } else {
+            li = e;
+            ls = side ? ns - 1 : 0;
+         }
+         lj = s0 + ls;
+      }
+      const int q = DIM == 3 ? qbase + lj + ls : qbase + ls;
+      if ((li & 1) != row_ioffset(q, offset)) continue;  // not of the active colour
+      const int tgt = reinterpret_cast<const int *>(stage + h->off_push[f])[e];
+      if (tgt < -1) continue;  // coarse-fine face: no push
+      const int c = DIM == 3 ? (li + 1) + gx * ((lj + 1) + gy * (ls + 1))
+                             : (li + 1) + gx * (ls + 1);
+      const T v = su[c];
+      if (tgt >= 0) {
+         u[tgt] = v;
+      } else {
+         const int step = a == 0 ? 1 : (a == 1 ? gx : sz);
+         gu[side ? c + step : c - step] = robin<T>(v, f, (T)h->dx[a], 1, bc);
+      }
+   }
+}
 
 template <int DIM, bool DVAR, int CKIND, class T>
 __global__ void __launch_bounds__(kStageBlock)
 k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restrict__ copies,
-            StageBases bases, int stage_bytes, T *__restrict__ u, int offset, T dconst,
-            T cconst, BcCoefs bc, int *__restrict__ err)
+            StageBases bases, int stage_bytes, int depth, T *__restrict__ u, int offset,
+            T dconst, T cconst, BcCoefs bc, int *__restrict__ err)
 {
    extern __shared__ __align__(128) unsigned char smem[];
    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem);
-   unsigned long long *empty = full + kStages;
-   StageBases *sbases = reinterpret_cast<StageBases *>(smem + 2 * kStages * 8);
+   unsigned long long *empty = full + kStageDepthMax;
+   StageBases *sbases = reinterpret_cast<StageBases *>(smem + 2 * kStageDepthMax * 8);
    unsigned char *stages = smem + kBarrierBytes;
    // the list holds active problems only (compacted), so the units of this
    // block are w = blockIdx.x, + gridDim.x, ... up to the end marker
    auto valid = [&](int w) { return w < nwork && chunks[w].patch >= 0; };
    if (threadIdx.x == 0) {
-      for (int k = 0; k < kStages; ++k) {
+      for (int k = 0; k < depth; ++k) {
          mbar_init_count(&full[k], 1);
          mbar_init_count(&empty[k], kConsumerWarps);
       }
@@ -153,9 +410,9 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
          const Chunk chn = wn < nwork ? chunks[wn] : Chunk{-1, 0, 0, 0};  // prefetch
          UnitCopy cp = {0, 0, 0, 0, 0};
          if (lane < ch.count) cp = copies[ch.begin + lane];
-         const int st = k % kStages;
+         const int st = k % depth;
          bool ok = true;
-         if (k >= kStages && lane == 0) ok = wait_phase(&empty[st], ((k / kStages) & 1) ^ 1u);
+         if (k >= depth && lane == 0) ok = wait_phase(&empty[st], ((k / depth) & 1) ^ 1u);
          if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
             if (lane == 0) atomicExch(err, 1);
             return;
@@ -176,170 +433,21 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
    bool cur = valid(blockIdx.x);
    for (int w = blockIdx.x; cur; w += gridDim.x, ++k) {
       const bool nxt = valid(w + gridDim.x);  // prefetched, used at the loop end
-      const int st = k % kStages;
+      const int st = k % depth;
+      const unsigned par = (k / depth) & 1;
       unsigned char *stage = stages + st * stage_bytes;
-      if (!wait_phase(&full[st], (k / kStages) & 1)) {
-         atomicExch(err, 1);
-         wait_phase(&full[st], (k / kStages) & 1);
+      const bool ok = wait_phase(&full[st], par);
+      if (ok) stage_update<DIM, DVAR, CKIND, T>(stage, tid, u, offset, dconst, cconst);
+      // every consumer passes here once per unit: all leave together when
+      // any wait ran out, and the pushes read the updated stage
+      if (consumers_any(!ok)) {
+         if (tid == 0) atomicExch(err, 1);
+         wait_phase(&full[st], par);  // copies still in flight land before the exit
          return;
       }
-      const UnitHdr *h = reinterpret_cast<const UnitHdr *>(stage);
-      const int s0 = h->s0, ns = h->ns;
-      const int lo0 = h->lo[0], lo1 = h->lo[1], lo2 = DIM == 3 ? h->lo[2] : 0;
-      const int nx = h->hi[0] - lo0 + 1;
-      const int ny = h->hi[1] - lo1 + 1;
-      const int gx = nx + 2, gy = ny + 2;
-      const int sy = gx, sz = gx * gy;
-      const T *su = reinterpret_cast<const T *>(stage + h->off_u);
-      const T *sf = reinterpret_cast<const T *>(stage + h->off_f);
-      const T *sdx = reinterpret_cast<const T *>(stage + h->off_d[0]);
-      const T *sdy = reinterpret_cast<const T *>(stage + h->off_d[1]);
-      const T *sdz = reinterpret_cast<const T *>(stage + h->off_d[2]);
-      const T *sc = reinterpret_cast<const T *>(stage + h->off_c);
-      const bool has_cf = (h->flags & 1) != 0;
-      const int fmask = h->fmask;
-      // global element of staged u element 0 (the slice before the unit)
-      T *gu = u + h->off1 + (long long)s0 * (DIM == 3 ? (long long)sz : (long long)gx);
-      const int hx = h->hx;
-      const int nslots = h->nslots;
-      const unsigned mhx = h->mhx, mny = h->mny;
-      const T one = (T)1;
-      const bool f64 = sizeof(T) == 8;
-      const T dxi = f64 ? (T)h->dxi_d[0] : (T)h->dxi_f[0];
-      const T dyi = f64 ? (T)h->dxi_d[1] : (T)h->dxi_f[1];
-      const T dzi = DIM == 3 ? (f64 ? (T)h->dxi_d[2] : (T)h->dxi_f[2]) : (T)0;
-      const T rcoef = one;
-      // parity of the first cell of each row: lo1 + j (2-D), lo0 + j + k (3-D)
-      const int qbase = DIM == 3 ? lo0 + lo1 + lo2 + s0 : 2 * lo1 + s0;
-      for (int t = tid; t < nslots; t += kConsumers) {
-         const int row = udiv(t, mhx);
-         const int mm = t - row * hx;
-         int lj, ls;
-         if (DIM == 3) {
-            ls = udiv(row, mny);
-            lj = row - ls * ny;
-         } else {
-            lj = s0 + row;
-            ls = row;
-         }
-         const int q = DIM == 3 ? qbase + lj + ls : qbase + row;
-         const int ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
-         const int li = ioffset + 2 * mm;
-         if (li >= nx) continue;
-         const int c = DIM == 3 ? (li + 1) + gx * ((lj + 1) + gy * (ls + 1))
-                                : (li + 1) + gx * (ls + 1);
-         const T uc = su[c];
-         T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
-         if (DVAR) {
-            if (DIM == 3) {
-               const int bx = li + (nx + 1) * (lj + ny * ls);
-               dx0 = sdx[bx];
-               dx1 = sdx[bx + 1];
-               const int by = li + nx * (lj + (ny + 1) * ls);
-               dy0 = sdy[by];
-               dy1 = sdy[by + nx];
-               const int bz = li + nx * (lj + ny * ls);
-               dz0 = sdz[bz];
-               dz1 = sdz[bz + nx * ny];
-            } else {
-               const int bx = li + (nx + 1) * ls;
-               dx0 = sdx[bx];
-               dx1 = sdx[bx + 1];
-               const int by = li + nx * ls;
-               dy0 = sdy[by];
-               dy1 = sdy[by + nx];
-            }
-         } else {
-            dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
-         }
-         const T nxl = su[c - 1], nxh = su[c + 1];
-         const T nyl = su[c - sy], nyh = su[c + sy];
-         T nzl = (T)0, nzh = (T)0;
-         if (DIM == 3) {
-            nzl = su[c - sz];
-            nzh = su[c + sz];
-         }
-         T fxl = dxi * dx0 * (uc - nxl);
-         T fxh = dxi * dx1 * (nxh - uc);
-         T fyl = dyi * dy0 * (uc - nyl);
-         T fyh = dyi * dy1 * (nyh - uc);
-         T fzl = (T)0, fzh = (T)0;
-         if (DIM == 3) {
-            fzl = dzi * dz0 * (uc - nzl);
-            fzh = dzi * dz1 * (nzh - uc);
-         }
-         // faces of the unit this cell lies on (bit 2*axis+side)
-         int on = 0;
-         on |= li == 0 ? 1 : 0;
-         on |= li == nx - 1 ? 2 : 0;
-         if (DIM == 3) {
-            on |= lj == 0 ? 4 : 0;
-            on |= lj == ny - 1 ? 8 : 0;
-            on |= ls == 0 ? 16 : 0;
-            on |= ls == ns - 1 ? 32 : 0;
-         } else {
-            on |= lj == 0 ? 4 : 0;
-            on |= lj == ny - 1 ? 8 : 0;
-         }
-         on &= fmask;
-         // index of the cell in a face region of axis a
-         auto face_entry = [&](int fid) -> int {
-            const int a = fid >> 1;
-            if (a == 0) return DIM == 3 ? lj + ny * ls : ls;
-            if (a == DIM - 1) return DIM == 3 ? li + nx * lj : li;
-            return li + nx * ls;
-         };
-         if (has_cf && on) {
-#pragma unroll
-            for (int fid = 0; fid < 2 * DIM; ++fid) {
-               if (!(on & (1 << fid))) continue;
-               const int e = face_entry(fid);
-               if (reinterpret_cast<const int *>(stage + h->off_push[fid])[e] != -2) continue;
-               const T fl = reinterpret_cast<const T *>(stage + h->off_cff[fid])[e];
-               switch (fid) {
-                  case 0: fxl = fl; break;
-                  case 1: fxh = fl; break;
-                  case 2: fyl = fl; break;
-                  case 3: fyh = fl; break;
-                  case 4: fzl = fl; break;
-                  default: fzh = fl; break;
-               }
-            }
-         }
-         const int l0 = DIM == 3 ? li + nx * (lj + ny * ls) : li + nx * ls;
-         const T scv = CKIND == 2 ? sc[l0] : (CKIND == 1 ? cconst : (T)0);
-         const T fv = sf[l0];
-         T residual, dudr;
-         if (DIM == 2) {
-            residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - scv * uc;
-            dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - scv);
-         } else {
-            const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
-            residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
-                       scv * uc;
-            dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
-                          scv);
-         }
-         const T du = -residual * dudr;
-         const T v = uc + du * rcoef;
-         // the new value, and its copies where the ghost fill puts them
-         gu[c] = v;
-         if (on) {
-#pragma unroll
-            for (int fid = 0; fid < 2 * DIM; ++fid) {
-               if (!(on & (1 << fid))) continue;
-               const int tgt = reinterpret_cast<const int *>(stage + h->off_push[fid])[face_entry(fid)];
-               if (tgt >= 0) {
-                  u[tgt] = v;
-               } else if (tgt == -1) {
-                  const int a = fid >> 1;
-                  const int step = a == 0 ? 1 : (a == 1 ? gx : sz);
-                  gu[(fid & 1) ? c + step : c - step] = robin<T>(v, fid, (T)h->dx[a], 1, bc);
-               }
-            }
-         }
-      }
-      // release the stage: every lane of this warp is done with it
+      stage_push<DIM, T>(stage, tid, u, offset, bc);
+      // the next copies into this stage (async proxy) follow the stores above
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);
       cur = nxt;
@@ -347,7 +455,7 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
 }
 
 template <int DIM, bool DVAR, int CK, class T>
-void staged_inst(cudaStream_t s, int nunits, int stage_bytes, const Chunk *units,
+void staged_inst(cudaStream_t s, int nunits, int stage_bytes, int depth, const Chunk *units,
                  const UnitCopy *copies, const StageBases &bases, T *u, int offset,
                  double dconst, double cconst, const BcCoefs &bc, int *err)
 {
@@ -361,7 +469,7 @@ void staged_inst(cudaStream_t s, int nunits, int stage_bytes, const Chunk *units
          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
       attr = true;
    }
-   const int smem = kBarrierBytes + kStages * stage_bytes;
+   const int smem = kBarrierBytes + depth * stage_bytes;
    // one wave of resident blocks: each walks its share of the units
    int per_sm = 1;
    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_staged<DIM, DVAR, CK, T>,
@@ -369,14 +477,15 @@ void staged_inst(cudaStream_t s, int nunits, int stage_bytes, const Chunk *units
    per_sm = per_sm < 1 ? 1 : per_sm;
    const int grid = nunits < nsm * per_sm ? nunits : nsm * per_sm;
    k_rb_staged<DIM, DVAR, CK, T><<<grid, kStageBlock, smem, s>>>(
-      units, nunits, copies, bases, stage_bytes, u, offset, (T)dconst, (T)cconst, bc, err);
+      units, nunits, copies, bases, stage_bytes, depth, u, offset, (T)dconst, (T)cconst, bc,
+      err);
 }
 
 }  // namespace
 
 template <class T>
 void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nunits,
-                      int stage_bytes, const Chunk *units, const UnitCopy *copies,
+                      int stage_bytes, int depth, const Chunk *units, const UnitCopy *copies,
                       const unsigned char *headers, T *u, const T *f, const T *dside,
                       const T *cfield, const T *cfflux, int offset, const int *pushmap,
                       const BcCoefs &bc, int *err)
@@ -392,7 +501,7 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
    bases.p[kSrcFlux] = reinterpret_cast<const char *>(cfflux);
    bases.p[kSrcHdr] = reinterpret_cast<const char *>(headers);
 #define SG(D, V, C)                                                                       \
-   staged_inst<D, V, C, T>(s, nunits, stage_bytes, units, copies, bases, u, offset,      \
+   staged_inst<D, V, C, T>(s, nunits, stage_bytes, depth, units, copies, bases, u, offset, \
                            spec.d_const, spec.c_const, bc, err)
    if (dim == 2) {
       if (spec.d_variable) {
@@ -419,7 +528,7 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
 }
 
 #define INST_STAGED(T)                                                                       \
-   template void launch_rb_staged<T>(cudaStream_t, int, const PoissonSpec &, int, int,         \
+   template void launch_rb_staged<T>(cudaStream_t, int, const PoissonSpec &, int, int, int,    \
                                      const Chunk *, const UnitCopy *, const unsigned char *,   \
                                      T *, const T *, const T *, const T *, const T *, int,     \
                                      const int *, const BcCoefs &, int *);

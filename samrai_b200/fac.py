@@ -74,7 +74,9 @@ def load_library(build_if_missing=True):
         "fac_learned_samples": (ctypes.c_int, [vp, ctypes.c_int, vp, dp]),
         "fac_set_fused_residual": (ctypes.c_int, [vp, ctypes.c_int]),
         "fac_set_stage_budget": (ctypes.c_int, [vp, ctypes.c_int]),
-        "fac_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), dp]),
+        "fac_set_stage_depth": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int), dp]),
         "fac_field_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, szp]),
         "fac_side_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
         "fac_oside_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, szp]),
@@ -164,6 +166,7 @@ class FacContext:
         self.dim = problems[0].dim
         self.nlev = problems[0].nlev
         self.device = device
+        self.stage_depth = 2
         h = ctypes.c_void_p()
         _check(L.fac_ctx_create(ctypes.byref(h), self.dim, device))
         self.h = h
@@ -338,15 +341,23 @@ class FacContext:
         _check(load_library().fac_synchronize(self.h))
 
     def autotune(self):
-        """Pick the staged pass's stage size by timing (before a solve);
-        returns (chosen bytes, ms per candidate)."""
+        """Pick the staged pass's stage size and depth by timing (before a
+        solve); returns (chosen bytes, ms per candidate) with the candidates
+        of depth 2 then depth 3; the depth is in stage_depth."""
         chosen = ctypes.c_int(0)
-        ms = np.zeros(5)
-        _check(load_library().fac_autotune(self.h, ctypes.byref(chosen), _dp(ms)))
+        depth = ctypes.c_int(0)
+        ms = np.zeros(10)
+        _check(load_library().fac_autotune(self.h, ctypes.byref(chosen), ctypes.byref(depth),
+                                           _dp(ms)))
+        self.stage_depth = depth.value
         return chosen.value, ms
 
     def set_stage_budget(self, nbytes):
         _check(load_library().fac_set_stage_budget(self.h, int(nbytes)))
+
+    def set_stage_depth(self, depth):
+        _check(load_library().fac_set_stage_depth(self.h, int(depth)))
+        self.stage_depth = int(depth)
 
     def set_fused_residual(self, on=True):
         _check(load_library().fac_set_fused_residual(self.h, int(on)))

@@ -256,12 +256,18 @@ def test_fused_and_staged_colour_passes_match_filled(case, precision, require_gp
         probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (41, 42)]
     prm = dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=2 if case == "config2" else 6)
     out = []
-    # fused passes on staged shared-memory units, fused passes reading HBM,
-    # and passes between ghost fills
-    for fused, staged in ((True, True), (True, False), (False, False)):
+    # fused passes on staged shared-memory units (default stages; three and
+    # four stages of small units, so that patches are cut into several
+    # units), fused passes reading HBM, and passes between ghost fills
+    for fused, staged, depth, budget in ((True, True, None, None), (True, True, 3, 8192),
+                                         (True, True, 4, 4096), (True, False, None, None),
+                                         (False, False, None, None)):
         g = fac.FacContext(probs, params=prm, precision=precision)
         g.set_fused(fused)
         g.set_staged(staged)
+        if depth:
+            g.set_stage_depth(depth)
+            g.set_stage_budget(budget)
         conv, its, res = g.solve()
         fields = [g.download(U, i, ln) for i in range(len(probs)) for ln in range(probs[0].nlev)]
         g.smooth(E, R, probs[0].nlev - 1, 3)
@@ -314,7 +320,8 @@ def test_autotune_keeps_results(require_gpu):
         if tune:
             chosen, ms = g.autotune()
             assert chosen in (12288, 16384, 24576, 32768, 49152)
-            assert np.all(ms > 0)
+            assert g.stage_depth in (2, 3)
+            assert ms.shape == (10,) and np.all(ms > 0)
         g.zero(U)
         conv, its, res = g.solve()
         out.append((its.copy(), res.copy(), [g.download(U, i, ln) for i in range(2)
