@@ -263,6 +263,7 @@ def main():
         ctx.close()
         ctx = fac.FacContext(mg, params=dict(PARAMS_MG, max_cycles=args.cycles),
                              device=local_rank, precision=args.precision)
+        ctx.set_krylov(args.krylov)
         ctx.timer_start()
         conv, its, res = ctx.solve()
         ms = ctx.timer_stop()

@@ -276,12 +276,15 @@ int fac_trace_read(fac_ctx *ctx, char *buf, int cap, int *len);
 /* Kernels launched by this process so far, over all contexts. */
 int fac_kernel_launches(long long *n);
 /* Record CUDA events around every red-black colour pass (kind 0 FP64,
- * kind 2 FP32) and ghost fill (kind 1 FP64, kind 3 FP32) from now on;
- * clears earlier records.  Bytes count only problems still iterating. */
+ * kind 2 FP32), ghost fill (kind 1 FP64, kind 3 FP32) and FGMRES vector
+ * operation (kind 4 multi-dot, kind 5 linear combination; per level) from
+ * now on; clears earlier records.  Bytes count only problems still
+ * iterating. */
 int fac_profile_enable(fac_ctx *ctx, int on);
 /* Totals over the records of one kind: launches, device milliseconds and
  * algorithmic bytes (colour pass: 8*(ghosted cells + cells) + 8*dim*cells
- * when D is variable; ghost fill: 16 bytes per ghost cell written). */
+ * when D is variable; ghost fill: 16 bytes per ghost cell written; vector
+ * operations on K vectors: 8*(K+2) bytes per cell). */
 int fac_profile_read(fac_ctx *ctx, int kind, long long *launches, double *ms,
                      double *bytes);
 int fac_profile_reset(fac_ctx *ctx);

@@ -10,11 +10,23 @@ namespace samrai_b200 {
 namespace dev {
 
 constexpr int kThreads = 256;
-// Blocks of a chunk kernel: enough to fill the GPU; each block walks the
-// work list with a grid stride.
+// Blocks of a chunk kernel when the occupancy query fails: enough to fill
+// the GPU; each block walks the work list with a grid stride.
 constexpr int kGridCap = 148 * 8;
 
-inline int work_grid(int nchunks) { return nchunks < kGridCap ? nchunks : kGridCap; }
+// Blocks of kernel fn (kThreads threads, no dynamic shared memory) that fit
+// on the device at once: the SMs times the resident blocks per SM, queried
+// once per kernel.
+int resident_blocks(const void *fn);
+
+// Grid of a chunk kernel: one wave of resident blocks at most, so that no
+// block of a second partial wave is left to run alone at the end.
+template <class F>
+inline int work_grid(F *fn, int nchunks)
+{
+   const int cap = resident_blocks(reinterpret_cast<const void *>(fn));
+   return nchunks < cap ? nchunks : cap;
+}
 
 // Grid-stride walk over a work list of nwork entries.  The list is compacted
 // on the device whenever the set of iterating problems changes: the chunks of

@@ -262,6 +262,20 @@ struct ItemList {
    }
 };
 
+// A ghost fill as a gather list: per element of the copy and constant-refine
+// items its destination, source element (coarser level: -source - 1) and
+// problem; the physical-boundary items stay items (bc).
+struct FillGather {
+   std::vector<unsigned> to;
+   std::vector<int> from;
+   std::vector<unsigned short> prob;
+   DevArray<unsigned> d_to;
+   DevArray<int> d_from;
+   DevArray<unsigned short> d_prob;
+   ItemList<FillItem> bc;
+   bool ok = false;  // element indices and problems fit their fields
+};
+
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
@@ -325,9 +339,19 @@ struct LevelState {
    WorkSrc ws_cell, ws_slot, ws_flux;
    std::vector<int> prob_cell_chunk_begin;
    DevArray<int> d_prob_cell_chunk_begin;
+   // Krylov vector chunks: runs of up to kSpanChunk ghost-0 cells of one
+   // problem, {problem, first cell, cells, chunk index}; a problem's patches
+   // are contiguous in the ghost-0 buffers
+   std::vector<Chunk> span_chunks;
+   DevArray<Chunk> d_span_chunks;
+   WorkSrc ws_span;
+   std::vector<int> prob_span_begin;
+   DevArray<int> d_prob_span_begin;
+   std::vector<double> cells_prob;  // ghost-0 cells per problem
    DevArray<double2> norm_partial;
 
    ItemList<FillItem> fill_nc, fill_wc;   // ghost fill without / with coarser level
+   FillGather gather_nc, gather_wc;       // the same fills as gather lists
    std::vector<CfFace> cf;
    DevArray<CfFace> d_cf;
    ItemList<RestrictItem> restrict_g1, restrict_g0;  // from level ln+1 into this
@@ -412,7 +436,7 @@ struct fac_ctx {
       long long n = 0;
       double ms = 0, bytes = 0;
    };
-   KindAcc graph_acc[4];
+   KindAcc graph_acc[6];
    // per-operation wall time with a stream synchronisation on both sides
    // (tbox::Timer::barrierAndStart semantics, tbox/Timer.C:174)
    bool tracing = false;
@@ -1183,6 +1207,28 @@ void build_chunks(fac_ctx *c, int ln)
    L.d_slot_chunks.upload(L.slot_chunks, c->stream);
    L.d_flux_chunks.upload(L.flux_chunks, c->stream);
    L.d_prob_cell_chunk_begin.upload(L.prob_cell_chunk_begin, c->stream);
+   L.span_chunks.clear();
+   L.prob_span_begin.assign(np + 1, 0);
+   for (int p = 0; p < np; ++p) {
+      L.prob_span_begin[p] = (int)L.span_chunks.size();
+      const int pb = L.prob_patch_begin[p], pe = L.prob_patch_begin[p + 1];
+      if (pb == pe) continue;
+      const long long b0 = L.hp[pb].off0;
+      long long e0 = b0;
+      for (int ip = pb; ip < pe; ++ip) {
+         if (L.hp[ip].off0 != e0) throw FacError(FAC_ERR_ARG, "problem cells not contiguous");
+         e0 += L.box[ip].size();
+      }
+      if (e0 >= (1ll << 31)) throw FacError(FAC_ERR_ARG, "level too large for 32-bit chunks");
+      for (long long q = b0; q < e0; q += kSpanChunk)
+         L.span_chunks.push_back({p, (int)q, (int)std::min<long long>(kSpanChunk, e0 - q),
+                                  (int)L.span_chunks.size()});
+   }
+   L.prob_span_begin[np] = (int)L.span_chunks.size();
+   L.cells_prob.assign(np, 0.0);
+   for (int ip = 0; ip < L.npatch; ++ip) L.cells_prob[L.hp[ip].prob] += (double)L.box[ip].size();
+   L.d_span_chunks.upload(L.span_chunks, c->stream);
+   L.d_prob_span_begin.upload(L.prob_span_begin, c->stream);
    L.norm_partial.alloc(std::max<size_t>(1, L.cell_chunks.size()));
    std::vector<int> last(np, 0);
    for (int p = 0; p < np; ++p) last[p] = L.prob_patch_begin[p + 1] - 1;
@@ -1538,6 +1584,70 @@ void validate_fill(ItemList<FillItem> &L, long long dstlen, long long samelen,
    validate_chunks(L, "fill chunk range");
 }
 
+// Gather list of a validated fill.  Falls back to the item kernel (ok =
+// false) when an element index does not fit its 32-bit field or two items
+// share a destination element.
+void build_fill_gather(fac_ctx *c, ItemList<FillItem> &F, FillGather &G, long long dstlen,
+                       long long samelen, long long coarselen)
+{
+   G.to.clear();
+   G.from.clear();
+   G.prob.clear();
+   G.bc.clear();
+   G.ok = dstlen <= 0xffffffffll && samelen < (1ll << 31) && coarselen < (1ll << 31) &&
+          nprob(c) <= 0xffff;
+   auto idx = [](const ArrDesc &A, int i, int j, int k) {
+      return A.base + (long long)(i - A.lo[0]) +
+             (long long)A.n[0] * ((long long)(j - A.lo[1]) + (long long)A.n[1] * (k - A.lo[2]));
+   };
+   auto crs = [](int i, int r) { return i < 0 ? (i + 1) / r - 1 : i / r; };
+   std::vector<unsigned char> seen(G.ok ? std::max<long long>(1, dstlen) : 1, 0);
+   for (const FillItem &it : F.items) {
+      if (!G.ok) break;
+      const Box b = item_box(it.lo, it.hi);
+      if (it.kind == kFillBc) {
+         for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+            for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+               for (int i = b.lo[0]; i <= b.hi[0]; ++i) {
+                  const long long d = idx(it.dst, i, j, k);
+                  if (seen[d]) G.ok = false;
+                  seen[d] = 1;
+               }
+         G.bc.add(it, b.size());
+         continue;
+      }
+      const bool coarse = it.src_is_coarse != 0;
+      const long long slen = coarse ? coarselen : samelen;
+      for (int k = b.lo[2]; k <= b.hi[2] && G.ok; ++k)
+         for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+            for (int i = b.lo[0]; i <= b.hi[0]; ++i) {
+               const long long d = idx(it.dst, i, j, k);
+               const long long sidx =
+                  it.kind == kFillCopy
+                     ? idx(it.src, i, j, k)
+                     : idx(it.src, crs(i, it.ratio[0]), crs(j, it.ratio[1]), crs(k, it.ratio[2]));
+               vcheck(d >= 0 && d < dstlen && sidx >= 0 && sidx < slen, "fill gather element");
+               if (seen[d]) G.ok = false;
+               seen[d] = 1;
+               G.to.push_back((unsigned)d);
+               G.from.push_back(coarse ? -(int)sidx - 1 : (int)sidx);
+               G.prob.push_back((unsigned short)it.prob);
+            }
+      if (G.to.size() >= (size_t)1 << 31) G.ok = false;
+   }
+   if (!G.ok) {
+      G.to.clear();
+      G.from.clear();
+      G.prob.clear();
+      G.bc.clear();
+      return;
+   }
+   G.d_to.upload(G.to, c->stream);
+   G.d_from.upload(G.from, c->stream);
+   G.d_prob.upload(G.prob, c->stream);
+   G.bc.upload(c->stream);
+}
+
 void validate_tables(fac_ctx *c)
 {
    const int dim = c->dim;
@@ -1659,8 +1769,12 @@ void register_work_lists(fac_ctx *c)
       register_work(c, L.ws_cell, L.cell_chunks, L.d_cell_chunks.p, pp);
       register_work(c, L.ws_slot, L.slot_chunks, L.d_slot_chunks.p, pp);
       register_work(c, L.ws_flux, L.flux_chunks, L.d_flux_chunks.p, pp);
+      register_work(c, L.ws_span, L.span_chunks, L.d_span_chunks.p,
+                    [](const Chunk &ch) { return ch.patch; });
       register_items(c, L.fill_nc);
       register_items(c, L.fill_wc);
+      for (FillGather *G : {&L.gather_nc, &L.gather_wc})
+         if (G->ok) register_items(c, G->bc);
       register_items(c, L.restrict_g1);
       register_items(c, L.restrict_g0);
       register_items(c, L.fcoarsen);
@@ -1750,6 +1864,9 @@ void initialize(fac_ctx *c)
       L.d_patches.upload(L.hp, c->stream);  // after cf flags are set
       L.fill_nc.upload(c->stream);
       L.fill_wc.upload(c->stream);
+      const long long clen = ln > 0 ? c->L[ln - 1].n1 : 0;
+      build_fill_gather(c, L.fill_nc, L.gather_nc, L.n1, L.n1, clen);
+      build_fill_gather(c, L.fill_wc, L.gather_wc, L.n1, L.n1, clen);
    }
    register_work_lists(c);
    c->kerr.alloc(1);
@@ -1780,9 +1897,15 @@ void ghost_fill(fac_ctx *c, int fid, int ln, bool with_coarse, int homogeneous, 
    double *dst = field_ptr(L, fid);
    const double *coarse = ln > 0 ? field_ptr(c->L[ln - 1], fid) : nullptr;
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
+   FillGather &G = (with_coarse && ln > 0) ? L.gather_wc : L.gather_nc;
    const int pi = prof_begin(c, 1, L.fill_bytes_prob, 1.0);
-   launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, dst, dst, coarse,
-               homogeneous, c->bc, mask);
+   if (G.ok)
+      launch_fill_gather(c->stream, (long long)G.to.size(), G.d_to.p, G.d_from.p, G.d_prob.p,
+                         G.bc.d_items.p, G.bc.d_chunks.p, G.bc.nchunks(), G.bc.d_prefix.p, dst,
+                         dst, coarse, homogeneous, c->bc, mask);
+   else
+      launch_fill(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, dst, dst,
+                  coarse, homogeneous, c->bc, mask);
    prof_end(c, pi);
 }
 
@@ -2036,10 +2159,16 @@ void ghost_fill32(fac_ctx *c, int ln, bool with_coarse, int homogeneous, const i
    LevelState &L = c->L[ln];
    const float *coarse = ln > 0 ? c->L[ln - 1].e32.p : nullptr;
    ItemList<FillItem> &it = (with_coarse && ln > 0) ? L.fill_wc : L.fill_nc;
-   const int pi =
-      prof_begin(c, 3, L.fill_bytes_prob, 0.5);
-   launch_fill<float>(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, L.e32.p, L.e32.p,
-                      coarse, homogeneous, c->bc, mask);
+   FillGather &G = (with_coarse && ln > 0) ? L.gather_wc : L.gather_nc;
+   const int pi = prof_begin(c, 3, L.fill_bytes_prob, 0.5);
+   if (G.ok)
+      launch_fill_gather<float>(c->stream, (long long)G.to.size(), G.d_to.p, G.d_from.p,
+                                G.d_prob.p, G.bc.d_items.p, G.bc.d_chunks.p, G.bc.nchunks(),
+                                G.bc.d_prefix.p, L.e32.p, L.e32.p, coarse, homogeneous, c->bc,
+                                mask);
+   else
+      launch_fill<float>(c->stream, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p,
+                         L.e32.p, L.e32.p, coarse, homogeneous, c->bc, mask);
    prof_end(c, pi);
 }
 
@@ -2258,13 +2387,15 @@ void solve(fac_ctx *c, int *converged, int *iterations, double *residual)
    if (c->mixed) mixed_prepare(c);
    // one FACPreconditioner cycle up to the norm kernels (no host sync)
    auto cycle_body = [&]() {
-      zero_field(c, FAC_E);
       if (c->mixed) {
+         // the error lives in e32; E is the FP64 coarsest-level solve's
+         CUDA_CHECK(cudaMemsetAsync(c->L[0].e.p, 0, c->L[0].e.n * sizeof(double), c->stream));
          for (int ln = 0; ln < c->nlev; ++ln)
             CUDA_CHECK(cudaMemsetAsync(c->L[ln].e32.p, 0, c->L[ln].e32.n * sizeof(float),
                                        c->stream));
          fac_cycle_mixed(c, c->nlev - 1);
       } else {
+         zero_field(c, FAC_E);
          fac_cycle_recursive(c, c->nlev - 1);
       }
       for (int ln = 0; ln < c->nlev; ++ln) {
@@ -2383,7 +2514,7 @@ void kry_alloc(fac_ctx *c, int m)
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
       L.kry.alloc((size_t)(2 * m + 1) * (size_t)std::max<long long>(1, L.n0));
-      L.kry_partial.alloc((size_t)std::max<size_t>(1, L.cell_chunks.size()) * (m + 1));
+      L.kry_partial.alloc((size_t)std::max<size_t>(1, L.span_chunks.size()) * (m + 1));
       // finite contents: slots a problem did not reach enter x += Z y with y = 0
       CUDA_CHECK(cudaMemsetAsync(L.kry.p, 0, L.kry.n * sizeof(double), c->stream));
    }
@@ -2396,14 +2527,17 @@ void kry_alloc(fac_ctx *c, int m)
 // out[p*K + i] = <x, V_i> (weighted) over all levels, for i < K
 void kry_dots(fac_ctx *c, int xslot, int vslot, int K, std::vector<double> &out)
 {
+   OpTimer ot(c, "kry_dots", -1);
    const int np = nprob(c);
    CUDA_CHECK(cudaMemsetAsync(c->kry_dots.p, 0, (size_t)np * K * sizeof(double), c->stream));
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
-      launch_multidot(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
-                      L.d_cell_chunks.p, L.w.p, kry_vec(c, ln, xslot), kry_vec(c, ln, vslot),
-                      std::max<long long>(1, L.n0), K, L.kry_partial.p,
-                      L.d_prob_cell_chunk_begin.p, np, c->active.p, c->kry_dots.p);
+      const int pi = prof_begin(c, 4, L.cells_prob, 8.0 * (K + 2));
+      launch_multidot(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p, L.w.p,
+                      kry_vec(c, ln, xslot), kry_vec(c, ln, vslot),
+                      std::max<long long>(1, L.n0), K, L.kry_partial.p, L.d_prob_span_begin.p,
+                      np, c->active.p, c->kry_dots.p);
+      prof_end(c, pi);
    }
    out.resize((size_t)np * K);
    CUDA_CHECK(cudaMemcpyAsync(out.data(), c->kry_dots.p, (size_t)np * K * sizeof(double),
@@ -2415,6 +2549,7 @@ void kry_dots(fac_ctx *c, int xslot, int vslot, int K, std::vector<double> &out)
 void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot, int K,
                  const std::vector<double> &coef)
 {
+   OpTimer ot(c, "kry_combine", -1);
    const int np = nprob(c);
    CUDA_CHECK(cudaMemcpyAsync(c->kry_a.p, a.data(), np * sizeof(double), cudaMemcpyHostToDevice,
                               c->stream));
@@ -2423,10 +2558,11 @@ void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot,
                                  cudaMemcpyHostToDevice, c->stream));
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
-      launch_combine(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
-                     L.d_cell_chunks.p, kry_vec(c, ln, xslot), c->kry_a.p,
-                     K > 0 ? kry_vec(c, ln, vslot) : nullptr, std::max<long long>(1, L.n0), K,
-                     c->kry_coef.p);
+      const int pi = prof_begin(c, 5, L.cells_prob, 8.0 * (K + 2));
+      launch_combine(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
+                     kry_vec(c, ln, xslot), c->kry_a.p, K > 0 ? kry_vec(c, ln, vslot) : nullptr,
+                     std::max<long long>(1, L.n0), K, c->kry_coef.p);
+      prof_end(c, pi);
    }
 }
 
@@ -2503,13 +2639,16 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
    for (int p = 0; p < np; ++p)
       if (!(res[p] > eff[p])) done[p] = 1;
    auto prec_body = [&]() {
-      zero_field(c, FAC_E);
       if (c->mixed) {
+         // the mixed cycle keeps the error in e32 and solves the coarsest
+         // level in FP64 on E: only level 0 of E needs its zero start
+         CUDA_CHECK(cudaMemsetAsync(c->L[0].e.p, 0, c->L[0].e.n * sizeof(double), c->stream));
          for (int ln = 0; ln < c->nlev; ++ln)
             CUDA_CHECK(cudaMemsetAsync(c->L[ln].e32.p, 0, c->L[ln].e32.n * sizeof(float),
                                        c->stream));
          fac_cycle_mixed(c, c->nlev - 1);
       } else {
+         zero_field(c, FAC_E);
          fac_cycle_recursive(c, c->nlev - 1);
       }
    };
@@ -2565,7 +2704,10 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                                        std::max<long long>(1, L.n0) * sizeof(double),
                                        cudaMemcpyDeviceToDevice, c->stream));
          }
-         run_graph(c, c->prec_exec, c->prec_launches, prec_body);
+         {
+            OpTimer ot(c, "kry_precondition", -1);
+            run_graph(c, c->prec_exec, c->prec_launches, prec_body);
+         }
          for (int ln = 0; ln < c->nlev; ++ln) {
             LevelState &L = c->L[ln];
             if (c->mixed)
@@ -2584,7 +2726,10 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
                             L.d_cell_chunks.p, kry_vec(c, ln, zslot0 + j), L.e.p);
          }
-         run_graph(c, c->apply_exec, c->apply_launches, apply_body);
+         {
+            OpTimer ot(c, "kry_apply", -1);
+            run_graph(c, c->apply_exec, c->apply_launches, apply_body);
+         }
          for (int ln = 0; ln < c->nlev; ++ln) {
             LevelState &L = c->L[ln];
             CUDA_CHECK(cudaMemcpyAsync(kry_vec(c, ln, j + 1), L.tr.p,
@@ -3492,7 +3637,7 @@ int fac_profile_read(fac_ctx *ctx, int kind, long long *launches, double *ms, do
    return guarded([&] {
       check_ops(ctx);
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-      if (kind < 0 || kind > 3) throw FacError(FAC_ERR_ARG, "profile kind out of range");
+      if (kind < 0 || kind > 5) throw FacError(FAC_ERR_ARG, "profile kind out of range");
       long long n = ctx->graph_acc[kind].n;
       double t = ctx->graph_acc[kind].ms, b = ctx->graph_acc[kind].bytes;
       for (const auto &r : ctx->prof) {

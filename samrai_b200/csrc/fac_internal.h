@@ -15,6 +15,7 @@ namespace samrai_b200 {
 
 constexpr int kMaxLevels = 8;
 constexpr int kChunk = 1024;  // cells per work chunk of the cell kernels
+constexpr int kSpanChunk = 8192;  // cells per chunk of the Krylov vector kernels
 
 // One patch of a (batched) level.
 struct PatchDesc {

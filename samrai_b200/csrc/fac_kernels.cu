@@ -12,6 +12,9 @@
 
 #include <atomic>
 #include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <unordered_map>
 
 #include "fac_device.h"
 #include "fac_internal.h"
@@ -32,6 +35,61 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, doub
 // ghost fill
 // ---------------------------------------------------------------------------
 
+// Cell lin of fill item it (x fastest, then y, then z).
+template <class T>
+__device__ __forceinline__ void fill_element(const FillItem &it, int lin, T *__restrict__ dst,
+                                             const T *__restrict__ src_same,
+                                             const T *__restrict__ src_coarse, int homogeneous,
+                                             const BcCoefs &bc)
+{
+   const T *src = it.src_is_coarse ? src_coarse : src_same;
+   const int nx = it.hi[0] - it.lo[0] + 1;
+   const int ny = it.hi[1] - it.lo[1] + 1;
+   const int i = it.lo[0] + lin % nx;
+   const int r = lin / nx;
+   const int j = it.lo[1] + r % ny;
+   const int k = it.lo[2] + r / ny;
+   T v;
+   if (it.kind == kFillCopy) {
+      v = src[aidx(it.src, i, j, k)];
+   } else if (it.kind == kFillCoarse) {
+      v = src[aidx(it.src, coarsen_index(i, it.ratio[0]), coarsen_index(j, it.ratio[1]),
+                   coarsen_index(k, it.ratio[2]))];
+   } else {
+      // Every ghost value of codimension m depends only on the interior
+      // cell reached by moving inward along all m outside axes
+      // (settype1/2/3cells{2,3}d applied in codimension order).
+      const T uin = src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
+      T f[3];
+      int m = 0;
+      for (int a = 0; a < 3; ++a) {
+         if (it.side[a]) {
+            f[a] = robin<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc);
+            ++m;
+         } else {
+            f[a] = (T)0;
+         }
+      }
+      if (m == 1) {
+         v = it.side[0] ? f[0] : (it.side[1] ? f[1] : f[2]);
+      } else if (m == 2) {
+         T s0 = (T)0, s1 = (T)0;
+         int n = 0;
+         for (int a = 0; a < 3; ++a)
+            if (it.side[a]) {
+               if (n == 0) s0 = f[a];
+               else s1 = f[a];
+               ++n;
+            }
+         v = -uin + (s1 + s0);
+      } else {
+         const T two3 = (T)(2.0f / 3.0f);
+         v = -uin + two3 * ((f[0] + f[1]) + f[2]);
+      }
+   }
+   dst[aidx(it.dst, i, j, k)] = v;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kThreads)
 k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks, int nwork,
@@ -44,54 +102,62 @@ k_fill(const FillItem *__restrict__ items, const Chunk *__restrict__ chunks, int
          int lin;
          const FillItem &it = items[chunk_item(ch, prefix, t, lin)];
          if (active && !active[it.prob]) continue;
-         const T *src = it.src_is_coarse ? src_coarse : src_same;
-         const int nx = it.hi[0] - it.lo[0] + 1;
-         const int ny = it.hi[1] - it.lo[1] + 1;
-         const int i = it.lo[0] + lin % nx;
-         const int r = lin / nx;
-         const int j = it.lo[1] + r % ny;
-         const int k = it.lo[2] + r / ny;
-         T v;
-         if (it.kind == kFillCopy) {
-            v = src[aidx(it.src, i, j, k)];
-         } else if (it.kind == kFillCoarse) {
-            v = src[aidx(it.src, coarsen_index(i, it.ratio[0]),
-                         coarsen_index(j, it.ratio[1]),
-                         coarsen_index(k, it.ratio[2]))];
-         } else {
-            // Every ghost value of codimension m depends only on the interior
-            // cell reached by moving inward along all m outside axes
-            // (settype1/2/3cells{2,3}d applied in codimension order).
-            const T uin =
-               src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
-            T f[3];
-            int m = 0;
-            for (int a = 0; a < 3; ++a) {
-               if (it.side[a]) {
-                  f[a] = robin<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc);
-                  ++m;
-               } else {
-                  f[a] = (T)0;
-               }
-            }
-            if (m == 1) {
-               v = it.side[0] ? f[0] : (it.side[1] ? f[1] : f[2]);
-            } else if (m == 2) {
-               T s0 = (T)0, s1 = (T)0;
-               int n = 0;
-               for (int a = 0; a < 3; ++a)
-                  if (it.side[a]) {
-                     if (n == 0) s0 = f[a];
-                     else s1 = f[a];
-                     ++n;
-                  }
-               v = -uin + (s1 + s0);
-            } else {
-               const T two3 = (T)(2.0f / 3.0f);
-               v = -uin + two3 * ((f[0] + f[1]) + f[2]);
-            }
+         fill_element<T>(it, lin, dst, src_same, src_coarse, homogeneous, bc);
+      }
+   }
+}
+
+// Ghost fill from a gather list: element e sets dst[to[e]] from the same
+// level (from[e] >= 0) or from the coarser level's element -from[e] - 1
+// (constant refine), when its problem prob[e] is active.  A flat launch:
+// each thread of the first nblk blocks has kFillPer elements in flight (its
+// index loads, then its value loads).  The blocks after them walk the
+// physical-boundary items of the same fill.
+constexpr int kFillPer = 4;
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+k_fill_gather(long long n, int nblk, const unsigned *__restrict__ to,
+              const int *__restrict__ from, const unsigned short *__restrict__ prob,
+              const FillItem *__restrict__ bc_items, const Chunk *__restrict__ bc_chunks, int nbc,
+              const int *__restrict__ bc_prefix, T *__restrict__ dst,
+              const T *__restrict__ src_same, const T *__restrict__ src_coarse, int homogeneous,
+              BcCoefs bc, const int *__restrict__ active)
+{
+   if ((int)blockIdx.x < nblk) {
+      const long long e0 = (long long)blockIdx.x * (kThreads * kFillPer) + threadIdx.x;
+      unsigned d[kFillPer];
+      int sx[kFillPer];
+      bool on[kFillPer];
+#pragma unroll
+      for (int q = 0; q < kFillPer; ++q) {
+         const long long e = e0 + q * kThreads;
+         on[q] = e < n;
+         d[q] = 0u;
+         sx[q] = 0;
+         if (on[q]) {
+            d[q] = to[e];
+            sx[q] = from[e];
+            if (active) on[q] = active[prob[e]] != 0;
          }
-         dst[aidx(it.dst, i, j, k)] = v;
+      }
+      T v[kFillPer];
+#pragma unroll
+      for (int q = 0; q < kFillPer; ++q)
+         if (on[q]) v[q] = sx[q] >= 0 ? src_same[sx[q]] : src_coarse[-(sx[q] + 1)];
+#pragma unroll
+      for (int q = 0; q < kFillPer; ++q)
+         if (on[q]) dst[d[q]] = v[q];
+      return;
+   }
+   for (int w = (int)blockIdx.x - nblk; w < nbc; w += (int)gridDim.x - nblk) {
+      const Chunk ch = bc_chunks[w];
+      if (ch.patch < 0) break;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         int lin;
+         const FillItem &it = bc_items[chunk_item(ch, bc_prefix, t, lin)];
+         if (active && !active[it.prob]) continue;
+         fill_element<T>(it, lin, dst, src_same, src_coarse, homogeneous, bc);
       }
    }
 }
@@ -1187,31 +1253,48 @@ k_compact(const WorkReg *__restrict__ regs, const int *__restrict__ active, int 
 // level, one vector every vstride elements), per problem, deterministic
 // ---------------------------------------------------------------------------
 
-// partial[chunk * K + i] = sum over the chunk of w x V_i
-template <int DIM>
+// Vectors a multi-dot or combination takes per pass over the cells: their
+// loads are independent, so a thread keeps that many in flight.
+constexpr int kVecBlock = 8;
+
+// partial[chunk * K + i] = sum over the chunk of w x V_i, chunks being runs
+// of one problem's cells {problem, first cell, cells, chunk index}: one pass
+// over the cells reads w and x once per kVecBlock vectors; each sum
+// accumulates thread-strided cells, then a warp tree, then warps in order.
 __global__ void __launch_bounds__(kThreads)
-k_multidot(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
-           const double *__restrict__ w, const double *__restrict__ x,
-           const double *__restrict__ V, long long vstride, int K,
+k_multidot(const Chunk *__restrict__ chunks, int nwork, const double *__restrict__ w,
+           const double *__restrict__ x, const double *__restrict__ V, long long vstride, int K,
            double *__restrict__ partial)
 {
-   __shared__ double red[kThreads / 32];
+   __shared__ double red[kVecBlock][kThreads / 32];
    WORK_LOOP(ch) {
-      const PatchDesc &p = patches[ch.patch];
-      for (int i = 0; i < K; ++i) {
-         const double *vi = V + (long long)i * vstride;
-         double sum = 0.0;
+      const long long c0 = ch.begin;
+      for (int i0 = 0; i0 < K; i0 += kVecBlock) {
+         const int nb = K - i0 < kVecBlock ? K - i0 : kVecBlock;
+         const double *vb = V + (long long)i0 * vstride;
+         double sum[kVecBlock];
+#pragma unroll
+         for (int q = 0; q < kVecBlock; ++q) sum[q] = 0.0;
          for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-            const long long c = p.off0 + ch.begin + t;
-            sum += w[c] * x[c] * vi[c];
+            const long long c = c0 + t;
+            const double wx = w[c] * x[c];
+            double v[kVecBlock];
+#pragma unroll
+            for (int q = 0; q < kVecBlock; ++q) v[q] = q < nb ? vb[(long long)q * vstride + c] : 0.0;
+#pragma unroll
+            for (int q = 0; q < kVecBlock; ++q) sum[q] += wx * v[q];
          }
-         for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
-         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+#pragma unroll
+         for (int q = 0; q < kVecBlock; ++q) {
+            double b = sum[q];
+            for (int o = 16; o > 0; o >>= 1) b += __shfl_down_sync(0xffffffffu, b, o);
+            if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = b;
+         }
          __syncthreads();
-         if (threadIdx.x == 0) {
+         if ((int)threadIdx.x < nb) {
             double b = 0.0;
-            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) b += red[q];
-            partial[(long long)ch.aux * K + i] = b;
+            for (int r = 0; r < (int)(blockDim.x >> 5); ++r) b += red[threadIdx.x][r];
+            partial[(long long)ch.aux * K + i0 + threadIdx.x] = b;
          }
          __syncthreads();
       }
@@ -1238,22 +1321,31 @@ __global__ void k_multidot_reduce(const double *__restrict__ partial,
    if (threadIdx.x == 0) out[(long long)p * K + i] += red[0];
 }
 
-// x = a[p] x + sum_i coef[p * K + i] V_i
-template <int DIM>
+// x = a[p] x + sum_i coef[p * K + i] V_i over the chunks of problem runs,
+// summed in the order of i; the loads of kVecBlock vectors are issued ahead
+// of their terms
 __global__ void __launch_bounds__(kThreads)
-k_combine(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
-          double *__restrict__ x, const double *__restrict__ a,
-          const double *__restrict__ V, long long vstride, int K,
+k_combine(const Chunk *__restrict__ chunks, int nwork, double *__restrict__ x,
+          const double *__restrict__ a, const double *__restrict__ V, long long vstride, int K,
           const double *__restrict__ coef)
 {
    WORK_LOOP(ch) {
-      const PatchDesc &p = patches[ch.patch];
-      const double ap = a[p.prob];
-      const double *cp = coef + (long long)p.prob * K;
+      const double ap = a[ch.patch];
+      const double *cp = coef + (long long)ch.patch * K;
+      // four cells of a thread at a time keep (K + 1) x 4 loads in flight
+#pragma unroll 4
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const long long c = p.off0 + ch.begin + t;
+         const long long c = (long long)ch.begin + t;
          double v = ap * x[c];
-         for (int i = 0; i < K; ++i) v = v + cp[i] * V[(long long)i * vstride + c];
+         for (int i0 = 0; i0 < K; i0 += kVecBlock) {
+            const double *vb = V + (long long)i0 * vstride + c;
+            double vv[kVecBlock];
+#pragma unroll
+            for (int q = 0; q < kVecBlock; ++q) vv[q] = i0 + q < K ? vb[(long long)q * vstride] : 0.0;
+#pragma unroll
+            for (int q = 0; q < kVecBlock; ++q)
+               if (i0 + q < K) v = v + cp[i0 + q] * vv[q];
+         }
          x[c] = v;
       }
    }
@@ -1300,7 +1392,15 @@ k_add_combination(const PatchDesc *__restrict__ patches, const Chunk *__restrict
          const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
          const long long c0 = p.off0 + lin;
          double s = 0.0;
-         for (int q = 0; q < K; ++q) s = s + yp[q] * Z[(long long)q * zstride + c0];
+         for (int q0 = 0; q0 < K; q0 += kVecBlock) {
+            const double *zb = Z + (long long)q0 * zstride + c0;
+            double zz[kVecBlock];
+#pragma unroll
+            for (int q = 0; q < kVecBlock; ++q) zz[q] = q0 + q < K ? zb[(long long)q * zstride] : 0.0;
+#pragma unroll
+            for (int q = 0; q < kVecBlock; ++q)
+               if (q0 + q < K) s = s + yp[q0 + q] * zz[q];
+         }
          const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
          u[c1] = u[c1] + s;
       }
@@ -1309,44 +1409,60 @@ k_add_combination(const PatchDesc *__restrict__ patches, const Chunk *__restrict
 
 std::atomic<long long> g_launches{0};
 
+std::mutex g_occ_mutex;
+std::unordered_map<const void *, int> g_occ;
+
 }  // namespace
+
+namespace dev {
+
+int resident_blocks(const void *fn)
+{
+   std::lock_guard<std::mutex> lock(g_occ_mutex);
+   const auto it = g_occ.find(fn);
+   if (it != g_occ.end()) return it->second;
+   int device = 0, nsm = 0, per_sm = 0;
+   int cap = kGridCap;
+   if (cudaGetDevice(&device) == cudaSuccess &&
+       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) == cudaSuccess &&
+       nsm > 0 && per_sm > 0)
+      cap = nsm * per_sm;
+   else
+      (void)cudaGetLastError();  // the launch reports real faults
+   g_occ[fn] = cap;
+   return cap;
+}
+
+}  // namespace dev
 
 long long kernel_launch_count() { return g_launches.load(); }
 
 void add_kernel_launches(long long n) { g_launches += n; }
 
-void launch_multidot(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                     const Chunk *chunks, const double *w, const double *x, const double *V,
-                     long long vstride, int K, double *partial, const int *prob_chunk_begin,
-                     int nprob, const int *active, double *out)
+void launch_multidot(cudaStream_t s, int nchunks, const Chunk *chunks, const double *w,
+                     const double *x, const double *V, long long vstride, int K,
+                     double *partial, const int *prob_chunk_begin, int nprob, const int *active,
+                     double *out)
 {
    if (K <= 0) return;
    if (nchunks > 0) {
       g_launches.fetch_add(1, std::memory_order_relaxed);
-      if (dim == 2)
-         k_multidot<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, w, x, V,
-                                                                vstride, K, partial);
-      else
-         k_multidot<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, w, x, V,
-                                                                vstride, K, partial);
+      k_multidot<<<work_grid(k_multidot, nchunks), kThreads, 0, s>>>(chunks, nchunks, w, x, V,
+                                                                     vstride, K, partial);
    }
    g_launches.fetch_add(1, std::memory_order_relaxed);
    k_multidot_reduce<<<dim3(nprob, K), kThreads, 0, s>>>(partial, prob_chunk_begin, K, active,
                                                          out);
 }
 
-void launch_combine(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                    const Chunk *chunks, double *x, const double *a, const double *V,
-                    long long vstride, int K, const double *coef)
+void launch_combine(cudaStream_t s, int nchunks, const Chunk *chunks, double *x, const double *a,
+                    const double *V, long long vstride, int K, const double *coef)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   if (dim == 2)
-      k_combine<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, a, V,
-                                                            vstride, K, coef);
-   else
-      k_combine<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, a, V,
-                                                            vstride, K, coef);
+   k_combine<<<work_grid(k_combine, nchunks), kThreads, 0, s>>>(chunks, nchunks, x, a, V, vstride,
+                                                               K, coef);
 }
 
 template <class TS>
@@ -1356,9 +1472,9 @@ void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patc
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_g1_to_g0<2, TS><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+      k_g1_to_g0<2, TS><<<work_grid(k_g1_to_g0<2, TS>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
    else
-      k_g1_to_g0<3, TS><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+      k_g1_to_g0<3, TS><<<work_grid(k_g1_to_g0<3, TS>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
 }
 template void launch_g1_to_g0<double>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
                                       const double *, double *);
@@ -1372,10 +1488,10 @@ void launch_add_combination(cudaStream_t s, int dim, int nchunks, const PatchDes
    if (nchunks <= 0 || K <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_add_combination<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, Z,
+      k_add_combination<2><<<work_grid(k_add_combination<2>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, Z,
                                                                     zstride, K, y);
    else
-      k_add_combination<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, Z,
+      k_add_combination<3><<<work_grid(k_add_combination<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, Z,
                                                                     zstride, K, y);
 }
 
@@ -1397,8 +1513,25 @@ void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_fill<T><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, dst, src_same, src_coarse,
+   k_fill<T><<<work_grid(k_fill<T>, nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, dst, src_same, src_coarse,
                                           homogeneous, bc, active);
+}
+
+template <class T>
+void launch_fill_gather(cudaStream_t s, long long n, const unsigned *to, const int *from,
+                        const unsigned short *prob, const FillItem *bc_items,
+                        const Chunk *bc_chunks, int nbc, const int *bc_prefix, T *dst,
+                        const T *src_same, const T *src_coarse, int homogeneous,
+                        const BcCoefs &bc, const int *active)
+{
+   const long long nblk = (n + kThreads * kFillPer - 1) / (kThreads * kFillPer);
+   const int gbc = nbc > 0 ? work_grid(k_fill_gather<T>, nbc) : 0;
+   if (nblk + gbc <= 0) return;
+   if (nblk + gbc > (1ll << 31) - 1) throw std::runtime_error("fill gather list too long");
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_fill_gather<T><<<(unsigned)(nblk + gbc), kThreads, 0, s>>>(
+      n, (int)nblk, to, from, prob, bc_items, bc_chunks, nbc, bc_prefix, dst, src_same,
+      src_coarse, homogeneous, bc, active);
 }
 
 template <class T>
@@ -1426,11 +1559,11 @@ static void rbgs_inst(cudaStream_t s, int nchunks, const PatchDesc *patches,
                       const long long *facemap, const BcCoefs &bc)
 {
    if (facemap)
-      k_rbgs<DIM, DVAR, CK, T, true><<<work_grid(nchunks), kThreads, 0, s>>>(
+      k_rbgs<DIM, DVAR, CK, T, true><<<work_grid(k_rbgs<DIM, DVAR, CK, T, true>, nchunks), kThreads, 0, s>>>(
          patches, chunks, nchunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
          maxres, run, facemap, bc);
    else
-      k_rbgs<DIM, DVAR, CK, T, false><<<work_grid(nchunks), kThreads, 0, s>>>(
+      k_rbgs<DIM, DVAR, CK, T, false><<<work_grid(k_rbgs<DIM, DVAR, CK, T, false>, nchunks), kThreads, 0, s>>>(
          patches, chunks, nchunks, u, f, dside, cfield, cfflux, cfmask, offset, (T)dconst, (T)cconst,
          maxres, run, facemap, bc);
 }
@@ -1486,20 +1619,20 @@ void launch_flux(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
    }
    if (dim == 2) {
       if (spec.d_variable)
-         k_flux<2, true, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
+         k_flux<2, true, TU><<<work_grid(k_flux<2, true, TU>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                           spec.d_const, cfmask, w, ratio_dev,
                                                           flux, run);
       else
-         k_flux<2, false, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
+         k_flux<2, false, TU><<<work_grid(k_flux<2, false, TU>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                            spec.d_const, cfmask, w,
                                                            ratio_dev, flux, run);
    } else {
       if (spec.d_variable)
-         k_flux<3, true, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
+         k_flux<3, true, TU><<<work_grid(k_flux<3, true, TU>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                           spec.d_const, cfmask, w, ratio_dev,
                                                           flux, run);
       else
-         k_flux<3, false, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
+         k_flux<3, false, TU><<<work_grid(k_flux<3, false, TU>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, dside,
                                                            spec.d_const, cfmask, w,
                                                            ratio_dev, flux, run);
    }
@@ -1519,7 +1652,7 @@ void launch_flux_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int nch
       w.longwt[a] = longwt[a];
    }
 #define FC(D, V)                                                                            \
-   k_flux_cells<D, V, TU><<<work_grid(nchunks), kThreads, 0, s>>>(                          \
+   k_flux_cells<D, V, TU><<<work_grid(k_flux_cells<D, V, TU>, nchunks), kThreads, 0, s>>>(                          \
       patches, cell_chunks, nchunks, u, dside, spec.d_const, cfmask, w, ratio_dev, flux, run)
    if (dim == 2) {
       if (spec.d_variable) FC(2, true);
@@ -1563,7 +1696,7 @@ void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int
       w.longwt[a] = longwt[a];
    }
 #define RF(D, V, C)                                                                         \
-   k_residual_fused<D, V, C, TU><<<work_grid(nchunks), kThreads, 0, s>>>(                   \
+   k_residual_fused<D, V, C, TU><<<work_grid(k_residual_fused<D, V, C, TU>, nchunks), kThreads, 0, s>>>(                   \
       patches, chunks, nchunks, u, dside, spec.d_const, cfmask, w, ratio_dev, fcmask, fcflux, \
       f, cfield, spec.c_const, res, oflux, run)
    if (dim == 2) {
@@ -1599,7 +1732,7 @@ void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchun
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
 #define RS(D, C)                                                                         \
-   k_residual<D, C, TU><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, f, flux, cfield, \
+   k_residual<D, C, TU><<<work_grid(k_residual<D, C, TU>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, f, flux, cfield, \
                                                      spec.c_const, res, oflux, run)
    if (dim == 2) {
       if (spec.c_kind == 2) RS(2, 2);
@@ -1620,7 +1753,7 @@ void launch_flux_coarsen(cudaStream_t s, const FluxCoarsenItem *items, const Chu
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_flux_coarsen<<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
+   k_flux_coarsen<<<work_grid(k_flux_coarsen, nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
                                                           coarse, oflux_fine, flux_coarse, run);
 }
 
@@ -1632,10 +1765,10 @@ void launch_restrict(cudaStream_t s, int dim, const RestrictItem *items, const C
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_restrict<2><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
+      k_restrict<2><<<work_grid(k_restrict<2>, nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
                                                             coarse, src, src_g, dst, dst_g, run);
    else
-      k_restrict<3><<<work_grid(nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
+      k_restrict<3><<<work_grid(k_restrict<3>, nchunks), kThreads, 0, s>>>(items, chunks, nchunks, prefix, fine,
                                                             coarse, src, src_g, dst, dst_g, run);
 }
 
@@ -1647,10 +1780,10 @@ void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_prolong_add<2, T><<<work_grid(nchunks), kThreads, 0, s>>>(
+      k_prolong_add<2, T><<<work_grid(k_prolong_add<2, T>, nchunks), kThreads, 0, s>>>(
          items, chunks, nchunks, prefix, fine, tmp, dxc_prob, ratio[0], ratio[1], ratio[2], e, run);
    else
-      k_prolong_add<3, T><<<work_grid(nchunks), kThreads, 0, s>>>(
+      k_prolong_add<3, T><<<work_grid(k_prolong_add<3, T>, nchunks), kThreads, 0, s>>>(
          items, chunks, nchunks, prefix, fine, tmp, dxc_prob, ratio[0], ratio[1], ratio[2], e, run);
 }
 
@@ -1661,9 +1794,9 @@ void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_add_interior<2, T><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, e, run);
+      k_add_interior<2, T><<<work_grid(k_add_interior<2, T>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, e, run);
    else
-      k_add_interior<3, T><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, e, run);
+      k_add_interior<3, T><<<work_grid(k_add_interior<3, T>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, u, e, run);
 }
 
 template <class S, class D>
@@ -1681,9 +1814,9 @@ void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
    if (nchunks <= 0) return;
    g_launches.fetch_add(2, std::memory_order_relaxed);
    if (dim == 2)
-      k_norm_partial<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
+      k_norm_partial<2><<<work_grid(k_norm_partial<2>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
    else
-      k_norm_partial<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
+      k_norm_partial<3><<<work_grid(k_norm_partial<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
    k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
 }
 
@@ -1708,8 +1841,8 @@ void launch_g0_to_g1(cudaStream_t s, int dim, int nchunks, const PatchDesc *patc
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   if (dim == 2) k_g0_to_g1<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
-   else k_g0_to_g1<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+   if (dim == 2) k_g0_to_g1<2><<<work_grid(k_g0_to_g1<2>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
+   else k_g0_to_g1<3><<<work_grid(k_g0_to_g1<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, src, dst);
 }
 
 void launch_patch_rms(cudaStream_t s, int dim, int npatch, const PatchDesc *patches,
@@ -1739,9 +1872,9 @@ void launch_scatter_samples(cudaStream_t s, int dim, int nchunks, const PatchDes
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_scatter_samples<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, y, scale, S, dst);
+      k_scatter_samples<2><<<work_grid(k_scatter_samples<2>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, y, scale, S, dst);
    else
-      k_scatter_samples<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, y, scale, S, dst);
+      k_scatter_samples<3><<<work_grid(k_scatter_samples<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, y, scale, S, dst);
 }
 
 void launch_dot_pair(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
@@ -1751,9 +1884,9 @@ void launch_dot_pair(cudaStream_t s, int dim, int nchunks, const PatchDesc *patc
    if (nchunks <= 0) return;
    g_launches.fetch_add(2, std::memory_order_relaxed);
    if (dim == 2)
-      k_dot_pair<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, r, r2, w, partial);
+      k_dot_pair<2><<<work_grid(k_dot_pair<2>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, r, r2, w, partial);
    else
-      k_dot_pair<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, r, r2, w, partial);
+      k_dot_pair<3><<<work_grid(k_dot_pair<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, r, r2, w, partial);
    k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
 }
 
@@ -1771,9 +1904,9 @@ void launch_apply_alpha(cudaStream_t s, int dim, int nchunks, const PatchDesc *p
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
-      k_apply_alpha<2><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, alpha, u, e, r, r2);
+      k_apply_alpha<2><<<work_grid(k_apply_alpha<2>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, alpha, u, e, r, r2);
    else
-      k_apply_alpha<3><<<work_grid(nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, alpha, u, e, r, r2);
+      k_apply_alpha<3><<<work_grid(k_apply_alpha<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, alpha, u, e, r, r2);
 }
 
 void launch_gather(cudaStream_t s, const long long *idx, long long n, const double *src,
@@ -1797,6 +1930,11 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
 #define INST_T(T)                                                                          \
    template void launch_fill<T>(cudaStream_t, const FillItem *, const Chunk *, int, const int *, T *,    \
                                 const T *, const T *, int, const BcCoefs &, const int *);   \
+   template void launch_fill_gather<T>(cudaStream_t, long long, const unsigned *,           \
+                                       const int *, const unsigned short *,                 \
+                                       const FillItem *, const Chunk *, int, const int *,   \
+                                       T *, const T *, const T *, int, const BcCoefs &,     \
+                                       const int *);                                        \
    template void launch_cf_flux<T>(cudaStream_t, const CfFace *, int, const PatchDesc *,    \
                                    const T *, const T *, int, double, const double *,       \
                                    const double *, T *, const int *);                       \

@@ -29,17 +29,17 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
                       const BcCoefs &bc, int *err);
 
 // Krylov vector operations on composite vectors: ghost-0 level arrays, one
-// vector every vstride elements; per-problem coefficients; cell chunks with
-// aux = chunk index (partial is nchunks x K).
+// vector every vstride elements; per-problem coefficients; chunks are runs
+// of one problem's cells {problem, first cell, cells, chunk index} (partial
+// is nchunks x K).
 // out[p*K+i] += sum_w x V_i over problem p's chunks of this level.
-void launch_multidot(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                     const Chunk *chunks, const double *w, const double *x, const double *V,
-                     long long vstride, int K, double *partial, const int *prob_chunk_begin,
-                     int nprob, const int *active, double *out);
+void launch_multidot(cudaStream_t s, int nchunks, const Chunk *chunks, const double *w,
+                     const double *x, const double *V, long long vstride, int K,
+                     double *partial, const int *prob_chunk_begin, int nprob, const int *active,
+                     double *out);
 // x = a[p] x + sum_i coef[p*K+i] V_i
-void launch_combine(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                    const Chunk *chunks, double *x, const double *a, const double *V,
-                    long long vstride, int K, const double *coef);
+void launch_combine(cudaStream_t s, int nchunks, const Chunk *chunks, double *x, const double *a,
+                    const double *V, long long vstride, int K, const double *coef);
 // dst (ghost-0) = interior of src (ghost-1), converted to FP64
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
@@ -56,6 +56,14 @@ template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
                  const int *prefix, T *dst, const T *src_same, const T *src_coarse, int homogeneous,
                  const BcCoefs &bc, const int *active);
+// Ghost fill from a gather list of n elements (copies and constant refines,
+// see k_fill_gather) plus the physical-boundary items of the same fill.
+template <class T>
+void launch_fill_gather(cudaStream_t s, long long n, const unsigned *to, const int *from,
+                        const unsigned short *prob, const FillItem *bc_items,
+                        const Chunk *bc_chunks, int nbc, const int *bc_prefix, T *dst,
+                        const T *src_same, const T *src_coarse, int homogeneous,
+                        const BcCoefs &bc, const int *active);
 
 template <class T>
 void launch_cf_flux(cudaStream_t s, const CfFace *faces, int nfaces, const PatchDesc *patches,
