@@ -98,6 +98,25 @@ __device__ __forceinline__ long long oidx(const PatchDesc &p, int a, int s, int 
    return p.offo[a][s] + t;
 }
 
+// Cell (li, lj, lk) of linear index lin (x fastest) of a patch's cells:
+// quotients by reciprocal multiplication when the patch carries its
+// divisors (q / d = umulhi(q, ceil(2^32 / d)) for q d < 2^32).
+__device__ __forceinline__ void patch_cell(const PatchDesc &p, int lin, int nx, int ny, int &li,
+                                           int &lj, int &lk)
+{
+   if (p.mx) {
+      const int r = (int)__umulhi((unsigned)lin, p.mx);
+      li = lin - r * nx;
+      lk = (int)__umulhi((unsigned)r, p.my);
+      lj = r - lk * ny;
+   } else {
+      li = lin % nx;
+      const int r = lin / nx;
+      lj = r % ny;
+      lk = r / ny;
+   }
+}
+
 __device__ __forceinline__ int coarsen_index(int i, int r)
 {
    return i < 0 ? (i + 1) / r - 1 : i / r;

@@ -679,6 +679,14 @@ void build_level_layout(fac_ctx *c, int ln)
          }
          d.prob = p;
          d.flags = 0;
+         {
+            const long long nx = b.hi[0] - b.lo[0] + 1, ny = dim > 1 ? b.hi[1] - b.lo[1] + 1 : 1;
+            const long long cells = b.size();
+            if (nx > 0 && ny > 0 && cells * std::max(nx, ny) < (1ll << 32)) {
+               d.mx = (unsigned)(((1ull << 32) + nx - 1) / nx);
+               d.my = (unsigned)(((1ull << 32) + ny - 1) / ny);
+            }
+         }
          d.off1 = o1;
          d.off0 = o0;
          o1 += cell_count(dim, b, 1);
@@ -2654,12 +2662,14 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
    };
    auto apply_body = [&]() {
       // as for u in the solve: finer values restricted onto covered cells
-      // first, then the composite residual level by level
+      // first (finest first, so each level passes on what it received),
+      // then the composite residual level by level.  Each residual fills
+      // its level's ghost cells itself (homogeneous boundary values of the
+      // error equation), so the restrictions need no fills of their own.
       const int lmax = c->nlev - 1;
-      for (int ln = lmax - 1; ln >= 0; --ln) restrict_solution(c, FAC_E, ln);
+      for (int ln = lmax - 1; ln >= 0; --ln) restrict_op(c, FAC_E, FAC_E, ln);
       comp_residual(c, FAC_TR, FAC_E, kFieldZero, lmax, 1);
       for (int ln = lmax - 1; ln >= 0; --ln) {
-         restrict_solution(c, FAC_E, ln);
          comp_residual(c, FAC_TR, FAC_E, kFieldZero, ln, 1);
          restrict_op(c, FAC_TR, FAC_TR, ln);
       }

@@ -15,13 +15,16 @@ namespace samrai_b200 {
 
 constexpr int kMaxLevels = 8;
 constexpr int kChunk = 1024;  // cells per work chunk of the cell kernels
-constexpr int kSpanChunk = 8192;  // cells per chunk of the Krylov vector kernels
+constexpr int kSpanChunk = 2048;  // cells per chunk of the Krylov vector kernels
 
 // One patch of a (batched) level.
 struct PatchDesc {
    int lo[3], hi[3];
    int prob;           // problem index within the context
    int flags;          // bit0: has coarse-fine boundary faces
+   // ceil(2^32 / nx), ceil(2^32 / ny) for the cell decode of a linear
+   // index (exact while cells * max(nx, ny) < 2^32); 0: divide instead
+   unsigned mx, my;
    long long off1;     // start of this patch in ghost-1 cell buffers
    long long off0;     // start in ghost-0 cell buffers
    long long offs[3];  // start of the side array of each axis

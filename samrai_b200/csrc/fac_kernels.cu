@@ -482,10 +482,8 @@ k_flux_cells(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ ch
       const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int li = lin % nx;
-         const int r = lin / nx;
-         const int lj = r % ny;
-         const int lk = DIM == 3 ? r / ny : 0;
+         int li, lj, lk;
+         patch_cell(p, lin, nx, ny, li, lj, lk);
          const int c = (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0);
          const double uc = (double)up[c];
          // side-array positions of the cell's lower faces
@@ -561,10 +559,8 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
       const double *fz = DIM == 3 ? flux + p.offs[2] : nullptr;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int li = lin % nx;
-         const int r = lin / nx;
-         const int lj = r % ny;
-         const int lk = DIM == 3 ? r / ny : 0;
+         int li, lj, lk;
+         patch_cell(p, lin, nx, ny, li, lj, lk);
          const int sx = li + (nx + 1) * (lj + ny * lk);
          const int sy = li + nx * (lj + (ny + 1) * lk);
          const double fxl = fx[sx], fxh = fx[sx + 1];
@@ -628,10 +624,8 @@ k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict_
       const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int li = lin % nx;
-         const int r = lin / nx;
-         const int lj = r % ny;
-         const int lk = DIM == 3 ? r / ny : 0;
+         int li, lj, lk;
+         patch_cell(p, lin, nx, ny, li, lj, lk);
          const int c = (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0);
          const double uc = (double)up[c];
          const int sx = li + (nx + 1) * (lj + ny * lk);
@@ -844,10 +838,11 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
          const int nx = p.hi[0] - p.lo[0] + 1;
          const int ny = p.hi[1] - p.lo[1] + 1;
          const double *dxc = dxc_prob + 3 * it.prob;
-         const int i = p.lo[0] + lin % nx;
-         const int rr = lin / nx;
-         const int j = p.lo[1] + rr % ny;
-         const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
          const int fi[3] = {i, j, k};
          int ic[3];
          T x[3];
@@ -906,10 +901,11 @@ k_add_interior(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ 
       const int ny = p.hi[1] - p.lo[1] + 1;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
-         const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
          const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
          u[c] = u[c] + (double)e[c];
       }
@@ -941,10 +937,11 @@ k_norm_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ 
       } else {
          for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
             const int lin = ch.begin + t;
-            const int i = p.lo[0] + lin % nx;
-            const int r = lin / nx;
-            const int j = p.lo[1] + r % ny;
-            const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+            int ci, cj, ck;
+            patch_cell(p, lin, nx, ny, ci, cj, ck);
+            const int i = p.lo[0] + ci;
+            const int j = p.lo[1] + cj;
+            const int k = DIM == 3 ? p.lo[2] + ck : 0;
             const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
             const double wv = w[p.off0 + lin];
             sd += xv * xv * wv;
@@ -1063,10 +1060,11 @@ k_g0_to_g1(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
       const int ny = p.hi[1] - p.lo[1] + 1;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
-         const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
          dst[cidx<DIM>(p, p.off1, 1, i, j, k)] = src[cidx<DIM>(p, p.off0, 0, i, j, k)];
       }
    }
@@ -1209,10 +1207,11 @@ k_apply_alpha(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ c
       const int ny = p.hi[1] - p.lo[1] + 1;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
-         const int rr = lin / nx;
-         const int j = p.lo[1] + rr % ny;
-         const int k = DIM == 3 ? p.lo[2] + rr / ny : 0;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
          const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
          const long long c0 = p.off0 + lin;
          u[c1] = u[c1] + al * e[c1];
@@ -1363,10 +1362,11 @@ k_g1_to_g0(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
       const int ny = p.hi[1] - p.lo[1] + 1;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
-         const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
          dst[p.off0 + lin] = (double)src[cidx<DIM>(p, p.off1, 1, i, j, k)];
       }
    }
@@ -1386,10 +1386,11 @@ k_add_combination(const PatchDesc *__restrict__ patches, const Chunk *__restrict
       const double *yp = y + (long long)p.prob * K;
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
-         const int i = p.lo[0] + lin % nx;
-         const int r = lin / nx;
-         const int j = p.lo[1] + r % ny;
-         const int k = DIM == 3 ? p.lo[2] + r / ny : 0;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
          const long long c0 = p.off0 + lin;
          double s = 0.0;
          for (int q0 = 0; q0 < K; q0 += kVecBlock) {
