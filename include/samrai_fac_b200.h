@@ -74,8 +74,9 @@ int fac_ctx_destroy(fac_ctx *ctx);
 
 /* Add one problem.  n0: level-0 cells per axis (physical domain is the
  * box [0,n0-1]); xlo/xup: physical extent; ratio: nlev x 3 refinement
- * ratios to the next coarser level (level 0: 1 1 1); npatch: patches per
- * level; boxes: lo0 lo1 lo2 hi0 hi1 hi2 per patch in level order.
+ * ratios to the next coarser level, 1 .. 16 per axis (level 0: 1 1 1);
+ * npatch: patches per level; boxes: lo0 lo1 lo2 hi0 hi1 hi2 per patch in
+ * level order.
  * Returns the problem index through *problem. */
 int fac_add_problem(fac_ctx *ctx, const int *n0, const double *xlo,
                     const double *xup, int nlev, const int *ratio,

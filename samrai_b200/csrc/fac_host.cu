@@ -2976,8 +2976,8 @@ int fac_add_problem(fac_ctx *ctx, const int *n0, const double *xlo, const double
       for (int ln = 0; ln < nlev; ++ln) {
          for (int a = 0; a < 3; ++a) {
             P.ratio[ln][a] = a < dim ? ratio[3 * ln + a] : 1;
-            if (P.ratio[ln][a] < 1 || P.ratio[ln][a] > 255)
-               throw FacError(FAC_ERR_ARG, "bad ratio");
+            if (P.ratio[ln][a] < 1 || P.ratio[ln][a] > kProlongRatioMax)
+               throw FacError(FAC_ERR_ARG, "bad ratio (1 .. 16 per axis)");
          }
          if (npatch[ln] < 1) throw FacError(FAC_ERR_ARG, "empty level");
          for (int ip = 0; ip < npatch[ln]; ++ip, ++off) {

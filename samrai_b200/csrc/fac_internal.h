@@ -16,6 +16,9 @@ namespace samrai_b200 {
 constexpr int kMaxLevels = 8;
 constexpr int kChunk = 1024;  // cells per work chunk of the cell kernels
 constexpr int kSpanChunk = 2048;  // cells per chunk of the Krylov vector kernels
+// Largest refinement ratio per axis: the prolongation tabulates its
+// interpolation offsets per chunk in shared memory.
+constexpr int kProlongRatioMax = 16;
 
 // One patch of a (batched) level.
 struct PatchDesc {

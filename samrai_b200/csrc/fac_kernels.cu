@@ -829,56 +829,77 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
 {
    const T half = (T)0.5, one = (T)1;
    const int r[3] = {ratio0, ratio1, ratio2};
+   // per axis and fine offset ir within the coarse cell: the interpolation
+   // weight x and the shift of the lower coarse cell (0 or -1).  They
+   // depend on the problem only (all patches of a problem on a level share
+   // dx), and a chunk holds one problem's cells.
+   __shared__ T s_x[3][kProlongRatioMax];
+   __shared__ int s_sh[3][kProlongRatioMax];
    WORK_LOOP(ch) {
+      const int prob = items[ch.patch].prob;
+      if (run && !run[prob]) continue;
+      __syncthreads();  // the previous chunk's table is no longer read
+      if ((int)threadIdx.x < DIM * kProlongRatioMax) {
+         const int a = threadIdx.x / kProlongRatioMax, ir = threadIdx.x % kProlongRatioMax;
+         if (ir < r[a]) {
+            const double *dxc = dxc_prob + 3 * prob;
+            const PatchDesc &p0 = fine[items[ch.patch].fine_patch];
+            const T deltax = ((T)ir + half) * (T)p0.dx[a] - (T)dxc[a] * half;
+            T x = deltax / (T)dxc[a];
+            int sh = 0;
+            if (x < 0.0) {
+               sh = -1;
+               x = x + one;
+            }
+            s_x[a][ir] = x;
+            s_sh[a][ir] = sh;
+         }
+      }
+      __syncthreads();
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          int lin;
          const ProlongItem &it = items[chunk_item(ch, prefix, t, lin)];
-         if (run && !run[it.prob]) continue;
          const PatchDesc &p = fine[it.fine_patch];
          const int nx = p.hi[0] - p.lo[0] + 1;
          const int ny = p.hi[1] - p.lo[1] + 1;
-         const double *dxc = dxc_prob + 3 * it.prob;
          int ci, cj, ck;
          patch_cell(p, lin, nx, ny, ci, cj, ck);
-         const int i = p.lo[0] + ci;
-         const int j = p.lo[1] + cj;
-         const int k = DIM == 3 ? p.lo[2] + ck : 0;
-         const int fi[3] = {i, j, k};
-         int ic[3];
+         const int fi[3] = {p.lo[0] + ci, p.lo[1] + cj, DIM == 3 ? p.lo[2] + ck : 0};
+         int ic[3] = {0, 0, 0};
          T x[3];
+#pragma unroll
          for (int a = 0; a < DIM; ++a) {
-            ic[a] = coarsen_index(fi[a], r[a]);
-            const int ir = fi[a] - ic[a] * r[a];
-            const T deltax = ((T)ir + half) * (T)p.dx[a] - (T)dxc[a] * half;
-            x[a] = deltax / (T)dxc[a];
-            if (x[a] < 0.0) {
-               ic[a] = ic[a] - 1;
-               x[a] = x[a] + one;
-            }
+            const int c0 = coarsen_index(fi[a], r[a]);
+            const int ir = fi[a] - c0 * r[a];
+            x[a] = s_x[a][ir];
+            ic[a] = c0 + s_sh[a][ir];
          }
-         T v;
          const ArrDesc &A = it.tmp;
+         const long long b = aidx(A, ic[0], ic[1], ic[2]);
+         const int sy = A.n[0];
+         T v;
          if (DIM == 2) {
-            const T c00 = tmp[aidx(A, ic[0], ic[1], 0)];
-            const T c10 = tmp[aidx(A, ic[0] + 1, ic[1], 0)];
-            const T c01 = tmp[aidx(A, ic[0], ic[1] + 1, 0)];
-            const T c11 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, 0)];
+            const T c00 = tmp[b];
+            const T c10 = tmp[b + 1];
+            const T c01 = tmp[b + sy];
+            const T c11 = tmp[b + sy + 1];
             v = (c00 + (c10 - c00) * x[0]) * (one - x[1]) + (c01 + (c11 - c01) * x[0]) * x[1];
          } else {
-            const T c000 = tmp[aidx(A, ic[0], ic[1], ic[2])];
-            const T c100 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2])];
-            const T c010 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2])];
-            const T c110 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2])];
-            const T c001 = tmp[aidx(A, ic[0], ic[1], ic[2] + 1)];
-            const T c101 = tmp[aidx(A, ic[0] + 1, ic[1], ic[2] + 1)];
-            const T c011 = tmp[aidx(A, ic[0], ic[1] + 1, ic[2] + 1)];
-            const T c111 = tmp[aidx(A, ic[0] + 1, ic[1] + 1, ic[2] + 1)];
+            const int sz = A.n[0] * A.n[1];
+            const T c000 = tmp[b];
+            const T c100 = tmp[b + 1];
+            const T c010 = tmp[b + sy];
+            const T c110 = tmp[b + sy + 1];
+            const T c001 = tmp[b + sz];
+            const T c101 = tmp[b + sz + 1];
+            const T c011 = tmp[b + sz + sy];
+            const T c111 = tmp[b + sz + sy + 1];
             const T y = x[1], z = x[2], xx = x[0];
             v = ((c000 + (c100 - c000) * xx) * (one - y) + (c010 + (c110 - c010) * xx) * y) *
                    (one - z) +
                 ((c001 + (c101 - c001) * xx) * (one - y) + (c011 + (c111 - c011) * xx) * y) * z;
          }
-         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+         const long long c = cidx<DIM>(p, p.off1, 1, fi[0], fi[1], fi[2]);
          e[c] = e[c] + v;
       }
    }
