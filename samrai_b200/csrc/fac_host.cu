@@ -352,6 +352,7 @@ struct LevelState {
 
    ItemList<FillItem> fill_nc, fill_wc;   // ghost fill without / with coarser level
    FillGather gather_nc, gather_wc;       // the same fills as gather lists
+   FillGather gather_tmp;                 // tmp_fill as a gather list
    std::vector<CfFace> cf;
    DevArray<CfFace> d_cf;
    ItemList<RestrictItem> restrict_g1, restrict_g0;  // from level ln+1 into this
@@ -1365,6 +1366,9 @@ void build_coarsen_tables(fac_ctx *c, int ln)
 
 // Coarse interpolation arrays for prolongation into level ln
 // (RefineSchedule coarse interpolation level, RefineSchedule.C:1353-1560).
+void build_fill_gather(fac_ctx *c, ItemList<FillItem> &F, FillGather &G, long long dstlen,
+                       long long samelen, long long coarselen);
+
 void build_prolong_tables(fac_ctx *c, int ln)
 {
    LevelState &Fl = c->L[ln];
@@ -1441,6 +1445,8 @@ void build_prolong_tables(fac_ctx *c, int ln)
    if (!g_dry)
       CUDA_CHECK(cudaMemsetAsync(Fl.tmp.p, 0xff, Fl.tmp.n * sizeof(double), c->stream));
    Fl.tmp_fill.upload(c->stream);
+   // every source of the interpolation array is on the coarser level
+   build_fill_gather(c, Fl.tmp_fill, Fl.gather_tmp, toff, 0, C.n1);
    Fl.prolong.upload(c->stream);
    std::vector<double> dxc(3 * nprob(c));
    for (int p = 0; p < nprob(c); ++p)
@@ -1787,6 +1793,7 @@ void register_work_lists(fac_ctx *c)
       register_items(c, L.restrict_g0);
       register_items(c, L.fcoarsen);
       register_items(c, L.tmp_fill);
+      if (L.gather_tmp.ok) register_items(c, L.gather_tmp.bc);
       register_items(c, L.prolong);
       for (int t = 0; t < 2; ++t)
          register_work(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
@@ -2045,9 +2052,16 @@ void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
    LevelState &C = c->L[dest_ln - 1];
    if (field_ghost(fid_src) != 1 || field_ghost(fid_dst) != 1)
       throw FacError(FAC_ERR_ARG, "prolongation needs ghosted cell fields");
-   launch_fill<double>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
-                       Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1, c->bc,
-                       c->active.p);
+   const FillGather &G = Fl.gather_tmp;
+   if (G.ok)
+      launch_fill_gather<double>(c->stream, (long long)G.to.size(), G.d_to.p, G.d_from.p,
+                                 G.d_prob.p, G.bc.d_items.p, G.bc.d_chunks.p, G.bc.nchunks(),
+                                 G.bc.d_prefix.p, Fl.tmp.p, nullptr, field_ptr(C, fid_src), 1,
+                                 c->bc, c->active.p);
+   else
+      launch_fill<double>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
+                          Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp.p, nullptr,
+                          field_ptr(C, fid_src), 1, c->bc, c->active.p);
    launch_prolong_add(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
                       Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp.p, Fl.dxc_prob.p, Fl.ratio,
                       field_ptr(Fl, fid_dst), c->active.p);
@@ -2261,9 +2275,16 @@ void prolong32(fac_ctx *c, int dest_ln)
    OpTimer ot(c, "prolong32", dest_ln);
    LevelState &Fl = c->L[dest_ln];
    LevelState &C = c->L[dest_ln - 1];
-   launch_fill<float>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
-                      Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp32.p, nullptr, C.e32.p, 1, c->bc,
-                      c->active.p);
+   const FillGather &G = Fl.gather_tmp;
+   if (G.ok)
+      launch_fill_gather<float>(c->stream, (long long)G.to.size(), G.d_to.p, G.d_from.p,
+                                G.d_prob.p, G.bc.d_items.p, G.bc.d_chunks.p, G.bc.nchunks(),
+                                G.bc.d_prefix.p, Fl.tmp32.p, nullptr, C.e32.p, 1, c->bc,
+                                c->active.p);
+   else
+      launch_fill<float>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
+                         Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp32.p, nullptr,
+                         C.e32.p, 1, c->bc, c->active.p);
    launch_prolong_add<float>(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
                              Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp32.p, Fl.dxc_prob.p,
                              Fl.ratio, Fl.e32.p, c->active.p);
