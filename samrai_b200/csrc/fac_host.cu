@@ -362,6 +362,7 @@ struct LevelState {
    DevArray<double> tmp;
    DevArray<double> dxc_prob;                        // per problem dx of level ln-1
    DevArray<unsigned long long> maxres_red, maxres_blk;
+   bool one_patch_per_prob = false;  // patch p is problem p's only patch, <= 16384 cells
    DevArray<int> last_patch;
    std::vector<long long> dir_idx;
    DevArray<long long> d_dir_idx;
@@ -1244,6 +1245,10 @@ void build_chunks(fac_ctx *c, int ln)
    L.last_patch.upload(last, c->stream);
    L.maxres_red.alloc(std::max(1, L.npatch));
    L.maxres_blk.alloc(std::max(1, L.npatch));
+   // one block per problem pays off for small patches only
+   L.one_patch_per_prob = L.npatch == np;
+   for (int ip = 0; ip < L.npatch; ++ip)
+      if (L.hp[ip].prob != ip || L.box[ip].size() > 16384) L.one_patch_per_prob = false;
    // one colour pass reads u over the ghosted boxes, f at the active half,
    // writes u at the active half, and reads D on all faces when variable
    double n = 0, ng = 0;
@@ -1944,7 +1949,17 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
    if (ln > 0) ghost_fill(c, fid_e, ln, true, 1, c->run.p);
    else if (!fmap || staged) ghost_fill(c, fid_e, ln, false, 1, c->run.p);
    std::vector<int> hrun(np);
-   for (int isweep = 0; isweep < nsweeps; ++isweep) {
+   // smoothing to a tolerance on a level without a coarser one and with one
+   // patch per problem (the coarsest level): every sweep in one launch
+   const bool one_launch = tol >= 0.0 && ln == 0 && fmap && L.one_patch_per_prob;
+   if (one_launch) {
+      const int pi = prof_begin(c, 0, L.rb_bytes_prob, 2.0 * nsweeps);
+      launch_rbgs_solve<double>(c->stream, c->dim, c->spec, L.npatch, L.d_patches.p, e, r,
+                                L.d.p, L.c.p, fmap, c->bc, nsweeps, tol, c->run.p,
+                                c->sweeps_call.p, L.maxres_red.p, L.maxres_blk.p);
+      prof_end(c, pi);
+   }
+   for (int isweep = 0; isweep < (one_launch ? 0 : nsweeps); ++isweep) {
       if (tol >= 0.0 && isweep > 0 && isweep % c->check_interval == 0 && !c->capturing) {
          CUDA_CHECK(cudaMemcpyAsync(hrun.data(), c->run.p, np * sizeof(int),
                                     cudaMemcpyDeviceToHost, c->stream));

@@ -219,6 +219,136 @@ k_cf_flux(const CfFace *__restrict__ faces, int nfaces,
 // of the cell itself at a physical boundary (homogeneous, as the
 // smoother's fills are), or the precomputed Ewing flux at a coarse-fine
 // face -- so the three ghost fills around each colour pass are not needed.
+// One slot s of a colour pass over patch p (the cell of the active colour
+// in row s / hx): the update of compflux + rbgswithfluxmax and the running
+// maximum of |residual|.
+template <int DIM, bool DVAR, int CKIND, class T, bool FUSED>
+__device__ __forceinline__ void rb_slot(const PatchDesc &p, int s, int nx, int ny, int hx, T dxi,
+                                        T dyi, T dzi, bool has_cf, T *__restrict__ u,
+                                        const T *__restrict__ f, const T *__restrict__ dside,
+                                        const T *__restrict__ cfield,
+                                        const T *__restrict__ cfflux,
+                                        const unsigned char *__restrict__ cfmask, int offset,
+                                        T dconst, T cconst, const long long *__restrict__ facemap,
+                                        const BcCoefs &bc, double &maxres)
+{
+   const T one = (T)1;
+   const T rcoef = one;
+      const int row = s / hx;
+      const int mm = s - row * hx;
+      const int j = p.lo[1] + row % ny;
+      const int k = DIM == 3 ? p.lo[2] + row / ny : 0;
+      int ioffset;
+      if (DIM == 2) {
+         const int q = p.lo[1] + j;
+         ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
+      } else {
+         const int q = p.lo[0] + j + k;
+         ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
+      }
+      const int i = p.lo[0] + ioffset + 2 * mm;
+      if (i > p.hi[0]) return;
+      const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
+      const long long sx = 1;
+      const long long sy = nx + 2;
+      const long long sz = (long long)(nx + 2) * (ny + 2);
+      const T uc = u[c];
+      T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
+      if (DVAR) {
+         dx0 = dside[sidx(p, 0, i, j, k)];
+         dx1 = dside[sidx(p, 0, i + 1, j, k)];
+         dy0 = dside[sidx(p, 1, i, j, k)];
+         dy1 = dside[sidx(p, 1, i, j + 1, k)];
+         if (DIM == 3) {
+            dz0 = dside[sidx(p, 2, i, j, k)];
+            dz1 = dside[sidx(p, 2, i, j, k + 1)];
+         }
+      } else {
+         dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
+      }
+      T nxl, nxh, nyl, nyh, nzl = (T)0, nzh = (T)0;
+      if (FUSED) {
+         auto across = [&](int a, int sd, long long own) -> T {
+            const long long m = facemap[oidx(p, a, sd, i, j, k)];
+            if (m >= 0) return u[m];
+            if (m == -1) return robin<T>(uc, 2 * a + sd, (T)p.dx[a], 1, bc);
+            return u[own];
+         };
+         nxl = i == p.lo[0] ? across(0, 0, c - sx) : u[c - sx];
+         nxh = i == p.hi[0] ? across(0, 1, c + sx) : u[c + sx];
+         nyl = j == p.lo[1] ? across(1, 0, c - sy) : u[c - sy];
+         nyh = j == p.hi[1] ? across(1, 1, c + sy) : u[c + sy];
+         if (DIM == 3) {
+            nzl = k == p.lo[2] ? across(2, 0, c - sz) : u[c - sz];
+            nzh = k == p.hi[2] ? across(2, 1, c + sz) : u[c + sz];
+         }
+      } else {
+         nxl = u[c - sx];
+         nxh = u[c + sx];
+         nyl = u[c - sy];
+         nyh = u[c + sy];
+         if (DIM == 3) {
+            nzl = u[c - sz];
+            nzh = u[c + sz];
+         }
+      }
+      T fxl = dxi * dx0 * (uc - nxl);
+      T fxh = dxi * dx1 * (nxh - uc);
+      T fyl = dyi * dy0 * (uc - nyl);
+      T fyh = dyi * dy1 * (nyh - uc);
+      T fzl = (T)0, fzh = (T)0;
+      if (DIM == 3) {
+         fzl = dzi * dz0 * (uc - nzl);
+         fzh = dzi * dz1 * (nzh - uc);
+      }
+      if (has_cf) {
+         if (i == p.lo[0]) {
+            const long long o = oidx(p, 0, 0, i, j, k);
+            if (cfmask[o]) fxl = cfflux[o];
+         }
+         if (i == p.hi[0]) {
+            const long long o = oidx(p, 0, 1, i, j, k);
+            if (cfmask[o]) fxh = cfflux[o];
+         }
+         if (j == p.lo[1]) {
+            const long long o = oidx(p, 1, 0, i, j, k);
+            if (cfmask[o]) fyl = cfflux[o];
+         }
+         if (j == p.hi[1]) {
+            const long long o = oidx(p, 1, 1, i, j, k);
+            if (cfmask[o]) fyh = cfflux[o];
+         }
+         if (DIM == 3) {
+            if (k == p.lo[2]) {
+               const long long o = oidx(p, 2, 0, i, j, k);
+               if (cfmask[o]) fzl = cfflux[o];
+            }
+            if (k == p.hi[2]) {
+               const long long o = oidx(p, 2, 1, i, j, k);
+               if (cfmask[o]) fzh = cfflux[o];
+            }
+         }
+      }
+      const T sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
+                              : (CKIND == 1 ? cconst : (T)0);
+      const T fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
+      T residual, dudr;
+      if (DIM == 2) {
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
+         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
+      } else {
+         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
+                    sf * uc;
+         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
+                       sf);
+      }
+      const T du = -residual * dudr;
+      u[c] = uc + du * rcoef;
+      const double ar = fabs((double)residual);
+      if (maxres < ar) maxres = ar;
+}
+
 template <int DIM, bool DVAR, int CKIND, class T, bool FUSED>
 __global__ void __launch_bounds__(kThreads, 3)
 k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
@@ -239,124 +369,11 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, 
       const T dxi = one / (T)p.dx[0], dyi = one / (T)p.dx[1];
       const T dzi = DIM == 3 ? one / (T)p.dx[2] : (T)0;
       const bool has_cf = (p.flags & 1) != 0;
-      const T rcoef = one;
       double maxres = 0.0;
-      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const int s = ch.begin + t;
-         const int row = s / hx;
-         const int mm = s - row * hx;
-         const int j = p.lo[1] + row % ny;
-         const int k = DIM == 3 ? p.lo[2] + row / ny : 0;
-         int ioffset;
-         if (DIM == 2) {
-            const int q = p.lo[1] + j;
-            ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
-         } else {
-            const int q = p.lo[0] + j + k;
-            ioffset = (q - (q / 2) * 2) != offset ? 1 : 0;
-         }
-         const int i = p.lo[0] + ioffset + 2 * mm;
-         if (i > p.hi[0]) continue;
-         const long long c = cidx<DIM>(p, p.off1, 1, i, j, k);
-         const long long sx = 1;
-         const long long sy = nx + 2;
-         const long long sz = (long long)(nx + 2) * (ny + 2);
-         const T uc = u[c];
-         T dx0, dx1, dy0, dy1, dz0 = (T)0, dz1 = (T)0;
-         if (DVAR) {
-            dx0 = dside[sidx(p, 0, i, j, k)];
-            dx1 = dside[sidx(p, 0, i + 1, j, k)];
-            dy0 = dside[sidx(p, 1, i, j, k)];
-            dy1 = dside[sidx(p, 1, i, j + 1, k)];
-            if (DIM == 3) {
-               dz0 = dside[sidx(p, 2, i, j, k)];
-               dz1 = dside[sidx(p, 2, i, j, k + 1)];
-            }
-         } else {
-            dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
-         }
-         T nxl, nxh, nyl, nyh, nzl = (T)0, nzh = (T)0;
-         if (FUSED) {
-            auto across = [&](int a, int sd, long long own) -> T {
-               const long long m = facemap[oidx(p, a, sd, i, j, k)];
-               if (m >= 0) return u[m];
-               if (m == -1) return robin<T>(uc, 2 * a + sd, (T)p.dx[a], 1, bc);
-               return u[own];
-            };
-            nxl = i == p.lo[0] ? across(0, 0, c - sx) : u[c - sx];
-            nxh = i == p.hi[0] ? across(0, 1, c + sx) : u[c + sx];
-            nyl = j == p.lo[1] ? across(1, 0, c - sy) : u[c - sy];
-            nyh = j == p.hi[1] ? across(1, 1, c + sy) : u[c + sy];
-            if (DIM == 3) {
-               nzl = k == p.lo[2] ? across(2, 0, c - sz) : u[c - sz];
-               nzh = k == p.hi[2] ? across(2, 1, c + sz) : u[c + sz];
-            }
-         } else {
-            nxl = u[c - sx];
-            nxh = u[c + sx];
-            nyl = u[c - sy];
-            nyh = u[c + sy];
-            if (DIM == 3) {
-               nzl = u[c - sz];
-               nzh = u[c + sz];
-            }
-         }
-         T fxl = dxi * dx0 * (uc - nxl);
-         T fxh = dxi * dx1 * (nxh - uc);
-         T fyl = dyi * dy0 * (uc - nyl);
-         T fyh = dyi * dy1 * (nyh - uc);
-         T fzl = (T)0, fzh = (T)0;
-         if (DIM == 3) {
-            fzl = dzi * dz0 * (uc - nzl);
-            fzh = dzi * dz1 * (nzh - uc);
-         }
-         if (has_cf) {
-            if (i == p.lo[0]) {
-               const long long o = oidx(p, 0, 0, i, j, k);
-               if (cfmask[o]) fxl = cfflux[o];
-            }
-            if (i == p.hi[0]) {
-               const long long o = oidx(p, 0, 1, i, j, k);
-               if (cfmask[o]) fxh = cfflux[o];
-            }
-            if (j == p.lo[1]) {
-               const long long o = oidx(p, 1, 0, i, j, k);
-               if (cfmask[o]) fyl = cfflux[o];
-            }
-            if (j == p.hi[1]) {
-               const long long o = oidx(p, 1, 1, i, j, k);
-               if (cfmask[o]) fyh = cfflux[o];
-            }
-            if (DIM == 3) {
-               if (k == p.lo[2]) {
-                  const long long o = oidx(p, 2, 0, i, j, k);
-                  if (cfmask[o]) fzl = cfflux[o];
-               }
-               if (k == p.hi[2]) {
-                  const long long o = oidx(p, 2, 1, i, j, k);
-                  if (cfmask[o]) fzh = cfflux[o];
-               }
-            }
-         }
-         const T sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
-                                 : (CKIND == 1 ? cconst : (T)0);
-         const T fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
-         T residual, dudr;
-         if (DIM == 2) {
-            residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
-            dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
-         } else {
-            const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
-            residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
-                       sf * uc;
-            dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
-                          sf);
-         }
-         const T du = -residual * dudr;
-         u[c] = uc + du * rcoef;
-         const double ar = fabs((double)residual);
-         if (maxres < ar) maxres = ar;
-      }
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x)
+         rb_slot<DIM, DVAR, CKIND, T, FUSED>(p, ch.begin + t, nx, ny, hx, dxi, dyi, dzi, has_cf, u,
+                                             f, dside, cfield, cfflux, cfmask, offset, dconst,
+                                             cconst, facemap, bc, maxres);
       // block max, then one atomic per block
       __shared__ double red[kThreads / 32];
       for (int o = 16; o > 0; o >>= 1) {
@@ -371,6 +388,68 @@ k_rbgs(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, 
          if (maxres_patch) atomic_max_nonneg(&maxres_patch[ch.patch], m);
       }
       __syncthreads();  // shared memory is reused by the next chunk
+   }
+}
+
+// Red-black smoothing to a tolerance of a level with one patch per problem
+// and no coarser level, all sweeps in one launch: block b owns patch b
+// (problem patches[b].prob) and runs up to nsweeps sweeps of a red and a
+// black pass, __syncthreads between passes, with the fused neighbour reads
+// (physical boundaries through the facemap).  After each sweep the block
+// applies the sweep check of smoothErrorByRedBlack: the sweep counts, and
+// with tol >= 0 the problem stops once max(red, black) max |residual| <=
+// tol.  Same cells, order and arithmetic as k_rbgs + k_sweep_check, so the
+// same bits.
+template <int DIM, bool DVAR, int CKIND, class T>
+__global__ void __launch_bounds__(kThreads)
+k_rbgs_solve(const PatchDesc *__restrict__ patches, T *__restrict__ u, const T *__restrict__ f,
+             const T *__restrict__ dside, const T *__restrict__ cfield, T dconst, T cconst,
+             const long long *__restrict__ facemap, BcCoefs bc, int nsweeps, double tol,
+             int *__restrict__ run, long long *__restrict__ sweeps,
+             unsigned long long *__restrict__ maxres_red,
+             unsigned long long *__restrict__ maxres_blk)
+{
+   const int ip = blockIdx.x;
+   const PatchDesc p = patches[ip];
+   const int pr = p.prob;
+   if (!run[pr]) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
+   const int hx = (nx + 1) >> 1;
+   const int nslots = hx * ny * nz;
+   const T one = (T)1;
+   const T dxi = one / (T)p.dx[0], dyi = one / (T)p.dx[1];
+   const T dzi = DIM == 3 ? one / (T)p.dx[2] : (T)0;
+   __shared__ double red[kThreads / 32];
+   bool going = true;
+   double mcol[2] = {0.0, 0.0};
+   for (int sw = 0; sw < nsweeps && going; ++sw) {
+      for (int color = 0; color < 2; ++color) {
+         double maxres = 0.0;
+         for (int t = threadIdx.x; t < nslots; t += blockDim.x)
+            rb_slot<DIM, DVAR, CKIND, T, true>(p, t, nx, ny, hx, dxi, dyi, dzi, false, u, f,
+                                               dside, cfield, nullptr, nullptr, color, dconst,
+                                               cconst, facemap, bc, maxres);
+         for (int o = 16; o > 0; o >>= 1) {
+            const double other = __shfl_down_sync(0xffffffffu, maxres, o);
+            maxres = other > maxres ? other : maxres;
+         }
+         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxres;
+         // the pass's writes and maxima are visible to the whole block
+         __syncthreads();
+         double m = red[0];
+         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
+         mcol[color] = m;
+         __syncthreads();  // red is reused
+      }
+      if (threadIdx.x == 0) sweeps[pr] += 1;
+      if (tol >= 0.0) going = (mcol[0] > mcol[1] ? mcol[0] : mcol[1]) > tol;
+   }
+   if (threadIdx.x == 0) {
+      run[pr] = going ? 1 : 0;
+      maxres_red[ip] = (unsigned long long)__double_as_longlong(mcol[0]);
+      maxres_blk[ip] = (unsigned long long)__double_as_longlong(mcol[1]);
    }
 }
 
@@ -1540,6 +1619,44 @@ void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int
 }
 
 template <class T>
+void launch_rbgs_solve(cudaStream_t s, int dim, const PoissonSpec &spec, int npatch,
+                       const PatchDesc *patches, T *u, const T *f, const T *dside,
+                       const T *cfield, const long long *facemap, const BcCoefs &bc,
+                       int nsweeps, double tol, int *run, long long *sweeps,
+                       unsigned long long *maxres_red, unsigned long long *maxres_blk)
+{
+   if (npatch <= 0 || nsweeps <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   const T dc = (T)spec.d_const, cc = (T)spec.c_const;
+#define RS(D, V, C)                                                                        \
+   k_rbgs_solve<D, V, C, T><<<npatch, kThreads, 0, s>>>(patches, u, f, dside, cfield, dc, cc, \
+                                                        facemap, bc, nsweeps, tol, run,      \
+                                                        sweeps, maxres_red, maxres_blk)
+   if (dim == 2) {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RS(2, true, 2);
+         else if (spec.c_kind == 1) RS(2, true, 1);
+         else RS(2, true, 0);
+      } else {
+         if (spec.c_kind == 2) RS(2, false, 2);
+         else if (spec.c_kind == 1) RS(2, false, 1);
+         else RS(2, false, 0);
+      }
+   } else {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RS(3, true, 2);
+         else if (spec.c_kind == 1) RS(3, true, 1);
+         else RS(3, true, 0);
+      } else {
+         if (spec.c_kind == 2) RS(3, false, 2);
+         else if (spec.c_kind == 1) RS(3, false, 1);
+         else RS(3, false, 0);
+      }
+   }
+#undef RS
+}
+
+template <class T>
 void launch_fill_gather(cudaStream_t s, long long n, const unsigned *to, const int *from,
                         const unsigned short *prob, const FillItem *bc_items,
                         const Chunk *bc_chunks, int nbc, const int *bc_prefix, T *dst,
@@ -1952,6 +2069,11 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
 #define INST_T(T)                                                                          \
    template void launch_fill<T>(cudaStream_t, const FillItem *, const Chunk *, int, const int *, T *,    \
                                 const T *, const T *, int, const BcCoefs &, const int *);   \
+   template void launch_rbgs_solve<T>(cudaStream_t, int, const PoissonSpec &, int,          \
+                                      const PatchDesc *, T *, const T *, const T *,         \
+                                      const T *, const long long *, const BcCoefs &, int,   \
+                                      double, int *, long long *, unsigned long long *,     \
+                                      unsigned long long *);                                \
    template void launch_fill_gather<T>(cudaStream_t, long long, const unsigned *,           \
                                        const int *, const unsigned short *,                 \
                                        const FillItem *, const Chunk *, int, const int *,   \

@@ -56,6 +56,16 @@ template <class T>
 void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int nchunks,
                  const int *prefix, T *dst, const T *src_same, const T *src_coarse, int homogeneous,
                  const BcCoefs &bc, const int *active);
+// Red-black smoothing to a tolerance, all sweeps in one launch, of a level
+// without a coarser level and with one patch per problem (patch b of
+// problem patches[b].prob); run, sweeps and the per-patch red / black
+// residual maxima as the per-pass launches and the sweep check leave them.
+template <class T>
+void launch_rbgs_solve(cudaStream_t s, int dim, const PoissonSpec &spec, int npatch,
+                       const PatchDesc *patches, T *u, const T *f, const T *dside,
+                       const T *cfield, const long long *facemap, const BcCoefs &bc,
+                       int nsweeps, double tol, int *run, long long *sweeps,
+                       unsigned long long *maxres_red, unsigned long long *maxres_blk);
 // Ghost fill from a gather list of n elements (copies and constant refines,
 // see k_fill_gather) plus the physical-boundary items of the same fill.
 template <class T>
