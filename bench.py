@@ -52,8 +52,8 @@ MG_LEVELS = {"c5": 3, "c2": 4, "c1": 3, "c3": 3}
 # headline: FGMRES(KRYLOV) with one FAC cycle as the flexible preconditioner
 KRYLOV = 20
 # DRAM bytes per algorithmic byte of the FP32 staged colour pass, from one ncu
-# capture (profiles/k_rb_staged_f32_config5x8_finest-level.md: 67.2 MB read +
-# write for 54.6 MB algorithmic on 2.48 M cells); traffic per launch is this
+# capture of the pass on the finest level of 8 config-5 problems (67.2 MB read
+# + write for 54.6 MB algorithmic on 2.48 M cells); traffic per launch is this
 # times the launch's algorithmic bytes (scaling by cells processed)
 STAGED_F32_TRAFFIC_RATIO = 67.2 / 54.6
 
