@@ -2046,9 +2046,9 @@ void restrict_op(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
    LevelState &Fl = c->L[dest_ln + 1];
    const int sg = field_ghost(fid_src), dg = field_ghost(fid_dst);
    ItemList<RestrictItem> &it = dg ? C.restrict_g1 : C.restrict_g0;
-   launch_restrict(c->stream, c->dim, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p, Fl.d_patches.p,
-                   C.d_patches.p, field_ptr(Fl, fid_src), sg, field_ptr(C, fid_dst), dg,
-                   c->active.p);
+   launch_restrict(c->stream, c->dim, it.d_items.p, it.d_chunks.p, it.nchunks(), it.d_prefix.p,
+                   Fl.d_patches.p, C.d_patches.p, field_ptr(Fl, fid_src), sg,
+                   field_ptr(C, fid_dst), dg, c->active.p);
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -2209,7 +2209,10 @@ void ghost_fill32(fac_ctx *c, int ln, bool with_coarse, int homogeneous, const i
    prof_end(c, pi);
 }
 
-void smooth32(fac_ctx *c, int ln, int nsweeps)
+// zero_start: e32 of this level and of the coarser level are zero (interior
+// and ghosts), so the entry fill, which would write the zeros the ghost
+// cells already hold, is skipped.
+void smooth32(fac_ctx *c, int ln, int nsweeps, bool zero_start = false)
 {
    OpTimer ot(c, "smooth32", ln);
    LevelState &L = c->L[ln];
@@ -2217,8 +2220,14 @@ void smooth32(fac_ctx *c, int ln, int nsweeps)
    const int *run = c->active.p;
    const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
    const bool staged = fmap && c->staged && L.unit_smem[1] > 0;
-   if (ln > 0) ghost_fill32(c, ln, true, 1, run);
-   else if (!fmap || staged) ghost_fill32(c, ln, false, 1, run);
+   if (zero_start && fmap) {
+      // entry fill skipped (see above); passes that fill around themselves
+      // (!fmap) fill as usual
+   } else if (ln > 0) {
+      ghost_fill32(c, ln, true, 1, run);
+   } else if (!fmap || staged) {
+      ghost_fill32(c, ln, false, 1, run);
+   }
    for (int isweep = 0; isweep < nsweeps; ++isweep) {
       for (int color = 0; color < 2; ++color) {
          if (!fmap) ghost_fill32(c, ln, false, 1, run);
@@ -2315,7 +2324,9 @@ void fac_cycle_mixed(fac_ctx *c, int ln)
       return;
    }
    launch_convert<double, float>(c->stream, L.r.p, L.r32.p, (long long)L.r.n);
-   smooth32(c, ln, c->pre_sweeps);
+   // every e32 is zeroed before the cycle, and coarser levels are reached
+   // only after this pre-smoothing
+   smooth32(c, ln, c->pre_sweeps, true);
    comp_residual_mixed(c, ln);
    restrict_op(c, FAC_TR, FAC_R, ln - 1);
    fac_cycle_mixed(c, ln - 1);
