@@ -185,6 +185,8 @@ __device__ __forceinline__ void stage_update(unsigned char *stage, int tid, T *_
    const T rcoef = one;
    // parity of the first cell of each row: lo1 + j (2-D), lo0 + j + k (3-D)
    const int qbase = DIM == 3 ? lo0 + lo1 + lo2 + s0 : 2 * lo1 + s0;
+   // two slots per thread in flight: their shared-memory loads overlap
+#pragma unroll 2
    for (int t = tid; t < nslots; t += kConsumers) {
       const int row = udiv(t, mhx);
       const int mm = t - row * hx;
