@@ -184,6 +184,29 @@ def test_config2_one_cycle(require_gpu):
     _solution_check(p, o, g)
 
 
+def test_coarsest_one_launch_solve_matches_oracle(require_gpu):
+    """Smoothing to a tolerance on a coarsest level with one patch per problem
+    runs every sweep in one launch (one block per problem, the sweep check
+    inside); per problem the sweep count and the result must equal the
+    oracle's, for problems that stop after different sweep counts."""
+    probs = [configs.extend_hierarchy(configs.small_3d(seed=s), k=2) for s in (71, 72, 73)]
+    prm = dict(coarse_tol=1e-3, coarse_max_it=200)
+    g = fac.FacContext(probs, params=prm)
+    oracles = [Oracle(p, params=prm) for p in probs]
+    rng = np.random.default_rng(74)
+    for i, o in enumerate(oracles):
+        for fid in (E, R):
+            v = rng.standard_normal(o.size(fid, 0)) * (1.0 + 3.0 * i)
+            o.set(fid, 0, v)
+            g.upload(fid, i, 0, v)
+    n_g = g.smooth(E, R, 0, 200, 1e-3)
+    for i, o in enumerate(oracles):
+        n_o, _ = o.smooth(E, R, 0, 200, 1e-3)
+        assert int(n_g[i]) == n_o
+        assert np.array_equal(g.download(E, i, 0), o.get(E, 0))
+    g.close()
+
+
 def test_mg_extended_hierarchy_matches_oracle(require_gpu):
     """The fast variant (hierarchy extended by fully covered coarser levels)
     against the oracle run on the same extended hierarchy, and its converged
