@@ -2601,8 +2601,10 @@ void kry_dots(fac_ctx *c, int xslot, int vslot, int K, std::vector<double> &out)
 }
 
 // V_x = a[p] V_x + sum_i coef[p*K+i] V_{vslot+i}
+// With norm: also norm[p] = <V_x, V_x> (weighted) of the result, the same
+// numbers as kry_dots(c, xslot, xslot, 1, norm) without rereading V_x.
 void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot, int K,
-                 const std::vector<double> &coef)
+                 const std::vector<double> &coef, std::vector<double> *norm = nullptr)
 {
    OpTimer ot(c, "kry_combine", -1);
    const int np = nprob(c);
@@ -2611,13 +2613,29 @@ void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot,
    if (K > 0)
       CUDA_CHECK(cudaMemcpyAsync(c->kry_coef.p, coef.data(), (size_t)np * K * sizeof(double),
                                  cudaMemcpyHostToDevice, c->stream));
+   if (norm) CUDA_CHECK(cudaMemsetAsync(c->kry_dots.p, 0, (size_t)np * sizeof(double), c->stream));
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
-      const int pi = prof_begin(c, 5, L.cells_prob, 8.0 * (K + 2));
-      launch_combine(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
-                     kry_vec(c, ln, xslot), c->kry_a.p, K > 0 ? kry_vec(c, ln, vslot) : nullptr,
-                     std::max<long long>(1, L.n0), K, c->kry_coef.p);
+      const int pi = prof_begin(c, 5, L.cells_prob, 8.0 * (K + (norm ? 3 : 2)));
+      if (norm)
+         launch_combine_norm(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
+                             kry_vec(c, ln, xslot), c->kry_a.p,
+                             K > 0 ? kry_vec(c, ln, vslot) : nullptr,
+                             std::max<long long>(1, L.n0), K, c->kry_coef.p, L.w.p,
+                             L.kry_partial.p, L.d_prob_span_begin.p, np, c->active.p,
+                             c->kry_dots.p);
+      else
+         launch_combine(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
+                        kry_vec(c, ln, xslot), c->kry_a.p,
+                        K > 0 ? kry_vec(c, ln, vslot) : nullptr, std::max<long long>(1, L.n0),
+                        K, c->kry_coef.p);
       prof_end(c, pi);
+   }
+   if (norm) {
+      norm->resize(np);
+      CUDA_CHECK(cudaMemcpyAsync(norm->data(), c->kry_dots.p, (size_t)np * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream));
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
    }
 }
 
@@ -2808,8 +2826,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                coef[(size_t)p * K + i] = -hi;
             }
          }
-         kry_combine(c, j + 1, a, 0, K, coef);
-         kry_dots(c, j + 1, j + 1, 1, dots);  // ||W||^2
+         kry_combine(c, j + 1, a, 0, K, coef, &dots);  // and ||W||^2
          bool again = false;
          std::vector<int> reo(np, 0);
          for (int p = 0; p < np; ++p)
@@ -2824,8 +2841,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                   coef[(size_t)p * K + i] = -d;
                }
             }
-            kry_combine(c, j + 1, a, 0, K, coef);
-            kry_dots(c, j + 1, j + 1, 1, dots);
+            kry_combine(c, j + 1, a, 0, K, coef, &dots);
          }
          for (int p = 0; p < np; ++p) {
             if (!act[p]) {

@@ -1422,15 +1422,22 @@ __global__ void k_multidot_reduce(const double *__restrict__ partial,
 
 // x = a[p] x + sum_i coef[p * K + i] V_i over the chunks of problem runs,
 // summed in the order of i; the loads of kVecBlock vectors are issued ahead
-// of their terms
+// of their terms.  NORM: also partial[chunk] = sum over the chunk of w x x
+// of the new x, accumulated exactly as k_multidot accumulates <x, x> (the
+// same cells per thread in the same order, the same warp tree, warps in
+// order), so the pass that would reread x for its norm is saved.
+template <bool NORM>
 __global__ void __launch_bounds__(kThreads)
 k_combine(const Chunk *__restrict__ chunks, int nwork, double *__restrict__ x,
           const double *__restrict__ a, const double *__restrict__ V, long long vstride, int K,
-          const double *__restrict__ coef)
+          const double *__restrict__ coef, const double *__restrict__ w,
+          double *__restrict__ partial)
 {
+   __shared__ double red[NORM ? kThreads / 32 : 1];
    WORK_LOOP(ch) {
       const double ap = a[ch.patch];
       const double *cp = coef + (long long)ch.patch * K;
+      double sum = 0.0;
       // four cells of a thread at a time keep (K + 1) x 4 loads in flight
 #pragma unroll 4
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
@@ -1446,6 +1453,21 @@ k_combine(const Chunk *__restrict__ chunks, int nwork, double *__restrict__ x,
                if (i0 + q < K) v = v + cp[i0 + q] * vv[q];
          }
          x[c] = v;
+         if (NORM) {
+            const double wx = w[c] * v;
+            sum += wx * v;
+         }
+      }
+      if (NORM) {
+         for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+         __syncthreads();
+         if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int r = 0; r < (int)(blockDim.x >> 5); ++r) b += red[r];
+            partial[ch.aux] = b;
+         }
+         __syncthreads();
       }
    }
 }
@@ -1562,8 +1584,23 @@ void launch_combine(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_combine<<<work_grid(k_combine, nchunks), kThreads, 0, s>>>(chunks, nchunks, x, a, V, vstride,
-                                                               K, coef);
+   k_combine<false><<<work_grid(k_combine<false>, nchunks), kThreads, 0, s>>>(
+      chunks, nchunks, x, a, V, vstride, K, coef, nullptr, nullptr);
+}
+
+void launch_combine_norm(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
+                         const double *a, const double *V, long long vstride, int K,
+                         const double *coef, const double *w, double *partial,
+                         const int *prob_chunk_begin, int nprob, const int *active, double *out)
+{
+   if (nchunks > 0) {
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      k_combine<true><<<work_grid(k_combine<true>, nchunks), kThreads, 0, s>>>(
+         chunks, nchunks, x, a, V, vstride, K, coef, w, partial);
+   }
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_multidot_reduce<<<dim3(nprob, 1), kThreads, 0, s>>>(partial, prob_chunk_begin, 1, active,
+                                                         out);
 }
 
 template <class TS>

@@ -40,6 +40,12 @@ void launch_multidot(cudaStream_t s, int nchunks, const Chunk *chunks, const dou
 // x = a[p] x + sum_i coef[p*K+i] V_i
 void launch_combine(cudaStream_t s, int nchunks, const Chunk *chunks, double *x, const double *a,
                     const double *V, long long vstride, int K, const double *coef);
+// The same, and out[p] += <x, x> (weighted, the new x) over problem p's
+// chunks of this level, equal to launch_multidot(x, x, K = 1).
+void launch_combine_norm(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
+                         const double *a, const double *V, long long vstride, int K,
+                         const double *coef, const double *w, double *partial,
+                         const int *prob_chunk_begin, int nprob, const int *active, double *out);
 // dst (ghost-0) = interior of src (ghost-1), converted to FP64
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
