@@ -58,22 +58,26 @@ KRYLOV = 20
 STAGED_F32_TRAFFIC_RATIO = 67.2 / 54.6
 
 
+def workload_desc(name, nprob):
+    return {"c5": (f"config5: {nprob} independent 3-D variable-coefficient problems "
+                   f"(3 levels, coarse 64^3..128^3, D=exp(g) contrast 1e3)"),
+            "c2": "config2: 3-D 128^3 coarse + 2 random-box levels, f = 4 Gaussian bumps",
+            "c3": "config3: 2-D 64^2 + 64^2 fine, D = exp(g) contrast 1e3",
+            "c1": "config1: 2-D sine, 64^2 coarse + 64^2 fine box"}[name]
+
+
+def workload_seeds(name, nprob, rank):
+    """Seeds of this rank's problems (config 5: a disjoint block per rank)."""
+    return list(range(rank * nprob, (rank + 1) * nprob)) if name == "c5" else [rank]
+
+
 def make_workload(name, nprob, rank):
     from samrai_b200 import configs
     if name == "c5":
         probs = configs.config5(nprob, first_seed=rank * nprob)
-        desc = (f"config5: {nprob} independent 3-D variable-coefficient problems "
-                f"(3 levels, coarse 64^3..128^3, D=exp(g) contrast 1e3)")
-    elif name == "c2":
-        probs = [configs.config2(seed=2 + rank)]
-        desc = "config2: 3-D 128^3 coarse + 2 random-box levels, f = 4 Gaussian bumps"
-    elif name == "c3":
-        probs = [configs.config3()]
-        desc = "config3: 2-D 64^2 + 64^2 fine, D = exp(g) contrast 1e3"
     else:
-        probs = [configs.config1()]
-        desc = "config1: 2-D sine, 64^2 coarse + 64^2 fine box"
-    return probs, desc
+        probs = [_make_problem(name, rank)]
+    return probs, workload_desc(name, nprob)
 
 
 class ClockSampler:
@@ -145,48 +149,160 @@ def measured_peaks():
 # CPU baseline (oracle = CPU restatement of the reference path)
 # ---------------------------------------------------------------------------
 
-def _cpu_cycle_sample(args):
-    """Time one complete FAC cycle (V-cycle with the 500-sweep coarse solve,
-    u += e, restriction and the full composite residual) of one problem on
-    one core; returns (seconds, cells)."""
-    name, seed, nprob = args
-    sys.path.insert(0, ROOT)
+# Plain FAC cycle counts of the config-5 problems to the 1e-10 relative
+# residual (capped at max_cycles = 100), per seed.
+PLAIN_CYCLES_FILE = os.path.join(ROOT, "oracle", "c5_plain_cycles.json")
+
+
+def _make_problem(name, seed):
     from samrai_b200 import configs
-    from oracle.oracle import Oracle
     if name == "c5":
-        p = configs.config5_problem(seed)
-    elif name == "c2":
-        p = configs.config2()
-    elif name == "c3":
-        p = configs.config3()
-    else:
-        p = configs.config1()
-    prm = dict(PARAMS)
-    prm["max_cycles"] = 1
-    o = Oracle(p, params=prm)
-    t = time.perf_counter()
-    o.solve()
-    dt = time.perf_counter() - t
-    return dt, p.num_cells()
+        return configs.config5_problem(seed)
+    if name == "c2":
+        return configs.config2(seed=2 + seed)
+    if name == "c3":
+        return configs.config3()
+    return configs.config1()
 
 
-def cpu_estimate(name, nprob, cycles, cells_total, workers, samples):
-    """Oracle time for one cycle on `samples` problems (in parallel on
-    `workers` processes), scaled to the whole workload: seconds per cell per
-    cycle x cells x cycles / workers."""
-    import multiprocessing as mp
-    jobs = [(name, s, nprob) for s in range(samples)]
+def _ref_init(lib_path):
+    """Pool initializer: every worker loads the timing build of the oracle
+    and keeps numpy to one thread (one worker per core)."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    oracle.use_library(lib_path)
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(1)
+    except ImportError:
+        pass
+
+
+def _ref_sample(job):
+    """CPU seconds of one plain FAC cycle of one problem on one core.
+
+    The plain cycle's coarsest solve runs exactly coarse_max_it red-black
+    sweeps (tolerance 1e-300), each the same work, so the cycle is timed as
+    (two cycles - one cycle, both without coarse sweeps: the outer-loop
+    work of one cycle) + coarse_max_it x (one coarse sweep, the mean of
+    `sweeps` sweeps)."""
+    name, seed, sweeps = job
+    from oracle.oracle import Oracle, E, R
+    p = _make_problem(name, seed)
+    t = []
+    for cyc in (1, 2):
+        o = Oracle(p, params=dict(PARAMS, max_cycles=cyc, coarse_max_it=0))
+        t0 = time.perf_counter()
+        o.solve()
+        t.append(time.perf_counter() - t0)
     t0 = time.perf_counter()
-    if workers > 1:
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(workers) as pool:
-            res = pool.map(_cpu_cycle_sample, jobs)
-    else:
-        res = [_cpu_cycle_sample(j) for j in jobs]
-    wall = time.perf_counter() - t0
-    per_cell = sum(r[0] for r in res) / sum(r[1] for r in res)
-    est_s = per_cell * cells_total * cycles / max(workers, 1)
-    return est_s * 1e3, wall, res
+    o.smooth(E, R, 0, sweeps, -1.0)
+    t_sweep = (time.perf_counter() - t0) / sweeps
+    t_rest = max(t[1] - t[0], 0.0)
+    return {"seed": seed, "cells": p.num_cells(), "t_rest": t_rest, "t_sweep": t_sweep,
+            "t_cycle": t_rest + PARAMS["coarse_max_it"] * t_sweep}
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def plain_cycles(name, seeds):
+    """Cycle counts of the plain variant per seed: config 5 from the table
+    measured by the plain FP64 path (its counts equal the oracle's cycle for
+    cycle, by the parity tests); seeds missing from it get the table's mean.
+    Returns (counts, number of seeds found in the table)."""
+    table = {}
+    if name == "c5" and os.path.exists(PLAIN_CYCLES_FILE):
+        with open(PLAIN_CYCLES_FILE) as fh:
+            table = {int(k): int(v) for k, v in json.load(fh)["cycles"].items()}
+    mean = statistics.mean(table.values()) if table else 50.0
+    return [table.get(s, mean) for s in seeds], sum(1 for s in seeds if s in table)
+
+
+def lpt_makespan(costs, workers):
+    """Wall time of independent jobs on `workers` processes, longest first."""
+    import heapq
+    heap = [0.0] * max(1, workers)
+    for c in sorted(costs, reverse=True):
+        heapq.heappush(heap, heapq.heappop(heap) + c)
+    return max(heap)
+
+
+class CpuReference:
+    """Times the CPU restatement of the reference's plain FAC (timing build,
+    -O3 -march=native, one process per core) on samples of the workload and
+    turns them into the time to solve the whole workload on those cores."""
+
+    def __init__(self, name, seeds, workers=None, sweeps=20):
+        import multiprocessing as mp
+        from oracle import oracle
+        self.name, self.seeds, self.sweeps = name, list(seeds), sweeps
+        self.workers = max(1, min(workers or host_cores(), len(self.seeds)))
+        self.lib_path = oracle.build_timing()
+        self.pool = mp.get_context("spawn").Pool(self.workers, initializer=_ref_init,
+                                                 initargs=(self.lib_path,))
+        self.samples = {}
+        self.next = 0
+
+    def round(self, keep=True):
+        """One sampling round: every worker times one cycle of the next
+        problem in turn; returns the round's wall seconds."""
+        jobs = []
+        for _ in range(self.workers):
+            jobs.append((self.name, self.seeds[self.next % len(self.seeds)], self.sweeps))
+            self.next += 1
+        t0 = time.perf_counter()
+        res = self.pool.map(_ref_sample, jobs)
+        wall = time.perf_counter() - t0
+        if keep:
+            for r in res:
+                self.samples.setdefault(r["seed"], []).append(r)
+        return wall
+
+    def estimate(self, cells=None):
+        """(ms to solve every problem, details): per problem the mean
+        sampled cycle time times its plain cycle count; the problems spread
+        over the worker processes longest first.  Problems without a sample
+        (only when `cells`, seed -> cells, is given) take the sampled
+        problems' seconds per cell times their cells."""
+        tc = {x: statistics.mean(r["t_cycle"] for r in rs) for x, rs in self.samples.items()}
+        per_cell = sum(tc.values()) / sum(rs[0]["cells"] for rs in self.samples.values())
+        missing = [x for x in self.seeds if x not in tc]
+        if missing and cells is None:
+            raise RuntimeError(f"problems without a sample: {missing}")
+        for x in missing:
+            tc[x] = per_cell * cells[x]
+        cyc, known = plain_cycles(self.name, self.seeds)
+        costs = [tc[x] * c for x, c in zip(self.seeds, cyc)]
+        ms = lpt_makespan(costs, self.workers) * 1e3
+        return ms, {"problems": len(self.seeds), "sampled": len(self.samples),
+                    "cycles_from_table": known,
+                    "cycles_total": float(sum(cyc)), "core_seconds": round(sum(costs), 1),
+                    "samples": sum(len(v) for v in self.samples.values())}
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_small_solves(names=("c1", "c3")):
+    """Full plain FAC solves of the small 2-D configurations on one core
+    with the timing build (measured, not scaled)."""
+    from oracle import oracle
+    from oracle.oracle import Oracle
+    out = {}
+    for n in names:
+        p = _make_problem(n, 0)
+        o = Oracle(p, params=dict(PARAMS))
+        t0 = time.perf_counter()
+        ok, its, res, _ = o.solve()
+        out[n] = {"cpu_ms": round((time.perf_counter() - t0) * 1e3, 2), "cycles": int(its),
+                  "converged": bool(ok)}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -201,8 +317,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3"])
     ap.add_argument("--nprob", type=int, default=64)
-    ap.add_argument("--plain-problems", type=int, default=8,
+    ap.add_argument("--plain-problems", type=int, default=64,
                     help="problems of the workload the plain variant is timed on")
+    ap.add_argument("--plain-cycles-out", default=None, metavar="PATH",
+                    help="write the plain variant's cycle count per seed to PATH (JSON)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
@@ -399,6 +517,14 @@ def main():
                 num += float(np.sum((a - b) ** 2))
                 den += float(np.sum(b ** 2))
             diffs.append(math.sqrt(num / max(den, 1e-300)))
+        if args.plain_cycles_out and rank == 0:
+            seeds = workload_seeds(args.config, len(probs), rank)
+            with open(args.plain_cycles_out, "w") as fh:
+                json.dump({"what": "plain FAC cycles to a 1e-10 relative composite residual "
+                                   "(max_cycles 100, 500-sweep coarsest solve) per seed",
+                           "workload": desc,
+                           "cycles": {str(x): int(c) for x, c in zip(seeds, pits)}}, fh,
+                          indent=1)
         plain = {"ms": round(p_ms, 1), "problems": len(sub), "cells": sub_cells,
                  "ms_scaled_to_workload": round(p_ms * cells / sub_cells, 1),
                  "converged": int(np.sum(pconv)), "cycles": [int(x) for x in pits],
@@ -469,15 +595,35 @@ def main():
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cyc = float(np.mean(plain["cycles"])) if plain else 50.0
-        ms_est, wall, res_s = cpu_estimate(args.config, args.nprob, cyc, cells, 1, 1)
+        # the reference arm's estimate on a bounded sample: one round of one
+        # problem per core (unsampled problems scaled by their cells)
+        seeds = workload_seeds(args.config, len(probs), 0)
+        ref = CpuReference(args.config, seeds)
+        wall = ref.round()
+        ms_est, info = ref.estimate(cells={x: p.num_cells() for x, p in zip(seeds, probs)})
+        ref.close()
         out["cpu_baseline"] = {
-            "value": round(ms_est, 1), "unit": "ms", "cores": 1, "kind": "port",
-            "sample": (f"CPU restatement of the reference FAC (plain semantics, gcc -O2 "
-                       f"-ffp-contract=off): one full cycle of problem 0 ({res_s[0][1]} cells) "
-                       f"took {res_s[0][0]:.2f} s; scaled by cells ({cells}) and the mean plain "
-                       f"cycle count ({cyc:.1f})"),
+            "value": round(ms_est, 1), "unit": "ms", "cores": ref.workers, "kind": "port",
+            "sample": (f"CPU restatement of the reference FAC, plain semantics (gcc -O3 "
+                       f"-march=native -ffp-contract=off), one process per core: one plain "
+                       f"cycle of each of {info['sampled']} problems timed ({wall:.1f} s wall), "
+                       f"the rest scaled by cells; each problem's plain cycle count "
+                       f"({info['cycles_from_table']} of {info['problems']} from the measured "
+                       f"table), problems spread over {ref.workers} processes"),
         }
+        # measured full solves of the small 2-D configurations, CPU and GPU
+        small = cpu_small_solves()
+        for n in small:
+            sp = [_make_problem(n, 0)]
+            sctx = fac.FacContext(sp, params=PARAMS, device=local_rank)
+            sctx.solve()
+            sctx.zero(fac.U)
+            sctx.timer_start()
+            _, sits, _ = sctx.solve()
+            small[n]["gpu_plain_fp64_ms"] = round(sctx.timer_stop(), 3)
+            small[n]["gpu_cycles"] = int(sits[0])
+            sctx.close()
+        out["cpu_small_configs"] = {"kind": "measured", "cores": 1, "configs": small}
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -487,23 +633,39 @@ def main():
 
 
 def run_reference(args, world):
-    """CPU reference arm: the CPU restatement of the reference FAC (plain
-    semantics) on all host cores.  Each step times one full FAC cycle of as
-    many problems as there are worker processes; the value is that cost
-    scaled to every cell of the workload and to REFERENCE_CYCLES cycles
-    (the plain cycle count, identical on CPU and GPU by the parity tests)."""
-    workers = os.cpu_count() or 1
-    probs, desc = make_workload(args.config, args.nprob, 0)
-    cells = sum(p.num_cells() for p in probs)
-    cycles = REFERENCE_CYCLES.get(args.config, 50.0)
-    samples = max(1, min(workers, len(probs), 16))
-    vals = []
-    for it in range(args.warmup + args.steps):
-        ms_est, wall, res = cpu_estimate(args.config, args.nprob, cycles, cells, samples,
-                                         samples)
-        if it >= args.warmup:
-            vals.append(ms_est)
-    value = statistics.mean(vals)
+    """CPU reference arm: the CPU restatement of the reference's plain FAC
+    on all host cores (one process per core, -O3 -march=native).  A step is
+    one sampling round, in which every process times one plain cycle of the
+    next problem in turn (`_ref_sample`); the rounds run until every problem
+    of the workload has a sample.  The value is the time to solve the
+    workload: per problem its mean cycle time times its plain cycle count,
+    the problems spread over the processes longest first."""
+    seeds = workload_seeds(args.config, args.nprob, 0)
+    desc = workload_desc(args.config, args.nprob)
+    if args.config in ("c1", "c3"):
+        # small enough to solve outright
+        vals = []
+        for it in range(args.warmup + args.steps):
+            r = cpu_small_solves((args.config,))[args.config]
+            if it >= args.warmup:
+                vals.append(r["cpu_ms"])
+        value, cores = statistics.mean(vals), 1
+        sample = f"full plain FAC solve, {r['cycles']} cycles, one core, measured"
+        info = {}
+    else:
+        ref = CpuReference(args.config, seeds)
+        for _ in range(args.warmup):
+            ref.round(keep=False)
+        rounds = max(args.steps, -(-len(seeds) // ref.workers))
+        walls = [ref.round() for _ in range(rounds)]
+        value, info = ref.estimate()
+        ref.close()
+        cores = ref.workers
+        sample = (f"{rounds} rounds of one plain cycle per process ({sum(walls):.1f} s wall): "
+                  f"cycle = outer-loop work + 500 x one coarse red-black sweep, timed per "
+                  f"problem; per-problem plain cycle counts ({info['cycles_from_table']} of "
+                  f"{info['problems']} from the measured table); problems spread over "
+                  f"{cores} processes longest first")
     out = {
         "metric": METRIC,
         "impl": "reference",
@@ -518,22 +680,18 @@ def run_reference(args, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": desc, "variant": "CPU FAC, reference semantics (oracle port)",
-                   "cycles_assumed": cycles},
-        "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": samples,
-                         "kind": "port",
-                         "sample": (f"one full FAC cycle of {samples} problems on {samples} "
-                                    f"processes, scaled to {cells} cells and {cycles} cycles")},
+        "config": {"workload": desc,
+                   "variant": "CPU FAC, reference semantics (oracle port, gcc -O3 "
+                              "-march=native -ffp-contract=off), plain cycle, 500-sweep "
+                              "red-black coarsest solve",
+                   **info},
+        "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": cores,
+                         "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
     return 0
-
-
-# Plain-FAC cycle counts per workload (mean over problems), as measured on
-# the GPU path whose cycle counts equal the CPU oracle's (parity tests).
-REFERENCE_CYCLES = {"c5": 50.0, "c2": 72.0, "c1": 20.0, "c3": 48.0}
 
 
 if __name__ == "__main__":

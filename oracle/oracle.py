@@ -25,6 +25,25 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
+def build_timing():
+    """Compile the -O3 -march=native timing build of the oracle into a fresh
+    temporary directory (the CPU it targets is the one running this) and
+    return its path; the results are bit-identical to the default build."""
+    import tempfile
+    d = tempfile.mkdtemp(prefix="facoracle_timing_")
+    subprocess.run(["make", "-s", "-C", _HERE, "timing", f"TIMING_DIR={d}"], check=True)
+    return os.path.join(d, "libfacoracle.so")
+
+
+def use_library(path):
+    """Load the oracle from `path` (a timing build) instead of the default
+    build; must precede the first call into the oracle in this process."""
+    global _LIB_PATH
+    if _lib is not None and path != _LIB_PATH:
+        raise RuntimeError("oracle library already loaded")
+    _LIB_PATH = path
+
+
 def lib():
     global _lib
     if _lib is None:
