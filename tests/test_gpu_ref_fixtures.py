@@ -1,0 +1,78 @@
+"""The CUDA path against the reference's own FAC solver.
+
+The same golden solves as tests/test_ref_fixtures.py (SAMRAI's
+CellPoissonFACSolver built from the reference's sources), reached through
+the drop-in solver class samrai_b200.fac.CellPoissonFACSolver with the
+reference's input keys: the cycle count and convergence flag must be equal,
+the residual norm after every cycle within 1e-11 relative, the convergence
+factors within 1e-10, and the solution on every level within 1e-12
+relative (all cells where the fixture keeps the whole array, else every
+97th value and the level's fingerprint).  Where the result is bit-identical
+to the reference's, the digests agree as well; the test reports it.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ref_cases
+from samrai_b200 import fac
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("name", list(ref_cases.CASES))
+def test_gpu_solver_matches_reference_solver(name, require_gpu):
+    fx = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    build, prm, bc, full = ref_cases.CASES[name]
+    p = build()
+    solver = fac.CellPoissonFACSolver(p.dim, "solver", {
+        "max_cycles": prm["max_cycles"], "residual_tol": prm["residual_tol"],
+        "relative_residual_tol": prm["relative_residual_tol"],
+        "num_pre_sweeps": prm["pre_sweeps"], "num_post_sweeps": prm["post_sweeps"],
+        "coarse_solver_choice": "redblack", "coarse_solver_tolerance": prm["coarse_tol"],
+        "coarse_solver_max_iterations": prm["coarse_max_it"],
+        "cf_discretization": "Ewing", "prolongation_method": "LINEAR_REFINE"})
+    if p.d_variable:
+        solver.setDPatchDataId()
+    else:
+        solver.setDConstant(p.d_const)
+    if p.c_kind == 2:
+        solver.setCPatchDataId()
+    if bc is None:
+        solver.setBoundaries("Dirichlet")
+    else:
+        solver.setBcObject(*bc)
+    solver.initializeSolverState(p)
+    converged = solver.solveSystem()
+    assert solver.getNumberOfIterations() == int(fx["iterations"][0])
+    assert converged == bool(fx["converged"][0])
+    assert rel(solver.getResidualNorm(), fx["residual"]) <= 1e-11
+    hist = solver._ctx.residual_history(0)
+    assert rel(hist[1:], fx["hist"]) <= 1e-11
+    avg, fin = solver.getConvergenceFactors()
+    assert rel([avg, fin], fx["factors"]) <= 1e-10
+    bit = []
+    for ln in range(p.nlev):
+        u = p.u[ln]
+        m = ref_cases.interior_mask(p, ln)
+        if full:
+            want = fx[f"u{ln}"]
+            assert rel(u[m], want[m]) <= 1e-12, ln
+            if bc is None:
+                assert rel(u, want) <= 1e-12, ln
+        else:
+            assert rel(u[::ref_cases.SAMPLE], fx[f"u{ln}_sample"]) <= 1e-12, ln
+            s = ref_cases.summarize(u)
+            assert s[0] == fx[f"u{ln}_summary"][0]
+            assert rel(s[1:], fx[f"u{ln}_summary"][1:]) <= 1e-10, ln
+        bit.append(bool(np.array_equal(ref_cases.digest(u[m]), fx[f"u{ln}_sha_interior"])))
+    solver.deallocateSolverState()
+    print(f"{name}: interior bit-identical to the reference per level: {bit}")
