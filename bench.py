@@ -13,8 +13,10 @@ Multi-GPU (torchrun, one rank per GPU): the independent problems are
 sharded, each rank solving its own batch of the same size (weak scaling, no
 data-path collective); the step time is the maximum over ranks.
 
-``--impl reference`` times the CPU restatement of the reference's FAC path
-(oracle/, kind "port") on all host cores.
+``--impl reference`` times the reference's own FAC solver on all host cores:
+its C++ built from its sources with its Fortran kernels translated to C
+(oracle/_ref, kind "reference"), or the oracle's restatement of it (kind
+"port") where that build is absent.
 """
 from __future__ import annotations
 
@@ -167,10 +169,12 @@ def _make_problem(name, seed):
 
 def _ref_init(lib_path):
     """Pool initializer: every worker loads the timing build of the oracle
-    and keeps numpy to one thread (one worker per core)."""
+    (when the port is timed) and keeps numpy to one thread (one worker per
+    core)."""
     sys.path.insert(0, ROOT)
-    from oracle import oracle
-    oracle.use_library(lib_path)
+    if lib_path:
+        from oracle import oracle
+        oracle.use_library(lib_path)
     try:
         from threadpoolctl import threadpool_limits
         threadpool_limits(1)
@@ -182,25 +186,35 @@ def _ref_sample(job):
     """CPU seconds of one plain FAC cycle of one problem on one core.
 
     The plain cycle's coarsest solve runs exactly coarse_max_it red-black
-    sweeps (tolerance 1e-300), each the same work, so the cycle is timed as
-    (two cycles - one cycle, both without coarse sweeps: the outer-loop
-    work of one cycle) + coarse_max_it x (one coarse sweep, the mean of
-    `sweeps` sweeps)."""
-    name, seed, sweeps = job
-    from oracle.oracle import Oracle, E, R
+    sweeps (tolerance 1e-300), each the same work, so the cycle is timed in
+    parts: T(c cycles, m coarse sweeps) for (1, m0), (2, m0) and (1, m0 +
+    sweeps); the cycle is T(2, m0) - T(1, m0) plus (coarse_max_it - m0) x
+    one sweep, a sweep being (T(1, m0 + sweeps) - T(1, m0)) / sweeps.
+    kind "reference" runs the reference's own CellPoissonFACSolver
+    (oracle/_ref/fac_ref_driver, solveSystem timed inside; the reference
+    needs m0 >= 1), kind "port" the oracle's restatement of it (m0 = 0)."""
+    name, seed, sweeps, kind = job
     p = _make_problem(name, seed)
-    t = []
-    for cyc in (1, 2):
-        o = Oracle(p, params=dict(PARAMS, max_cycles=cyc, coarse_max_it=0))
+    m0 = 1 if kind == "reference" else 0
+
+    def solve_seconds(cyc, m):
+        prm = dict(PARAMS, max_cycles=cyc, coarse_max_it=m)
+        if kind == "reference":
+            from oracle.ref import refio
+            return float(refio.run_reference(p, prm, solution=False)["seconds"][1])
+        from oracle.oracle import Oracle
+        o = Oracle(p, params=prm)
         t0 = time.perf_counter()
         o.solve()
-        t.append(time.perf_counter() - t0)
-    t0 = time.perf_counter()
-    o.smooth(E, R, 0, sweeps, -1.0)
-    t_sweep = (time.perf_counter() - t0) / sweeps
-    t_rest = max(t[1] - t[0], 0.0)
+        return time.perf_counter() - t0
+
+    t_a = solve_seconds(1, m0)
+    t_b = solve_seconds(2, m0)
+    t_c = solve_seconds(1, m0 + sweeps)
+    t_sweep = max(t_c - t_a, 0.0) / sweeps
+    t_rest = max(t_b - t_a, 0.0)
     return {"seed": seed, "cells": p.num_cells(), "t_rest": t_rest, "t_sweep": t_sweep,
-            "t_cycle": t_rest + PARAMS["coarse_max_it"] * t_sweep}
+            "t_cycle": t_rest + (PARAMS["coarse_max_it"] - m0) * t_sweep}
 
 
 def host_cores():
@@ -232,17 +246,29 @@ def lpt_makespan(costs, workers):
     return max(heap)
 
 
+CPU_KIND_TEXT = {
+    "reference": "the reference's CellPoissonFACSolver built from its sources (g++ -O2 "
+                 "-ffp-contract=off, Fortran kernels translated to C)",
+    "port": "the oracle's C restatement of the reference FAC (gcc -O3 -march=native "
+            "-ffp-contract=off)"}
+
+
 class CpuReference:
-    """Times the CPU restatement of the reference's plain FAC (timing build,
-    -O3 -march=native, one process per core) on samples of the workload and
-    turns them into the time to solve the whole workload on those cores."""
+    """Times the reference's plain FAC on the CPU -- its own solver built
+    from its sources (oracle/_ref, g++ -O2) when present, else the oracle's
+    restatement (timing build, gcc -O3 -march=native) -- one process per
+    core, on samples of the workload, and turns them into the time to solve
+    the whole workload on those cores."""
 
     def __init__(self, name, seeds, workers=None, sweeps=20):
         import multiprocessing as mp
         from oracle import oracle
+        from oracle.ref import refio
         self.name, self.seeds, self.sweeps = name, list(seeds), sweeps
         self.workers = max(1, min(workers or host_cores(), len(self.seeds)))
-        self.lib_path = oracle.build_timing()
+        # the reference's own solver when its build is present, else the port
+        self.kind = "reference" if refio.available() else "port"
+        self.lib_path = oracle.build_timing() if self.kind == "port" else None
         self.pool = mp.get_context("spawn").Pool(self.workers, initializer=_ref_init,
                                                  initargs=(self.lib_path,))
         self.samples = {}
@@ -253,7 +279,8 @@ class CpuReference:
         problem in turn; returns the round's wall seconds."""
         jobs = []
         for _ in range(self.workers):
-            jobs.append((self.name, self.seeds[self.next % len(self.seeds)], self.sweeps))
+            jobs.append((self.name, self.seeds[self.next % len(self.seeds)], self.sweeps,
+                         self.kind))
             self.next += 1
         t0 = time.perf_counter()
         res = self.pool.map(_ref_sample, jobs)
@@ -603,10 +630,10 @@ def main():
         ms_est, info = ref.estimate(cells={x: p.num_cells() for x, p in zip(seeds, probs)})
         ref.close()
         out["cpu_baseline"] = {
-            "value": round(ms_est, 1), "unit": "ms", "cores": ref.workers, "kind": "port",
-            "sample": (f"CPU restatement of the reference FAC, plain semantics (gcc -O3 "
-                       f"-march=native -ffp-contract=off), one process per core: one plain "
-                       f"cycle of each of {info['sampled']} problems timed ({wall:.1f} s wall), "
+            "value": round(ms_est, 1), "unit": "ms", "cores": ref.workers, "kind": ref.kind,
+            "sample": (f"{CPU_KIND_TEXT[ref.kind]}, plain semantics, one process per core: "
+                       f"one plain cycle of each of {info['sampled']} problems timed "
+                       f"({wall:.1f} s wall), "
                        f"the rest scaled by cells; each problem's plain cycle count "
                        f"({info['cycles_from_table']} of {info['problems']} from the measured "
                        f"table), problems spread over {ref.workers} processes"),
@@ -649,7 +676,7 @@ def run_reference(args, world):
             r = cpu_small_solves((args.config,))[args.config]
             if it >= args.warmup:
                 vals.append(r["cpu_ms"])
-        value, cores = statistics.mean(vals), 1
+        value, cores, kind = statistics.mean(vals), 1, "port"
         sample = f"full plain FAC solve, {r['cycles']} cycles, one core, measured"
         info = {}
     else:
@@ -660,7 +687,7 @@ def run_reference(args, world):
         walls = [ref.round() for _ in range(rounds)]
         value, info = ref.estimate()
         ref.close()
-        cores = ref.workers
+        cores, kind = ref.workers, ref.kind
         sample = (f"{rounds} rounds of one plain cycle per process ({sum(walls):.1f} s wall): "
                   f"cycle = outer-loop work + 500 x one coarse red-black sweep, timed per "
                   f"problem; per-problem plain cycle counts ({info['cycles_from_table']} of "
@@ -681,12 +708,11 @@ def run_reference(args, world):
         "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": desc,
-                   "variant": "CPU FAC, reference semantics (oracle port, gcc -O3 "
-                              "-march=native -ffp-contract=off), plain cycle, 500-sweep "
-                              "red-black coarsest solve",
+                   "variant": f"{CPU_KIND_TEXT[kind]}: plain cycle, 500-sweep red-black "
+                              f"coarsest solve",
                    **info},
         "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": cores,
-                         "kind": "port", "sample": sample},
+                         "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -26,11 +26,14 @@
  * a field).  Arrays of a level are its patches' ghosted arrays in patch
  * order, each column-major (pdat::ArrayData layout); side data per patch,
  * axis 0..dim-1.
+ * With a "skip_u" record the solution is not written back.
  * Output records: converged, iterations, residual, hist (composite residual
- * norm after each cycle), factors (average, final), u<ln> (ghost 1).
+ * norm after each cycle), factors (average, final), seconds (wall time of
+ * initializeSolverState and of solveSystem), u<ln> (ghost 1).
  */
 #include "SAMRAI/SAMRAI_config.h"
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -372,9 +375,13 @@ int run(Records &in, const char *out_path)
    else solver.setCConstant(ckind == 1 ? poisson[3] : 0.0);
    if (robin_bc) solver.setBcObject(&robin);
    else solver.setBoundaries("Dirichlet");
+   using clock = std::chrono::steady_clock;
+   const clock::time_point t0 = clock::now();
    solver.initializeSolverState(u_id, f_id, hierarchy, 0, nlev - 1);
    TRACE("state initialized");
+   const clock::time_point t1 = clock::now();
    const int converged = solver.solveSystem(u_id, f_id) ? 1 : 0;
+   const clock::time_point t2 = clock::now();
    TRACE("solved");
    double avg = 0.0, fin = 0.0;
    solver.getConvergenceFactors(avg, fin);
@@ -384,8 +391,12 @@ int run(Records &in, const char *out_path)
    write_record(out, "residual", {solver.getResidualNorm()});
    write_record(out, "factors", {avg, fin});
    write_record(out, "hist", ops->hist);
-   for (int ln = 0; ln < nlev; ++ln)
-      write_record(out, "u" + std::to_string(ln), save_cell(hierarchy->getPatchLevel(ln), u_id));
+   write_record(out, "seconds", {std::chrono::duration<double>(t1 - t0).count(),
+                                 std::chrono::duration<double>(t2 - t1).count()});
+   if (!in.i32.count("skip_u"))
+      for (int ln = 0; ln < nlev; ++ln)
+         write_record(out, "u" + std::to_string(ln),
+                      save_cell(hierarchy->getPatchLevel(ln), u_id));
    solver.deallocateSolverState();
    return 0;
 }

@@ -76,12 +76,20 @@ def problem_records(prob, params, bc=None):
     return recs
 
 
-def run_reference(prob, params, bc=None, driver=DRIVER, timeout=3600):
+def available(driver=DRIVER):
+    return os.access(driver, os.X_OK)
+
+
+def run_reference(prob, params, bc=None, driver=DRIVER, timeout=3600, solution=True):
     """Solve `prob` with the reference's CellPoissonFACSolver; returns the
-    driver's output records."""
+    driver's output records (without the solution arrays when `solution`
+    is false)."""
     with tempfile.TemporaryDirectory() as d:
         fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
-        write(fin, problem_records(prob, params, bc))
+        recs = problem_records(prob, params, bc)
+        if not solution:
+            recs.append(("skip_u", np.array([1], dtype=np.int32)))
+        write(fin, recs)
         r = subprocess.run([driver, fin, fout], capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"fac_ref_driver failed ({r.returncode}): {r.stderr[-2000:]}")
