@@ -363,7 +363,14 @@ int fac_learned_samples(fac_ctx *ctx, int level, float *x, double *scale);
  * with the device current); make that first call before any stream capture.
  * All calls share the array: calls whose work can overlap on the GPU (two
  * streams, or two host threads) race and must be serialised by the caller.
- * Every partial sum a call reads it first writes, so no clearing is needed. */
+ * Every partial sum a call reads it first writes, so no clearing is needed.
+ * The looked-up address is kept for the life of the process: do not use
+ * this entry point on a device after cudaDeviceReset.  An error already
+ * pending on the calling thread when the call starts (left by earlier,
+ * unrelated work) is reported as FAC_ERR_CUDA and left in place for its
+ * owner; the call then launches nothing.  An empty segment's norm is 0.
+ * Each segment is reduced by 64 blocks, so a call with few large segments
+ * runs below memory bandwidth. */
 #define FAC_NOALLOC_MAX_SEGMENTS 256
 int fac_rms_norm_noalloc(const double *x, const double *w,
                          const long long *seg_offsets, int nseg, double *norms,

@@ -132,5 +132,47 @@ __device__ __forceinline__ T robin(T uin, int loc, T h, int hom, const BcCoefs &
    return (h * (T)bc.g[loc] + uin * (b - half * h * a)) / (b + half * h * a);
 }
 
+// One red-black point update from the six face fluxes (low/high per axis),
+// the six face coefficients, C and f (rbgswithfluxmax*, 2d.f:136-160,
+// 3d.f:196-226): returns the new value and the residual.  FP64 keeps the
+// Fortran's evaluation order with every product and sum rounded separately
+// (the build has no contraction).  FP32, used only for the error equation
+// inside the mixed cycle whose FP64 outer loop restores the accuracy, fuses
+// the sums of products into FMAs; the reciprocal is the correctly rounded
+// one in both.
+template <int DIM, class T>
+__device__ __forceinline__ T rb_point(T fv, T uc, T scv, T dxi, T dyi, T dzi, T fxl, T fxh,
+                                      T fyl, T fyh, T fzl, T fzh, T dx0, T dx1, T dy0, T dy1,
+                                      T dz0, T dz1, T &residual)
+{
+   const T one = (T)1;
+   if constexpr (sizeof(T) == 8) {
+      T dudr;
+      if (DIM == 2) {
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - scv * uc;
+         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - scv);
+      } else {
+         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
+         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - scv * uc;
+         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) - scv);
+      }
+      const T du = -residual * dudr;
+      const T rcoef = one;
+      return uc + du * rcoef;
+   } else {
+      T div = dxi * (fxh - fxl);
+      div = __fmaf_rn(dyi, fyh - fyl, div);
+      T diag = dxi * dxi * (dx1 + dx0);
+      diag = __fmaf_rn(dyi * dyi, dy1 + dy0, diag);
+      if (DIM == 3) {
+         div = __fmaf_rn(dzi, fzh - fzl, div);
+         diag = __fmaf_rn(dzi * dzi, dz1 + dz0, diag);
+      }
+      residual = __fmaf_rn(-scv, uc, fv - div);
+      const T dudr = __frcp_rn(diag - scv);
+      return __fmaf_rn(-residual, dudr, uc);
+   }
+}
+
 }  // namespace dev
 }  // namespace samrai_b200

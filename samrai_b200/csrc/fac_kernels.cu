@@ -232,8 +232,6 @@ __device__ __forceinline__ void rb_slot(const PatchDesc &p, int s, int nx, int n
                                         T dconst, T cconst, const long long *__restrict__ facemap,
                                         const BcCoefs &bc, double &maxres)
 {
-   const T one = (T)1;
-   const T rcoef = one;
       const int row = s / hx;
       const int mm = s - row * hx;
       const int j = p.lo[1] + row % ny;
@@ -332,19 +330,9 @@ __device__ __forceinline__ void rb_slot(const PatchDesc &p, int s, int nx, int n
       const T sf = CKIND == 2 ? cfield[cidx<DIM>(p, p.off0, 0, i, j, k)]
                               : (CKIND == 1 ? cconst : (T)0);
       const T fv = f[cidx<DIM>(p, p.off0, 0, i, j, k)];
-      T residual, dudr;
-      if (DIM == 2) {
-         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - sf * uc;
-         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - sf);
-      } else {
-         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
-         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) -
-                    sf * uc;
-         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) -
-                       sf);
-      }
-      const T du = -residual * dudr;
-      u[c] = uc + du * rcoef;
+      T residual;
+      u[c] = rb_point<DIM, T>(fv, uc, sf, dxi, dyi, dzi, fxl, fxh, fyl, fyh, fzl, fzh, dx0, dx1,
+                              dy0, dy1, dz0, dz1, residual);
       const double ar = fabs((double)residual);
       if (maxres < ar) maxres = ar;
 }

@@ -105,6 +105,11 @@ extern "C" int fac_rms_norm_noalloc(const double *x, const double *w,
          return FAC_ERR_ARG;
       }
    }
+   // an error left pending by earlier work belongs to its owner: report it
+   // without consuming it, so that any error after the launches is ours
+   if (cudaPeekAtLastError() != cudaSuccess) {
+      return FAC_ERR_CUDA;
+   }
    int dev = 0;
    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
       return FAC_ERR_CUDA;

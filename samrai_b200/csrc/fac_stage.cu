@@ -177,12 +177,10 @@ __device__ __forceinline__ void stage_update(unsigned char *stage, int tid, T *_
    const int hx = h->hx;
    const int nslots = h->nslots;
    const unsigned mhx = h->mhx, mny = h->mny;
-   const T one = (T)1;
    const bool f64 = sizeof(T) == 8;
    const T dxi = f64 ? (T)h->dxi_d[0] : (T)h->dxi_f[0];
    const T dyi = f64 ? (T)h->dxi_d[1] : (T)h->dxi_f[1];
    const T dzi = DIM == 3 ? (f64 ? (T)h->dxi_d[2] : (T)h->dxi_f[2]) : (T)0;
-   const T rcoef = one;
    // parity of the first cell of each row: lo1 + j (2-D), lo0 + j + k (3-D)
    const int qbase = DIM == 3 ? lo0 + lo1 + lo2 + s0 : 2 * lo1 + s0;
    // two slots per thread in flight: their shared-memory loads overlap
@@ -279,17 +277,9 @@ __device__ __forceinline__ void stage_update(unsigned char *stage, int tid, T *_
       const int l0 = DIM == 3 ? li + nx * (lj + ny * ls) : li + nx * ls;
       const T scv = CKIND == 2 ? sc[l0] : (CKIND == 1 ? cconst : (T)0);
       const T fv = sf[l0];
-      T residual, dudr;
-      if (DIM == 2) {
-         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - scv * uc;
-         dudr = one / ((dxi * dxi * (dx1 + dx0) + dyi * dyi * (dy1 + dy0)) - scv);
-      } else {
-         const T dxi2 = dxi * dxi, dyi2 = dyi * dyi, dzi2 = dzi * dzi;
-         residual = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - scv * uc;
-         dudr = one / ((dxi2 * (dx1 + dx0) + dyi2 * (dy1 + dy0) + dzi2 * (dz1 + dz0)) - scv);
-      }
-      const T du = -residual * dudr;
-      const T v = uc + du * rcoef;
+      T residual;
+      const T v = rb_point<DIM, T>(fv, uc, scv, dxi, dyi, dzi, fxl, fxh, fyl, fyh, fzl, fzh, dx0,
+                                   dx1, dy0, dy1, dz0, dz1, residual);
       gu[c] = v;
       su[c] = v;
    }

@@ -1,9 +1,12 @@
 """fac_rms_norm_noalloc: the weighted RMS norm for callers that cannot
-allocate device memory (a pool allocator owns all of it, or the call sits
-inside a CUDA graph capture).  Its partial sums live in a static device
-array instead of context scratch; here it must agree with fac_rms_norm on
-the same data, on two calls in a row (the second call reuses the array the
-first one left behind).  Kept in its own file, collected last."""
+allocate device memory when they need a norm (all device memory handed to a
+pool allocator up front, or a time step that may not call cudaMalloc because
+it synchronises the device).  Its partial sums live in a static device array
+instead of context scratch.  Here it must agree with fac_rms_norm on the
+same data on two calls in a row (the second call reuses the array the first
+one left behind), leave the device's free memory unchanged, give 0 for an
+empty segment, accept the full FAC_NOALLOC_MAX_SEGMENTS segments and reject
+one more.  Kept in its own file, collected last."""
 import ctypes
 
 import numpy as np
@@ -12,6 +15,8 @@ import pytest
 from samrai_b200 import configs, fac
 
 pytestmark = pytest.mark.gpu
+
+MAX_SEGMENTS = 256  # FAC_NOALLOC_MAX_SEGMENTS
 
 
 def _single_level_problem(n, seed):
@@ -22,14 +27,24 @@ def _single_level_problem(n, seed):
     return p
 
 
+def _entry():
+    lib = fac.load_library()
+    fn = lib.fac_rms_norm_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                   ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    return fn
+
+
+def _offsets(offs):
+    offs = np.ascontiguousarray(offs, dtype=np.int64)
+    return offs, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+
+
 def test_no_alloc_norm_matches_context_norm(require_gpu):
     import torch
 
-    lib = fac.load_library()
-    lib.fac_rms_norm_noalloc.restype = ctypes.c_int
-    lib.fac_rms_norm_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
-                                         ctypes.POINTER(ctypes.c_longlong), ctypes.c_int,
-                                         ctypes.c_void_p, ctypes.c_void_p]
+    norm = _entry()
     probs = [_single_level_problem(n, s) for s, n in enumerate((16, 32, 48))]
     ctx = fac.FacContext(probs)
     rng = np.random.default_rng(7)
@@ -43,22 +58,41 @@ def test_no_alloc_norm_matches_context_norm(require_gpu):
 
     x = torch.from_numpy(np.concatenate(xs)).cuda()
     w = torch.from_numpy(np.concatenate(ws)).cuda()
-    offs = np.concatenate([[0], np.cumsum([a.size for a in xs])]).astype(np.int64)
-    off_p = offs.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+    offs, off_p = _offsets(np.concatenate([[0], np.cumsum([a.size for a in xs])]))
     stream = torch.cuda.current_stream().cuda_stream
+    out = torch.full((MAX_SEGMENTS,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free = []
     for _ in range(2):
-        out = torch.full((len(probs),), float("nan"), dtype=torch.float64, device="cuda")
-        rc = lib.fac_rms_norm_noalloc(x.data_ptr(), w.data_ptr(), off_p, len(probs),
-                                      out.data_ptr(), stream)
+        out.fill_(float("nan"))
+        rc = norm(x.data_ptr(), w.data_ptr(), off_p, len(probs), out.data_ptr(), stream)
         assert rc == 0
         torch.cuda.synchronize()
-        got = out.cpu().numpy()
+        free.append(torch.cuda.mem_get_info()[0])
+        got = out[:len(probs)].cpu().numpy()
         np.testing.assert_allclose(got, want, rtol=1e-13, atol=0)
+    # nothing allocated by the second call (the first may load the module)
+    assert free[1] == free[0]
 
-    # sizes beyond the static array are rejected, not truncated
-    big = np.zeros(258, dtype=np.int64)
-    rc = lib.fac_rms_norm_noalloc(x.data_ptr(), w.data_ptr(),
-                                  big.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), 257,
-                                  out.data_ptr(), stream)
+    # the full segment count, with empty segments among them: every
+    # segment's norm against numpy, an empty one is 0
+    cuts = np.sort(rng.integers(0, x.numel(), MAX_SEGMENTS - 1))
+    cuts[10] = cuts[11]  # segment 11 is empty
+    offs, off_p = _offsets(np.concatenate([[0], cuts, [x.numel()]]))
+    rc = norm(x.data_ptr(), w.data_ptr(), off_p, MAX_SEGMENTS, out.data_ptr(), stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    xh, wh = x.cpu().numpy(), w.cpu().numpy()
+    for s in range(MAX_SEGMENTS):
+        a, b = offs[s], offs[s + 1]
+        sw = wh[a:b].sum()
+        ref = np.sqrt((xh[a:b] ** 2 * wh[a:b]).sum()) / np.sqrt(sw) if sw > 0 else 0.0
+        np.testing.assert_allclose(got[s], ref, rtol=1e-12, atol=0)
+    assert got[11] == 0.0
+
+    # one segment beyond the static array is rejected, not truncated
+    big, big_p = _offsets(np.zeros(MAX_SEGMENTS + 2))
+    rc = norm(x.data_ptr(), w.data_ptr(), big_p, MAX_SEGMENTS + 1, out.data_ptr(), stream)
     assert rc == 1
     ctx.close()
