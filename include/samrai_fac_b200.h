@@ -82,6 +82,23 @@ int fac_add_problem(fac_ctx *ctx, const int *n0, const double *xlo,
                     const double *xup, int nlev, const int *ratio,
                     const int *npatch, const int *boxes, int *problem);
 
+/* Multigrid coarsest-level solve (no counterpart in the reference, whose
+ * equivalent is its hypre coarse solver, CellPoissonFACOps.C:1741-1781):
+ * every problem added after this call gets `levels` extra levels below its
+ * level 0, each one patch covering the domain at half the previous
+ * resolution, so the FAC cycle continues as a multigrid V-cycle whose
+ * coarsest solve is small.  The added cells are all covered, so the
+ * composite problem, its weights and norms are unchanged.  Requires a level
+ * 0 that covers the domain with n0 divisible by 2^levels; call before
+ * fac_add_problem.  Level numbers in every other call count the added
+ * levels: the caller's level l is level l + levels, and the host tables of
+ * fac_solve_host hold the caller's levels only.  D (and C) on the added
+ * levels derive from the caller's level 0 (face means; C, f and u zero);
+ * solves redo that after D or C of that level was uploaded, and
+ * fac_extend_coefficients does it on demand. */
+int fac_set_coarse_extension(fac_ctx *ctx, int levels);
+int fac_extend_coefficients(fac_ctx *ctx);
+
 /* PoissonSpecifications (solv/PoissonSpecifications.h:51-345):
  * div(D grad u) + C u = f.  d_variable: D is side data (fac_upload_side);
  * c_kind 0 = zero, 1 = constant c_const, 2 = cell field FAC_C. */
@@ -244,7 +261,8 @@ int fac_solve(fac_ctx *ctx, int *converged, int *iterations,
 
 /* Solve from host memory: uploads f (and u0, when not NULL) for every
  * problem and level, solves, and downloads u.  Array k of f_host/u_host
- * holds level (k % nlev) of problem (k / nlev) in the host layout. */
+ * holds level (k % nlev) of problem (k / nlev) in the host layout (nlev:
+ * the caller's levels, without those of fac_set_coarse_extension). */
 int fac_solve_host(fac_ctx *ctx, const double *const *f_host,
                    const double *const *u0_host, double *const *u_host,
                    int *converged, int *iterations, double *residual);

@@ -408,6 +408,11 @@ struct fac_ctx {
    int kry_m = 0;
    DevArray<double> kry_dots, kry_coef, kry_a;
    int krylov = 0;  // > 0: fac_solve runs FGMRES(krylov) around the FAC cycle
+   // fac_set_coarse_extension: domain-covering coarser levels added below
+   // every problem's level 0, and whether their coefficients need to be
+   // derived again from the caller's level 0 before the next solve
+   int ext_levels = 0;
+   bool ext_dirty = false;
    // learned correction after every cycle (fac_set_learned)
    fac_cnn *cnn = nullptr;
    int learned_level = -1;
@@ -2579,32 +2584,50 @@ void kry_alloc(fac_ctx *c, int m)
    c->kry_m = m;
 }
 
-// out[p*K + i] = <x, V_i> (weighted) over all levels, for i < K
-void kry_dots(fac_ctx *c, int xslot, int vslot, int K, std::vector<double> &out)
+// Krylov operands that are not slots: the residual field TR (the operator's
+// output) and R (the preconditioner's input), ghost-0 level arrays of the
+// same layout as the slots
+constexpr int kNoField = -1;
+
+double *kry_field(fac_ctx *c, int ln, int field)
+{
+   if (field == FAC_TR) return c->L[ln].tr.p;
+   if (field == FAC_R) return c->L[ln].r.p;
+   return nullptr;
+}
+
+// out[p*KT + i] = <x, V_i> (weighted) over all levels, for i < K, x slot
+// xslot or the field xfield; with self_dot KT = K + 1 and entry K is <x, x>
+void kry_dots(fac_ctx *c, int xslot, int vslot, int K, std::vector<double> &out,
+              int xfield = kNoField, bool self_dot = false)
 {
    OpTimer ot(c, "kry_dots", -1);
    const int np = nprob(c);
-   CUDA_CHECK(cudaMemsetAsync(c->kry_dots.p, 0, (size_t)np * K * sizeof(double), c->stream));
+   const int KT = K + (self_dot ? 1 : 0);
+   CUDA_CHECK(cudaMemsetAsync(c->kry_dots.p, 0, (size_t)np * KT * sizeof(double), c->stream));
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
       const int pi = prof_begin(c, 4, L.cells_prob, 8.0 * (K + 2));
-      launch_multidot(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p, L.w.p,
-                      kry_vec(c, ln, xslot), kry_vec(c, ln, vslot),
-                      std::max<long long>(1, L.n0), K, L.kry_partial.p, L.d_prob_span_begin.p,
-                      np, c->active.p, c->kry_dots.p);
+      const double *x = xfield != kNoField ? kry_field(c, ln, xfield) : kry_vec(c, ln, xslot);
+      launch_multidot(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p, L.w.p, x,
+                      kry_vec(c, ln, vslot), std::max<long long>(1, L.n0), K, L.kry_partial.p,
+                      L.d_prob_span_begin.p, np, c->active.p, c->kry_dots.p, self_dot);
       prof_end(c, pi);
    }
-   out.resize((size_t)np * K);
-   CUDA_CHECK(cudaMemcpyAsync(out.data(), c->kry_dots.p, (size_t)np * K * sizeof(double),
+   out.resize((size_t)np * KT);
+   CUDA_CHECK(cudaMemcpyAsync(out.data(), c->kry_dots.p, (size_t)np * KT * sizeof(double),
                               cudaMemcpyDeviceToHost, c->stream));
    CUDA_CHECK(cudaStreamSynchronize(c->stream));
 }
 
-// V_x = a[p] V_x + sum_i coef[p*K+i] V_{vslot+i}
-// With norm: also norm[p] = <V_x, V_x> (weighted) of the result, the same
-// numbers as kry_dots(c, xslot, xslot, 1, norm) without rereading V_x.
+// V_x = a[p] X + sum_i coef[p*K+i] V_{vslot+i}, X = V_x or the field
+// xin_field; the result also goes to the field x2_field when one is given
+// (not with norm).  With norm: also norm[p] = <V_x, V_x> (weighted) of the
+// result, the same numbers as kry_dots(c, xslot, xslot, 1, norm) without
+// rereading V_x.
 void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot, int K,
-                 const std::vector<double> &coef, std::vector<double> *norm = nullptr)
+                 const std::vector<double> &coef, std::vector<double> *norm = nullptr,
+                 int xin_field = kNoField, int x2_field = kNoField)
 {
    OpTimer ot(c, "kry_combine", -1);
    const int np = nprob(c);
@@ -2617,18 +2640,20 @@ void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot,
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
       const int pi = prof_begin(c, 5, L.cells_prob, 8.0 * (K + (norm ? 3 : 2)));
+      const double *xin = xin_field != kNoField ? kry_field(c, ln, xin_field) : nullptr;
       if (norm)
          launch_combine_norm(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
                              kry_vec(c, ln, xslot), c->kry_a.p,
                              K > 0 ? kry_vec(c, ln, vslot) : nullptr,
                              std::max<long long>(1, L.n0), K, c->kry_coef.p, L.w.p,
                              L.kry_partial.p, L.d_prob_span_begin.p, np, c->active.p,
-                             c->kry_dots.p);
+                             c->kry_dots.p, xin);
       else
          launch_combine(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
                         kry_vec(c, ln, xslot), c->kry_a.p,
                         K > 0 ? kry_vec(c, ln, vslot) : nullptr, std::max<long long>(1, L.n0),
-                        K, c->kry_coef.p);
+                        K, c->kry_coef.p, xin,
+                        x2_field != kNoField ? kry_field(c, ln, x2_field) : nullptr);
       prof_end(c, pi);
    }
    if (norm) {
@@ -2753,12 +2778,6 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
       c->host_active = act;
       // V_0 = r / beta
       std::vector<int> cyc = act;
-      for (int ln = 0; ln < c->nlev; ++ln) {
-         LevelState &L = c->L[ln];
-         CUDA_CHECK(cudaMemcpyAsync(kry_vec(c, ln, 0), L.r.p,
-                                    std::max<long long>(1, L.n0) * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, c->stream));
-      }
       std::fill(g.begin(), g.end(), 0.0);
       std::fill(h.begin(), h.end(), 0.0);
       for (int p = 0; p < np; ++p) {
@@ -2767,18 +2786,13 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
          a[p] = cyc[p] && beta > 0 ? 1.0 / beta : 0.0;
          kp[p] = 0;
       }
-      kry_combine(c, 0, a, 0, 0, coef);
+      // V_0 = R / beta, also back into R, the preconditioner's input
+      kry_combine(c, 0, a, 0, 0, coef, nullptr, FAC_R, FAC_R);
       for (int j = 0; j < m; ++j) {
          bool live = false;
          for (int v : act) live = live || v;
          if (!live) break;
-         // Z_j = M^-1 V_j: one FAC cycle on the residual V_j
-         for (int ln = 0; ln < c->nlev; ++ln) {
-            LevelState &L = c->L[ln];
-            CUDA_CHECK(cudaMemcpyAsync(L.r.p, kry_vec(c, ln, j),
-                                       std::max<long long>(1, L.n0) * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, c->stream));
-         }
+         // Z_j = M^-1 V_j: one FAC cycle on the residual V_j (R holds V_j)
          {
             OpTimer ot(c, "kry_precondition", -1);
             run_graph(c, c->prec_exec, c->prec_launches, prec_body);
@@ -2805,16 +2819,11 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             OpTimer ot(c, "kry_apply", -1);
             run_graph(c, c->apply_exec, c->apply_launches, apply_body);
          }
-         for (int ln = 0; ln < c->nlev; ++ln) {
-            LevelState &L = c->L[ln];
-            CUDA_CHECK(cudaMemcpyAsync(kry_vec(c, ln, j + 1), L.tr.p,
-                                       std::max<long long>(1, L.n0) * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, c->stream));
-         }
-         // classical Gram-Schmidt, W = -TR - sum h_i V_i, repeated once for
-         // the problems whose W lost more than half its norm (cancellation)
+         // classical Gram-Schmidt, W = -TR - sum h_i V_i into slot j + 1,
+         // repeated once for the problems whose W lost more than half its
+         // norm (cancellation)
          const int K = j + 1;
-         kry_dots(c, j + 1, 0, K + 1, dots);  // <TR, V_i>, i <= j, and <TR, TR>
+         kry_dots(c, 0, 0, K, dots, FAC_TR, true);  // <TR, V_i>, i <= j, and <TR, TR>
          std::vector<double> before(np, 0.0);
          coef.assign((size_t)np * K, 0.0);
          for (int p = 0; p < np; ++p) {
@@ -2826,7 +2835,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                coef[(size_t)p * K + i] = -hi;
             }
          }
-         kry_combine(c, j + 1, a, 0, K, coef, &dots);  // and ||W||^2
+         kry_combine(c, j + 1, a, 0, K, coef, &dots, FAC_TR);  // and ||W||^2
          bool again = false;
          std::vector<int> reo(np, 0);
          for (int p = 0; p < np; ++p)
@@ -2874,7 +2883,8 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             c->hist[p].push_back(est);
             if (!(est > eff[p]) || its[p] >= c->max_cycles || !(hn > 0)) act[p] = 0;
          }
-         kry_combine(c, j + 1, a, 0, 0, coef);  // V_{j+1} = W / ||W||
+         // V_{j+1} = W / ||W||, also into R for the next preconditioning
+         kry_combine(c, j + 1, a, 0, 0, coef, nullptr, kNoField, FAC_R);
          set_active(c, act);
          c->host_active = act;
       }
@@ -2970,6 +2980,181 @@ extern "C" {
 
 const char *fac_last_error(void) { return g_last_error.c_str(); }
 
+namespace {
+
+// The problem with k domain-covering levels below its level 0, each
+// coarsening the domain by 2 (one patch each): every cell of an added level
+// is covered by the next finer level, so the composite problem, its weights
+// and its residual norm are unchanged and the FAC cycle becomes a full
+// multigrid V-cycle whose coarsest solve is cheap (the reference reaches the
+// same end with its hypre coarse solver, CellPoissonFACOps.C:1741-1781).
+HostProblem extend_problem(const HostProblem &P, int k, int dim)
+{
+   if (P.nlev + k > kMaxLevels) throw FacError(FAC_ERR_ARG, "too many levels with the extension");
+   long long domain = 1, covered = 0;
+   for (int a = 0; a < dim; ++a) {
+      if (P.n0[a] % (1 << k) != 0)
+         throw FacError(FAC_ERR_ARG, "level 0 not divisible by 2^levels for the extension");
+      domain *= P.n0[a];
+   }
+   for (const Box &b : P.boxes[0]) covered += b.size();
+   if (covered != domain)
+      throw FacError(FAC_ERR_ARG, "the extension needs a level 0 that covers the domain");
+   HostProblem E;
+   for (int a = 0; a < 3; ++a) {
+      E.n0[a] = a < dim ? P.n0[a] >> k : 1;
+      E.xlo[a] = P.xlo[a];
+      E.xup[a] = P.xup[a];
+   }
+   E.nlev = P.nlev + k;
+   for (int j = k; j >= 1; --j) {
+      const int ln = k - j;
+      Box b;
+      for (int a = 0; a < 3; ++a) {
+         b.lo[a] = 0;
+         b.hi[a] = a < dim ? (P.n0[a] >> j) - 1 : 0;
+         E.ratio[ln][a] = (ln == 0 || a >= dim) ? 1 : 2;
+      }
+      E.boxes[ln].push_back(b);
+   }
+   for (int ln = 0; ln < P.nlev; ++ln) {
+      for (int a = 0; a < 3; ++a)
+         E.ratio[ln + k][a] = ln == 0 ? (a < dim ? 2 : 1) : P.ratio[ln][a];
+      E.boxes[ln + k] = P.boxes[ln];
+   }
+   return E;
+}
+
+// D on the added levels from D of the caller's level 0 (level k): on each
+// coarse face the mean of the 2^(dim-1) fine faces it covers, averaged in
+// pairs along the tangential axes in increasing order; f, u and C there
+// are zero (covered cells).  Host side, once per change of D.
+void extend_coefficients(fac_ctx *c)
+{
+   const int k = c->ext_levels, dim = c->dim;
+   for (int ln = 0; ln < k; ++ln) {
+      LevelState &L = c->L[ln];
+      CUDA_CHECK(cudaMemsetAsync(L.f.p, 0, L.f.n * sizeof(double), c->stream));
+      CUDA_CHECK(cudaMemsetAsync(L.u.p, 0, L.u.n * sizeof(double), c->stream));
+      if (c->spec.c_kind == 2)
+         CUDA_CHECK(cudaMemsetAsync(L.c.p, 0, L.c.n * sizeof(double), c->stream));
+   }
+   if (c->spec.d_variable) {
+      const LevelState &L0 = c->L[k];
+      for (int p = 0; p < nprob(c); ++p) {
+         const HostProblem &P = c->probs[p];
+         // dense per-axis face arrays of the caller's level 0 (patches in
+         // order; a face two patches share takes the later patch's value)
+         int n[3];
+         for (int a = 0; a < 3; ++a) n[a] = a < dim ? P.n0[a] << k : 1;
+         std::vector<double> fine(L0.prob_offs[p + 1] - L0.prob_offs[p]);
+         CUDA_CHECK(cudaMemcpyAsync(fine.data(), L0.d.p + L0.prob_offs[p],
+                                    fine.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+         CUDA_CHECK(cudaStreamSynchronize(c->stream));
+         std::vector<std::vector<double> > dense(dim);
+         int ext[3][3];
+         for (int a = 0; a < dim; ++a) {
+            for (int q = 0; q < 3; ++q) ext[a][q] = n[q] + (q == a ? 1 : 0);
+            dense[a].assign((size_t)ext[a][0] * ext[a][1] * ext[a][2], 0.0);
+         }
+         size_t off = 0;
+         for (const Box &b : P.boxes[k]) {
+            for (int a = 0; a < dim; ++a) {
+               const Box sb = side_box(b, a);
+               for (int z = sb.lo[2]; z <= sb.hi[2]; ++z)
+                  for (int y = sb.lo[1]; y <= sb.hi[1]; ++y)
+                     for (int x = sb.lo[0]; x <= sb.hi[0]; ++x)
+                        dense[a][((size_t)z * ext[a][1] + y) * ext[a][0] + x] = fine[off++];
+            }
+         }
+         for (int ln = k - 1; ln >= 0; --ln) {
+            for (int q = 0; q < 3; ++q) n[q] = q < dim ? n[q] / 2 : 1;
+            std::vector<std::vector<double> > coarse(dim);
+            for (int a = 0; a < dim; ++a) {
+               int ce[3];
+               for (int q = 0; q < 3; ++q) ce[q] = n[q] + (q == a ? 1 : 0);
+               // every other face along the normal, then pair means along
+               // each tangential axis in turn
+               std::vector<double> t = dense[a];
+               int te[3] = {ext[a][0], ext[a][1], ext[a][2]};
+               auto take = [&](int ax) {
+                  int ne[3] = {te[0], te[1], te[2]};
+                  const bool normal = ax == a;
+                  ne[ax] = normal ? (te[ax] + 1) / 2 : te[ax] / 2;
+                  std::vector<double> o((size_t)ne[0] * ne[1] * ne[2]);
+                  for (int z = 0; z < ne[2]; ++z)
+                     for (int y = 0; y < ne[1]; ++y)
+                        for (int x = 0; x < ne[0]; ++x) {
+                           int i0[3] = {x, y, z};
+                           int i1[3] = {x, y, z};
+                           i0[ax] *= 2;
+                           i1[ax] = i0[ax] + 1;
+                           const double v0 =
+                              t[((size_t)i0[2] * te[1] + i0[1]) * te[0] + i0[0]];
+                           o[((size_t)z * ne[1] + y) * ne[0] + x] =
+                              normal ? v0
+                                     : 0.5 * (v0 + t[((size_t)i1[2] * te[1] + i1[1]) * te[0] +
+                                                     i1[0]]);
+                        }
+                  t.swap(o);
+                  for (int q = 0; q < 3; ++q) te[q] = ne[q];
+               };
+               take(a);
+               for (int tt = 0; tt < dim; ++tt)
+                  if (tt != a) take(tt);
+               for (int q = 0; q < 3; ++q)
+                  if (te[q] != ce[q]) throw FacError(FAC_ERR_STATE, "extension face count");
+               coarse[a].swap(t);
+               for (int q = 0; q < 3; ++q) ext[a][q] = ce[q];
+            }
+            dense.swap(coarse);
+            // the added level is one patch over the domain: its side arrays
+            // per axis are the dense arrays
+            const LevelState &L = c->L[ln];
+            long long o = L.prob_offs[p];
+            for (int a = 0; a < dim; ++a) {
+               if (o + (long long)dense[a].size() > L.prob_offs[p + 1])
+                  throw FacError(FAC_ERR_STATE, "extension side layout");
+               CUDA_CHECK(cudaMemcpyAsync(L.d.p + o, dense[a].data(),
+                                          dense[a].size() * sizeof(double),
+                                          cudaMemcpyHostToDevice, c->stream));
+               o += (long long)dense[a].size();
+            }
+            CUDA_CHECK(cudaStreamSynchronize(c->stream));
+         }
+      }
+   }
+   c->ext_dirty = false;
+}
+
+void ensure_extension(fac_ctx *c)
+{
+   if (c->ext_levels > 0 && c->ext_dirty) extend_coefficients(c);
+}
+
+}  // namespace
+
+int fac_set_coarse_extension(fac_ctx *ctx, int levels)
+{
+   return guarded([&] {
+      check_state(ctx, false);
+      if (!ctx->probs.empty())
+         throw FacError(FAC_ERR_STATE, "set the extension before adding problems");
+      if (levels < 0 || levels > kMaxLevels - 1) throw FacError(FAC_ERR_ARG, "bad level count");
+      ctx->ext_levels = levels;
+   });
+}
+
+int fac_extend_coefficients(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      ctx->ext_dirty = true;
+      ensure_extension(ctx);
+   });
+}
+
 int fac_ctx_create(fac_ctx **ctx, int dim, int device)
 {
    return guarded([&] {
@@ -3054,6 +3239,7 @@ int fac_add_problem(fac_ctx *ctx, const int *n0, const double *xlo, const double
             P.boxes[ln].push_back(b);
          }
       }
+      if (ctx->ext_levels > 0) P = extend_problem(P, ctx->ext_levels, dim);
       ctx->probs.push_back(P);
       if (problem) *problem = (int)ctx->probs.size() - 1;
    });
@@ -3305,6 +3491,7 @@ int fac_initialize(fac_ctx *ctx)
    return guarded([&] {
       check_state(ctx, false);
       initialize(ctx);
+      ctx->ext_dirty = ctx->ext_levels > 0;
    });
 }
 
@@ -3346,6 +3533,7 @@ int fac_upload_field(fac_ctx *ctx, int fid, int problem, int ln, const double *h
       check_pl(ctx, problem, ln);
       if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
       if (fid == FAC_C && ctx->spec.c_kind != 2) throw FacError(FAC_ERR_ARG, "C is not variable");
+      if (fid == FAC_C && ln == ctx->ext_levels) ctx->ext_dirty = true;
       long long off;
       const size_t n = field_slice(ctx, fid, problem, ln, off);
       CUDA_CHECK(cudaMemcpyAsync(field_ptr(ctx->L[ln], fid) + off, host, n * sizeof(double),
@@ -3374,6 +3562,7 @@ int fac_upload_side(fac_ctx *ctx, int problem, int ln, const double *host)
       check_ops(ctx);
       check_pl(ctx, problem, ln);
       if (!ctx->spec.d_variable) throw FacError(FAC_ERR_ARG, "D is not variable");
+      if (ln == ctx->ext_levels) ctx->ext_dirty = true;
       if (!host) throw FacError(FAC_ERR_ARG, "null host pointer");
       const LevelState &L = ctx->L[ln];
       const long long off = L.prob_offs[problem], n = L.prob_offs[problem + 1] - off;
@@ -3557,6 +3746,7 @@ int fac_solve(fac_ctx *ctx, int *converged, int *iterations, double *residual)
 {
    return guarded([&] {
       check_ops(ctx);
+      ensure_extension(ctx);
       solve(ctx, converged, iterations, residual);
    });
 }
@@ -3574,6 +3764,7 @@ int fac_solve_fgmres(fac_ctx *ctx, int restart, int *converged, int *iterations,
 {
    return guarded([&] {
       check_ops(ctx);
+      ensure_extension(ctx);
       fgmres_solve(ctx, restart, converged, iterations, residual);
    });
 }
@@ -3584,10 +3775,17 @@ int fac_solve_host(fac_ctx *ctx, const double *const *f_host, const double *cons
    return guarded([&] {
       check_ops(ctx);
       if (!f_host || !u_host) throw FacError(FAC_ERR_ARG, "null host array table");
+      ensure_extension(ctx);
       const int np = nprob(ctx);
+      // the tables hold the caller's levels; the added coarser ones keep
+      // their zero f and start from a zero u
+      const int lx = ctx->ext_levels, nl = ctx->nlev - lx;
+      for (int ln = 0; ln < lx; ++ln)
+         CUDA_CHECK(cudaMemsetAsync(ctx->L[ln].u.p, 0, ctx->L[ln].u.n * sizeof(double),
+                                    ctx->stream));
       for (int p = 0; p < np; ++p)
-         for (int ln = 0; ln < ctx->nlev; ++ln) {
-            const int k = p * ctx->nlev + ln;
+         for (int ln = lx; ln < ctx->nlev; ++ln) {
+            const int k = p * nl + ln - lx;
             long long off;
             size_t n = field_slice(ctx, FAC_F, p, ln, off);
             CUDA_CHECK(cudaMemcpyAsync(ctx->L[ln].f.p + off, f_host[k], n * sizeof(double),
@@ -3602,8 +3800,8 @@ int fac_solve_host(fac_ctx *ctx, const double *const *f_host, const double *cons
          }
       solve(ctx, converged, iterations, residual);
       for (int p = 0; p < np; ++p)
-         for (int ln = 0; ln < ctx->nlev; ++ln) {
-            const int k = p * ctx->nlev + ln;
+         for (int ln = lx; ln < ctx->nlev; ++ln) {
+            const int k = p * nl + ln - lx;
             long long off;
             const size_t n = field_slice(ctx, FAC_U, p, ln, off);
             CUDA_CHECK(cudaMemcpyAsync(u_host[k], ctx->L[ln].u.p + off, n * sizeof(double),

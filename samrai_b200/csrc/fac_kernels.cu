@@ -1348,26 +1348,32 @@ constexpr int kVecBlock = 8;
 // of one problem's cells {problem, first cell, cells, chunk index}: one pass
 // over the cells reads w and x once per kVecBlock vectors; each sum
 // accumulates thread-strided cells, then a warp tree, then warps in order.
+// With SELF, entry K is <x, x>: x taken as one more vector after the K.
+template <bool SELF>
 __global__ void __launch_bounds__(kThreads)
 k_multidot(const Chunk *__restrict__ chunks, int nwork, const double *__restrict__ w,
            const double *__restrict__ x, const double *__restrict__ V, long long vstride, int K,
            double *__restrict__ partial)
 {
    __shared__ double red[kVecBlock][kThreads / 32];
+   const int KT = K + (SELF ? 1 : 0);
    WORK_LOOP(ch) {
       const long long c0 = ch.begin;
-      for (int i0 = 0; i0 < K; i0 += kVecBlock) {
-         const int nb = K - i0 < kVecBlock ? K - i0 : kVecBlock;
+      for (int i0 = 0; i0 < KT; i0 += kVecBlock) {
+         const int nb = KT - i0 < kVecBlock ? KT - i0 : kVecBlock;
          const double *vb = V + (long long)i0 * vstride;
          double sum[kVecBlock];
 #pragma unroll
          for (int q = 0; q < kVecBlock; ++q) sum[q] = 0.0;
          for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
             const long long c = c0 + t;
-            const double wx = w[c] * x[c];
+            const double xc = x[c];
+            const double wx = w[c] * xc;
             double v[kVecBlock];
 #pragma unroll
-            for (int q = 0; q < kVecBlock; ++q) v[q] = q < nb ? vb[(long long)q * vstride + c] : 0.0;
+            for (int q = 0; q < kVecBlock; ++q)
+               v[q] = i0 + q < K ? vb[(long long)q * vstride + c]
+                                 : (SELF && i0 + q == K ? xc : 0.0);
 #pragma unroll
             for (int q = 0; q < kVecBlock; ++q) sum[q] += wx * v[q];
          }
@@ -1381,7 +1387,7 @@ k_multidot(const Chunk *__restrict__ chunks, int nwork, const double *__restrict
          if ((int)threadIdx.x < nb) {
             double b = 0.0;
             for (int r = 0; r < (int)(blockDim.x >> 5); ++r) b += red[threadIdx.x][r];
-            partial[(long long)ch.aux * K + i0 + threadIdx.x] = b;
+            partial[(long long)ch.aux * KT + i0 + threadIdx.x] = b;
          }
          __syncthreads();
       }
@@ -1414,13 +1420,18 @@ __global__ void k_multidot_reduce(const double *__restrict__ partial,
 // of the new x, accumulated exactly as k_multidot accumulates <x, x> (the
 // same cells per thread in the same order, the same warp tree, warps in
 // order), so the pass that would reread x for its norm is saved.
+// The old x is read from xin (x itself when xin is null) and the new one
+// is also written to x2 when that is not null, so a copy before or after
+// the combination needs no pass of its own; xin and x2 may be the same
+// array (each element is read before it is written, by the same thread).
 template <bool NORM>
 __global__ void __launch_bounds__(kThreads)
-k_combine(const Chunk *__restrict__ chunks, int nwork, double *__restrict__ x,
-          const double *__restrict__ a, const double *__restrict__ V, long long vstride, int K,
-          const double *__restrict__ coef, const double *__restrict__ w,
-          double *__restrict__ partial)
+k_combine(const Chunk *__restrict__ chunks, int nwork, double *x, const double *xin,
+          double *x2, const double *__restrict__ a, const double *__restrict__ V,
+          long long vstride, int K, const double *__restrict__ coef,
+          const double *__restrict__ w, double *__restrict__ partial)
 {
+   if (!xin) xin = x;
    __shared__ double red[NORM ? kThreads / 32 : 1];
    WORK_LOOP(ch) {
       const double ap = a[ch.patch];
@@ -1430,7 +1441,7 @@ k_combine(const Chunk *__restrict__ chunks, int nwork, double *__restrict__ x,
 #pragma unroll 4
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const long long c = (long long)ch.begin + t;
-         double v = ap * x[c];
+         double v = ap * xin[c];
          for (int i0 = 0; i0 < K; i0 += kVecBlock) {
             const double *vb = V + (long long)i0 * vstride + c;
             double vv[kVecBlock];
@@ -1441,6 +1452,7 @@ k_combine(const Chunk *__restrict__ chunks, int nwork, double *__restrict__ x,
                if (i0 + q < K) v = v + cp[i0 + q] * vv[q];
          }
          x[c] = v;
+         if (x2) x2[c] = v;
          if (NORM) {
             const double wx = w[c] * v;
             sum += wx * v;
@@ -1554,37 +1566,44 @@ void add_kernel_launches(long long n) { g_launches += n; }
 void launch_multidot(cudaStream_t s, int nchunks, const Chunk *chunks, const double *w,
                      const double *x, const double *V, long long vstride, int K,
                      double *partial, const int *prob_chunk_begin, int nprob, const int *active,
-                     double *out)
+                     double *out, bool self_dot)
 {
-   if (K <= 0) return;
+   const int KT = K + (self_dot ? 1 : 0);
+   if (KT <= 0) return;
    if (nchunks > 0) {
       g_launches.fetch_add(1, std::memory_order_relaxed);
-      k_multidot<<<work_grid(k_multidot, nchunks), kThreads, 0, s>>>(chunks, nchunks, w, x, V,
-                                                                     vstride, K, partial);
+      if (self_dot)
+         k_multidot<true><<<work_grid(k_multidot<true>, nchunks), kThreads, 0, s>>>(
+            chunks, nchunks, w, x, V, vstride, K, partial);
+      else
+         k_multidot<false><<<work_grid(k_multidot<false>, nchunks), kThreads, 0, s>>>(
+            chunks, nchunks, w, x, V, vstride, K, partial);
    }
    g_launches.fetch_add(1, std::memory_order_relaxed);
-   k_multidot_reduce<<<dim3(nprob, K), kThreads, 0, s>>>(partial, prob_chunk_begin, K, active,
-                                                         out);
+   k_multidot_reduce<<<dim3(nprob, KT), kThreads, 0, s>>>(partial, prob_chunk_begin, KT, active,
+                                                          out);
 }
 
 void launch_combine(cudaStream_t s, int nchunks, const Chunk *chunks, double *x, const double *a,
-                    const double *V, long long vstride, int K, const double *coef)
+                    const double *V, long long vstride, int K, const double *coef,
+                    const double *xin, double *x2)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    k_combine<false><<<work_grid(k_combine<false>, nchunks), kThreads, 0, s>>>(
-      chunks, nchunks, x, a, V, vstride, K, coef, nullptr, nullptr);
+      chunks, nchunks, x, xin, x2, a, V, vstride, K, coef, nullptr, nullptr);
 }
 
 void launch_combine_norm(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
                          const double *a, const double *V, long long vstride, int K,
                          const double *coef, const double *w, double *partial,
-                         const int *prob_chunk_begin, int nprob, const int *active, double *out)
+                         const int *prob_chunk_begin, int nprob, const int *active, double *out,
+                         const double *xin)
 {
    if (nchunks > 0) {
       g_launches.fetch_add(1, std::memory_order_relaxed);
       k_combine<true><<<work_grid(k_combine<true>, nchunks), kThreads, 0, s>>>(
-         chunks, nchunks, x, a, V, vstride, K, coef, w, partial);
+         chunks, nchunks, x, xin, nullptr, a, V, vstride, K, coef, w, partial);
    }
    g_launches.fetch_add(1, std::memory_order_relaxed);
    k_multidot_reduce<<<dim3(nprob, 1), kThreads, 0, s>>>(partial, prob_chunk_begin, 1, active,

@@ -32,20 +32,24 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
 // vector every vstride elements; per-problem coefficients; chunks are runs
 // of one problem's cells {problem, first cell, cells, chunk index} (partial
 // is nchunks x K).
-// out[p*K+i] += sum_w x V_i over problem p's chunks of this level.
+// out[p*KT+i] += sum_w x V_i over problem p's chunks of this level, KT = K
+// (+1 with self_dot: entry K is <x, x>, the same sum as taking x as V_K).
 void launch_multidot(cudaStream_t s, int nchunks, const Chunk *chunks, const double *w,
                      const double *x, const double *V, long long vstride, int K,
                      double *partial, const int *prob_chunk_begin, int nprob, const int *active,
-                     double *out);
-// x = a[p] x + sum_i coef[p*K+i] V_i
+                     double *out, bool self_dot = false);
+// x = a[p] xin + sum_i coef[p*K+i] V_i (xin null: x itself), also written
+// to x2 when it is not null
 void launch_combine(cudaStream_t s, int nchunks, const Chunk *chunks, double *x, const double *a,
-                    const double *V, long long vstride, int K, const double *coef);
-// The same, and out[p] += <x, x> (weighted, the new x) over problem p's
-// chunks of this level, equal to launch_multidot(x, x, K = 1).
+                    const double *V, long long vstride, int K, const double *coef,
+                    const double *xin = nullptr, double *x2 = nullptr);
+// The same (without x2), and out[p] += <x, x> (weighted, the new x) over
+// problem p's chunks of this level, equal to launch_multidot(x, x, K = 1).
 void launch_combine_norm(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
                          const double *a, const double *V, long long vstride, int K,
                          const double *coef, const double *w, double *partial,
-                         const int *prob_chunk_begin, int nprob, const int *active, double *out);
+                         const int *prob_chunk_begin, int nprob, const int *active, double *out,
+                         const double *xin = nullptr);
 // dst (ghost-0) = interior of src (ghost-1), converted to FP64
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,

@@ -57,6 +57,8 @@ def load_library(build_if_missing=True):
         "fac_ctx_create": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int]),
         "fac_ctx_destroy": (ctypes.c_int, [vp]),
         "fac_add_problem": (ctypes.c_int, [vp, ip, dp, dp, ctypes.c_int, ip, ip, ip, ip]),
+        "fac_set_coarse_extension": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_extend_coefficients": (ctypes.c_int, [vp]),
         "fac_set_poisson": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double]),
         "fac_set_bc": (ctypes.c_int, [vp, dp, dp, dp]),
@@ -157,14 +159,17 @@ class FacContext:
     """A batch of FAC problems on one GPU (device=-1: host-only table check)."""
 
     def __init__(self, problems: Sequence, params: Optional[dict] = None, device: int = 0,
-                 bc=None, precision: str = "fp64"):
+                 bc=None, precision: str = "fp64", coarse_extension: int = 0):
         L = load_library()
         problems = list(problems)
         if not problems:
             raise ValueError("no problems")
         self.problems = problems
         self.dim = problems[0].dim
-        self.nlev = problems[0].nlev
+        # fac_set_coarse_extension: the library adds this many coarser
+        # levels; level numbers below count them
+        self.ext = int(coarse_extension)
+        self.nlev = problems[0].nlev + self.ext
         self.device = device
         self.stage_depth = 2
         h = ctypes.c_void_p()
@@ -185,6 +190,8 @@ class FacContext:
                                 prm["relative_residual_tol"], prm["pre_sweeps"],
                                 prm["post_sweeps"], prm["coarse_tol"], prm["coarse_max_it"],
                                 prm["ewing"]))
+        if self.ext:
+            _check(L.fac_set_coarse_extension(h, self.ext))
         for prob in problems:
             n0 = np.array(prob.n0, dtype=np.int32)
             xlo = np.array(prob.xlo, dtype=np.float64)
@@ -203,15 +210,16 @@ class FacContext:
         _check(L.fac_initialize(h))
         if device >= 0:
             for ip_, prob in enumerate(problems):
-                for ln in range(self.nlev):
+                for pl in range(prob.nlev):
+                    ln = pl + self.ext
                     if prob.f:
-                        self.upload(F, ip_, ln, prob.f[ln])
+                        self.upload(F, ip_, ln, prob.f[pl])
                     if prob.u0:
-                        self.upload(U, ip_, ln, prob.u0[ln])
+                        self.upload(U, ip_, ln, prob.u0[pl])
                     if prob.d_variable:
-                        self.upload_side(ip_, ln, prob.d[ln])
+                        self.upload_side(ip_, ln, prob.d[pl])
                     if prob.c_kind == 2:
-                        self.upload(C, ip_, ln, prob.c[ln])
+                        self.upload(C, ip_, ln, prob.c[pl])
 
     def close(self):
         if getattr(self, "h", None):

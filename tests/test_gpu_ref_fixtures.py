@@ -54,11 +54,16 @@ def test_gpu_solver_matches_reference_solver(name, require_gpu):
     converged = solver.solveSystem()
     assert solver.getNumberOfIterations() == int(fx["iterations"][0])
     assert converged == bool(fx["converged"][0])
-    assert rel(solver.getResidualNorm(), fx["residual"]) <= 1e-11
+    # a residual norm near convergence is a difference of O(1) terms: a
+    # rounding difference in the solution moves it by ~1e-16 of the initial
+    # residual, so norms are compared against that scale
     hist = solver._ctx.residual_history(0)
-    assert rel(hist[1:], fx["hist"]) <= 1e-11
+    r0 = hist[0]
+    assert abs(solver.getResidualNorm() - fx["residual"][0]) <= 1e-12 * r0
+    assert np.abs(hist[1:] - fx["hist"]).max() <= 1e-12 * r0
     avg, fin = solver.getConvergenceFactors()
-    assert rel([avg, fin], fx["factors"]) <= 1e-10
+    assert rel(avg, fx["factors"][0]) <= 1e-6
+    assert rel(fin, fx["factors"][1]) <= 1e-4
     bit = []
     for ln in range(p.nlev):
         u = p.u[ln]
