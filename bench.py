@@ -9,9 +9,10 @@ host buffers with the copies inside the timed region for ``e2e``).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config c5|c2|c1|c3] [--nprob P]
 
-Multi-GPU (torchrun, one rank per GPU): the independent problems are
-sharded, each rank solving its own batch of the same size (weak scaling, no
-data-path collective); the step time is the maximum over ranks.
+Multi-GPU (torchrun, one rank per GPU): nprob x N independent problems are
+spread over the ranks by samrai_b200.parallel.partition (cell-balanced, about
+nprob per rank: weak scaling, no data-path collective); the step time is the
+maximum over ranks.
 
 ``--impl reference`` times the reference's own FAC solver on all host cores:
 its C++ built from its sources with its Fortran kernels translated to C
@@ -68,15 +69,22 @@ def workload_desc(name, nprob):
             "c1": "config1: 2-D sine, 64^2 coarse + 64^2 fine box"}[name]
 
 
-def workload_seeds(name, nprob, rank):
-    """Seeds of this rank's problems (config 5: a disjoint block per rank)."""
-    return list(range(rank * nprob, (rank + 1) * nprob)) if name == "c5" else [rank]
+def workload_seeds(name, nprob, rank, world=1):
+    """Seeds of this rank's problems.  Config 5: nprob x world problems
+    (weak scaling: nprob per GPU) spread over the ranks by
+    parallel.partition, longest first by coarse cells."""
+    if name != "c5":
+        return [rank]
+    from samrai_b200 import configs, parallel
+    seeds = list(range(nprob * world))
+    return [seeds[i] for i in parallel.shard([configs.config5_cost(x) for x in seeds], rank,
+                                             world)]
 
 
-def make_workload(name, nprob, rank):
+def make_workload(name, nprob, rank, world=1):
     from samrai_b200 import configs
     if name == "c5":
-        probs = configs.config5(nprob, first_seed=rank * nprob)
+        probs = configs.config5(seeds=workload_seeds(name, nprob, rank, world))
     else:
         probs = [_make_problem(name, rank)]
     return probs, workload_desc(name, nprob)
@@ -379,7 +387,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
 
     from samrai_b200 import configs, fac
-    probs, desc = make_workload(args.config, args.nprob, rank)
+    probs, desc = make_workload(args.config, args.nprob, rank, world)
     mg = [configs.extend_hierarchy(p, k=MG_LEVELS[args.config]) for p in probs]
     ctx = fac.FacContext(mg, params=PARAMS_MG, device=local_rank, precision=args.precision)
     ctx.set_krylov(args.krylov)
@@ -545,7 +553,7 @@ def main():
                 den += float(np.sum(b ** 2))
             diffs.append(math.sqrt(num / max(den, 1e-300)))
         if args.plain_cycles_out and rank == 0:
-            seeds = workload_seeds(args.config, len(probs), rank)
+            seeds = workload_seeds(args.config, args.nprob, rank, world)
             with open(args.plain_cycles_out, "w") as fh:
                 json.dump({"what": "plain FAC cycles to a 1e-10 relative composite residual "
                                    "(max_cycles 100, 500-sweep coarsest solve) per seed",
@@ -624,7 +632,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the reference arm's estimate on a bounded sample: one round of one
         # problem per core (unsampled problems scaled by their cells)
-        seeds = workload_seeds(args.config, len(probs), 0)
+        seeds = workload_seeds(args.config, args.nprob, 0)
         ref = CpuReference(args.config, seeds)
         wall = ref.round()
         ms_est, info = ref.estimate(cells={x: p.num_cells() for x, p in zip(seeds, probs)})

@@ -107,7 +107,9 @@ int fac_set_poisson(fac_ctx *ctx, int d_variable, double d_const,
 
 /* Robin boundary coefficients a u + b du/dn = g per location index
  * 0..2*dim-1 (solv/RobinBcCoefStrategy.h; Dirichlet a=1,b=0 as
- * SimpleCellRobinBcCoefs::setBcCoefs, SimpleCellRobinBcCoefs.C:283-290). */
+ * SimpleCellRobinBcCoefs::setBcCoefs, SimpleCellRobinBcCoefs.C:283-290).
+ * May be called again after fac_initialize; later operations use the new
+ * coefficients. */
 int fac_set_bc(fac_ctx *ctx, const double *a, const double *b,
                const double *g);
 
@@ -224,6 +226,17 @@ int fac_download_oside(fac_ctx *ctx, int problem, int ln, double *host);
  * (CellPoissonFACOps.C:2861-2900). */
 int fac_ghost_fill(fac_ctx *ctx, int fid, int ln, int with_coarse,
                    int homogeneous);
+/* The copies a ghost fill of level ln makes (the transactions of the
+ * reference's RefineSchedule, RefineSchedule.C:4821-4866, element by
+ * element), for splitting a hierarchy over ranks as tbox::Schedule splits
+ * transactions into local, send and receive sets (tbox/Schedule.C:98-175):
+ * element q copies into dst[q] (an index of the level's ghost-1 cell array)
+ * from src[q] >= 0 (the same level) or, with_coarse, from -src[q]-1 of the
+ * next coarser level's ghost-1 array (constant refine).  Physical-boundary
+ * ghost cells are not in the table (each patch fills its own).  cap = 0
+ * returns the count in *n only.  Works on host-only contexts. */
+int fac_fill_table(fac_ctx *ctx, int ln, int with_coarse, long long *dst,
+                   long long *src, size_t cap, size_t *n);
 /* smoothErrorByRedBlack (CellPoissonFACOps.C:1339-1514): nsweeps red-black
  * Gauss-Seidel sweeps of field fid_e against right-hand side fid_r; tol < 0
  * disables the convergence test.  sweeps (optional, one int per problem)
@@ -357,6 +370,25 @@ int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level);
  * patch scales (RMS of r) into the host array scale (may be NULL).  Uses
  * FAC_E of that level as scratch. */
 int fac_learned_samples(fac_ctx *ctx, int level, float *x, double *scale);
+
+/* ---- composite-vector operations (solv/SAMRAIVectorReal.C: dot :889,
+ *      RMSNorm :821, L2Norm, maxNorm, linearSum), for Krylov and nonlinear
+ *      solvers that call FAC as a preconditioner
+ *      (source/test/nonlinear/ModifiedBratuProblem.C:2283-2352).
+ * A vector is one cell field over every level of a problem; the inner
+ * products carry the control-volume weights FAC_W (zero under finer
+ * levels), as SAMRAIVectorReal's do when made with those weights.  Interior
+ * cells only; one result per problem, every problem of the context. */
+/* dots[p] = sum w x y */
+int fac_vec_dot(fac_ctx *ctx, int fid_x, int fid_y, double *dots);
+/* norms[p] = sqrt(sum w x^2) */
+int fac_vec_l2_norm(fac_ctx *ctx, int fid, double *norms);
+/* norms[p] = max |x| over cells with w > 0 */
+int fac_vec_max_norm(fac_ctx *ctx, int fid, double *norms);
+/* z = a[p] x + b[p] y (host arrays a, b of one scalar per problem; z may be
+ * x or y).  RMS norm: fac_rms_norm. */
+int fac_vec_linear_sum(fac_ctx *ctx, int fid_z, const double *a, int fid_x,
+                       const double *b, int fid_y);
 
 /* ---- allocation-free norm.  No counterpart in the reference.
  *

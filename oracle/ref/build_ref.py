@@ -18,7 +18,9 @@ the configure step and the compilers would:
    kernel files translated to C (f77c.py), compiled with gcc;
 4. abort() stubs for the Fortran symbols the compiled units reference but
    the FAC path never calls (complex data, other centerings);
-5. fac_ref_driver.C linked with all of it: oracle/_ref/fac_ref_driver.
+5. fac_ref_driver.C linked with all of it: oracle/_ref/fac_ref_driver;
+   and, when the CUDA library is built, the same driver on the drop-in
+   operators (samrai_b200/dropin): oracle/_ref/fac_dropin_driver.
 
 Nothing is copied from the reference into the repository: the generated
 files and objects live under oracle/_ref/, which git ignores.  Everything is
@@ -189,7 +191,31 @@ def main():
     exe = os.path.join(OUT, "fac_ref_driver")
     run(["g++", "-o", exe, drv_obj, *objs, kobj, sobj, "-lm"])
     print(f"build_ref: {exe}", flush=True)
+    dropin(inc, objs + [kobj, sobj])
     return 0
+
+
+def dropin(inc, objs):
+    """fac_dropin_driver: the driver with the reference's CellPoissonFACOps
+    replaced by samrai_b200's B200CellPoissonFACOps (compiled here against
+    the reference's headers), linked with the CUDA library; skipped when
+    that library is not built."""
+    root = os.path.dirname(os.path.dirname(HERE))
+    lib_dir = os.path.join(root, "samrai_b200", "_build")
+    if not os.path.exists(os.path.join(lib_dir, "libsamrai_fac_b200.so")):
+        print("build_ref: no CUDA library, fac_dropin_driver not built", flush=True)
+        return
+    src_dir = os.path.join(root, "samrai_b200", "dropin")
+    flags = [*CXXFLAGS, "-I" + inc, "-I" + src_dir, "-I" + os.path.join(root, "include")]
+    ops_obj = os.path.join(OUT, "obj", "B200CellPoissonFACOps.o")
+    run(["g++", *flags, "-c", os.path.join(src_dir, "B200CellPoissonFACOps.C"), "-o", ops_obj])
+    drv_obj = os.path.join(OUT, "obj", "fac_dropin_driver.o")
+    run(["g++", *flags, "-DWITH_B200_OPS", "-c", os.path.join(HERE, "fac_ref_driver.C"), "-o",
+         drv_obj])
+    exe = os.path.join(OUT, "fac_dropin_driver")
+    run(["g++", "-o", exe, drv_obj, ops_obj, *objs, "-L" + lib_dir, "-lsamrai_fac_b200",
+         "-Wl,-rpath,$ORIGIN/../../samrai_b200/_build", "-lm"])
+    print(f"build_ref: {exe}", flush=True)
 
 
 if __name__ == "__main__":

@@ -12,6 +12,11 @@
  *
  *    fac_ref_driver <in.bin> <out.bin>
  *
+ * Built with WITH_B200_OPS (fac_dropin_driver), the same solver runs the
+ * B200 library's operators through samrai_b200::B200CellPoissonFACOps in
+ * place of CellPoissonFACOps: the drop-in, checked against the reference's
+ * own results.
+ *
  * File format (both directions): records of
  *    int32 name length, name bytes, int32 type (0 = f64, 1 = i32),
  *    int64 count, count values.
@@ -62,6 +67,14 @@
 #include "SAMRAI/tbox/MemoryDatabase.h"
 #include "SAMRAI/tbox/SAMRAIManager.h"
 #include "SAMRAI/tbox/SAMRAI_MPI.h"
+
+#ifdef WITH_B200_OPS
+// the drop-in: SAMRAI's solver running the B200 library's operators
+#include "B200CellPoissonFACOps.h"
+typedef samrai_b200::B200CellPoissonFACOps BaseOps;
+#else
+typedef SAMRAI::solv::CellPoissonFACOps BaseOps;
+#endif
 
 using namespace SAMRAI;
 
@@ -148,18 +161,18 @@ private:
  * cycle: FACPreconditioner::solveSystem calls postprocessOneCycle after it
  * has stored the new norm (FACPreconditioner.C:425-436).
  */
-class RecordingOps : public solv::CellPoissonFACOps {
+class RecordingOps : public BaseOps {
 public:
    RecordingOps(const tbox::Dimension &dim, const std::string &name,
                 const std::shared_ptr<tbox::Database> &db)
-      : solv::CellPoissonFACOps(dim, name, db) {}
+      : BaseOps(dim, name, db) {}
 
    void setRecordingPreconditioner(const solv::FACPreconditioner *p) { d_pre = p; }
 
    void postprocessOneCycle(int it, const solv::SAMRAIVectorReal<double> &u,
                             const solv::SAMRAIVectorReal<double> &r) override
    {
-      solv::CellPoissonFACOps::postprocessOneCycle(it, u, r);
+      BaseOps::postprocessOneCycle(it, u, r);
       hist.push_back(d_pre->getResidualNorm());
    }
 

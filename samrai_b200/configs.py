@@ -453,10 +453,20 @@ def small_3d(seed=7, n0=32) -> Problem:
     return p
 
 
-def config5(nprob=64, first_seed=0, workers=None):
-    """64 independent 3-D variable-coefficient problems (seeds 0..63),
-    generated in parallel worker processes."""
-    seeds = list(range(first_seed, first_seed + nprob))
+def config5_cost(seed) -> int:
+    """Coarse cells of config-5 problem `seed` (its n0 draw, without building
+    the problem): the weight of the problem when problems are spread over
+    ranks."""
+    n0 = int(np.random.default_rng(10_000 + seed).integers(8, 17)) * 8
+    return n0 ** 3
+
+
+def config5(nprob=64, first_seed=0, workers=None, seeds=None):
+    """64 independent 3-D variable-coefficient problems (seeds 0..63, or the
+    given seeds), generated in parallel worker processes."""
+    if seeds is None:
+        seeds = list(range(first_seed, first_seed + nprob))
+    seeds = list(seeds)
     if workers is None:
         import os
         workers = min(len(seeds), os.cpu_count() or 1, 32)

@@ -407,6 +407,7 @@ struct fac_ctx {
    long long prec_launches = 0, apply_launches = 0;
    int kry_m = 0;
    DevArray<double> kry_dots, kry_coef, kry_a;
+   DevArray<double> vec_coef;  // per-problem scalars of fac_vec_linear_sum
    int krylov = 0;  // > 0: fac_solve runs FGMRES(krylov) around the FAC cycle
    // fac_set_coarse_extension: domain-covering coarser levels added below
    // every problem's level 0, and whether their coefficients need to be
@@ -3155,6 +3156,100 @@ int fac_extend_coefficients(fac_ctx *ctx)
    });
 }
 
+namespace {
+
+// Composite-vector operations act on every problem: lists compacted to
+// converged problems are restored first.
+void vec_all_active(fac_ctx *c)
+{
+   const int np = nprob(c);
+   bool all = (int)c->host_active.size() == np;
+   for (int v : c->host_active) all = all && v;
+   if (!all) {
+      c->host_active.assign(np, 1);
+      set_active(c, c->host_active);
+   }
+}
+
+std::vector<double2> vec_reduce(fac_ctx *c, int mode, int fid_x, int fid_y)
+{
+   vec_all_active(c);
+   const int np = nprob(c);
+   const int gx = field_ghost(fid_x), gy = field_ghost(fid_y);
+   CUDA_CHECK(cudaMemsetAsync(c->norm_acc.p, 0, np * sizeof(double2), c->stream));
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      launch_vec_reduce(c->stream, c->dim, mode, (int)L.cell_chunks.size(), L.d_patches.p,
+                        L.d_cell_chunks.p, field_ptr(L, fid_x), gx, field_ptr(L, fid_y), gy,
+                        L.w.p, L.norm_partial.p, L.d_prob_cell_chunk_begin.p, np,
+                        c->norm_acc.p);
+   }
+   CUDA_CHECK(cudaGetLastError());
+   std::vector<double2> acc(np);
+   CUDA_CHECK(cudaMemcpyAsync(acc.data(), c->norm_acc.p, np * sizeof(double2),
+                              cudaMemcpyDeviceToHost, c->stream));
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   return acc;
+}
+
+}  // namespace
+
+int fac_vec_dot(fac_ctx *ctx, int fid_x, int fid_y, double *dots)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!dots) throw FacError(FAC_ERR_ARG, "null output");
+      const std::vector<double2> acc = vec_reduce(ctx, 0, fid_x, fid_y);
+      for (int p = 0; p < nprob(ctx); ++p) dots[p] = acc[p].x;
+   });
+}
+
+int fac_vec_l2_norm(fac_ctx *ctx, int fid, double *norms)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!norms) throw FacError(FAC_ERR_ARG, "null output");
+      const std::vector<double2> acc = vec_reduce(ctx, 0, fid, fid);
+      for (int p = 0; p < nprob(ctx); ++p) norms[p] = std::sqrt(acc[p].x);
+   });
+}
+
+int fac_vec_max_norm(fac_ctx *ctx, int fid, double *norms)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!norms) throw FacError(FAC_ERR_ARG, "null output");
+      const std::vector<double2> acc = vec_reduce(ctx, 1, fid, fid);
+      for (int p = 0; p < nprob(ctx); ++p) norms[p] = acc[p].x;
+   });
+}
+
+int fac_vec_linear_sum(fac_ctx *ctx, int fid_z, const double *a, int fid_x, const double *b,
+                       int fid_y)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      if (!a || !b) throw FacError(FAC_ERR_ARG, "null coefficients");
+      if (fid_z == FAC_W) throw FacError(FAC_ERR_ARG, "the weights are not a vector");
+      vec_all_active(ctx);
+      const int np = nprob(ctx);
+      ctx->vec_coef.alloc(2 * (size_t)np);
+      CUDA_CHECK(cudaMemcpyAsync(ctx->vec_coef.p, a, np * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+      CUDA_CHECK(cudaMemcpyAsync(ctx->vec_coef.p + np, b, np * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+      const int gz = field_ghost(fid_z), gx = field_ghost(fid_x), gy = field_ghost(fid_y);
+      for (int ln = 0; ln < ctx->nlev; ++ln) {
+         LevelState &L = ctx->L[ln];
+         launch_vec_lincomb(ctx->stream, ctx->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                            L.d_cell_chunks.p, field_ptr(L, fid_z), gz, field_ptr(L, fid_x), gx,
+                            field_ptr(L, fid_y), gy, ctx->vec_coef.p, ctx->vec_coef.p + np);
+      }
+      CUDA_CHECK(cudaGetLastError());
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
 int fac_ctx_create(fac_ctx **ctx, int dim, int device)
 {
    return guarded([&] {
@@ -3266,6 +3361,9 @@ int fac_set_bc(fac_ctx *ctx, const double *a, const double *b, const double *g)
          ctx->bc.b[l] = b[l];
          ctx->bc.g[l] = g[l];
       }
+      // kernels take the coefficients by value: graphs captured with the
+      // old ones are captured again
+      ctx->drop_graph();
    });
 }
 
@@ -3611,6 +3709,27 @@ int fac_download_oside(fac_ctx *ctx, int problem, int ln, double *host)
       CUDA_CHECK(cudaMemcpyAsync(host, ctx->L[ln].oflux.p + off, n * sizeof(double),
                                  cudaMemcpyDeviceToHost, ctx->stream));
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+int fac_fill_table(fac_ctx *ctx, int ln, int with_coarse, long long *dst, long long *src,
+                   size_t cap, size_t *n)
+{
+   return guarded([&] {
+      check_state(ctx, true);
+      check_pl(ctx, 0, ln);
+      if (!n) throw FacError(FAC_ERR_ARG, "null count");
+      if (with_coarse && ln == 0) throw FacError(FAC_ERR_ARG, "level 0 has no coarser level");
+      const FillGather &G = with_coarse ? ctx->L[ln].gather_wc : ctx->L[ln].gather_nc;
+      if (!G.ok)
+         throw FacError(FAC_ERR_STATE, "this level's fill has no element table (item fill)");
+      *n = G.to.size();
+      if (cap == 0) return;
+      if (cap < G.to.size() || !dst || !src) throw FacError(FAC_ERR_ARG, "table too small");
+      for (size_t q = 0; q < G.to.size(); ++q) {
+         dst[q] = (long long)G.to[q];
+         src[q] = (long long)G.from[q];
+      }
    });
 }
 

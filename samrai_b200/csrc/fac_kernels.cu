@@ -1052,6 +1052,119 @@ k_norm_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ 
    }
 }
 
+// Composite-vector reductions (SAMRAIVectorReal::dot and maxNorm with
+// control volumes, SAMRAIVectorReal.C:821-960 over HierarchyCellDataOpsReal
+// dot/maxNorm, HierarchyCellDataOpsReal.C:877-1036): MODE 0, per chunk the
+// sum of w x y (and of w); MODE 1, the largest |x| over cells with w > 0.
+// Interior cells of fields of any ghost width.
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(kThreads)
+k_vec_partial(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
+              const double *__restrict__ x, int xg, const double *__restrict__ y, int yg,
+              const double *__restrict__ w, double2 *__restrict__ partial)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const long long xoff = xg ? p.off1 : p.off0, yoff = yg ? p.off1 : p.off0;
+      double sd = 0.0, sv = 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
+         const double xv = x[cidx<DIM>(p, xoff, xg, i, j, k)];
+         const double wv = w[p.off0 + lin];
+         if (MODE == 0) {
+            const double yv = y[cidx<DIM>(p, yoff, yg, i, j, k)];
+            sd += xv * yv * wv;
+            sv += wv;
+         } else if (wv > 0.0) {
+            sd = fmax(sd, fabs(xv));
+         }
+      }
+      __shared__ double rs[kThreads], rv[kThreads];
+      rs[threadIdx.x] = sd;
+      rv[threadIdx.x] = sv;
+      __syncthreads();
+      for (int o = kThreads / 2; o > 0; o >>= 1) {
+         if ((int)threadIdx.x < o) {
+            rs[threadIdx.x] = MODE == 0 ? rs[threadIdx.x] + rs[threadIdx.x + o]
+                                        : fmax(rs[threadIdx.x], rs[threadIdx.x + o]);
+            rv[threadIdx.x] += rv[threadIdx.x + o];
+         }
+         __syncthreads();
+      }
+      if (threadIdx.x == 0) partial[ch.aux] = make_double2(rs[0], rv[0]);
+      __syncthreads();
+   }
+}
+
+// Per problem: the partials of its chunks in chunk order, added to (MODE 0)
+// or maxed into (MODE 1) acc[prob]; levels in level order by the caller.
+template <int MODE>
+__global__ void k_vec_reduce(const double2 *__restrict__ partial,
+                             const int *__restrict__ prob_chunk_begin, int nprob,
+                             double2 *__restrict__ acc)
+{
+   const int pr = blockIdx.x;
+   if (pr >= nprob) return;
+   const int b = prob_chunk_begin[pr], e = prob_chunk_begin[pr + 1];
+   __shared__ double rs[kThreads], rv[kThreads];
+   double sd = 0.0, sv = 0.0;
+   for (int c = b + threadIdx.x; c < e; c += blockDim.x) {
+      sd = MODE == 0 ? sd + partial[c].x : fmax(sd, partial[c].x);
+      sv += partial[c].y;
+   }
+   rs[threadIdx.x] = sd;
+   rv[threadIdx.x] = sv;
+   __syncthreads();
+   for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) {
+         rs[threadIdx.x] = MODE == 0 ? rs[threadIdx.x] + rs[threadIdx.x + o]
+                                     : fmax(rs[threadIdx.x], rs[threadIdx.x + o]);
+         rv[threadIdx.x] += rv[threadIdx.x + o];
+      }
+      __syncthreads();
+   }
+   if (threadIdx.x == 0) {
+      double2 a = acc[pr];
+      a.x = MODE == 0 ? a.x + rs[0] : fmax(a.x, rs[0]);
+      a.y += rv[0];
+      acc[pr] = a;
+   }
+}
+
+// z = a[prob] x + b[prob] y on interior cells (SAMRAIVectorReal::linearSum,
+// ArrayDataBasicOps: dst = alpha src1 + beta src2)
+template <int DIM>
+__global__ void __launch_bounds__(kThreads)
+k_vec_lincomb(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
+              double *z, int zg, const double *x, int xg, const double *y, int yg,
+              const double *__restrict__ a, const double *__restrict__ b)
+{
+   WORK_LOOP(ch) {
+      const PatchDesc p = patches[ch.patch];
+      const int nx = p.hi[0] - p.lo[0] + 1;
+      const int ny = p.hi[1] - p.lo[1] + 1;
+      const double ap = a[p.prob], bp = b[p.prob];
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const int lin = ch.begin + t;
+         int ci, cj, ck;
+         patch_cell(p, lin, nx, ny, ci, cj, ck);
+         const int i = p.lo[0] + ci;
+         const int j = p.lo[1] + cj;
+         const int k = DIM == 3 ? p.lo[2] + ck : 0;
+         const double xv = x[cidx<DIM>(p, xg ? p.off1 : p.off0, xg, i, j, k)];
+         const double yv = y[cidx<DIM>(p, yg ? p.off1 : p.off0, yg, i, j, k)];
+         z[cidx<DIM>(p, zg ? p.off1 : p.off0, zg, i, j, k)] = ap * xv + bp * yv;
+      }
+   }
+}
+
 // Per problem: sum the partials of its chunks (in chunk order) and add them
 // to acc[prob] (levels are summed in level order by the caller).
 __global__ void k_norm_reduce(const double2 *__restrict__ partial,
@@ -2001,6 +2114,42 @@ void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
    else
       k_norm_partial<3><<<work_grid(k_norm_partial<3>, nchunks), kThreads, 0, s>>>(patches, chunks, nchunks, x, xg, w, partial);
    k_norm_reduce<<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
+}
+
+void launch_vec_reduce(cudaStream_t s, int dim, int mode, int nchunks, const PatchDesc *patches,
+                       const Chunk *chunks, const double *x, int xg, const double *y, int yg,
+                       const double *w, double2 *partial, const int *prob_chunk_begin,
+                       int nprob, double2 *acc)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(2, std::memory_order_relaxed);
+#define VP(D, M)                                                                          \
+   k_vec_partial<D, M><<<work_grid(k_vec_partial<D, M>, nchunks), kThreads, 0, s>>>(       \
+      patches, chunks, nchunks, x, xg, y, yg, w, partial)
+   if (dim == 2) {
+      if (mode == 0) VP(2, 0);
+      else VP(2, 1);
+   } else {
+      if (mode == 0) VP(3, 0);
+      else VP(3, 1);
+   }
+#undef VP
+   if (mode == 0) k_vec_reduce<0><<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
+   else k_vec_reduce<1><<<nprob, kThreads, 0, s>>>(partial, prob_chunk_begin, nprob, acc);
+}
+
+void launch_vec_lincomb(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                        const Chunk *chunks, double *z, int zg, const double *x, int xg,
+                        const double *y, int yg, const double *a, const double *b)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_vec_lincomb<2><<<work_grid(k_vec_lincomb<2>, nchunks), kThreads, 0, s>>>(
+         patches, chunks, nchunks, z, zg, x, xg, y, yg, a, b);
+   else
+      k_vec_lincomb<3><<<work_grid(k_vec_lincomb<3>, nchunks), kThreads, 0, s>>>(
+         patches, chunks, nchunks, z, zg, x, xg, y, yg, a, b);
 }
 
 void launch_sweep_check(cudaStream_t s, const unsigned long long *red,

@@ -164,6 +164,18 @@ void launch_norm(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                  const Chunk *chunks, const double *x, int xg, const double *w,
                  double2 *partial, const int *prob_chunk_begin, int nprob, double2 *acc);
 
+// Composite-vector reductions over interior cells, per problem added into
+// acc: mode 0 acc += (sum w x y, sum w); mode 1 acc.x = max(acc.x, max |x|
+// where w > 0).
+void launch_vec_reduce(cudaStream_t s, int dim, int mode, int nchunks, const PatchDesc *patches,
+                       const Chunk *chunks, const double *x, int xg, const double *y, int yg,
+                       const double *w, double2 *partial, const int *prob_chunk_begin,
+                       int nprob, double2 *acc);
+// z = a[prob] x + b[prob] y on interior cells
+void launch_vec_lincomb(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                        const Chunk *chunks, double *z, int zg, const double *x, int xg,
+                        const double *y, int yg, const double *a, const double *b);
+
 void launch_sweep_check(cudaStream_t s, const unsigned long long *red,
                         const unsigned long long *blk, const int *last_patch, int nprob,
                         double tol, int *run, long long *sweeps);

@@ -58,6 +58,15 @@ def load_library(build_if_missing=True):
         "fac_ctx_destroy": (ctypes.c_int, [vp]),
         "fac_add_problem": (ctypes.c_int, [vp, ip, dp, dp, ctypes.c_int, ip, ip, ip, ip]),
         "fac_set_coarse_extension": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_fill_table": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_longlong),
+                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_size_t,
+                                          szp]),
+        "fac_vec_dot": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
+        "fac_vec_l2_norm": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "fac_vec_max_norm": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+        "fac_vec_linear_sum": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, dp,
+                                              ctypes.c_int]),
         "fac_extend_coefficients": (ctypes.c_int, [vp]),
         "fac_set_poisson": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double]),
@@ -257,6 +266,11 @@ class FacContext:
         arr = np.ascontiguousarray(arr, dtype=np.float64)
         _check(load_library().fac_upload_side(self.h, prob, ln, _dp(arr)))
 
+    def download_side(self, prob, ln):
+        out = np.empty(self._side_n(prob, ln))
+        _check(load_library().fac_download_side(self.h, prob, ln, _dp(out)))
+        return out
+
     def _side_n(self, prob, ln):
         n = ctypes.c_size_t(0)
         _check(load_library().fac_side_size(self.h, prob, ln, ctypes.byref(n)))
@@ -319,8 +333,9 @@ class FacContext:
         return conv.astype(bool), its, res
 
     def solve_host(self, f_arrays, u_out, u0_arrays=None):
-        """End-to-end solve from host buffers (one per problem x level)."""
-        n = self.nprob * self.nlev
+        """End-to-end solve from host buffers (one per problem x level of the
+        caller's hierarchy, without the levels of the coarse extension)."""
+        n = self.nprob * (self.nlev - self.ext)
         DP = ctypes.POINTER(ctypes.c_double)
         ftab = (DP * n)(*[_dp(a) for a in f_arrays])
         utab = (DP * n)(*[_dp(a) for a in u_out])
@@ -441,6 +456,40 @@ class FacContext:
         buf = ctypes.create_string_buffer(n.value + 1)
         _check(load_library().fac_trace_read(self.h, buf, n.value + 1, ctypes.byref(n)))
         return json.loads(buf.value.decode())
+
+    def fill_table(self, ln, with_coarse):
+        """(dst, src) element copies of a ghost fill of level ln
+        (fac_fill_table); src < 0 is element -src-1 of the coarser level."""
+        L = load_library()
+        n = ctypes.c_size_t(0)
+        _check(L.fac_fill_table(self.h, ln, int(with_coarse), None, None, 0, ctypes.byref(n)))
+        dst = np.zeros(n.value, dtype=np.int64)
+        src = np.zeros(n.value, dtype=np.int64)
+        lp = ctypes.POINTER(ctypes.c_longlong)
+        _check(L.fac_fill_table(self.h, ln, int(with_coarse), dst.ctypes.data_as(lp),
+                                src.ctypes.data_as(lp), n.value, ctypes.byref(n)))
+        return dst, src
+
+    # composite-vector operations (SAMRAIVectorReal dot, norms, linearSum)
+    def vec_dot(self, fx, fy):
+        out = np.zeros(self.nprob)
+        _check(load_library().fac_vec_dot(self.h, fx, fy, _dp(out)))
+        return out
+
+    def vec_l2_norm(self, fid):
+        out = np.zeros(self.nprob)
+        _check(load_library().fac_vec_l2_norm(self.h, fid, _dp(out)))
+        return out
+
+    def vec_max_norm(self, fid):
+        out = np.zeros(self.nprob)
+        _check(load_library().fac_vec_max_norm(self.h, fid, _dp(out)))
+        return out
+
+    def vec_linear_sum(self, fz, a, fx, b, fy):
+        a = np.ascontiguousarray(np.broadcast_to(a, self.nprob), dtype=np.float64)
+        b = np.ascontiguousarray(np.broadcast_to(b, self.nprob), dtype=np.float64)
+        _check(load_library().fac_vec_linear_sum(self.h, fz, _dp(a), fx, _dp(b), fy))
 
     def timer_start(self):
         _check(load_library().fac_timer(self.h, 0, None))

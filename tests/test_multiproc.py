@@ -62,3 +62,82 @@ def test_two_gloo_ranks_shard_and_reduce():
     for rank, _, ms, conv in res:
         assert ms == 20.0
         assert conv == len(costs)
+
+
+# ---------------------------------------------------------------------------
+# one hierarchy split over ranks: ghost fills through split transaction tables
+# ---------------------------------------------------------------------------
+
+def test_morton_partition_balances_cells():
+    import numpy as np
+    from samrai_b200 import configs
+    p = configs.config2()
+    for world in (2, 4, 8):
+        for lv in p.levels:
+            own = parallel.morton_partition(lv.boxes, world)
+            cells = np.prod(lv.boxes[:, 3:] - lv.boxes[:, :3] + 1, axis=1)
+            loads = np.bincount(own, weights=cells, minlength=world)
+            assert set(own.tolist()) <= set(range(world))
+            assert loads.max() <= 1.35 * loads.mean()
+
+
+def _fill_worker(rank, world, port, q):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from samrai_b200 import configs, fac
+    from oracle.oracle import Oracle, U
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        p = configs.small_3d(seed=9)
+        g = fac.FacContext([p], device=-1)          # tables only
+        rng = np.random.default_rng(3)
+        data = [rng.standard_normal(configs.field_size(p, ln, 1)) for ln in range(p.nlev)]
+        powner = [parallel.morton_partition(lv.boxes, world) for lv in p.levels]
+        eowner = [parallel.element_owner(p, ln, powner[ln]) for ln in range(p.nlev)]
+        report = []
+        for ln in range(p.nlev):
+            for wc in ((0, 1) if ln else (0,)):
+                # the single-rank fill of the whole level
+                o = Oracle(p)
+                for l2 in range(p.nlev):
+                    o.set(U, l2, data[l2])
+                o.ghost_fill(U, ln, wc, 0)
+                want = o.get(U, ln)
+                dst, src = g.fill_table(ln, wc)
+                plan = parallel.FillPlan(dst, src, eowner[ln], eowner[ln],
+                                         eowner[ln - 1] if ln else None, rank)
+                # this rank sees only its own patches: the others' values are NaN
+                x = torch.from_numpy(np.where(eowner[ln] == rank, data[ln], np.nan))
+                xc = (torch.from_numpy(np.where(eowner[ln - 1] == rank, data[ln - 1], np.nan))
+                      if ln else None)
+                parallel.exchange(plan, x, xc, dist)
+                mine = dst[eowner[ln][dst] == rank]
+                ok = bool(np.array_equal(x.numpy()[mine], want[mine]))
+                report.append((ln, wc, ok, plan.volume()))
+        q.put((rank, report))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_fill_tables_two_gloo_ranks_match_single_rank_fill():
+    import torch.multiprocessing as mp
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_fill_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank in (0, 1):
+        for ln, wc, ok, vol in res[rank]:
+            assert ok, (rank, ln, wc)
+    # what one rank sends the other receives, fill by fill
+    for a, b in zip(res[0], res[1]):
+        assert a[3][1] == b[3][2] and a[3][2] == b[3][1]
+        assert a[3][1] + a[3][2] > 0      # the split really crosses ranks
