@@ -371,6 +371,54 @@ int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level);
  * FAC_E of that level as scratch. */
 int fac_learned_samples(fac_ctx *ctx, int level, float *x, double *scale);
 
+/* ---- other centerings: time interpolation and index boxes (no part of the
+ *      FAC path; the reference's RefineSchedule applies them to any patch
+ *      data: xfer/RefineSchedule.C:2037 fillData with time interpolation,
+ *      pdat/CellDoubleLinearTimeInterpolateOp.C:86 and its side, face, node
+ *      and edge twins over pdat_m4lintimeintops{2,3}d.i). */
+enum fac_centering {
+   FAC_CELL = 0,
+   FAC_SIDE = 1,   /* SideGeometry::toSideBox: upper+1 along the axis */
+   FAC_FACE = 2,   /* FaceGeometry::toFaceBox: axis first, upper+1 along it */
+   FAC_NODE = 3,   /* NodeGeometry::toNodeBox: upper+1 along every axis */
+   FAC_EDGE = 4    /* EdgeGeometry::toEdgeBox: upper+1 along the other axes */
+};
+/* The index box of centering (and axis, for side, face and edge data) of the
+ * cell box lo..hi, in the storage order of that data. */
+int fac_centered_box(int dim, int centering, int axis, const int *lo, const int *hi,
+                     int *out_lo, int *out_hi);
+/* One box of a time interpolation: device arrays (one component, column-
+ * major over their boxes, first index fastest), each box in the data's own
+ * index space (fac_centered_box), where inside all three. */
+typedef struct fac_time_box {
+   const double *old_data;
+   const double *new_data;
+   double *dst_data;
+   int where_lo[3], where_hi[3];
+   int old_lo[3], old_hi[3];
+   int new_lo[3], new_hi[3];
+   int dst_lo[3], dst_hi[3];
+} fac_time_box;
+/* dst = old (1 - t) + new t over every box, t = (dst_time - old_time) /
+ * (new_time - old_time) (0 when the times coincide), the arithmetic of the
+ * reference's LinearTimeInterpolateOps; queued on stream (a cudaStream_t,
+ * NULL: legacy default), nothing allocated.  A where box outside an array's
+ * box returns FAC_ERR_ARG before anything runs. */
+int fac_time_interpolate(int dim, const fac_time_box *boxes, int nboxes,
+                         double old_time, double new_time, double dst_time,
+                         void *stream);
+
+/* ---- bounded device waits (no counterpart in the reference).
+ * The staged colour pass's consumer warps wait for each unit's copies at
+ * most limit_cycles SM clock cycles (default 4e9, about 2 s) and then set
+ * the context's device error flag, which the next norm or solve reports as
+ * FAC_ERR_CUDA; every copy a block issued lands before the block exits, so
+ * the context stays usable.  never = 1 makes that wait be for a phase no
+ * copy completes: a test of the bound that ends with the error.
+ * fac_clear_device_error resets the flag. */
+int fac_set_wait_test(fac_ctx *ctx, long long limit_cycles, int never);
+int fac_clear_device_error(fac_ctx *ctx);
+
 /* ---- composite-vector operations (solv/SAMRAIVectorReal.C: dot :889,
  *      RMSNorm :821, L2Norm, maxNorm, linearSum), for Krylov and nonlinear
  *      solvers that call FAC as a preconditioner

@@ -137,6 +137,10 @@ def compile_kernels(ref):
         fh.write("\n\n".join(chunks) + "\n")
     obj = os.path.join(gen, "kernels.o")
     run(["gcc", *CFLAGS, "-c", src, "-o", obj])
+    # the same kernels as a shared library, for tests that call the
+    # reference's routines one by one
+    run(["gcc", *CFLAGS, "-fPIC", "-shared", src, "-o", os.path.join(OUT, "libref_kernels.so"),
+         "-lm"])
     print(f"build_ref: {len(names)} Fortran routines translated", flush=True)
     return obj
 

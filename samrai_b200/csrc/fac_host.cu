@@ -399,6 +399,7 @@ struct fac_ctx {
    int stage_budget = 32 * 1024;  // shared memory of one stage (unit) of the staged pass
    int stage_depth = 2;           // stages per CTA of the staged pass
    DevArray<int> kerr;       // set by kernels whose bounded waits ran out
+   WaitTest wait_test;       // bound of the staged pass's waits (fac_set_wait_test)
    bool capturing = false;   // inside stream capture: no host synchronisation
    cudaGraphExec_t cycle_exec = nullptr;
    // captured FGMRES pieces: FAC cycle on R into E (the preconditioner) and
@@ -1989,7 +1990,8 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
             launch_rb_staged<double>(c->stream, c->dim, c->spec, (int)L.units[0].size(),
                                      L.unit_smem[0], c->stage_depth, L.d_units[0].p,
                                      L.d_copies[0].p, L.d_hdrs[0].p, e, r, L.d.p, L.c.p,
-                                     L.cfflux.p, color, L.pushmap.p, c->bc, c->kerr.p);
+                                     L.cfflux.p, color, L.pushmap.p, c->bc, c->kerr.p,
+                                     c->wait_test);
          else
             launch_rbgs(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(), L.d_patches.p,
                         L.d_slot_chunks.p, e, r, L.d.p, L.c.p, L.cfflux.p, L.cfmask.p, color,
@@ -2111,7 +2113,9 @@ void rms_norm_read(fac_ctx *c, std::vector<double> &out)
    int kerr = 0;
    CUDA_CHECK(cudaMemcpyAsync(&kerr, c->kerr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
    CUDA_CHECK(cudaStreamSynchronize(c->stream));
-   if (kerr) throw FacError(FAC_ERR_CUDA, "a staged colour pass lost its shared-memory copies");
+   if (kerr)
+      throw FacError(FAC_ERR_CUDA, "a bounded wait of a staged colour pass ran out (device error "
+                                   "flag; fac_clear_device_error resets it)");
    out.resize(np);
    for (int p = 0; p < np; ++p) {
       const double num = std::sqrt(acc[p].x);
@@ -2248,7 +2252,7 @@ void smooth32(fac_ctx *c, int ln, int nsweeps, bool zero_start = false)
                                     L.unit_smem[1], c->stage_depth, L.d_units[1].p,
                                     L.d_copies[1].p, L.d_hdrs[1].p, L.e32.p, L.r32.p,
                                     L.d32.p, L.c32.p, L.cfflux32.p, color, L.pushmap.p,
-                                    c->bc, c->kerr.p);
+                                    c->bc, c->kerr.p, c->wait_test);
          else
             launch_rbgs<float>(c->stream, c->dim, c->spec, (int)L.slot_chunks.size(),
                                L.d_patches.p, L.d_slot_chunks.p, L.e32.p, L.r32.p, L.d32.p,
@@ -3491,6 +3495,26 @@ int fac_autotune(fac_ctx *ctx, int *chosen_bytes, int *chosen_depth, double *ms_
       set_stage_shape(ctx, best, best_depth);
       if (chosen_bytes) *chosen_bytes = best;
       if (chosen_depth) *chosen_depth = best_depth;
+   });
+}
+
+int fac_set_wait_test(fac_ctx *ctx, long long limit_cycles, int never)
+{
+   return guarded([&] {
+      if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
+      if (limit_cycles < 1 || never < 0 || never > 1) throw FacError(FAC_ERR_ARG, "bad wait test");
+      ctx->wait_test.limit = limit_cycles;
+      ctx->wait_test.never = never;
+      ctx->drop_graph();  // launches take the bound by value
+   });
+}
+
+int fac_clear_device_error(fac_ctx *ctx)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      CUDA_CHECK(cudaMemsetAsync(ctx->kerr.p, 0, sizeof(int), ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
    });
 }
 

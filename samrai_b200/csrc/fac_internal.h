@@ -135,6 +135,15 @@ struct BcCoefs {
    double a[6], b[6], g[6];
 };
 
+// The staged colour pass's wait for a unit's copies: it gives up after
+// `limit` SM clock cycles (about 2 s by default).  never = 1 is the test of
+// that bound: the wait is on an mbarrier nothing arrives on, so it runs
+// out (the stage's copies still land before the block exits).
+struct WaitTest {
+   long long limit = 4000000000ll;
+   int never = 0;
+};
+
 #ifdef __CUDACC__
 #define FAC_HD __host__ __device__
 #else

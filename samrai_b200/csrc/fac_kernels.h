@@ -26,7 +26,7 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
                       int stage_bytes, int depth, const Chunk *units, const UnitCopy *copies,
                       const unsigned char *headers, T *u, const T *f, const T *dside,
                       const T *cfield, const T *cfflux, int offset, const int *pushmap,
-                      const BcCoefs &bc, int *err);
+                      const BcCoefs &bc, int *err, const WaitTest &wt = WaitTest());
 
 // Krylov vector operations on composite vectors: ghost-0 level arrays, one
 // vector every vstride elements; per-problem coefficients; chunks are runs

@@ -108,11 +108,12 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long *bar)
 }
 
 // bounded wait of one thread; false on timeout
-__device__ __forceinline__ bool wait_phase(unsigned long long *bar, unsigned parity)
+__device__ __forceinline__ bool wait_phase(unsigned long long *bar, unsigned parity,
+                                           long long limit = kWaitCycles)
 {
    const long long t0 = clock64();
    while (!mbar_try_wait(bar, parity))
-      if (clock64() - t0 > kWaitCycles) return false;
+      if (clock64() - t0 > limit) return false;
    return true;
 }
 
@@ -140,7 +141,10 @@ struct StageBases {
    const char *p[kSrcCount];
 };
 
-static_assert(2 * kStageDepthMax * 8 + sizeof(StageBases) <= kBarrierBytes, "barrier area");
+// full[depth], empty[depth], the copy sources, and one mbarrier nothing
+// arrives on (the test of the bounded wait waits on it)
+static_assert(2 * kStageDepthMax * 8 + sizeof(StageBases) + 8 <= kBarrierBytes, "barrier area");
+static_assert((2 * kStageDepthMax * 8 + sizeof(StageBases)) % 8 == 0, "mbarrier alignment");
 
 // Red-black parity of a row of a unit: the first active cell of the row is
 // at li = ioffset (2d.f:141-147, 3d.f:201-207 with their integer modulo).
@@ -372,12 +376,14 @@ template <int DIM, bool DVAR, int CKIND, class T>
 __global__ void __launch_bounds__(kStageBlock)
 k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restrict__ copies,
             StageBases bases, int stage_bytes, int depth, T *__restrict__ u, int offset,
-            T dconst, T cconst, BcCoefs bc, int *__restrict__ err)
+            T dconst, T cconst, BcCoefs bc, int *__restrict__ err, WaitTest wt)
 {
    extern __shared__ __align__(128) unsigned char smem[];
    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem);
    unsigned long long *empty = full + kStageDepthMax;
    StageBases *sbases = reinterpret_cast<StageBases *>(smem + 2 * kStageDepthMax * 8);
+   unsigned long long *never_bar = reinterpret_cast<unsigned long long *>(
+      smem + 2 * kStageDepthMax * 8 + sizeof(StageBases));
    unsigned char *stages = smem + kBarrierBytes;
    // the list holds active problems only (compacted), so the units of this
    // block are w = blockIdx.x, + gridDim.x, ... up to the end marker
@@ -387,6 +393,7 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
          mbar_init_count(&full[k], 1);
          mbar_init_count(&empty[k], kConsumerWarps);
       }
+      mbar_init_count(never_bar, 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       *sbases = bases;
    }
@@ -397,7 +404,8 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
       // list, header first; its first entry carries the byte total)
       int w = blockIdx.x;
       Chunk ch = w < nwork ? chunks[w] : Chunk{-1, 0, 0, 0};
-      for (int k = 0; ch.patch >= 0; ++k) {
+      int k = 0;  // units issued
+      for (; ch.patch >= 0; ++k) {
          const int wn = w + gridDim.x;
          const Chunk chn = wn < nwork ? chunks[wn] : Chunk{-1, 0, 0, 0};  // prefetch
          UnitCopy cp = {0, 0, 0, 0, 0};
@@ -407,7 +415,7 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
          if (k >= depth && lane == 0) ok = wait_phase(&empty[st], ((k / depth) & 1) ^ 1u);
          if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) {
             if (lane == 0) atomicExch(err, 1);
-            return;
+            break;
          }
          unsigned char *stage = stages + st * stage_bytes;
          if (lane == 0) mbar_expect_tx(&full[st], (unsigned)cp.total);
@@ -418,6 +426,14 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
          w = wn;
          ch = chn;
       }
+      // the block's shared memory must outlive every copy issued into it:
+      // the last `depth` units (one per stage; no later unit was issued
+      // into those stages) have landed before this warp leaves, whether
+      // or not the consumers took them
+      if (lane == 0)
+         for (int q = k - 1; q >= 0 && q >= k - depth; --q)
+            if (!wait_phase(&full[q % depth], (q / depth) & 1)) atomicExch(err, 1);
+      __syncwarp();
       return;
    }
    const int tid = threadIdx.x;  // 0 .. kConsumers-1
@@ -428,7 +444,9 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
       const int st = k % depth;
       const unsigned par = (k / depth) & 1;
       unsigned char *stage = stages + st * stage_bytes;
-      const bool ok = wait_phase(&full[st], par);
+      // (the test of the bounded wait waits on a barrier nothing arrives on)
+      const bool ok = wt.never ? wait_phase(never_bar, 0u, wt.limit)
+                               : wait_phase(&full[st], par, wt.limit);
       if (ok) stage_update<DIM, DVAR, CKIND, T>(stage, tid, u, offset, dconst, cconst);
       // every consumer passes here once per unit: all leave together when
       // any wait ran out, and the pushes read the updated stage
@@ -449,7 +467,7 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
 template <int DIM, bool DVAR, int CK, class T>
 void staged_inst(cudaStream_t s, int nunits, int stage_bytes, int depth, const Chunk *units,
                  const UnitCopy *copies, const StageBases &bases, T *u, int offset,
-                 double dconst, double cconst, const BcCoefs &bc, int *err)
+                 double dconst, double cconst, const BcCoefs &bc, int *err, const WaitTest &wt)
 {
    static bool attr = false;
    static int nsm = 148;
@@ -470,7 +488,7 @@ void staged_inst(cudaStream_t s, int nunits, int stage_bytes, int depth, const C
    const int grid = nunits < nsm * per_sm ? nunits : nsm * per_sm;
    k_rb_staged<DIM, DVAR, CK, T><<<grid, kStageBlock, smem, s>>>(
       units, nunits, copies, bases, stage_bytes, depth, u, offset, (T)dconst, (T)cconst, bc,
-      err);
+      err, wt);
 }
 
 }  // namespace
@@ -480,7 +498,7 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
                       int stage_bytes, int depth, const Chunk *units, const UnitCopy *copies,
                       const unsigned char *headers, T *u, const T *f, const T *dside,
                       const T *cfield, const T *cfflux, int offset, const int *pushmap,
-                      const BcCoefs &bc, int *err)
+                      const BcCoefs &bc, int *err, const WaitTest &wt)
 {
    if (nunits <= 0) return;
    add_kernel_launches(1);
@@ -494,7 +512,7 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
    bases.p[kSrcHdr] = reinterpret_cast<const char *>(headers);
 #define SG(D, V, C)                                                                       \
    staged_inst<D, V, C, T>(s, nunits, stage_bytes, depth, units, copies, bases, u, offset, \
-                           spec.d_const, spec.c_const, bc, err)
+                           spec.d_const, spec.c_const, bc, err, wt)
    if (dim == 2) {
       if (spec.d_variable) {
          if (spec.c_kind == 2) SG(2, true, 2);
@@ -523,7 +541,7 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
    template void launch_rb_staged<T>(cudaStream_t, int, const PoissonSpec &, int, int, int,    \
                                      const Chunk *, const UnitCopy *, const unsigned char *,   \
                                      T *, const T *, const T *, const T *, const T *, int,     \
-                                     const int *, const BcCoefs &, int *);
+                                     const int *, const BcCoefs &, int *, const WaitTest &);
 INST_STAGED(double)
 INST_STAGED(float)
 #undef INST_STAGED

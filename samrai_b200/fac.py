@@ -58,6 +58,8 @@ def load_library(build_if_missing=True):
         "fac_ctx_destroy": (ctypes.c_int, [vp]),
         "fac_add_problem": (ctypes.c_int, [vp, ip, dp, dp, ctypes.c_int, ip, ip, ip, ip]),
         "fac_set_coarse_extension": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_wait_test": (ctypes.c_int, [vp, ctypes.c_longlong, ctypes.c_int]),
+        "fac_clear_device_error": (ctypes.c_int, [vp]),
         "fac_fill_table": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(ctypes.c_longlong),
                                           ctypes.POINTER(ctypes.c_longlong), ctypes.c_size_t,
