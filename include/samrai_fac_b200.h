@@ -112,6 +112,19 @@ int fac_set_poisson(fac_ctx *ctx, int d_variable, double d_const,
  * coefficients. */
 int fac_set_bc(fac_ctx *ctx, const double *a, const double *b,
                const double *g);
+/* Robin coefficients that vary along the boundary, as a
+ * RobinBcCoefStrategy::setBcCoefs fills them per boundary face
+ * (solv/RobinBcCoefStrategy.h:138-145): for one problem, level and
+ * location index, abg holds (a, b, g) triples over that level's whole
+ * domain face on that side (the lowest tangential axis fastest); sides
+ * without them keep the constants of fac_set_bc.  The coefficients of the
+ * coarse interpolation array of prolongation come from the coarser level's
+ * arrays, by position, as the reference's coefficient object evaluates
+ * them there.  While any are set, smoothing takes the fill-based colour
+ * passes (the fused and staged ones apply side constants).  After
+ * fac_initialize. */
+int fac_set_bc_faces(fac_ctx *ctx, int problem, int ln, int location,
+                     const double *abg);
 
 /* Input keys of FACPreconditioner (FACPreconditioner.C:80-114) and
  * CellPoissonFACOps (CellPoissonFACOps.C:692-739).  ewing: 1 selects

@@ -61,6 +61,9 @@ struct orc_hier {
    int c_kind;
    double c_const;
    double bc_a[6], bc_b[6], bc_g[6];
+   /* per-face Robin coefficients (a, b, g triples) over each level's domain
+    * face of each location index, or NULL for the constants above */
+   double *bcf[OMAXL][6];
    /* FACPreconditioner / CellPoissonFACOps parameters */
    int max_cycles;
    double residual_tol, rel_residual_tol;
@@ -269,6 +272,7 @@ void orc_destroy(orc_hier *h)
    if (!h) return;
    for (int ln = 0; ln < h->nlev; ++ln) {
       olevel *L = &h->L[ln];
+      for (int loc = 0; loc < 6; ++loc) free(h->bcf[ln][loc]);
       for (int ip = 0; ip < L->np; ++ip) {
          opatch *p = &L->p[ip];
          for (int f = 0; f < ORC_NCELL; ++f) free(p->cell[f]);
@@ -303,6 +307,20 @@ void orc_set_bc(orc_hier *h, const double *a, const double *b,
       h->bc_b[l] = b[l];
       h->bc_g[l] = g[l];
    }
+}
+
+void orc_set_bc_faces(orc_hier *h, int ln, int loc, const double *abg)
+{
+   if (ln < 0 || ln >= h->nlev || loc < 0 || loc >= 2 * h->dim) return;
+   const obox *d = &h->L[ln].domain;
+   long n = 1;
+   for (int t = 0; t < h->dim; ++t)
+      if (t != loc / 2) n *= d->hi[t] - d->lo[t] + 1;
+   free(h->bcf[ln][loc]);
+   h->bcf[ln][loc] = NULL;
+   if (!abg) return;
+   h->bcf[ln][loc] = malloc(3 * n * sizeof(double));
+   memcpy(h->bcf[ln][loc], abg, 3 * n * sizeof(double));
 }
 
 void orc_set_params(orc_hier *h, int max_cycles, double residual_tol,
@@ -479,8 +497,22 @@ static void compute_cf_masks(orc_hier *h, int ln)
  * Codimension 1 is done for all faces first, then 2, then 3, as in the
  * reference.
  */
+/* Index of the face at the tangential coordinates of cell c on location
+ * loc of a level's domain face: lowest tangential axis fastest. */
+static long face_index(int dim, const obox *domain, int loc, const int *c)
+{
+   const int a = loc / 2;
+   long idx = 0, stride = 1;
+   for (int t = 0; t < dim; ++t) {
+      if (t == a) continue;
+      idx += stride * (c[t] - domain->lo[t]);
+      stride *= domain->hi[t] - domain->lo[t] + 1;
+   }
+   return idx;
+}
+
 static void bc_fill_box(const orc_hier *h, oarr A, obox b, const obox *domain,
-                        const double *dx, int homogeneous)
+                        const double *dx, int homogeneous, double *const *faces)
 {
    const int dim = h->dim;
    obox gb = box_grow(b, dim, 1);
@@ -513,6 +545,15 @@ static void bc_fill_box(const orc_hier *h, oarr A, obox b, const obox *domain,
                   int ci[3] = {i, j, k};
                   ci[a] -= side[a];
                   double av = h->bc_a[loc], bv = h->bc_b[loc], gv = h->bc_g[loc];
+                  if (faces && faces[loc]) {
+                     /* the coefficients of the face between ghost and
+                      * interior cell (RobinBcCoefStrategy::setBcCoefs
+                      * arrays, RobinBcCoefStrategy.h:138-145) */
+                     const double *f = faces[loc] + 3 * face_index(dim, domain, loc, c);
+                     av = f[0];
+                     bv = f[1];
+                     gv = f[2];
+                  }
                   double hh = dx[a];
                   double uin = AT(A, ci[0], ci[1], ci[2]);
                   double v;
@@ -622,8 +663,8 @@ static void fill_physical(orc_hier *h, int fid, int ln, int homogeneous)
    if (k_cell_ghost[fid] < 1) return;
    for (int ip = 0; ip < L->np; ++ip) {
       opatch *p = &L->p[ip];
-      bc_fill_box(h, cell_arr(h, p, fid), p->box, &L->domain, L->dx,
-                  homogeneous);
+      bc_fill_box(h, cell_arr(h, p, fid), p->box, &L->domain, L->dx, homogeneous,
+                  h->bcf[ln]);
    }
 }
 
@@ -1108,7 +1149,7 @@ void orc_prolong_correct(orc_hier *h, int fid_src, int fid_dst, int dest_ln)
                for (int i = ov.lo[0]; i <= ov.hi[0]; ++i)
                   AT(T, i, j, k) = AT(S, i, j, k);
       }
-      bc_fill_box(h, T, B, &C->domain, C->dx, 1);
+      bc_fill_box(h, T, B, &C->domain, C->dx, 1, h->bcf[dest_ln - 1]);
       oarr D = cell_arr(h, fp, fid_dst);
       const obox b = fp->box;
       for (int k = b.lo[2]; k <= b.hi[2]; ++k) {

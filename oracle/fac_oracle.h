@@ -62,6 +62,10 @@ void orc_set_poisson(orc_hier *h, int d_variable, double d_const,
 /* Robin coefficients per location index 0..2*dim-1 (a u + b un = g). */
 void orc_set_bc(orc_hier *h, const double *a, const double *b,
                 const double *g);
+/* Robin coefficients per face of location index loc of level ln: abg holds
+ * (a, b, g) triples over the level's whole domain face, the lowest
+ * tangential axis fastest (NULL: back to the constants of orc_set_bc). */
+void orc_set_bc_faces(orc_hier *h, int ln, int loc, const double *abg);
 /* Solver parameters (FACPreconditioner / CellPoissonFACOps input keys). */
 void orc_set_params(orc_hier *h, int max_cycles, double residual_tol,
                     double relative_residual_tol, int pre_sweeps,

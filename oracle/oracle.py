@@ -58,6 +58,7 @@ def lib():
         L.orc_set_poisson.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_int, ctypes.c_double]
         L.orc_set_bc.argtypes = [ctypes.c_void_p, dp, dp, dp]
+        L.orc_set_bc_faces.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.orc_set_params.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_int, ctypes.c_int]
@@ -103,7 +104,7 @@ def _ip(a):
 class Oracle:
     """One FAC hierarchy on the CPU, set up like CellPoissonFACSolver."""
 
-    def __init__(self, prob, params=None, bc=None):
+    def __init__(self, prob, params=None, bc=None, bc_faces=None):
         L = lib()
         self.prob = prob
         dim = prob.dim
@@ -123,6 +124,12 @@ class Oracle:
         if bc is not None:
             a, b, g = (np.asarray(x, dtype=np.float64) for x in bc)
             L.orc_set_bc(self.h, _dp(a), _dp(b), _dp(g))
+        # per-face Robin coefficients: {(level, location): (n, 3) array}
+        self._faces = {}
+        for (ln, loc), abg in (bc_faces or {}).items():
+            arr = np.ascontiguousarray(abg, dtype=np.float64).reshape(-1)
+            self._faces[ln, loc] = arr
+            L.orc_set_bc_faces(self.h, int(ln), int(loc), _dp(arr))
         p = dict(max_cycles=100, residual_tol=1e-300, relative_residual_tol=1e-10,
                  pre_sweeps=2, post_sweeps=2, coarse_tol=1e-8, coarse_max_it=500, ewing=1)
         if params:

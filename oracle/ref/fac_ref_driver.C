@@ -24,7 +24,8 @@
  * boxes[npatch_total*6] (lo0 lo1 lo2 hi0 hi1 hi2 in the level's index space),
  * xlo[3], xup[3], poisson[4] (D variable, D constant, C kind, C constant),
  * bc[18] (a, b, g per location index 0..5; absent: Dirichlet through the
- * solver's setBoundaries, values from u0's ghost cells), params[7] (max_cycles,
+ * solver's setBoundaries, values from u0's ghost cells), bc_faces (present:
+ * Robin coefficients varying along the boundary, FaceRobin), params[7] (max_cycles,
  * residual_tol, relative_residual_tol, pre sweeps, post sweeps, coarse
  * tolerance, coarse max iterations), and per level f<ln> (cells, ghost 0),
  * u0<ln> (ghost 1), d<ln> (side data, when D is variable), c<ln> (when C is
@@ -154,6 +155,60 @@ public:
 private:
    const tbox::Dimension d_dim;
    std::vector<double> d_abg;
+};
+
+/*
+ * Robin coefficients varying along the boundary: a polynomial of the face
+ * centre's tangential coordinates (t = sum of x = xlo + (i + 1/2) dx over
+ * the tangential axes, dx of the patch's level), a = 1 + t/4, b = 1/2 + t/8,
+ * g = t/10 - 1/20 + location/100, written per face into the arrays the
+ * helper asks for, without tangential extensions.
+ */
+class FaceRobin : public solv::RobinBcCoefStrategy {
+public:
+   FaceRobin(const tbox::Dimension &dim, const std::vector<double> &xlo,
+             const std::vector<double> &xup, const std::vector<int> &n0)
+      : d_dim(dim), d_xlo(xlo), d_xup(xup), d_n0(n0) {}
+
+   void setBcCoefs(const std::shared_ptr<pdat::ArrayData<double> > &acoef_data,
+                   const std::shared_ptr<pdat::ArrayData<double> > &bcoef_data,
+                   const std::shared_ptr<pdat::ArrayData<double> > &gcoef_data,
+                   const std::shared_ptr<hier::Variable> &, const hier::Patch &patch,
+                   const hier::BoundaryBox &bdry_box, const double) const override
+   {
+      const int dim = d_dim.getValue();
+      const int loc = bdry_box.getLocationIndex();
+      const int normal = loc / 2;
+      const hier::IntVector &ratio = patch.getPatchGeometry()->getRatio();
+      double dx[3] = {1, 1, 1};
+      for (int a = 0; a < dim; ++a)
+         dx[a] = ((d_xup[a] - d_xlo[a]) / (double)d_n0[a]) / (double)ratio(a);
+      const std::shared_ptr<pdat::ArrayData<double> > arrs[3] = {acoef_data, bcoef_data,
+                                                                  gcoef_data};
+      for (int q = 0; q < 3; ++q) {
+         if (!arrs[q]) continue;
+         const hier::Box &box = arrs[q]->getBox();
+         for (hier::Box::iterator bi(box.begin()); bi != box.end(); ++bi) {
+            const hier::Index &idx = *bi;
+            double t = 0.0;
+            for (int a = 0; a < dim; ++a)
+               if (a != normal) t = t + (d_xlo[a] + ((double)idx(a) + 0.5) * dx[a]);
+            const double v = q == 0 ? 1.0 + 0.25 * t
+                                    : (q == 1 ? 0.5 + 0.125 * t : 0.1 * t - 0.05 + 0.01 * loc);
+            (*arrs[q])(idx, 0) = v;
+         }
+      }
+   }
+
+   hier::IntVector numberOfExtensionsFillable() const override
+   {
+      return hier::IntVector::getZero(d_dim);
+   }
+
+private:
+   const tbox::Dimension d_dim;
+   std::vector<double> d_xlo, d_xup;
+   std::vector<int> d_n0;
 };
 
 /*
@@ -330,6 +385,8 @@ int run(Records &in, const char *out_path)
       new solv::FACPreconditioner("fac_precond", ops, pre_db));
    ops->setRecordingPreconditioner(pre.get());
    ConstantRobin robin(dim, bc);
+   FaceRobin face_robin(dim, xlo, xup, n0);
+   const bool face_bc = in.i32.count("bc_faces") != 0;
    solv::CellPoissonFACSolver solver(dim, "solver", pre, ops);
    TRACE("solver made");
 
@@ -386,7 +443,8 @@ int run(Records &in, const char *out_path)
    else solver.setDConstant(poisson[1]);
    if (ckind == 2) solver.setCPatchDataId(c_id);
    else solver.setCConstant(ckind == 1 ? poisson[3] : 0.0);
-   if (robin_bc) solver.setBcObject(&robin);
+   if (face_bc) solver.setBcObject(&face_robin);
+   else if (robin_bc) solver.setBcObject(&robin);
    else solver.setBoundaries("Dirichlet");
    using clock = std::chrono::steady_clock;
    const clock::time_point t0 = clock::now();

@@ -47,7 +47,8 @@ def read(path):
 
 
 def problem_records(prob, params, bc=None):
-    """Input records of fac_ref_driver for a samrai_b200.configs.Problem."""
+    """Input records of fac_ref_driver for a samrai_b200.configs.Problem;
+    bc "faces" selects the driver's position-dependent Robin object."""
     boxes = np.concatenate([lv.boxes for lv in prob.levels]).astype(np.int32)
     recs = [("dim", [prob.dim]), ("nlev", [prob.nlev]),
             ("n0", np.array(list(prob.n0) + [1] * (3 - len(prob.n0)), dtype=np.int32)),
@@ -60,7 +61,9 @@ def problem_records(prob, params, bc=None):
             ("params", [params["max_cycles"], params["residual_tol"],
                         params["relative_residual_tol"], params["pre_sweeps"],
                         params["post_sweeps"], params["coarse_tol"], params["coarse_max_it"]])]
-    if bc is not None:
+    if isinstance(bc, str) and bc == "faces":
+        recs.append(("bc_faces", np.array([1], dtype=np.int32)))
+    elif bc is not None:
         # Robin a u + b du/dn = g per side; without it the solver's own
         # Dirichlet path, boundary values from u0's ghost cells
         recs.append(("bc", np.concatenate([np.asarray(x, dtype=np.float64) for x in bc])))

@@ -125,11 +125,43 @@ __device__ __forceinline__ int coarsen_index(int i, int r)
 // settype1cells{2,3}d (robinbchelper2d.f:10-72): ghost value from the
 // interior value next to the boundary.
 template <class T>
+__device__ __forceinline__ T robin_abg(T uin, T a, T b, T g, T h, int hom)
+{
+   const T half = (T)0.5;
+   if (hom) return (uin * (b - half * h * a)) / (b + half * h * a);
+   return (h * g + uin * (b - half * h * a)) / (b + half * h * a);
+}
+
+template <class T>
 __device__ __forceinline__ T robin(T uin, int loc, T h, int hom, const BcCoefs &bc)
 {
-   const T a = (T)bc.a[loc], b = (T)bc.b[loc], half = (T)0.5;
-   if (hom) return (uin * (b - half * h * a)) / (b + half * h * a);
-   return (h * (T)bc.g[loc] + uin * (b - half * h * a)) / (b + half * h * a);
+   return robin_abg<T>(uin, (T)bc.a[loc], (T)bc.b[loc], (T)bc.g[loc], h, hom);
+}
+
+// The Robin ghost value across location loc of a boundary item of level
+// lvl and problem prob, inward cell ci: the coefficients of that face when
+// the level has per-face coefficients on that side (RobinBcCoefStrategy::
+// setBcCoefs arrays), else the side's constants.
+template <class T>
+__device__ __forceinline__ T robin_at(T uin, int loc, T h, int hom, const BcCoefs &bc, int lvl,
+                                      int prob, const int *ci)
+{
+   if (bc.face_base) {
+      const long long off = bc.face_off[((long long)lvl * 6 + loc) * bc.face_nprob + prob];
+      if (off >= 0) {
+         const int *dm = bc.face_dom + ((long long)lvl * bc.face_nprob + prob) * 6;
+         const int a = loc >> 1;
+         long long idx = 0, stride = 1;
+         for (int t = 0; t < 3; ++t) {
+            if (t == a) continue;
+            idx += stride * (ci[t] - dm[t]);
+            stride *= dm[3 + t];
+         }
+         const double *f = bc.face_base + off + 3 * idx;
+         return robin_abg<T>(uin, (T)f[0], (T)f[1], (T)f[2], h, hom);
+      }
+   }
+   return robin<T>(uin, loc, h, hom, bc);
 }
 
 // One red-black point update from the six face fluxes (low/high per axis),

@@ -400,6 +400,16 @@ struct fac_ctx {
    int stage_depth = 2;           // stages per CTA of the staged pass
    DevArray<int> kerr;       // set by kernels whose bounded waits ran out
    WaitTest wait_test;       // bound of the staged pass's waits (fac_set_wait_test)
+   // Robin coefficients varying along the boundary (fac_set_bc_faces);
+   // while any are set the colour passes take the fill-based path, whose
+   // boundary fills read them
+   bool bc_faces = false;
+   std::vector<double> face_host;
+   std::vector<long long> face_off_host;
+   std::vector<int> face_dom_host;
+   DevArray<double> face_dev;
+   DevArray<long long> face_off_dev;
+   DevArray<int> face_dom_dev;
    bool capturing = false;   // inside stream capture: no host synchronisation
    cudaGraphExec_t cycle_exec = nullptr;
    // captured FGMRES pieces: FAC cycle on R into E (the preconditioner) and
@@ -814,6 +824,7 @@ void build_fill_tables(fac_ctx *c, int ln)
                it.side[a] = s[a];
                it.h[a] = L.dx[3 * p + a];
             }
+            it.bc_level = ln;
             it.dst = dst;
             it.src = dst;
             L.fill_nc.add(it, bb.size());
@@ -1435,6 +1446,7 @@ void build_prolong_tables(fac_ctx *c, int ln)
                it.side[a] = s[a];
                it.h[a] = C.dx[3 * p + a];
             }
+            it.bc_level = ln - 1;  // the coarse level's boundary coefficients
             it.dst = T;
             it.src = patch_desc(c, C, iq, 1);
             it.src_is_coarse = 1;
@@ -1947,7 +1959,7 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
    CUDA_CHECK(cudaMemcpyAsync(c->run.p, c->active.p, np * sizeof(int), cudaMemcpyDeviceToDevice,
                               c->stream));
    CUDA_CHECK(cudaMemsetAsync(c->sweeps_call.p, 0, np * sizeof(long long), c->stream));
-   const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
+   const long long *fmap = (c->fused && L.fused_ok && !c->bc_faces) ? L.facemap.p : nullptr;
    // the staged pass computes no residual maxima: fixed sweep counts only
    const bool staged = fmap && c->staged && tol < 0.0 && L.unit_smem[0] > 0;
    // The fill with the coarser level is a full fill.  Pulling fused passes
@@ -2228,7 +2240,7 @@ void smooth32(fac_ctx *c, int ln, int nsweeps, bool zero_start = false)
    LevelState &L = c->L[ln];
    const int np = nprob(c);
    const int *run = c->active.p;
-   const long long *fmap = (c->fused && L.fused_ok) ? L.facemap.p : nullptr;
+   const long long *fmap = (c->fused && L.fused_ok && !c->bc_faces) ? L.facemap.p : nullptr;
    const bool staged = fmap && c->staged && L.unit_smem[1] > 0;
    if (zero_start && fmap) {
       // entry fill skipped (see above); passes that fill around themselves
@@ -3495,6 +3507,50 @@ int fac_autotune(fac_ctx *ctx, int *chosen_bytes, int *chosen_depth, double *ms_
       set_stage_shape(ctx, best, best_depth);
       if (chosen_bytes) *chosen_bytes = best;
       if (chosen_depth) *chosen_depth = best_depth;
+   });
+}
+
+int fac_set_bc_faces(fac_ctx *ctx, int problem, int ln, int location, const double *abg)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      const int dim = ctx->dim, np = nprob(ctx);
+      if (location < 0 || location >= 2 * dim) throw FacError(FAC_ERR_ARG, "bad location index");
+      if (!abg) throw FacError(FAC_ERR_ARG, "null coefficients");
+      if (ctx->face_off_host.empty()) {
+         ctx->face_off_host.assign((size_t)kMaxLevels * 6 * np, -1);
+         ctx->face_dom_host.assign((size_t)kMaxLevels * np * 6, 0);
+         for (int l = 0; l < ctx->nlev; ++l)
+            for (int p = 0; p < np; ++p) {
+               const Box &d = ctx->L[l].domain[p];
+               int *dm = &ctx->face_dom_host[((size_t)l * np + p) * 6];
+               for (int a = 0; a < 3; ++a) {
+                  dm[a] = d.lo[a];
+                  dm[3 + a] = d.hi[a] - d.lo[a] + 1;
+               }
+            }
+      }
+      const Box &d = ctx->L[ln].domain[problem];
+      long long n = 1;
+      for (int t = 0; t < 3; ++t)
+         if (t != location / 2) n *= d.hi[t] - d.lo[t] + 1;
+      long long &off = ctx->face_off_host[((size_t)ln * 6 + location) * np + problem];
+      if (off < 0) {
+         off = (long long)ctx->face_host.size();
+         ctx->face_host.resize(ctx->face_host.size() + 3 * (size_t)n);
+      }
+      std::copy(abg, abg + 3 * n, ctx->face_host.begin() + off);
+      ctx->face_dev.upload(ctx->face_host, ctx->stream);
+      ctx->face_off_dev.upload(ctx->face_off_host, ctx->stream);
+      ctx->face_dom_dev.upload(ctx->face_dom_host, ctx->stream);
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      ctx->bc.face_base = ctx->face_dev.p;
+      ctx->bc.face_off = ctx->face_off_dev.p;
+      ctx->bc.face_dom = ctx->face_dom_dev.p;
+      ctx->bc.face_nprob = np;
+      ctx->bc_faces = true;
+      ctx->drop_graph();  // kernels take the coefficients by value
    });
 }
 

@@ -84,7 +84,7 @@ struct FillItem {
    ArrDesc src;
    double h[3];         // kFillBc: grid spacing of the destination
    int src_is_coarse;   // read from the coarser level's buffer
-   int pad;
+   int bc_level;        // kFillBc: level whose boundary coefficients apply
 };
 
 // A coarse-fine boundary face of a patch (Ewing fix-up).
@@ -133,6 +133,16 @@ struct ProlongItem {
 
 struct BcCoefs {
    double a[6], b[6], g[6];
+   // Robin coefficients varying along the boundary (fac_set_bc_faces):
+   // (a, b, g) triples; face_off[(level * 6 + location) * face_nprob +
+   // problem] is a problem's offset for one side of one level's domain
+   // face (-1: the constants above), face_dom[(level * face_nprob +
+   // problem) * 6] that level's domain box (lower corner, extents).  Null
+   // base: constants everywhere.
+   const double *face_base = nullptr;
+   const long long *face_off = nullptr;
+   const int *face_dom = nullptr;
+   int face_nprob = 0;
 };
 
 // The staged colour pass's wait for a unit's copies: it gives up after

@@ -59,12 +59,14 @@ __device__ __forceinline__ void fill_element(const FillItem &it, int lin, T *__r
       // Every ghost value of codimension m depends only on the interior
       // cell reached by moving inward along all m outside axes
       // (settype1/2/3cells{2,3}d applied in codimension order).
-      const T uin = src[aidx(it.src, i - it.side[0], j - it.side[1], k - it.side[2])];
+      const int ci[3] = {i - it.side[0], j - it.side[1], k - it.side[2]};
+      const T uin = src[aidx(it.src, ci[0], ci[1], ci[2])];
       T f[3];
       int m = 0;
       for (int a = 0; a < 3; ++a) {
          if (it.side[a]) {
-            f[a] = robin<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc);
+            f[a] = robin_at<T>(uin, 2 * a + (it.side[a] > 0), (T)it.h[a], homogeneous, bc,
+                               it.bc_level, it.prob, ci);
             ++m;
          } else {
             f[a] = (T)0;

@@ -12,6 +12,7 @@
  */
 #include "B200CellPoissonFACOps.h"
 
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -229,23 +230,37 @@ void B200CellPoissonFACOps::upload_coefficients()
    }
 }
 
-// Robin coefficients a, b, g of each side of the domain, from the boundary
-// object over every physical boundary box (the faces next to the patch,
-// without tangential extensions, as CartesianRobinBcHelper asks for them
-// from SimpleCellRobinBcCoefs, CartesianRobinBcHelper.C:215-241).  Queried
-// at the first operation of a solve, when the solver has cached its
-// Dirichlet values.
+// Robin coefficients a, b, g from the boundary object, asked over every
+// physical boundary box of every patch (the faces next to the patch,
+// without tangential extensions, as CartesianRobinBcHelper asks
+// SimpleCellRobinBcCoefs for them, CartesianRobinBcHelper.C:215-241), at
+// the first operation of a solve, when the solver has cached its Dirichlet
+// values.  Constant sides go to fac_set_bc (the fused and staged colour
+// passes stay on); otherwise every level's side arrays go to
+// fac_set_bc_faces.
 void B200CellPoissonFACOps::sync_bc()
 {
    if (d_bc_known) return;
    const solv::RobinBcCoefStrategy *bc = this->*member(BcTag());
    if (!bc) TBOX_ERROR("B200CellPoissonFACOps: no boundary condition object");
    const int dim = d_b200_dim.getValue();
+   const int nlev = (int)d_patches.size();
    double a[6] = {1, 1, 1, 1, 1, 1}, b[6] = {0, 0, 0, 0, 0, 0}, g[6] = {0, 0, 0, 0, 0, 0};
    bool seen[6] = {false, false, false, false, false, false};
+   bool varies = false;
+   // per level and side, the faces of the level's domain face: (a, b, g)
+   std::vector<std::vector<double> > faces((size_t)nlev * 6);
+   std::vector<std::array<int, 6> > dom(nlev);
    std::shared_ptr<hier::Variable> var;
-   for (auto &level : d_patches)
-      for (auto &patch : level) {
+   for (int ln = 0; ln < nlev; ++ln) {
+      const hier::BoxContainer &pd =
+         d_hier->getPatchLevel(ln)->getPhysicalDomain(hier::BlockId::zero());
+      const hier::Box &dbox = pd.front();
+      for (int t = 0; t < 3; ++t) {
+         dom[ln][t] = t < dim ? dbox.lower()(t) : 0;
+         dom[ln][3 + t] = t < dim ? dbox.upper()(t) - dbox.lower()(t) + 1 : 1;
+      }
+      for (auto &patch : d_patches[ln]) {
          std::shared_ptr<geom::CartesianPatchGeometry> pg(
             SAMRAI_SHARED_PTR_CAST<geom::CartesianPatchGeometry, hier::PatchGeometry>(
                patch->getPatchGeometry()));
@@ -263,32 +278,55 @@ void B200CellPoissonFACOps::sync_bc()
                               std::min(cells.upper()(t), patch->getBox().upper()(t)));
             }
             const hier::BoundaryBox trimmed(cells, 1, loc);
-            hier::Box faces(cells);
-            if (loc % 2 == 0) faces.shift(static_cast<tbox::Dimension::dir_t>(nd), 1);
+            hier::Box fbox(cells);
+            if (loc % 2 == 0) fbox.shift(static_cast<tbox::Dimension::dir_t>(nd), 1);
             std::shared_ptr<pdat::ArrayData<double> > ad(
-               std::make_shared<pdat::ArrayData<double> >(faces, 1));
+               std::make_shared<pdat::ArrayData<double> >(fbox, 1));
             std::shared_ptr<pdat::ArrayData<double> > bd(
-               std::make_shared<pdat::ArrayData<double> >(faces, 1));
+               std::make_shared<pdat::ArrayData<double> >(fbox, 1));
             std::shared_ptr<pdat::ArrayData<double> > gd(
-               std::make_shared<pdat::ArrayData<double> >(faces, 1));
+               std::make_shared<pdat::ArrayData<double> >(fbox, 1));
             bc->setBcCoefs(ad, bd, gd, var, *patch, trimmed, 0.0);
-            const size_t n = faces.size();
-            for (size_t q = 0; q < n; ++q) {
+            std::vector<double> &f = faces[(size_t)ln * 6 + loc];
+            if (f.empty()) {
+               size_t n = 1;
+               for (int t = 0; t < 3; ++t)
+                  if (t != nd) n *= (size_t)dom[ln][3 + t];
+               f.assign(3 * n, 0.0);
+            }
+            size_t q = 0;
+            for (hier::Box::iterator bi(fbox.begin()); bi != fbox.end(); ++bi, ++q) {
+               const hier::Index &idx = *bi;
                const double av = ad->getPointer()[q], bv = bd->getPointer()[q],
                             gv = gd->getPointer()[q];
+               long long fi = 0, stride = 1;
+               for (int t = 0; t < dim; ++t) {
+                  if (t == nd) continue;
+                  fi += stride * (idx(t) - dom[ln][t]);
+                  stride *= dom[ln][3 + t];
+               }
+               f[3 * fi] = av;
+               f[3 * fi + 1] = bv;
+               f[3 * fi + 2] = gv;
                if (!seen[loc]) {
                   a[loc] = av;
                   b[loc] = bv;
                   g[loc] = gv;
                   seen[loc] = true;
                } else if (av != a[loc] || bv != b[loc] || gv != g[loc]) {
-                  TBOX_ERROR("B200CellPoissonFACOps: Robin coefficients must be constant "
-                             "on each side of the domain");
+                  varies = true;
                }
             }
          }
       }
+   }
    check(fac_set_bc(d_ctx, a, b, g), "fac_set_bc");
+   if (varies)
+      for (int ln = 0; ln < nlev; ++ln)
+         for (int loc = 0; loc < 2 * dim; ++loc)
+            if (!faces[(size_t)ln * 6 + loc].empty())
+               check(fac_set_bc_faces(d_ctx, 0, ln, loc, faces[(size_t)ln * 6 + loc].data()),
+                     "fac_set_bc_faces");
    d_bc_known = true;
 }
 

@@ -18,9 +18,10 @@
  *
  * Supported as the GPU path implements them: prolongation_method
  * LINEAR_REFINE, cf_discretization Ewing, coarse_solver_choice redblack, a
- * level-0 domain of one box at the origin, levels from 0 up, Robin
- * coefficients that are constant on each side of the domain.  Other
- * settings stop with TBOX_ERROR in initializeOperatorState.
+ * level-0 domain of one box at the origin, levels from 0 up.  Robin
+ * coefficients may vary along the boundary (then the library's
+ * fill-based colour passes run).  Other settings stop with TBOX_ERROR in
+ * initializeOperatorState.
  */
 #ifndef SAMRAI_B200_CELL_POISSON_FAC_OPS_H
 #define SAMRAI_B200_CELL_POISSON_FAC_OPS_H

@@ -58,6 +58,7 @@ def load_library(build_if_missing=True):
         "fac_ctx_destroy": (ctypes.c_int, [vp]),
         "fac_add_problem": (ctypes.c_int, [vp, ip, dp, dp, ctypes.c_int, ip, ip, ip, ip]),
         "fac_set_coarse_extension": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fac_set_bc_faces": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]),
         "fac_set_wait_test": (ctypes.c_int, [vp, ctypes.c_longlong, ctypes.c_int]),
         "fac_clear_device_error": (ctypes.c_int, [vp]),
         "fac_fill_table": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
@@ -459,6 +460,14 @@ class FacContext:
         _check(load_library().fac_trace_read(self.h, buf, n.value + 1, ctypes.byref(n)))
         return json.loads(buf.value.decode())
 
+    def set_bc_faces(self, faces, prob=0):
+        """Robin coefficients varying along the boundary: {(level,
+        location): (n, 3) array of (a, b, g)} over each level's domain face
+        (fac_set_bc_faces); levels count the coarse extension's."""
+        for (ln, loc), abg in faces.items():
+            arr = np.ascontiguousarray(abg, dtype=np.float64).reshape(-1)
+            _check(load_library().fac_set_bc_faces(self.h, prob, int(ln), int(loc), _dp(arr)))
+
     def fill_table(self, ln, with_coarse):
         """(dst, src) element copies of a ghost fill of level ln
         (fac_fill_table); src < 0 is element -src-1 of the coarser level."""
@@ -570,6 +579,13 @@ class CellPoissonFACSolver:
     def setBcObject(self, a, b, g):
         self._bc = (a, b, g)
 
+    def setBcFaces(self, faces):
+        """Robin coefficients varying along the boundary, {(level,
+        location): (n, 3) array of (a, b, g) over the level's domain face}:
+        what a RobinBcCoefStrategy's setBcCoefs would fill, evaluated on
+        every boundary face."""
+        self._faces = dict(faces)
+
     def setMaxCycles(self, n):
         self._params["max_cycles"] = int(n)
 
@@ -600,6 +616,9 @@ class CellPoissonFACSolver:
                 p.c_kind, p.c_const = self._c_kind, self._c_const
         self._problems = list(problems)
         self._ctx = FacContext(self._problems, self._params, device=device, bc=self._bc)
+        if getattr(self, "_faces", None):
+            for i in range(len(self._problems)):
+                self._ctx.set_bc_faces(self._faces, prob=i)
 
     def deallocateSolverState(self):
         if self._ctx:

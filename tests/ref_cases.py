@@ -3,8 +3,9 @@
 coarse-fine boundaries, norms and FAC loop, with its Fortran kernels
 translated to C) are stored as golden fixtures in tests/golden/ref_*.npz.
 
-Each case: (problem builder, solver parameters, Robin coefficients or None
-for Dirichlet u = 0, whether the fixture keeps the full solution arrays).
+Each case: (problem builder, solver parameters, Robin coefficients -- a
+constant triple per side, "faces" for robin_face_coefs, or None for
+Dirichlet u = 0 -- and whether the fixture keeps the full solution arrays).
 Every fixture keeps, per level, SHA-256 digests of the solution's bytes
 (interior cells, and all cells with the ghost cells), a fingerprint and
 every SAMPLE-th value; the small 2-D cases keep the full arrays as well.
@@ -63,6 +64,32 @@ def config2_mg():
     return configs.extend_hierarchy(configs.config2(), k=4)
 
 
+def robin_face_coefs(prob, ln, loc):
+    """Robin (a, b, g) varying along every side of the domain, the same
+    polynomial of the face-centre coordinates that fac_ref_driver's
+    position-dependent coefficient object evaluates: t = sum over the
+    tangential axes of x = xlo + (i + 0.5) dx (level ln's dx), a = 1 +
+    t/4, b = 1/2 + t/8, g = t/10 - 1/20 + loc/100.  Returns the (n, 3)
+    array over the level's domain face, lowest tangential axis fastest."""
+    dim = prob.dim
+    a_n = loc // 2
+    lo, hi = prob.domain(ln)
+    dx = prob.dx(ln)
+    tang = [t for t in range(dim) if t != a_n]
+    axes = [np.arange(lo[t], hi[t] + 1) for t in tang]
+    grids = np.meshgrid(*axes[::-1], indexing="ij")[::-1]
+    t = np.zeros(grids[0].shape)
+    for g, ax in zip(grids, tang):
+        t = t + (prob.xlo[ax] + (g.astype(np.float64) + 0.5) * dx[ax])
+    t = t.reshape(-1)
+    return np.stack([1.0 + 0.25 * t, 0.5 + 0.125 * t, 0.1 * t - 0.05 + 0.01 * loc], axis=1)
+
+
+def all_face_coefs(prob):
+    return {(ln, loc): robin_face_coefs(prob, ln, loc)
+            for ln in range(prob.nlev) for loc in range(2 * prob.dim)}
+
+
 # Robin a u + b du/dn = g on the four sides (location index 0..3)
 ROBIN = (np.array([1.0, 2.0, 1.0, 0.5, 0, 0]), np.array([0.5, 1.0, 0.25, 1.0, 0, 0]),
          np.array([0.1, -0.2, 0.05, 0.3, 0, 0]))
@@ -80,6 +107,10 @@ CASES = {
     "mixed_parity_2d": (mixed_parity_2d, dict(BASE, coarse_tol=1e-300, coarse_max_it=200),
                         None, True),
     "robin_2d": (configs.config1, TIGHT, ROBIN, True),
+    # Robin coefficients varying along the boundary (robin_face_coefs)
+    "robin_faces_2d": (configs.config1, TIGHT, "faces", True),
+    "robin_faces_3d": (configs.small_3d, dict(BASE, coarse_tol=1e-300, coarse_max_it=100),
+                       "faces", False),
     "c_field_2d": (c_field_2d, TIGHT, None, True),
     "small_3d": (configs.small_3d, dict(BASE, coarse_tol=1e-300, coarse_max_it=100), None,
                  False),

@@ -24,8 +24,8 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 DRIVER = os.path.join(os.path.dirname(refio.DRIVER), "fac_dropin_driver")
-CASES = ["config1_tight", "config3_tight", "mixed_parity_2d", "robin_2d", "c_field_2d",
-         "small_3d"]
+CASES = ["config1_tight", "config3_tight", "mixed_parity_2d", "robin_2d", "robin_faces_2d",
+         "c_field_2d", "small_3d"]
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -41,7 +41,7 @@ def randomize(prob, o, g, rng, fields=(U, E, R, F, TR)):
 CONFIGS = [configs.config1, configs.config3, configs.small_3d]
 
 
-@pytest.mark.parametrize("mk", CONFIGS)
+@pytest.mark.parametrize("mk", CONFIGS + [configs.config2])
 @pytest.mark.parametrize("homogeneous", [0, 1])
 def test_ghost_fill_bit_exact(mk, homogeneous, require_gpu):
     p = mk()

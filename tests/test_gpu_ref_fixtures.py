@@ -48,6 +48,8 @@ def test_gpu_solver_matches_reference_solver(name, require_gpu):
         solver.setCPatchDataId()
     if bc is None:
         solver.setBoundaries("Dirichlet")
+    elif isinstance(bc, str):  # "faces": coefficients varying along the boundary
+        solver.setBcFaces(ref_cases.all_face_coefs(p))
     else:
         solver.setBcObject(*bc)
     solver.initializeSolverState(p)

@@ -36,7 +36,10 @@ def test_oracle_matches_reference_solver(name):
     fx = fixture(name)
     build, prm, bc, _ = ref_cases.CASES[name]
     p = build()
-    o = Oracle(p, params=prm, bc=bc)
+    if isinstance(bc, str):  # "faces": coefficients varying along the boundary
+        o = Oracle(p, params=prm, bc_faces=ref_cases.all_face_coefs(p))
+    else:
+        o = Oracle(p, params=prm, bc=bc)
     ok, its, res, hist = o.solve()
     assert its == int(fx["iterations"][0])
     assert ok == bool(fx["converged"][0])
