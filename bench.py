@@ -325,19 +325,27 @@ class CpuReference:
 
 
 def cpu_small_solves(names=("c1", "c3")):
-    """Full plain FAC solves of the small 2-D configurations on one core
-    with the timing build (measured, not scaled)."""
-    from oracle import oracle
-    from oracle.oracle import Oracle
+    """Full plain FAC solves of the small 2-D configurations on one core,
+    measured, not scaled: the reference's own CellPoissonFACSolver
+    (oracle/_ref, solveSystem timed inside the driver) when it is built,
+    else the oracle's restatement.  Returns (kind, results)."""
+    from oracle.ref import refio
+    kind = "reference" if refio.available() else "port"
     out = {}
     for n in names:
         p = _make_problem(n, 0)
-        o = Oracle(p, params=dict(PARAMS))
-        t0 = time.perf_counter()
-        ok, its, res, _ = o.solve()
-        out[n] = {"cpu_ms": round((time.perf_counter() - t0) * 1e3, 2), "cycles": int(its),
-                  "converged": bool(ok)}
-    return out
+        if kind == "reference":
+            r = refio.run_reference(p, dict(PARAMS), solution=False)
+            ms = float(r["seconds"][1]) * 1e3
+            its, ok = int(r["iterations"][0]), bool(r["converged"][0])
+        else:
+            from oracle.oracle import Oracle
+            o = Oracle(p, params=dict(PARAMS))
+            t0 = time.perf_counter()
+            ok, its, res, _ = o.solve()
+            ms = (time.perf_counter() - t0) * 1e3
+        out[n] = {"cpu_ms": round(ms, 2), "cycles": int(its), "converged": bool(ok)}
+    return kind, out
 
 
 # ---------------------------------------------------------------------------
@@ -647,7 +655,7 @@ def main():
                        f"table), problems spread over {ref.workers} processes"),
         }
         # measured full solves of the small 2-D configurations, CPU and GPU
-        small = cpu_small_solves()
+        small_kind, small = cpu_small_solves()
         for n in small:
             sp = [_make_problem(n, 0)]
             sctx = fac.FacContext(sp, params=PARAMS, device=local_rank)
@@ -658,7 +666,8 @@ def main():
             small[n]["gpu_plain_fp64_ms"] = round(sctx.timer_stop(), 3)
             small[n]["gpu_cycles"] = int(sits[0])
             sctx.close()
-        out["cpu_small_configs"] = {"kind": "measured", "cores": 1, "configs": small}
+        out["cpu_small_configs"] = {"kind": small_kind, "measured": True, "cores": 1,
+                                    "cpu": CPU_KIND_TEXT[small_kind], "configs": small}
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -668,23 +677,26 @@ def main():
 
 
 def run_reference(args, world):
-    """CPU reference arm: the CPU restatement of the reference's plain FAC
-    on all host cores (one process per core, -O3 -march=native).  A step is
-    one sampling round, in which every process times one plain cycle of the
-    next problem in turn (`_ref_sample`); the rounds run until every problem
-    of the workload has a sample.  The value is the time to solve the
-    workload: per problem its mean cycle time times its plain cycle count,
-    the problems spread over the processes longest first."""
+    """CPU reference arm: the reference's plain FAC on all host cores, one
+    process per core -- its own CellPoissonFACSolver built from its sources
+    (oracle/_ref) when present, else the oracle's restatement (-O3
+    -march=native).  A step is one sampling round, in which every process
+    times one plain cycle of the next problem in turn (`_ref_sample`); the
+    rounds run until every problem of the workload has a sample.  The value
+    is the time to solve the workload: per problem its mean cycle time times
+    its plain cycle count, the problems spread over the processes longest
+    first.  Configs 1 and 3 are solved outright on one core."""
     seeds = workload_seeds(args.config, args.nprob, 0)
     desc = workload_desc(args.config, args.nprob)
     if args.config in ("c1", "c3"):
         # small enough to solve outright
         vals = []
         for it in range(args.warmup + args.steps):
-            r = cpu_small_solves((args.config,))[args.config]
+            kind, rs = cpu_small_solves((args.config,))
+            r = rs[args.config]
             if it >= args.warmup:
                 vals.append(r["cpu_ms"])
-        value, cores, kind = statistics.mean(vals), 1, "port"
+        value, cores = statistics.mean(vals), 1
         sample = f"full plain FAC solve, {r['cycles']} cycles, one core, measured"
         info = {}
     else:

@@ -157,8 +157,9 @@ int fac_set_staged(fac_ctx *ctx, int on);
  * fluxes where the flux coarsening stored them.  Bit-identical to 0.
  * fac_comp_residual itself always stores the face fluxes (fac_download_flux);
  * the setting applies to the residuals inside fac_solve / fac_fac_cycle.
- * Default 0: on B200 the two bandwidth-bound kernels beat the one
- * index-heavy kernel. */
+ * on = 1: every level, 0: none, -1 (the default): the levels whose patches
+ * average at least 8192 cells, where on B200 the one pass is faster (on
+ * levels of 8^3..16^3 patches the two kernels are). */
 int fac_set_fused_residual(fac_ctx *ctx, int on);
 
 /* Shared-memory bytes of one stage (one work unit) of the staged pass,

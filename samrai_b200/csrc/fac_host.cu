@@ -191,6 +191,7 @@ struct DevArray {
 struct WorkSrc {
    DevArray<Chunk> all;
    DevArray<int> pcb;
+   DevArray<int> prob;  // per entry, for lists not in problem order
 };
 
 template <class I>
@@ -395,7 +396,9 @@ struct fac_ctx {
    int use_graph = 1;        // capture one FAC cycle into a CUDA graph and replay it
    int fused = 1;            // colour passes read across patch faces directly
    int staged = 1;           // fused passes on shared-memory staged units
-   int fused_residual = 0;   // residual kernels form the fluxes on the fly
+   // residual kernels form the fluxes on the fly: 1 on every level, 0 on
+   // none, -1 on the levels of large patches (fused_residual_on)
+   int fused_residual = -1;
    int stage_budget = 32 * 1024;  // shared memory of one stage (unit) of the staged pass
    int stage_depth = 2;           // stages per CTA of the staged pass
    DevArray<int> kerr;       // set by kernels whose bounded waits ran out
@@ -1101,6 +1104,13 @@ void build_stage_units(fac_ctx *c, int ln)
          }
          if (s0 != nslow) throw FacError(FAC_ERR_ARG, "staged units do not tile the patch");
       }
+      // largest units first: the blocks walk the list in a snake order
+      // (k_rb_staged), so every block ends with the small units and the
+      // blocks' totals come out nearly equal (the pass has no tail of a few
+      // blocks still working on large units)
+      std::stable_sort(U.begin(), U.end(), [&](const Chunk &a, const Chunk &b) {
+         return copies[a.begin].total > copies[b.begin].total;
+      });
       // stage_depth stages per CTA after the barriers and copy sources; a
       // level whose units do not fit runs the unstaged pass
       L.unit_smem[t] =
@@ -1383,6 +1393,7 @@ void build_coarsen_tables(fac_ctx *c, int ln)
                if (si < 0 || si >= C.ns) throw FacError(FAC_ERR_ARG, "flux coarsening face");
                fm[si] = 1;
             }
+      C.hp[it.coarse_patch].flags |= 2;
    }
    C.fcmask.upload(fm, c->stream);
 }
@@ -1788,7 +1799,28 @@ void register_work(fac_ctx *c, WorkSrc &ws, const std::vector<Chunk> &chunks, Ch
       throw FacError(FAC_ERR_STATE, "work list registered before its upload");
    ws.all.upload(chunks, c->stream);
    ws.pcb.upload(pcb, c->stream);
-   if (!chunks.empty()) c->work_regs.push_back({ws.all.p, list, ws.pcb.p, (int)chunks.size(), 0});
+   if (!chunks.empty())
+      c->work_regs.push_back({ws.all.p, list, ws.pcb.p, nullptr, (int)chunks.size(), 0});
+}
+
+// A work list in an order of its own (not by problem): the compaction keeps
+// that order over the entries of the active problems.
+template <class ProbOf>
+void register_work_ordered(fac_ctx *c, WorkSrc &ws, const std::vector<Chunk> &chunks,
+                           Chunk *list, ProbOf prob_of)
+{
+   const int np = nprob(c);
+   std::vector<int> prob(std::max<size_t>(1, chunks.size()), 0);
+   for (size_t q = 0; q < chunks.size(); ++q) {
+      prob[q] = prob_of(chunks[q]);
+      if (prob[q] < 0 || prob[q] >= np) throw FacError(FAC_ERR_ARG, "work list problem");
+   }
+   if (!chunks.empty() && !list && !g_dry)
+      throw FacError(FAC_ERR_STATE, "work list registered before its upload");
+   ws.all.upload(chunks, c->stream);
+   ws.prob.upload(prob, c->stream);
+   if (!chunks.empty())
+      c->work_regs.push_back({ws.all.p, list, nullptr, ws.prob.p, (int)chunks.size(), 0});
 }
 
 template <class I>
@@ -1820,7 +1852,7 @@ void register_work_lists(fac_ctx *c)
       if (L.gather_tmp.ok) register_items(c, L.gather_tmp.bc);
       register_items(c, L.prolong);
       for (int t = 0; t < 2; ++t)
-         register_work(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
+         register_work_ordered(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
    }
    c->d_work_regs.upload(c->work_regs, c->stream);
 }
@@ -2023,6 +2055,18 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
 }
 
 // CellPoissonFACOps::computeCompositeResidualOnLevel (CellPoissonFACOps.C:1792-1956).
+// Mean patch size (cells) from which the automatic setting fuses the
+// residual: on levels of 32^3 patches the one-pass kernel measured faster
+// than the flux-array pair, on levels of 8^3..16^3 patches slower.
+constexpr long long kFusedResidualCells = 8192;
+
+bool fused_residual_on(const fac_ctx *c, int ln)
+{
+   if (c->fused_residual >= 0) return c->fused_residual != 0;
+   const LevelState &L = c->L[ln];
+   return L.npatch > 0 && L.n0 >= kFusedResidualCells * (long long)L.npatch;
+}
+
 void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int error_eq)
 {
    OpTimer ot(c, "comp_residual", ln);
@@ -2031,7 +2075,8 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
    ghost_fill(c, fid_u, ln, ln > 0, error_eq, run);
    const double *u = field_ptr(L, fid_u);
    const bool finer = ln < c->nlev - 1;
-   if (!c->fused_residual) {
+   const bool fused = fused_residual_on(c, ln);
+   if (!fused) {
       launch_flux_cells(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
                         L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
                         L.d_ratio.p, L.flux.p, run);
@@ -2046,7 +2091,7 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
                           L.fcoarsen.nchunks(), L.fcoarsen.d_prefix.p, Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
-   if (c->fused_residual)
+   if (fused)
       launch_residual_fused(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                             L.d_patches.p, L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt,
                             L.longwt, L.d_ratio.p, finer ? L.fcmask.p : nullptr, L.flux.p,
@@ -2288,7 +2333,8 @@ void comp_residual_mixed(fac_ctx *c, int ln)
    const int *run = c->active.p;
    ghost_fill32(c, ln, ln > 0, 1, run);
    const bool finer = ln < c->nlev - 1;
-   if (!c->fused_residual) {
+   const bool fused = fused_residual_on(c, ln);
+   if (!fused) {
       launch_flux_cells<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                                L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
                                L.tranwt, L.longwt, L.d_ratio.p, L.flux.p, run);
@@ -2303,7 +2349,7 @@ void comp_residual_mixed(fac_ctx *c, int ln)
                           L.fcoarsen.nchunks(), L.fcoarsen.d_prefix.p, Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
-   if (c->fused_residual)
+   if (fused)
       launch_residual_fused<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                                    L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
                                    L.tranwt, L.longwt, L.d_ratio.p,
@@ -2681,6 +2727,42 @@ void kry_combine(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot,
    }
 }
 
+// V_x = a[p] X + sum_i coef[p*K+i] V_{vslot+i} as kry_combine, and
+// dots[p*(K+1)+i] = <V_x, V_{vslot+i}>, dots[p*(K+1)+K] = <V_x, V_x> of the
+// result: the numbers kry_dots(c, xslot, vslot, K, dots, kNoField, true)
+// would give, from the combination's own pass.  False (nothing done) when K
+// is outside the fused kernel's range.
+bool kry_combine_dots(fac_ctx *c, int xslot, const std::vector<double> &a, int vslot, int K,
+                      const std::vector<double> &coef, std::vector<double> &dots,
+                      int xin_field = kNoField)
+{
+   if (K < 1 || K > kCombineDotsMax) return false;
+   OpTimer ot(c, "kry_combine_dots", -1);
+   const int np = nprob(c);
+   const int KT = K + 1;
+   CUDA_CHECK(cudaMemcpyAsync(c->kry_a.p, a.data(), np * sizeof(double), cudaMemcpyHostToDevice,
+                              c->stream));
+   CUDA_CHECK(cudaMemcpyAsync(c->kry_coef.p, coef.data(), (size_t)np * K * sizeof(double),
+                              cudaMemcpyHostToDevice, c->stream));
+   CUDA_CHECK(cudaMemsetAsync(c->kry_dots.p, 0, (size_t)np * KT * sizeof(double), c->stream));
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      LevelState &L = c->L[ln];
+      const int pi = prof_begin(c, 5, L.cells_prob, 8.0 * (K + 3));
+      const double *xin = xin_field != kNoField ? kry_field(c, ln, xin_field) : nullptr;
+      launch_combine_dots(c->stream, (int)L.span_chunks.size(), L.d_span_chunks.p,
+                          kry_vec(c, ln, xslot), c->kry_a.p, kry_vec(c, ln, vslot),
+                          std::max<long long>(1, L.n0), K, c->kry_coef.p, L.w.p,
+                          L.kry_partial.p, L.d_prob_span_begin.p, np, c->active.p,
+                          c->kry_dots.p, xin);
+      prof_end(c, pi);
+   }
+   dots.resize((size_t)np * KT);
+   CUDA_CHECK(cudaMemcpyAsync(dots.data(), c->kry_dots.p, (size_t)np * KT * sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
+   CUDA_CHECK(cudaStreamSynchronize(c->stream));
+   return true;
+}
+
 // Run body() through a CUDA graph captured on first use (eager when graphs
 // are off or the context traces / profiles).
 template <class Body>
@@ -2852,22 +2934,56 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                coef[(size_t)p * K + i] = -hi;
             }
          }
-         kry_combine(c, j + 1, a, 0, K, coef, &dots, FAC_TR);  // and ||W||^2
+         // W' = -TR - sum h_i V_i into slot j + 1 with <W', W'>; with the
+         // fused pass also the second-pass coefficients d_i = <W', V_i>
+         std::vector<double> nw(np, 0.0), d2;
+         const bool fused = kry_combine_dots(c, j + 1, a, 0, K, coef, d2, FAC_TR);
+         if (fused) {
+            for (int p = 0; p < np; ++p) nw[p] = d2[(size_t)p * (K + 1) + K];
+         } else {
+            kry_combine(c, j + 1, a, 0, K, coef, &dots, FAC_TR);
+            for (int p = 0; p < np; ++p) nw[p] = dots[p];
+         }
          bool again = false;
          std::vector<int> reo(np, 0);
          for (int p = 0; p < np; ++p)
-            if (act[p] && dots[p] < 0.25 * before[p]) reo[p] = again = true;
-         if (again) {
-            kry_dots(c, j + 1, 0, K, dots);
+            if (act[p] && nw[p] < 0.25 * before[p]) reo[p] = again = true;
+         // squared norm of V_{j+1} before its normalisation, and -d_i of the
+         // second pass (0 for the problems that need none)
+         std::vector<double> hn2(nw), dcoef((size_t)np * K, 0.0);
+         bool exact = again && !fused;
+         if (again && fused) {
             for (int p = 0; p < np; ++p) {
-               a[p] = 1.0;
+               if (!reo[p]) continue;
+               double s2 = 0.0;
                for (int i = 0; i < K; ++i) {
-                  const double d = reo[p] ? dots[(size_t)p * K + i] : 0.0;
+                  const double d = d2[(size_t)p * (K + 1) + i];
                   h[((size_t)p * H + i) * m + j] += d;
-                  coef[(size_t)p * K + i] = -d;
+                  dcoef[(size_t)p * K + i] = -d;
+                  s2 += d * d;
                }
+               // W' - sum d_i V_i is orthogonal to the V_i: its norm follows
+               // from ||W'|| and the d_i while these are small against W'
+               hn2[p] = nw[p] - s2;
+               if (!(hn2[p] > 0.5 * nw[p])) exact = true;
             }
-            kry_combine(c, j + 1, a, 0, K, coef, &dots);
+         }
+         if (exact) {
+            // second pass as its own combination, with the norm of the result
+            if (!fused) {
+               kry_dots(c, j + 1, 0, K, dots);
+               for (int p = 0; p < np; ++p)
+                  for (int i = 0; i < K; ++i) {
+                     const double d = reo[p] ? dots[(size_t)p * K + i] : 0.0;
+                     h[((size_t)p * H + i) * m + j] += d;
+                     dcoef[(size_t)p * K + i] = -d;
+                  }
+            }
+            std::fill(a.begin(), a.end(), 1.0);
+            kry_combine(c, j + 1, a, 0, K, dcoef, &dots);
+            for (int p = 0; p < np; ++p) hn2[p] = dots[p];
+            std::fill(dcoef.begin(), dcoef.end(), 0.0);
+            again = false;
          }
          for (int p = 0; p < np; ++p) {
             if (!act[p]) {
@@ -2875,7 +2991,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                continue;
             }
             double *hp = &h[(size_t)p * H * m];
-            const double hn = std::sqrt(std::max(0.0, dots[p]));
+            const double hn = std::sqrt(std::max(0.0, hn2[p]));
             hp[(size_t)(j + 1) * m + j] = hn;
             a[p] = hn > 0 ? 1.0 / hn : 0.0;
             // Givens rotations on column j
@@ -2900,8 +3016,16 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             c->hist[p].push_back(est);
             if (!(est > eff[p]) || its[p] >= c->max_cycles || !(hn > 0)) act[p] = 0;
          }
-         // V_{j+1} = W / ||W||, also into R for the next preconditioning
-         kry_combine(c, j + 1, a, 0, 0, coef, nullptr, kNoField, FAC_R);
+         // V_{j+1} = (W' - sum d_i V_i) / ||.||, the second Gram-Schmidt pass
+         // and the normalisation in one combination, also into R for the
+         // next preconditioning
+         if (again) {
+            for (int p = 0; p < np; ++p)
+               for (int i = 0; i < K; ++i) dcoef[(size_t)p * K + i] *= a[p];
+            kry_combine(c, j + 1, a, 0, K, dcoef, nullptr, kNoField, FAC_R);
+         } else {
+            kry_combine(c, j + 1, a, 0, 0, coef, nullptr, kNoField, FAC_R);
+         }
          set_active(c, act);
          c->host_active = act;
       }
@@ -3447,7 +3571,8 @@ int fac_set_fused_residual(fac_ctx *ctx, int on)
 {
    return guarded([&] {
       if (!ctx) throw FacError(FAC_ERR_ARG, "null context");
-      ctx->fused_residual = on != 0;
+      if (on < -1 || on > 1) throw FacError(FAC_ERR_ARG, "fused residual setting must be -1, 0 or 1");
+      ctx->fused_residual = on;
       ctx->drop_graph();
    });
 }

@@ -24,7 +24,8 @@ constexpr int kProlongRatioMax = 16;
 struct PatchDesc {
    int lo[3], hi[3];
    int prob;           // problem index within the context
-   int flags;          // bit0: has coarse-fine boundary faces
+   int flags;          // bit0: has coarse-fine boundary faces; bit1: has faces
+                       // that take a coarsened finer-level flux
    // ceil(2^32 / nx), ceil(2^32 / ny) for the cell decode of a linear
    // index (exact while cells * max(nx, ny) < 2^32); 0: divide instead
    unsigned mx, my;
@@ -55,6 +56,9 @@ struct WorkReg {
    const Chunk *all;
    Chunk *list;
    const int *pcb;
+   // lists not in problem order (the staged units, largest first): the
+   // problem of every entry; the compaction keeps the order (pcb unused)
+   const int *prob;
    int n;
    int pad;
 };

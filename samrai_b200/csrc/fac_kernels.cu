@@ -688,6 +688,8 @@ k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict_
       const int ny = p.hi[1] - p.lo[1] + 1;
       const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
       const bool has_cf = (p.flags & 1) != 0;
+      // faces taking a coarsened finer-level flux exist on this patch
+      const bool has_fc = fcmask && (p.flags & 2) != 0;
       const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
       const TU *up = u + p.off1;
       const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
@@ -700,32 +702,52 @@ k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict_
          const int sx = li + (nx + 1) * (lj + ny * lk);
          const int sy = li + nx * (lj + (ny + 1) * lk);
          const int sz = li + nx * (lj + ny * lk);
+         // every face's loads are issued before any test of a mask: the
+         // plain fluxes first, then the Ewing fix on coarse-fine faces, then
+         // the coarsened finer-level fluxes over the faces that take them
          double fl[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+         double dd[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
          for (int a = 0; a < DIM; ++a) {
-            const int la = a == 0 ? li : (a == 1 ? lj : lk);
-            const int na = a == 0 ? nx : (a == 1 ? ny : nz);
             const int st = a == 0 ? 1 : (a == 1 ? gx : gxy);
             const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
             const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
                const long long si = sbase + (s ? sup : 0);
-               if (fcmask && fcmask[si]) {
-                  fl[a][s] = fcflux[si];
-                  continue;
-               }
                const double d = DVAR ? dside[si] : dconst;
                const double ulo = s ? uc : (double)up[c - st];
                const double uhi = s ? (double)up[c + st] : uc;
-               double v = dai[a] * d * (uhi - ulo);
-               if (has_cf && (s ? la == na - 1 : la == 0)) {
+               dd[a][s] = d;
+               fl[a][s] = dai[a] * d * (uhi - ulo);
+            }
+         }
+         if (has_cf) {
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) {
+               const int la = a == 0 ? li : (a == 1 ? lj : lk);
+               const int na = a == 0 ? nx : (a == 1 ? ny : nz);
+#pragma unroll
+               for (int s = 0; s < 2; ++s) {
+                  if (!(s ? la == na - 1 : la == 0)) continue;
                   const int i = p.lo[0] + li, j = p.lo[1] + lj;
                   const int k = DIM == 3 ? p.lo[2] + lk : 0;
                   if (cfmask[oidx(p, a, s, i, j, k)])
-                     v = ewing_face<DIM, TU>(p, u, a, s, i, j, k, v, d, w, ratio_to_coarser);
+                     fl[a][s] = ewing_face<DIM, TU>(p, u, a, s, i, j, k, fl[a][s], dd[a][s], w,
+                                                    ratio_to_coarser);
                }
-               fl[a][s] = v;
+            }
+         }
+         if (has_fc) {
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) {
+               const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
+               const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
+#pragma unroll
+               for (int s = 0; s < 2; ++s) {
+                  const long long si = sbase + (s ? sup : 0);
+                  if (fcmask[si]) fl[a][s] = fcflux[si];
+               }
             }
          }
          const long long c0 = p.off0 + lin;
@@ -1431,6 +1453,37 @@ k_compact(const WorkReg *__restrict__ regs, const int *__restrict__ active, int 
 {
    const WorkReg r = regs[blockIdx.x];
    const int p = blockIdx.y;
+   if (r.prob) {
+      // a list in its own order: one block keeps the order of the active
+      // problems' entries (a straight copy when every problem is active)
+      if (p != 0) return;
+      int all = 1;
+      for (int q = threadIdx.x; q < nprob; q += blockDim.x) all &= active[q] != 0;
+      if (__syncthreads_and(all)) {
+         for (int t = threadIdx.x; t < r.n; t += blockDim.x) r.list[t] = r.all[t];
+         return;
+      }
+      __shared__ int wsum[kThreads / 32];
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      int base = 0;
+      for (int t0 = 0; t0 < r.n; t0 += blockDim.x) {
+         const int t = t0 + threadIdx.x;
+         const bool keep = t < r.n && active[r.prob[t]] != 0;
+         const unsigned m = __ballot_sync(0xffffffffu, keep);
+         if (lane == 0) wsum[wid] = __popc(m);
+         __syncthreads();
+         int off = base, tot = 0;
+         for (int q = 0; q < kThreads / 32; ++q) {
+            if (q < wid) off += wsum[q];
+            tot += wsum[q];
+         }
+         if (keep) r.list[off + __popc(m & ((1u << lane) - 1u))] = r.all[t];
+         base += tot;
+         __syncthreads();
+      }
+      for (int t = base + threadIdx.x; t < r.n; t += blockDim.x) r.list[t] = Chunk{-1, 0, 0, 0};
+      return;
+   }
    int before = 0;
    for (int q = threadIdx.x; q < p; q += blockDim.x)
       if (active[q]) before += r.pcb[q + 1] - r.pcb[q];
@@ -1587,6 +1640,68 @@ k_combine(const Chunk *__restrict__ chunks, int nwork, double *x, const double *
    }
 }
 
+// x = a[p] xin + sum_i coef[p * K + i] V_i as k_combine (the same terms in
+// the same order), and in the same pass partial[chunk * (K + 1) + i] = sum
+// over the chunk of w x V_i of the new x, entry K being <x, x>: the
+// multi-dot of the new vector against the vectors it was formed from,
+// accumulated exactly as k_multidot<true> accumulates it (the same cells per
+// thread in the same order, the same warp tree, warps in order), so the
+// second Gram-Schmidt pass needs no multi-dot pass of its own.  The K vector
+// values of a cell stay in registers between the combination and the
+// products (K <= KB); the coefficients sit in shared memory.
+template <int KB>
+__global__ void __launch_bounds__(kThreads)
+k_combine_dots(const Chunk *__restrict__ chunks, int nwork, double *x, const double *xin,
+               const double *__restrict__ a, const double *__restrict__ V, long long vstride,
+               int K, const double *__restrict__ coef, const double *__restrict__ w,
+               double *__restrict__ partial)
+{
+   if (!xin) xin = x;
+   __shared__ double red[KB + 1][kThreads / 32];
+   __shared__ double scoef[KB];
+   const int KT = K + 1;
+   WORK_LOOP(ch) {
+      if ((int)threadIdx.x < K) scoef[threadIdx.x] = coef[(long long)ch.patch * K + threadIdx.x];
+      __syncthreads();
+      const double ap = a[ch.patch];
+      double sum[KB + 1];
+#pragma unroll
+      for (int q = 0; q <= KB; ++q) sum[q] = 0.0;
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         const long long c = (long long)ch.begin + t;
+         double vv[KB];
+#pragma unroll
+         for (int q = 0; q < KB; ++q) vv[q] = q < K ? V[(long long)q * vstride + c] : 0.0;
+         double v = ap * xin[c];
+#pragma unroll
+         for (int q = 0; q < KB; ++q)
+            if (q < K) v = v + scoef[q] * vv[q];
+         x[c] = v;
+         const double wx = w[c] * v;
+#pragma unroll
+         for (int q = 0; q < KB; ++q)
+            if (q < K) sum[q] += wx * vv[q];
+         sum[KB] += wx * v;
+      }
+#pragma unroll
+      for (int q = 0; q <= KB; ++q) {
+         if (q < K || q == KB) {
+            double b = sum[q];
+            for (int o = 16; o > 0; o >>= 1) b += __shfl_down_sync(0xffffffffu, b, o);
+            if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = b;
+         }
+      }
+      __syncthreads();
+      if ((int)threadIdx.x < KT) {
+         const int q = (int)threadIdx.x < K ? (int)threadIdx.x : KB;
+         double b = 0.0;
+         for (int r = 0; r < (int)(blockDim.x >> 5); ++r) b += red[q][r];
+         partial[(long long)ch.aux * KT + threadIdx.x] = b;
+      }
+      __syncthreads();
+   }
+}
+
 // dst (ghost-0, FP64) = src interior (ghost-1)
 template <int DIM, class TS>
 __global__ void __launch_bounds__(kThreads)
@@ -1723,6 +1838,32 @@ void launch_combine_norm(cudaStream_t s, int nchunks, const Chunk *chunks, doubl
    g_launches.fetch_add(1, std::memory_order_relaxed);
    k_multidot_reduce<<<dim3(nprob, 1), kThreads, 0, s>>>(partial, prob_chunk_begin, 1, active,
                                                          out);
+}
+
+bool launch_combine_dots(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
+                         const double *a, const double *V, long long vstride, int K,
+                         const double *coef, const double *w, double *partial,
+                         const int *prob_chunk_begin, int nprob, const int *active, double *out,
+                         const double *xin)
+{
+   if (K < 1 || K > kCombineDotsMax) return false;
+   if (nchunks > 0) {
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      if (K <= 8)
+         k_combine_dots<8><<<work_grid(k_combine_dots<8>, nchunks), kThreads, 0, s>>>(
+            chunks, nchunks, x, xin, a, V, vstride, K, coef, w, partial);
+      else if (K <= 16)
+         k_combine_dots<16><<<work_grid(k_combine_dots<16>, nchunks), kThreads, 0, s>>>(
+            chunks, nchunks, x, xin, a, V, vstride, K, coef, w, partial);
+      else
+         k_combine_dots<kCombineDotsMax>
+            <<<work_grid(k_combine_dots<kCombineDotsMax>, nchunks), kThreads, 0, s>>>(
+               chunks, nchunks, x, xin, a, V, vstride, K, coef, w, partial);
+   }
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   k_multidot_reduce<<<dim3(nprob, K + 1), kThreads, 0, s>>>(partial, prob_chunk_begin, K + 1,
+                                                             active, out);
+   return true;
 }
 
 template <class TS>

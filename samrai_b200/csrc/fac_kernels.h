@@ -50,6 +50,18 @@ void launch_combine_norm(cudaStream_t s, int nchunks, const Chunk *chunks, doubl
                          const double *coef, const double *w, double *partial,
                          const int *prob_chunk_begin, int nprob, const int *active, double *out,
                          const double *xin = nullptr);
+// Largest K of launch_combine_dots.
+constexpr int kCombineDotsMax = 24;
+// x = a[p] xin + sum_i coef[p*K+i] V_i as launch_combine, and out[p*(K+1)+i]
+// += <x, V_i> for i < K, out[p*(K+1)+K] += <x, x> (weighted, the new x) over
+// problem p's chunks of this level: the numbers of launch_multidot(x, V, K,
+// self_dot) after the combination, from the same pass.  Returns false
+// (nothing launched) unless 1 <= K <= kCombineDotsMax.
+bool launch_combine_dots(cudaStream_t s, int nchunks, const Chunk *chunks, double *x,
+                         const double *a, const double *V, long long vstride, int K,
+                         const double *coef, const double *w, double *partial,
+                         const int *prob_chunk_begin, int nprob, const int *active, double *out,
+                         const double *xin = nullptr);
 // dst (ghost-0) = interior of src (ghost-1), converted to FP64
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,

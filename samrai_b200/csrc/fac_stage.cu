@@ -385,8 +385,16 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
    unsigned long long *never_bar = reinterpret_cast<unsigned long long *>(
       smem + 2 * kStageDepthMax * 8 + sizeof(StageBases));
    unsigned char *stages = smem + kBarrierBytes;
-   // the list holds active problems only (compacted), so the units of this
-   // block are w = blockIdx.x, + gridDim.x, ... up to the end marker
+   // the list holds active problems only (compacted), largest units first;
+   // unit k of this block is entry k G + b in even rounds and k G + G-1-b in
+   // odd ones (G blocks, b this block): a snake, so that the blocks that
+   // take the larger unit of one round take the smaller of the next.  The
+   // walk ends at the first end marker (patch < 0) or past the list: later
+   // rounds lie wholly after it.
+   auto unit_at = [&](int k) {
+      const int b = (k & 1) ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+      return k * (int)gridDim.x + b;
+   };
    auto valid = [&](int w) { return w < nwork && chunks[w].patch >= 0; };
    if (threadIdx.x == 0) {
       for (int k = 0; k < depth; ++k) {
@@ -402,11 +410,11 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
    if (warp == kConsumerWarps) {
       // producer warp: lane i issues copy i of a unit (the host-built copy
       // list, header first; its first entry carries the byte total)
-      int w = blockIdx.x;
+      int w = unit_at(0);
       Chunk ch = w < nwork ? chunks[w] : Chunk{-1, 0, 0, 0};
       int k = 0;  // units issued
       for (; ch.patch >= 0; ++k) {
-         const int wn = w + gridDim.x;
+         const int wn = unit_at(k + 1);
          const Chunk chn = wn < nwork ? chunks[wn] : Chunk{-1, 0, 0, 0};  // prefetch
          UnitCopy cp = {0, 0, 0, 0, 0};
          if (lane < ch.count) cp = copies[ch.begin + lane];
@@ -438,9 +446,9 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
    }
    const int tid = threadIdx.x;  // 0 .. kConsumers-1
    int k = 0;
-   bool cur = valid(blockIdx.x);
-   for (int w = blockIdx.x; cur; w += gridDim.x, ++k) {
-      const bool nxt = valid(w + gridDim.x);  // prefetched, used at the loop end
+   bool cur = valid(unit_at(0));
+   for (; cur; ++k) {
+      const bool nxt = valid(unit_at(k + 1));  // prefetched, used at the loop end
       const int st = k % depth;
       const unsigned par = (k / depth) & 1;
       unsigned char *stage = stages + st * stage_bytes;

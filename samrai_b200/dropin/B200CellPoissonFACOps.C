@@ -144,7 +144,7 @@ void B200CellPoissonFACOps::initializeOperatorState(
                          spec.dIsConstant() ? spec.getDConstant() : 1.0, ckind,
                          ckind == 1 ? spec.getCConstant() : 0.0),
          "fac_set_poisson");
-   check(fac_set_params(d_ctx, 1, 0.0, -1.0, 1, 1, this->*member(CoarseTolTag()),
+   check(fac_set_params(d_ctx, 1, 1e-300, -1.0, 1, 1, this->*member(CoarseTolTag()),
                         this->*member(CoarseMaxTag()), 1),
          "fac_set_params");
    int problem = 0;
@@ -456,7 +456,7 @@ int B200CellPoissonFACOps::solveCoarsestLevel(solv::SAMRAIVectorReal<double> &er
    sync_bc();
    // the coarse-solver setters may have changed the settings since the
    // operator state was made
-   check(fac_set_params(d_ctx, 1, 0.0, -1.0, 1, 1, this->*member(CoarseTolTag()),
+   check(fac_set_params(d_ctx, 1, 1e-300, -1.0, 1, 1, this->*member(CoarseTolTag()),
                         this->*member(CoarseMaxTag()), 1),
          "fac_set_params");
    upload(error, 0, FAC_E);

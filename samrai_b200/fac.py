@@ -386,6 +386,8 @@ class FacContext:
         self.stage_depth = int(depth)
 
     def set_fused_residual(self, on=True):
+        """One-pass composite residual: True on every level, False on none,
+        -1 (the default) on the levels of large patches."""
         _check(load_library().fac_set_fused_residual(self.h, int(on)))
 
     def set_learned(self, net, level):

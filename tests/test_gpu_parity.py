@@ -385,3 +385,26 @@ def test_fgmres_matches_fac_solution(case, precision, require_gpu):
     assert conv_f.all() and conv_k.all(), (its_f, res_f, its_k, res_k)
     assert (its_k <= its_f).all(), (its_k, its_f)
     assert _rel_l2(uk, uf) <= 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("mk", [configs.config1, configs.config3])
+def test_fgmres_matches_oracle_solution(mk, precision, require_gpu):
+    """FGMRES(20) around the FAC cycle, on the hierarchy extended by fully
+    covered coarser levels, converges to the oracle's solution of the
+    original hierarchy: both solved to 1e-12 relative residual, the
+    solutions agree to 1e-9 relative L2 over the original levels (the
+    converged-solution bar of the mixed-precision method)."""
+    p = mk()
+    x = configs.extend_hierarchy(p, k=3)
+    g = fac.FacContext([x], params=dict(coarse_tol=1e-300, coarse_max_it=20, max_cycles=100,
+                                        relative_residual_tol=1e-12), precision=precision)
+    conv, its, res = g.solve_fgmres(20)
+    k = x.virtual_levels
+    uk = [g.download(U, 0, ln + k) for ln in range(p.nlev)]
+    g.close()
+    assert conv[0], (its, res)
+    op = Oracle(p, params=dict(coarse_tol=1e-12, relative_residual_tol=1e-12))
+    assert op.solve()[0]
+    assert _rel_l2(uk, [op.get(U, ln) for ln in range(p.nlev)]) <= 1e-9
