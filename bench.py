@@ -324,6 +324,49 @@ class CpuReference:
         self.pool.join()
 
 
+def regrid_measure(ctx, probs, target=0.02):
+    """The regrid step on the finest level of every problem after the
+    solve: device tagging of the solution by the adaption estimate
+    (fac_tag_gradient) and Berger-Rigoutsos clustering of each problem's
+    tags within its level's bounding box (fac_cluster_tags: device
+    histograms, host decisions; min box 4, efficiency 0.8, combine 0.8).
+    The threshold is the one that tags about `target` of the cells (found
+    by bisection before the timing).  Wall time of one tagging plus the
+    clustering of every problem, synchronised."""
+    ln = ctx.nlev - 1
+    cells = sum(int(np.prod(p.levels[-1].boxes[:, 3:] - p.levels[-1].boxes[:, :3] + 1, axis=1).sum())
+                for p in probs)
+    lo_t, hi_t = 0.0, 1.0
+    while ctx.tag_gradient(fac.U, ln, hi_t).sum() > target * cells:
+        hi_t *= 4.0
+    for _ in range(24):
+        mid = 0.5 * (lo_t + hi_t)
+        if ctx.tag_gradient(fac.U, ln, mid).sum() > target * cells:
+            lo_t = mid
+        else:
+            hi_t = mid
+    thr = hi_t
+    bounds = []
+    for p in probs:
+        b = p.levels[-1].boxes
+        bounds.append([[int(b[:, 0].min()), int(b[:, 1].min()), int(b[:, 2].min()),
+                        int(b[:, 3].max()), int(b[:, 4].max()), int(b[:, 5].max())]])
+    ctx.tag_gradient(fac.U, ln, thr)  # warm-up
+    for i in range(len(probs)):
+        ctx.cluster_tags(i, ln, bounds[i], (4, 4, 4))
+    t0 = time.perf_counter()
+    tags = ctx.tag_gradient(fac.U, ln, thr)
+    nbox = 0
+    for i in range(len(probs)):
+        nbox += len(ctx.cluster_tags(i, ln, bounds[i], (4, 4, 4)))
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"ms": round(ms, 2), "level": "finest", "cells": cells, "tagged": int(tags.sum()),
+            "boxes": nbox, "threshold": thr,
+            "what": "fac_tag_gradient (AdaptivePoisson adaption estimate > threshold) and "
+                    "fac_cluster_tags (Berger-Rigoutsos, min box 4, efficiency 0.8, combine "
+                    "0.8) of every problem's finest level, wall time"}
+
+
 def cpu_small_solves(names=("c1", "c3")):
     """Full plain FAC solves of the small 2-D configurations on one core,
     measured, not scaled: the reference's own CellPoissonFACSolver
@@ -366,6 +409,8 @@ def main():
                     help="write the plain variant's cycle count per seed to PATH (JSON)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-regrid", dest="regrid", action="store_false",
+                    help="skip the regrid-step measurement (tagging and clustering)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the headline (multigrid-extended) variant")
     ap.add_argument("--smoother-only", type=int, default=0, metavar="SWEEPS",
@@ -575,6 +620,7 @@ def main():
                  "mg_vs_plain_rel_l2_max": max(diffs) if diffs else None}
         pctx.close()
 
+    regrid = regrid_measure(ctx, probs) if args.regrid else None
     peak, peak_kind = measured_peaks()
     achieved = rb_bytes / (rb_ms * 1e-3) / 1e9 if rb_ms > 0 else 0.0
     out = {
@@ -635,6 +681,7 @@ def main():
         "fp64_multigrid": fp64_mg,
         "stationary_fac": fac_only,
         "plain_fp64": plain,
+        "regrid": regrid,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -109,7 +109,12 @@ int fac_set_poisson(fac_ctx *ctx, int d_variable, double d_const,
  * 0..2*dim-1 (solv/RobinBcCoefStrategy.h; Dirichlet a=1,b=0 as
  * SimpleCellRobinBcCoefs::setBcCoefs, SimpleCellRobinBcCoefs.C:283-290).
  * May be called again after fac_initialize; later operations use the new
- * coefficients. */
+ * coefficients.  Once coefficients are set (here or by fac_set_bc_faces)
+ * the solves leave the physical-boundary ghost cells of u as their last
+ * fill leaves them, as CellPoissonFACSolver does with a caller's
+ * RobinBcCoefStrategy; without them (the solver's own Dirichlet object) the
+ * solves put back the ghost values u had (cacheDirichletData /
+ * restoreDirichletData, CellPoissonFACSolver.C:327-349). */
 int fac_set_bc(fac_ctx *ctx, const double *a, const double *b,
                const double *g);
 /* Robin coefficients that vary along the boundary, as a
@@ -147,8 +152,11 @@ int fac_set_fused(fac_ctx *ctx, int on);
 /* 1 (default): on levels where the fused pass is used, sweeps with a fixed
  * count (every sweep except the coarsest-level solve to a tolerance) run on
  * shared-memory staged units: TMA bulk copies bring a run of slices of one
- * patch into shared memory, the colour pass runs there and a bulk store
- * writes the slices back.  Results are bit-identical to 0. */
+ * patch into shared memory, the colour pass runs there and the new values
+ * go back to HBM.  The composite residuals inside the solves run staged the
+ * same way (fluxes and residual from the staged slices, then the cells on
+ * coarse-fine faces and next to finer-level faces redone by a fix-up pass).
+ * Results are bit-identical to 0. */
 int fac_set_staged(fac_ctx *ctx, int on);
 
 /* 1: the composite residual forms the face fluxes while it sums
@@ -451,6 +459,39 @@ int fac_vec_max_norm(fac_ctx *ctx, int fid, double *norms);
  * x or y).  RMS norm: fac_rms_norm. */
 int fac_vec_linear_sum(fac_ctx *ctx, int fid_z, const double *a, int fid_x,
                        const double *b, int fid_y);
+
+/* ---- regrid step: tagging and Berger-Rigoutsos clustering (the step
+ *      before FAC in an adaptive run: mesh/GriddingAlgorithm.C's tagging
+ *      and box generation).
+ * fac_tag_gradient tags the cells of level ln of every problem where the
+ * adaption estimate of the ghosted FP64 field fid (FAC_U or FAC_E) exceeds
+ * threshold: the estimate of source/test/FAC_adaptive/AdaptivePoisson.C:
+ * 622-720 (largest |u(+) + u(-) - 2u| along the axes, half of it along the
+ * face diagonals; ghost cells read as they are, so fill them first) and
+ * its threshold test (applyGradientDetector, :517-527).  ntagged (host,
+ * one per problem, may be NULL) gets the counts.  The tags stay on the
+ * device (fac_download_tags: one byte per cell, ghost-0 layout). */
+int fac_tag_gradient(fac_ctx *ctx, int fid, int ln, double threshold, long long *ntagged);
+int fac_download_tags(fac_ctx *ctx, int problem, int ln, unsigned char *host);
+/* Boxes covering the tags of level ln of one problem inside each of the
+ * nbound bound boxes (lo0 lo1 lo2 hi0 hi1 hi2 in the level's index space),
+ * as mesh::BergerRigoutsos::findBoxesContainingTags
+ * (mesh/BergerRigoutsos.C:251-420, BergerRigoutsosNode.C) forms them on one
+ * process: tag histograms per node (on the device, one launch per tree
+ * depth), the tags' bounding box, acceptance when the tagged fraction
+ * reaches efficiency (efficiency_tolerance) or no direction can be cut
+ * without a side below min_box, else a cut at the zero swath nearest the
+ * middle or at the strongest inflection of the histogram, and recombination
+ * of two accepted children whose cells are at least combine (combine_
+ * efficiency) of their parent's.  max_box (0 per axis: none) is
+ * max_box_size; the other input keys at the reference's defaults.  The
+ * product of two histogram Laplacians is formed in 64 bits (the reference
+ * uses int, which overflows only for planes of more than ~11,600 tags).
+ * Up to cap boxes go to boxes (6 ints each) in depth-first order; nboxes
+ * gets their number. */
+int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *bound,
+                     const int *min_box, const int *max_box, double efficiency,
+                     double combine, int cap, int *boxes, int *nboxes);
 
 /* ---- allocation-free norm.  No counterpart in the reference.
  *

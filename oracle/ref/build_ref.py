@@ -10,9 +10,9 @@ the configure step and the compilers would:
 1. SAMRAI_config.h from the reference's template for a serial build
    (mkconfig.py) and an include tree whose SAMRAI/<pkg> entries link to the
    reference's source directories;
-2. every .C unit of tbox, hier, pdat, geom, xfer, math and solv compiled
-   with g++ (the four template-implementation units that headers include
-   are skipped);
+2. every .C unit of tbox, hier, pdat, geom, xfer, math, solv, mesh and
+   appu compiled with g++ (the four template-implementation units that
+   headers include are skipped);
 3. the Fortran kernels those packages call: the m4 templates expanded
    (m4lite.py, as cmake/SetupM4.cmake runs m4) and every routine of the
    kernel files translated to C (f77c.py), compiled with gcc;
@@ -20,7 +20,11 @@ the configure step and the compilers would:
    the FAC path never calls (complex data, other centerings);
 5. fac_ref_driver.C linked with all of it: oracle/_ref/fac_ref_driver;
    and, when the CUDA library is built, the same driver on the drop-in
-   operators (samrai_b200/dropin): oracle/_ref/fac_dropin_driver.
+   operators (samrai_b200/dropin): oracle/_ref/fac_dropin_driver;
+6. br_ref_driver.C (tagging and Berger-Rigoutsos clustering) linked with
+   the same objects and the reference's FAC_adaptive test problem
+   (source/test/FAC_adaptive, all but its main.C), whose adaption estimate
+   it calls: oracle/_ref/br_ref_driver.
 
 Nothing is copied from the reference into the repository: the generated
 files and objects live under oracle/_ref/, which git ignores.  Everything is
@@ -36,7 +40,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(os.path.dirname(HERE), "_ref")
-PKGS = ["tbox", "hier", "pdat", "geom", "xfer", "math", "solv"]
+PKGS = ["tbox", "hier", "pdat", "geom", "xfer", "math", "solv", "mesh", "appu"]
 SKIP = {"pdat/ArrayDataOperationUtilities.C", "pdat/CopyOperation.C", "pdat/SumOperation.C",
         "tbox/MathUtilities.C"}
 CXXFLAGS = ["-std=c++11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-w"]
@@ -157,19 +161,19 @@ def symbols(objs, defined):
     return out
 
 
-def stubs(objs):
+def stubs(objs, name="stubs"):
     """abort() stubs for Fortran symbols (lower case, one trailing
     underscore) referenced but defined nowhere."""
     und = symbols(objs, False) - symbols(objs, True)
     f77 = sorted(s for s in und if re.fullmatch(r"[a-z][a-z0-9]*_", s))
     gen = os.path.join(OUT, "gen")
-    src = os.path.join(gen, "stubs.c")
+    src = os.path.join(gen, name + ".c")
     with open(src, "w") as fh:
         fh.write("/* Fortran routines the FAC path never calls. */\n#include <stdio.h>\n"
                  "#include <stdlib.h>\n")
         for s in f77:
             fh.write(f'void {s}(void) {{ fprintf(stderr, "{s} not built\\n"); abort(); }}\n')
-    obj = os.path.join(gen, "stubs.o")
+    obj = os.path.join(gen, name + ".o")
     run(["gcc", *CFLAGS, "-c", src, "-o", obj])
     print(f"build_ref: {len(f77)} Fortran symbols stubbed", flush=True)
     return obj
@@ -196,7 +200,33 @@ def main():
     run(["g++", "-o", exe, drv_obj, *objs, kobj, sobj, "-lm"])
     print(f"build_ref: {exe}", flush=True)
     dropin(inc, objs + [kobj, sobj])
+    br_driver(a.ref, inc, objs + [kobj], a.jobs)
     return 0
+
+
+def br_driver(ref, inc, objs, jobs):
+    """br_ref_driver: the reference's AdaptivePoisson tagging and its
+    BergerRigoutsos box generator on one level."""
+    tdir = os.path.join(ref, "source", "test", "FAC_adaptive")
+    odir = os.path.join(OUT, "obj", "FAC_adaptive")
+    os.makedirs(odir, exist_ok=True)
+    flags = [*CXXFLAGS, "-I" + inc, "-I" + tdir]
+    work, tobjs = [], []
+    for f in sorted(os.listdir(tdir)):
+        if not f.endswith(".C") or f == "main.C":
+            continue
+        src, obj = os.path.join(tdir, f), os.path.join(odir, f[:-2] + ".o")
+        tobjs.append(obj)
+        if newer(src, obj):
+            work.append((src, obj))
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        list(ex.map(lambda j: run(["g++", *flags, "-c", j[0], "-o", j[1]]), work))
+    drv_obj = os.path.join(OUT, "obj", "br_ref_driver.o")
+    run(["g++", *flags, "-c", os.path.join(HERE, "br_ref_driver.C"), "-o", drv_obj])
+    sobj = stubs(objs + tobjs + [drv_obj], name="br_stubs")
+    exe = os.path.join(OUT, "br_ref_driver")
+    run(["g++", "-o", exe, drv_obj, *tobjs, *objs, sobj, "-lm"])
+    print(f"build_ref: {exe}", flush=True)
 
 
 def dropin(inc, objs):

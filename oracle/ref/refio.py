@@ -12,6 +12,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DRIVER = os.path.join(os.path.dirname(HERE), "_ref", "fac_ref_driver")
+BR_DRIVER = os.path.join(os.path.dirname(HERE), "_ref", "br_ref_driver")
 
 
 def write(path, recs):
@@ -96,4 +97,31 @@ def run_reference(prob, params, bc=None, driver=DRIVER, timeout=3600, solution=T
         r = subprocess.run([driver, fin, fout], capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"fac_ref_driver failed ({r.returncode}): {r.stderr[-2000:]}")
+        return read(fout)
+
+
+def run_br(prob, threshold, bound, min_box, max_box, efficiency, combine, driver=BR_DRIVER,
+           timeout=600):
+    """Tag level 0 of `prob` (u from prob.u0[0]) by the reference's
+    AdaptivePoisson estimate and cluster the tags with its BergerRigoutsos
+    (oracle/_ref/br_ref_driver); returns the driver's records (tags, boxes,
+    seconds)."""
+    dim = prob.dim
+    pad = [1] * (3 - dim)
+    recs = [("dim", [dim]),
+            ("n0", np.array(list(prob.n0[:dim]) + pad, dtype=np.int32)),
+            ("boxes", np.asarray(prob.levels[0].boxes, dtype=np.int32).reshape(-1)),
+            ("xlo", np.array(list(prob.xlo[:dim]) + [0.0] * (3 - dim))),
+            ("xup", np.array(list(prob.xup[:dim]) + [1.0] * (3 - dim))),
+            ("u", prob.u0[0]), ("threshold", [float(threshold)]),
+            ("bound", np.asarray(bound, dtype=np.int32).reshape(-1)),
+            ("min_box", np.array(list(min_box[:dim]) + pad, dtype=np.int32)),
+            ("max_box", np.array(list(max_box[:dim]) + [0] * (3 - dim), dtype=np.int32)),
+            ("efficiency", [float(efficiency)]), ("combine", [float(combine)])]
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        write(fin, recs)
+        r = subprocess.run([driver, fin, fout], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"br_ref_driver failed ({r.returncode}): {r.stderr[-2000:]}")
         return read(fout)

@@ -17,7 +17,7 @@ OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libsamrai_fac_b200.so")
 
 SOURCES = ["fac_kernels.cu", "fac_stage.cu", "fac_host.cu", "fac_cnn.cu", "fac_noalloc.cu",
-           "fac_xfer.cu"]
+           "fac_xfer.cu", "fac_regrid.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-Wall"]

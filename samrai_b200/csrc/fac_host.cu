@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
+#include <climits>
+#include <limits>
 #include <map>
 #include <cmath>
 #include <cstdio>
@@ -191,7 +193,6 @@ struct DevArray {
 struct WorkSrc {
    DevArray<Chunk> all;
    DevArray<int> pcb;
-   DevArray<int> prob;  // per entry, for lists not in problem order
 };
 
 template <class I>
@@ -332,6 +333,21 @@ struct LevelState {
    DevArray<unsigned char> d_hdrs[2];
    WorkSrc ws_units[2];
    int unit_smem[2] = {0, 0};
+   // staged composite residual: units per ResKind (largest first) and
+   // their largest shared memory (0: the level runs the unstaged kernels)
+   std::vector<Chunk> runits[kResKinds];
+   DevArray<Chunk> d_runits[kResKinds];
+   DevArray<UnitCopy> d_rcopies[kResKinds];
+   DevArray<unsigned char> d_rhdrs[kResKinds];
+   WorkSrc ws_runits[kResKinds];
+   int runit_smem[kResKinds] = {0, 0, 0};
+   // cells the staged residual leaves to the fix-up pass
+   std::vector<CellRef> rfix;
+   DevArray<CellRef> d_rfix;
+   // host copies of cfmask and fcmask
+   std::vector<unsigned char> cfmask_h, fcmask_h;
+   // regrid step: tags of the level's cells (ghost-0 layout), allocated on first use
+   DevArray<unsigned char> tag;
    DevArray<int> d_ratio;
 
    // work chunks
@@ -396,6 +412,10 @@ struct fac_ctx {
    int use_graph = 1;        // capture one FAC cycle into a CUDA graph and replay it
    int fused = 1;            // colour passes read across patch faces directly
    int staged = 1;           // fused passes on shared-memory staged units
+   // coefficients came from fac_set_bc / fac_set_bc_faces (a caller's
+   // RobinBcCoefStrategy): the solves leave the boundary ghost values of u
+   // as their last fill leaves them instead of restoring them
+   bool bc_object = false;
    // residual kernels form the fluxes on the fly: 1 on every level, 0 on
    // none, -1 on the levels of large patches (fused_residual_on)
    int fused_residual = -1;
@@ -422,6 +442,7 @@ struct fac_ctx {
    int kry_m = 0;
    DevArray<double> kry_dots, kry_coef, kry_a;
    DevArray<double> vec_coef;  // per-problem scalars of fac_vec_linear_sum
+   DevArray<unsigned long long> tag_counts;  // per-problem tag counts
    int krylov = 0;  // > 0: fac_solve runs FGMRES(krylov) around the FAC cycle
    // fac_set_coarse_extension: domain-covering coarser levels added below
    // every problem's level 0, and whether their coefficients need to be
@@ -879,6 +900,7 @@ void build_cf_faces(fac_ctx *c, int ln)
    L.cf.clear();
    if (ln == 0) {
       L.cfmask.upload(mask, c->stream);
+      L.cfmask_h = mask;
       return;
    }
    for (int ip = 0; ip < L.npatch; ++ip) {
@@ -945,6 +967,7 @@ void build_cf_faces(fac_ctx *c, int ln)
          }
    }
    L.cfmask.upload(mask, c->stream);
+   L.cfmask_h = mask;
    L.d_cf.upload(L.cf, c->stream);
 }
 
@@ -1104,13 +1127,6 @@ void build_stage_units(fac_ctx *c, int ln)
          }
          if (s0 != nslow) throw FacError(FAC_ERR_ARG, "staged units do not tile the patch");
       }
-      // largest units first: the blocks walk the list in a snake order
-      // (k_rb_staged), so every block ends with the small units and the
-      // blocks' totals come out nearly equal (the pass has no tail of a few
-      // blocks still working on large units)
-      std::stable_sort(U.begin(), U.end(), [&](const Chunk &a, const Chunk &b) {
-         return copies[a.begin].total > copies[b.begin].total;
-      });
       // stage_depth stages per CTA after the barriers and copy sources; a
       // level whose units do not fit runs the unstaged pass
       L.unit_smem[t] =
@@ -1123,6 +1139,196 @@ void build_stage_units(fac_ctx *c, int ln)
       if (!hdrs.empty()) std::memcpy(raw.data(), hdrs.data(), raw.size());
       L.d_hdrs[t].upload(raw, c->stream);
    }
+}
+
+// Units of the staged composite residual, one list per ResKind: every
+// patch cut along its slowest axis into runs of slices whose plan fits the
+// stage budget (one slice at least), header and bulk-copy list per unit as
+// for the colour pass.
+void build_res_units(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   const bool dvar = c->spec.d_variable != 0, cvar = c->spec.c_kind == 2;
+   struct HdrRec {
+      ResHdr h;
+      char pad[kStageHeader - sizeof(ResHdr)];
+   };
+   static_assert(sizeof(HdrRec) == kStageHeader, "header record size");
+   for (int kind = 0; kind < kResKinds; ++kind) {
+      const int tu = kind == kResF32 ? 4 : 8;
+      const bool hasf = kind != kResF64Zero;
+      std::vector<Chunk> &U = L.runits[kind];
+      std::vector<UnitCopy> copies;
+      std::vector<HdrRec> hdrs;
+      U.clear();
+      int maxb = 0;
+      bool decode_ok = true;
+      for (int ip = 0; ip < L.npatch; ++ip) {
+         const Box &b = L.box[ip];
+         const PatchDesc &d = L.hp[ip];
+         const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+         const int nslow = dim == 3 ? b.hi[2] - b.lo[2] + 1 : ny;
+         const long long g1 = dim == 3 ? (long long)(nx + 2) * (ny + 2) : nx + 2;
+         const long long g0 = dim == 3 ? (long long)nx * ny : nx;
+         auto bytes = [&](int ns) { return res_plan(dim, nx, ny, ns, tu, hasf, dvar, cvar).bytes; };
+         int nsmax = 1;
+         while (nsmax < nslow && bytes(nsmax + 1) <= c->stage_budget) ++nsmax;
+         const int nunit = (nslow + nsmax - 1) / nsmax;
+         const int base = nslow / nunit, rem = nslow % nunit;
+         int s0 = 0;
+         for (int u = 0; u < nunit; ++u) {
+            const int ns = base + (u < rem ? 1 : 0);
+            const StagePlan sp = res_plan(dim, nx, ny, ns, tu, hasf, dvar, cvar);
+            maxb = std::max(maxb, sp.bytes);
+            HdrRec rec;
+            std::memset(&rec, 0, sizeof(rec));
+            ResHdr &h = rec.h;
+            for (int a = 0; a < 3; ++a) {
+               h.lo[a] = d.lo[a];
+               h.hi[a] = d.hi[a];
+               // the reciprocal the kernels would form: an IEEE division
+               h.dxi[a] = 1.0 / d.dx[a];
+               for (int sd = 0; sd < 2; ++sd) h.offo[a][sd] = a < dim ? d.offo[a][sd] : 0;
+            }
+            h.s0 = s0;
+            h.ns = ns;
+            h.ncells = (int)(g0 * ns);
+            h.has_oflux = ln > 0 ? 1 : 0;
+            h.mnx = (unsigned)(((1ull << 32) + nx - 1) / nx);
+            h.mny = (unsigned)(((1ull << 32) + ny - 1) / ny);
+            // exact magic divisions: cells by nx, rows by ny (3-D)
+            const long long lim = 1ll << 32;
+            if ((long long)h.ncells * nx >= lim || (long long)ny * ns * ny >= lim)
+               decode_ok = false;
+            h.off0s = d.off0 + (long long)s0 * g0;
+            h.off_u = h.off_f = h.off_c = -1;
+            for (int a = 0; a < 3; ++a) h.off_d[a] = -1;
+            const int first = (int)copies.size();
+            copies.push_back({(long long)hdrs.size() * kStageHeader, kSrcHdr, kStageHeader, 0, 0});
+            long long total = kStageHeader;
+            for (int r = 0; r < sp.nreg; ++r) {
+               // region r: u, then f (hasf), then D per axis (dvar), then C (cvar)
+               int q = r;
+               int what;  // 0 u, 1 f, 2.. D axis, 5 C
+               if (q == 0) what = 0;
+               else if (hasf && q == 1) what = 1;
+               else {
+                  q -= hasf ? 2 : 1;
+                  what = dvar && q < dim ? 2 + q : 5;
+               }
+               int src;
+               long long e0, limit;
+               if (what == 0) {
+                  src = kSrcU;
+                  e0 = d.off1 + (long long)s0 * g1;
+                  limit = std::min<long long>(L.n1, d.off1 + cell_count(dim, b, 1));
+               } else if (what == 1 || what == 5) {
+                  src = what == 1 ? kSrcF : kSrcC;
+                  e0 = d.off0 + (long long)s0 * g0;
+                  limit = std::min<long long>(L.n0, d.off0 + b.size());
+               } else {
+                  const int a = what - 2;
+                  const long long per =
+                     dim == 3 ? (a == 0 ? (long long)(nx + 1) * ny
+                                        : (a == 1 ? (long long)nx * (ny + 1) : g0))
+                              : (a == 0 ? nx + 1 : nx);
+                  src = kSrcD;
+                  e0 = d.offs[a] + (long long)s0 * per;
+                  limit = std::min<long long>(L.ns, d.offs[a] + side_box(b, a).size());
+               }
+               if (e0 < 0 || e0 + sp.count[r] > limit)
+                  throw FacError(FAC_ERR_ARG, "residual unit outside its patch arrays");
+               const long long b0 = e0 * sp.esize[r], b1 = b0 + sp.count[r] * sp.esize[r];
+               const long long a0 = b0 & ~15ll, a1 = (b1 + 15) & ~15ll;
+               const int off = sp.off[r] + (int)(b0 - a0);
+               if (what == 0) h.off_u = off;
+               else if (what == 1) h.off_f = off;
+               else if (what == 5) h.off_c = off;
+               else h.off_d[what - 2] = off;
+               copies.push_back({a0, src, (int)(a1 - a0), sp.off[r], 0});
+               total += a1 - a0;
+            }
+            copies[first].total = (int)total;
+            U.push_back({ip, first, (int)copies.size() - first, (int)hdrs.size()});
+            hdrs.push_back(rec);
+            s0 += ns;
+         }
+         if (s0 != nslow) throw FacError(FAC_ERR_ARG, "residual units do not tile the patch");
+      }
+      L.runit_smem[kind] =
+         decode_ok && kStageBarrierBytes + (long long)c->stage_depth * maxb <= kStageSmemMax
+            ? maxb
+            : 0;
+      L.d_runits[kind].upload(U, c->stream);
+      L.d_rcopies[kind].upload(copies, c->stream);
+      std::vector<unsigned char> raw(hdrs.size() * kStageHeader);
+      if (!hdrs.empty()) std::memcpy(raw.data(), hdrs.data(), raw.size());
+      L.d_rhdrs[kind].upload(raw, c->stream);
+   }
+}
+
+// Cells whose residual the staged pass leaves to the fix-up pass, each once
+// in patch order: a cell on a coarse-fine face of the level (the Ewing fix
+// changes that face's flux) and a cell next to a face that takes a
+// coarsened finer-level flux -- exactly the faces k_residual_fused treats
+// apart (patch flags bit 0 with cfmask, bit 1 with fcmask).
+void build_residual_fixups(fac_ctx *c, int ln)
+{
+   LevelState &L = c->L[ln];
+   const int dim = c->dim;
+   L.rfix.clear();
+   std::vector<unsigned char> mark;
+   for (int ip = 0; ip < L.npatch; ++ip) {
+      const PatchDesc &d = L.hp[ip];
+      if (!(d.flags & 3)) continue;
+      const int n[3] = {d.hi[0] - d.lo[0] + 1, d.hi[1] - d.lo[1] + 1,
+                        dim == 3 ? d.hi[2] - d.lo[2] + 1 : 1};
+      mark.assign((size_t)n[0] * n[1] * n[2], 0);
+      auto cell = [&](const int *x) { return x[0] + (long long)n[0] * (x[1] + (long long)n[1] * x[2]); };
+      if ((d.flags & 1) && !L.cfmask_h.empty()) {
+         for (int a = 0; a < dim; ++a) {
+            // outer-side layout: tangential axes t0 (fastest) and t1
+            const int t0 = a == 0 ? 1 : 0, t1 = a == 2 ? 1 : 2;
+            const int m0 = n[t0], m1 = dim == 3 ? n[t1] : 1;
+            for (int sd = 0; sd < 2; ++sd)
+               for (int q1 = 0; q1 < m1; ++q1)
+                  for (int q0 = 0; q0 < m0; ++q0) {
+                     const long long o = d.offo[a][sd] + q0 + (long long)m0 * q1;
+                     if (o < 0 || o >= (long long)L.cfmask_h.size())
+                        throw FacError(FAC_ERR_ARG, "coarse-fine mask index");
+                     if (!L.cfmask_h[o]) continue;
+                     int x[3] = {0, 0, 0};
+                     x[a] = sd ? n[a] - 1 : 0;
+                     x[t0] = q0;
+                     if (dim == 3) x[t1] = q1;
+                     mark[cell(x)] = 1;
+                  }
+         }
+      }
+      if ((d.flags & 2) && !L.fcmask_h.empty()) {
+         for (int a = 0; a < dim; ++a) {
+            const int e0 = n[0] + (a == 0), e1 = n[1] + (a == 1), e2 = n[2] + (dim == 3 && a == 2);
+            for (int k = 0; k < e2; ++k)
+               for (int j = 0; j < e1; ++j)
+                  for (int i = 0; i < e0; ++i) {
+                     const long long si = d.offs[a] + i + (long long)e0 * (j + (long long)e1 * k);
+                     if (si < 0 || si >= (long long)L.fcmask_h.size())
+                        throw FacError(FAC_ERR_ARG, "finer-flux mask index");
+                     if (!L.fcmask_h[si]) continue;
+                     int x[3] = {i, j, k};
+                     if (x[a] < n[a]) mark[cell(x)] = 1;  // the cell above the face
+                     if (x[a] > 0) {                      // and the one below
+                        --x[a];
+                        mark[cell(x)] = 1;
+                     }
+                  }
+         }
+      }
+      for (size_t q = 0; q < mark.size(); ++q)
+         if (mark[q]) L.rfix.push_back({ip, (int)q});
+   }
+   L.d_rfix.upload(L.rfix, c->stream);
 }
 
 // Same-level neighbour of every face cell of every patch (fused colour
@@ -1396,6 +1602,7 @@ void build_coarsen_tables(fac_ctx *c, int ln)
       C.hp[it.coarse_patch].flags |= 2;
    }
    C.fcmask.upload(fm, c->stream);
+   C.fcmask_h = std::move(fm);
 }
 
 // Coarse interpolation arrays for prolongation into level ln
@@ -1799,28 +2006,7 @@ void register_work(fac_ctx *c, WorkSrc &ws, const std::vector<Chunk> &chunks, Ch
       throw FacError(FAC_ERR_STATE, "work list registered before its upload");
    ws.all.upload(chunks, c->stream);
    ws.pcb.upload(pcb, c->stream);
-   if (!chunks.empty())
-      c->work_regs.push_back({ws.all.p, list, ws.pcb.p, nullptr, (int)chunks.size(), 0});
-}
-
-// A work list in an order of its own (not by problem): the compaction keeps
-// that order over the entries of the active problems.
-template <class ProbOf>
-void register_work_ordered(fac_ctx *c, WorkSrc &ws, const std::vector<Chunk> &chunks,
-                           Chunk *list, ProbOf prob_of)
-{
-   const int np = nprob(c);
-   std::vector<int> prob(std::max<size_t>(1, chunks.size()), 0);
-   for (size_t q = 0; q < chunks.size(); ++q) {
-      prob[q] = prob_of(chunks[q]);
-      if (prob[q] < 0 || prob[q] >= np) throw FacError(FAC_ERR_ARG, "work list problem");
-   }
-   if (!chunks.empty() && !list && !g_dry)
-      throw FacError(FAC_ERR_STATE, "work list registered before its upload");
-   ws.all.upload(chunks, c->stream);
-   ws.prob.upload(prob, c->stream);
-   if (!chunks.empty())
-      c->work_regs.push_back({ws.all.p, list, nullptr, ws.prob.p, (int)chunks.size(), 0});
+   if (!chunks.empty()) c->work_regs.push_back({ws.all.p, list, ws.pcb.p, (int)chunks.size(), 0});
 }
 
 template <class I>
@@ -1852,7 +2038,9 @@ void register_work_lists(fac_ctx *c)
       if (L.gather_tmp.ok) register_items(c, L.gather_tmp.bc);
       register_items(c, L.prolong);
       for (int t = 0; t < 2; ++t)
-         register_work_ordered(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
+         register_work(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
+      for (int k = 0; k < kResKinds; ++k)
+         register_work(c, L.ws_runits[k], L.runits[k], L.d_runits[k].p, pp);
    }
    c->d_work_regs.upload(c->work_regs, c->stream);
 }
@@ -1929,6 +2117,10 @@ void initialize(fac_ctx *c)
       if (ln > 0) build_prolong_tables(c, ln);
    }
    for (int ln = 0; ln + 1 < c->nlev; ++ln) build_coarsen_tables(c, ln);
+   for (int ln = 0; ln < c->nlev; ++ln) {
+      build_res_units(c, ln);
+      build_residual_fixups(c, ln);
+   }
    validate_tables(c);
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
@@ -2067,6 +2259,14 @@ bool fused_residual_on(const fac_ctx *c, int ln)
    return L.npatch > 0 && L.n0 >= kFusedResidualCells * (long long)L.npatch;
 }
 
+// The staged residual (TMA-staged units, then the fix-up of the special
+// cells) runs wherever the staged passes are on and the level's units fit
+// the shared memory; it gives the same bits as the other two forms.
+bool staged_residual_on(const fac_ctx *c, int ln, int kind)
+{
+   return c->staged && c->L[ln].runit_smem[kind] > 0 && !c->L[ln].runits[kind].empty();
+}
+
 void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int error_eq)
 {
    OpTimer ot(c, "comp_residual", ln);
@@ -2075,8 +2275,10 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
    ghost_fill(c, fid_u, ln, ln > 0, error_eq, run);
    const double *u = field_ptr(L, fid_u);
    const bool finer = ln < c->nlev - 1;
-   const bool fused = fused_residual_on(c, ln);
-   if (!fused) {
+   const int kind = fid_f == kFieldZero ? kResF64Zero : kResF64;
+   const bool staged = staged_residual_on(c, ln, kind);
+   const bool fused = !staged && fused_residual_on(c, ln);
+   if (!staged && !fused) {
       launch_flux_cells(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
                         L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
                         L.d_ratio.p, L.flux.p, run);
@@ -2091,16 +2293,28 @@ void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int erro
                           L.fcoarsen.nchunks(), L.fcoarsen.d_prefix.p, Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
-   if (fused)
+   if (staged) {
+      launch_res_staged<double>(c->stream, c->dim, c->spec, (int)L.runits[kind].size(),
+                                L.runit_smem[kind], c->stage_depth, L.d_runits[kind].p,
+                                L.d_rcopies[kind].p, L.d_rhdrs[kind].p, u,
+                                field_ptr(L, fid_f), L.d.p, L.c.p, field_ptr(L, fid_r),
+                                ln > 0 ? L.oflux.p : nullptr, c->kerr.p, c->wait_test);
+      launch_residual_cells<double>(c->stream, c->dim, c->spec, (int)L.rfix.size(), L.d_rfix.p,
+                                    L.d_patches.p, u, L.d.p, L.cfmask.p, L.tranwt, L.longwt,
+                                    L.d_ratio.p, finer ? L.fcmask.p : nullptr, L.flux.p,
+                                    field_ptr(L, fid_f), L.c.p, field_ptr(L, fid_r),
+                                    ln > 0 ? L.oflux.p : nullptr, run);
+   } else if (fused) {
       launch_residual_fused(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                             L.d_patches.p, L.d_cell_chunks.p, u, L.d.p, L.cfmask.p, L.tranwt,
                             L.longwt, L.d_ratio.p, finer ? L.fcmask.p : nullptr, L.flux.p,
                             field_ptr(L, fid_f), L.c.p, field_ptr(L, fid_r),
                             ln > 0 ? L.oflux.p : nullptr, run);
-   else
+   } else {
       launch_residual(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(), L.d_patches.p,
                       L.d_cell_chunks.p, u, field_ptr(L, fid_f), L.flux.p, L.c.p,
                       field_ptr(L, fid_r), ln > 0 ? L.oflux.p : nullptr, run);
+   }
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -2240,8 +2454,13 @@ void zero_field(fac_ctx *c, int fid)
    }
 }
 
+// CellPoissonFACSolver::solveSystem with the solver's own boundary object
+// (CellPoissonFACSolver.C:327-349): the physical-boundary ghost values of u
+// are cached before the solve and put back after it.  With a caller's
+// coefficient object the reference does neither.
 void dirichlet(fac_ctx *c, bool restore)
 {
+   if (c->bc_object) return;
    for (int ln = 0; ln < c->nlev; ++ln) {
       LevelState &L = c->L[ln];
       const long long n = (long long)L.dir_idx.size();
@@ -2333,8 +2552,9 @@ void comp_residual_mixed(fac_ctx *c, int ln)
    const int *run = c->active.p;
    ghost_fill32(c, ln, ln > 0, 1, run);
    const bool finer = ln < c->nlev - 1;
-   const bool fused = fused_residual_on(c, ln);
-   if (!fused) {
+   const bool staged = staged_residual_on(c, ln, kResF32);
+   const bool fused = !staged && fused_residual_on(c, ln);
+   if (!staged && !fused) {
       launch_flux_cells<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                                L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
                                L.tranwt, L.longwt, L.d_ratio.p, L.flux.p, run);
@@ -2349,16 +2569,28 @@ void comp_residual_mixed(fac_ctx *c, int ln)
                           L.fcoarsen.nchunks(), L.fcoarsen.d_prefix.p, Fl.d_patches.p, L.d_patches.p, Fl.oflux.p,
                           L.flux.p, run);
    }
-   if (fused)
+   if (staged) {
+      launch_res_staged<float>(c->stream, c->dim, c->spec, (int)L.runits[kResF32].size(),
+                               L.runit_smem[kResF32], c->stage_depth, L.d_runits[kResF32].p,
+                               L.d_rcopies[kResF32].p, L.d_rhdrs[kResF32].p, L.e32.p, L.r.p,
+                               L.d.p, L.c.p, L.tr.p, ln > 0 ? L.oflux.p : nullptr, c->kerr.p,
+                               c->wait_test);
+      launch_residual_cells<float>(c->stream, c->dim, c->spec, (int)L.rfix.size(), L.d_rfix.p,
+                                   L.d_patches.p, L.e32.p, L.d.p, L.cfmask.p, L.tranwt,
+                                   L.longwt, L.d_ratio.p, finer ? L.fcmask.p : nullptr,
+                                   L.flux.p, L.r.p, L.c.p, L.tr.p,
+                                   ln > 0 ? L.oflux.p : nullptr, run);
+   } else if (fused) {
       launch_residual_fused<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                                    L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.d.p, L.cfmask.p,
                                    L.tranwt, L.longwt, L.d_ratio.p,
                                    finer ? L.fcmask.p : nullptr, L.flux.p, L.r.p, L.c.p, L.tr.p,
                                    ln > 0 ? L.oflux.p : nullptr, run);
-   else
+   } else {
       launch_residual<float>(c->stream, c->dim, c->spec, (int)L.cell_chunks.size(),
                              L.d_patches.p, L.d_cell_chunks.p, L.e32.p, L.r.p, L.flux.p, L.c.p,
                              L.tr.p, ln > 0 ? L.oflux.p : nullptr, run);
+   }
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -3390,6 +3622,411 @@ int fac_vec_linear_sum(fac_ctx *ctx, int fid_z, const double *a, int fid_x, cons
    });
 }
 
+// ---------------------------------------------------------------------------
+// regrid step: tagging and Berger-Rigoutsos clustering
+// ---------------------------------------------------------------------------
+
+int fac_tag_gradient(fac_ctx *ctx, int fid, int ln, double threshold, long long *ntagged)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, ln);
+      if (field_ghost(fid) != 1 || fid == FAC_W)
+         throw FacError(FAC_ERR_ARG, "tagging reads a ghosted FP64 cell field (U or E)");
+      vec_all_active(ctx);
+      LevelState &L = ctx->L[ln];
+      const int np = nprob(ctx);
+      if (L.tag.n != (size_t)std::max<long long>(1, L.n0))
+         L.tag.alloc(std::max<long long>(1, L.n0));
+      ctx->tag_counts.alloc(np);
+      CUDA_CHECK(cudaMemsetAsync(ctx->tag_counts.p, 0, np * sizeof(unsigned long long),
+                                 ctx->stream));
+      launch_adaption_tags(ctx->stream, ctx->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                           L.d_cell_chunks.p, field_ptr(L, fid), threshold, L.tag.p,
+                           ctx->tag_counts.p, nullptr);
+      CUDA_CHECK(cudaGetLastError());
+      std::vector<unsigned long long> cnt(np);
+      CUDA_CHECK(cudaMemcpyAsync(cnt.data(), ctx->tag_counts.p, np * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      if (ntagged)
+         for (int p = 0; p < np; ++p) ntagged[p] = (long long)cnt[p];
+   });
+}
+
+int fac_download_tags(fac_ctx *ctx, int problem, int ln, unsigned char *host)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (!host) throw FacError(FAC_ERR_ARG, "null output");
+      LevelState &L = ctx->L[ln];
+      if (!L.tag.p) throw FacError(FAC_ERR_STATE, "no tags on this level (fac_tag_gradient)");
+      const long long off = L.prob_off0[problem], n = L.prob_off0[problem + 1] - off;
+      CUDA_CHECK(cudaMemcpyAsync(host, L.tag.p + off, (size_t)n, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+   });
+}
+
+namespace {
+
+// One node of the clustering tree (BergerRigoutsosNode on one process).
+struct BrTree {
+   int lo[3], hi[3];          // box (after the shrink to the tags' bounding box)
+   int left = -1, right = -1;
+   int state = 0;             // 1 accepted, 2 split, 3 no tag
+   std::vector<int> h[3];     // histograms of the (shrunken) box
+};
+
+// C integer division (toward zero), as the reference's int arithmetic
+inline int cdiv(int a, int b) { return a / b; }
+
+struct BrParams {
+   int dim;
+   int min_box[3], max_box[3];
+   double efficiency, combine;
+};
+
+// findZeroCutSwath (mesh/BergerRigoutsosNode.C:1636-1700)
+bool zero_cut(const BrParams &P, const BrTree &n, int a, int &cut_lo, int &cut_hi)
+{
+   const int lo = n.lo[a], hi = n.hi[a];
+   const int lim_lo = lo + P.min_box[a], lim_hi = hi - P.min_box[a];
+   const std::vector<int> &h = n.h[a];
+   cut_lo = cut_hi = cdiv(lo + hi, 2);
+   while (cut_lo >= lim_lo && cut_hi <= lim_hi) {
+      if (h[cut_lo - lo] == 0) {
+         cut_hi = cut_lo;
+         while (cut_lo > lim_lo && h[cut_lo - lo - 1] == 0) --cut_lo;
+         return true;
+      }
+      if (h[cut_hi - lo] == 0) {
+         cut_lo = cut_hi;
+         while (cut_hi < lim_hi && h[cut_hi - lo + 1] == 0) ++cut_hi;
+         return true;
+      }
+      --cut_lo;
+      ++cut_hi;
+   }
+   return false;
+}
+
+// cutAtInflection (mesh/BergerRigoutsosNode.C:1718-1812), with the
+// reference's defaults DEV_max_inflection_cut_from_center = 1 and
+// DEV_min_box_size_from_cutting = 0; the product of the two Laplacians is
+// formed in 64 bits (its sign is what the reference tests)
+void inflection_cut(const BrParams &P, const BrTree &n, int a, int &cut_pt, int &inflection)
+{
+   const std::vector<int> &h = n.h[a];
+   const int size = (int)h.size();
+   if (size < 4) {
+      cut_pt = 1;
+      for (int i = 2; i < size; ++i)
+         if (std::abs(h[cut_pt] - h[cut_pt - 1]) < std::abs(h[i] - h[i - 1])) cut_pt = i;
+      cut_pt += n.lo[a];
+      inflection = 0;
+      return;
+   }
+   const int min_size = std::max(P.min_box[a], 0);
+   const int box_lo = 0, box_hi = size - 1;
+   const int max_dist = (int)(1.0 * size / 2);
+   const int mid = cdiv(box_lo + box_hi + 1, 2);
+   const int lim_lo = std::max(box_lo + min_size, mid - max_dist);
+   const int lim_hi = std::min(box_hi - min_size + 1, mid + max_dist);
+   cut_pt = mid;
+   inflection = std::abs((h[cut_pt - 1] - 2 * h[cut_pt] + h[cut_pt + 1]) -
+                         (h[cut_pt - 2] - 2 * h[cut_pt - 1] + h[cut_pt]));
+   int cl = mid - 1, ch = mid + 1;
+   auto test = [&](int c) {
+      const int la = h[c - 1] - 2 * h[c] + h[c + 1];
+      const int lb = h[c - 2] - 2 * h[c - 1] + h[c];
+      if ((long long)la * (long long)lb <= 0) {
+         const int t = std::abs(la - lb);
+         if (t > inflection) {
+            cut_pt = c;
+            inflection = t;
+         }
+      }
+   };
+   while (cl > lim_lo || ch < lim_hi) {
+      if (cl > lim_lo) test(cl);
+      if (ch < lim_hi) test(ch);
+      --cl;
+      ++ch;
+   }
+   cut_pt += n.lo[a];
+}
+
+// computeMinimalBoundingBoxForTags + acceptOrSplitBox
+// (mesh/BergerRigoutsosNode.C:1251-1590) for a node whose histograms are
+// known: shrink, then accept (state 1), find no tags (3), or cut into the
+// children's boxes (state 2, boxes in lchild/rchild).
+void decide(const BrParams &P, BrTree &n, int lchild[6], int rchild[6])
+{
+   const int d = P.dim;
+   for (int a = 0; a < d; ++a) {
+      std::vector<int> &h = n.h[a];
+      int size = n.hi[a] - n.lo[a] + 1, b = 0, e = (int)h.size() - 1;
+      while (h[b] == 0 && size > P.min_box[a]) {
+         ++n.lo[a];
+         ++b;
+         --size;
+      }
+      while (h[e] == 0 && size > P.min_box[a]) {
+         --n.hi[a];
+         --e;
+         --size;
+      }
+      h = std::vector<int>(h.begin() + b, h.begin() + e + 1);
+   }
+   int dims[3] = {1, 1, 1};
+   long long size = 1;
+   for (int a = 0; a < d; ++a) {
+      dims[a] = n.hi[a] - n.lo[a] + 1;
+      size *= dims[a];
+   }
+   bool over = false;
+   for (int a = 0; a < d; ++a) over = over || dims[a] > P.max_box[a];
+   if (!over) {
+      long long tagged = 0;
+      for (int v : n.h[0]) tagged += v;
+      const double eff = size == 0 ? 1.0 : (double)tagged / (double)size;
+      if (eff >= P.efficiency) {
+         n.state = 1;
+         return;
+      }
+      if (tagged == 0) {
+         n.state = 3;
+         return;
+      }
+   }
+   int margin[3];
+   bool none = true;  // IntVector's < : no direction can be cut
+   for (int a = 0; a < d; ++a) {
+      margin[a] = dims[a] - 2 * P.min_box[a];
+      none = none && margin[a] < 0;
+   }
+   if (none) {
+      n.state = 1;
+      return;
+   }
+   int order[3] = {0, 1, 2};
+   for (int d0 = 0; d0 < d - 1; ++d0)
+      for (int d1 = d0 + 1; d1 < d; ++d1)
+         if (margin[order[d0]] < margin[order[d1]]) std::swap(order[d0], order[d1]);
+   int lft_hi[3] = {n.hi[0], n.hi[1], n.hi[2]}, rht_lo[3] = {n.lo[0], n.lo[1], n.lo[2]};
+   int cut_dir = 0, k = 0;
+   for (; k < d; ++k) {
+      cut_dir = order[k];
+      if (margin[cut_dir] < 0) continue;
+      int cl, ch;
+      if (zero_cut(P, n, cut_dir, cl, ch)) {
+         lft_hi[cut_dir] = cl - 1;
+         rht_lo[cut_dir] = ch + 1;
+         break;
+      }
+   }
+   if (k == d) {
+      // DEV_inflection_cut_threshold_ar = 0: only the direction(s) of the
+      // largest margin are cut
+      const int leave = dims[order[0]] - 1;
+      int inflection = -1, cut_pt = 0;
+      for (int a = 0; a < d; ++a) {
+         if (margin[a] < 0 || dims[a] <= leave) continue;
+         int cp, ti;
+         inflection_cut(P, n, a, cp, ti);
+         if (inflection < ti || (inflection == ti && margin[a] > margin[cut_dir])) {
+            cut_dir = a;
+            cut_pt = cp;
+            inflection = ti;
+         }
+      }
+      lft_hi[cut_dir] = cut_pt - 1;
+      rht_lo[cut_dir] = cut_pt;
+   }
+   for (int a = 0; a < 3; ++a) {
+      lchild[a] = n.lo[a];
+      lchild[3 + a] = lft_hi[a];
+      rchild[a] = rht_lo[a];
+      rchild[3 + a] = n.hi[a];
+   }
+   n.state = 2;
+}
+
+}  // namespace
+
+int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *bound,
+                     const int *min_box, const int *max_box, double efficiency, double combine,
+                     int cap, int *boxes, int *nboxes)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (nbound < 1 || !bound || !min_box || !max_box || !nboxes || (cap > 0 && !boxes))
+         throw FacError(FAC_ERR_ARG, "bad clustering arguments");
+      if (!(efficiency >= 0.0 && efficiency <= 1.0) || !(combine >= 0.0 && combine <= 1.0))
+         throw FacError(FAC_ERR_ARG, "efficiency and combine efficiency must lie in [0, 1]");
+      LevelState &L = ctx->L[ln];
+      if (!L.tag.p) throw FacError(FAC_ERR_STATE, "no tags on this level (fac_tag_gradient)");
+      const int d = ctx->dim;
+      BrParams P;
+      P.dim = d;
+      P.efficiency = efficiency;
+      P.combine = combine;
+      for (int a = 0; a < 3; ++a) {
+         P.min_box[a] = a < d ? min_box[a] : 1;
+         P.max_box[a] = a < d && max_box[a] > 0 ? max_box[a] : std::numeric_limits<int>::max();
+         if (a < d && P.min_box[a] < 1) throw FacError(FAC_ERR_ARG, "min_box must be >= 1");
+      }
+      // dense tag array over the bounding box of the problem's patches and
+      // the bound boxes (cells outside the patches hold no tags)
+      int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+      auto grow = [&](const int *blo, const int *bhi) {
+         for (int a = 0; a < 3; ++a) {
+            const int l = a < d ? blo[a] : 0, h = a < d ? bhi[a] : 0;
+            lo[a] = std::min(lo[a], l);
+            hi[a] = std::max(hi[a], h);
+         }
+      };
+      for (int ip = 0; ip < L.npatch; ++ip)
+         if (L.hp[ip].prob == problem) grow(L.hp[ip].lo, L.hp[ip].hi);
+      for (int b = 0; b < nbound; ++b) {
+         const int *bb = bound + 6 * b;
+         for (int a = 0; a < d; ++a)
+            if (bb[3 + a] < bb[a]) throw FacError(FAC_ERR_ARG, "empty bound box");
+         grow(bb, bb + 3);
+      }
+      int n[3];
+      long long cells = 1;
+      for (int a = 0; a < 3; ++a) {
+         n[a] = hi[a] - lo[a] + 1;
+         cells *= n[a];
+      }
+      DevArray<unsigned char> dense;
+      dense.alloc((size_t)cells);
+      CUDA_CHECK(cudaMemsetAsync(dense.p, 0, (size_t)cells, ctx->stream));
+      launch_tags_dense(ctx->stream, d, (int)L.cell_chunks.size(), L.d_patches.p,
+                        L.d_cell_chunks.p, L.tag.p, problem, lo, n, dense.p);
+      CUDA_CHECK(cudaGetLastError());
+      // breadth first over the tree: one histogram launch per depth
+      std::vector<BrTree> tree;
+      std::vector<int> roots, frontier;
+      for (int b = 0; b < nbound; ++b) {
+         BrTree t;
+         for (int a = 0; a < 3; ++a) {
+            t.lo[a] = a < d ? bound[6 * b + a] : 0;
+            t.hi[a] = a < d ? bound[6 * b + 3 + a] : 0;
+         }
+         roots.push_back((int)tree.size());
+         frontier.push_back((int)tree.size());
+         tree.push_back(t);
+      }
+      DevArray<BrNode> d_nodes;
+      DevArray<BrItem> d_items;
+      DevArray<int> d_hist;
+      while (!frontier.empty()) {
+         std::vector<BrNode> nodes;
+         std::vector<BrItem> items;
+         long long hsize = 0;
+         for (int q = 0; q < (int)frontier.size(); ++q) {
+            const BrTree &t = tree[frontier[q]];
+            BrNode nd;
+            int e[3];
+            for (int a = 0; a < 3; ++a) {
+               nd.lo[a] = t.lo[a];
+               nd.hi[a] = t.hi[a];
+               e[a] = t.hi[a] - t.lo[a] + 1;
+            }
+            if (e[0] > kBrThreads * kBrMaxXPerThread)
+               throw FacError(FAC_ERR_ARG, "clustering box too long along x");
+            nd.hoff = hsize;
+            hsize += e[0] + e[1] + e[2];
+            nodes.push_back(nd);
+            // runs of rows of at most ~64k cells per block
+            const int rows = e[1] * e[2];
+            const int per = std::max(1, 65536 / e[0]);
+            for (int r0 = 0; r0 < rows; r0 += per) items.push_back({q, r0, std::min(per, rows - r0), 0});
+         }
+         d_nodes.upload(nodes, ctx->stream);
+         d_items.upload(items, ctx->stream);
+         d_hist.alloc((size_t)std::max<long long>(1, hsize));
+         CUDA_CHECK(cudaMemsetAsync(d_hist.p, 0, (size_t)std::max<long long>(1, hsize) * sizeof(int),
+                                    ctx->stream));
+         launch_br_histogram(ctx->stream, (int)items.size(), d_items.p, d_nodes.p, dense.p, lo, n,
+                             d_hist.p);
+         CUDA_CHECK(cudaGetLastError());
+         std::vector<int> hist((size_t)std::max<long long>(1, hsize));
+         CUDA_CHECK(cudaMemcpyAsync(hist.data(), d_hist.p, hist.size() * sizeof(int),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+         std::vector<int> next;
+         for (int q = 0; q < (int)frontier.size(); ++q) {
+            const int id = frontier[q];
+            const BrNode &nd = nodes[q];
+            long long o = nd.hoff;
+            for (int a = 0; a < 3; ++a) {
+               const int e = nd.hi[a] - nd.lo[a] + 1;
+               if (a < d) tree[id].h[a].assign(hist.begin() + o, hist.begin() + o + e);
+               o += e;
+            }
+            int lc[6], rc[6];
+            decide(P, tree[id], lc, rc);
+            if (tree[id].state == 2) {
+               for (int side = 0; side < 2; ++side) {
+                  const int *cb = side ? rc : lc;
+                  BrTree t;
+                  for (int a = 0; a < 3; ++a) {
+                     t.lo[a] = cb[a];
+                     t.hi[a] = cb[3 + a];
+                  }
+                  (side ? tree[id].right : tree[id].left) = (int)tree.size();
+                  next.push_back((int)tree.size());
+                  tree.push_back(t);
+               }
+            }
+         }
+         frontier.swap(next);
+      }
+      // recombination, children before parents (runChildren_check,
+      // mesh/BergerRigoutsosNode.C:719-790)
+      auto box_size = [&](const BrTree &t) {
+         long long s = 1;
+         for (int a = 0; a < d; ++a) s *= t.hi[a] - t.lo[a] + 1;
+         return s;
+      };
+      for (int id = (int)tree.size() - 1; id >= 0; --id) {
+         BrTree &t = tree[id];
+         if (t.state != 2) continue;
+         const BrTree &l = tree[t.left], &r = tree[t.right];
+         bool fits = true;
+         for (int a = 0; a < d; ++a) fits = fits && t.hi[a] - t.lo[a] + 1 <= P.max_box[a];
+         const double reduction = (double)(box_size(l) + box_size(r)) / (double)box_size(t);
+         if (l.state == 1 && r.state == 1 && fits && reduction >= P.combine) t.state = 1;
+      }
+      // the accepted boxes, depth first, left before right
+      int count = 0;
+      std::vector<int> stack(roots.rbegin(), roots.rend());
+      while (!stack.empty()) {
+         const int id = stack.back();
+         stack.pop_back();
+         const BrTree &t = tree[id];
+         if (t.state == 1) {
+            if (count < cap)
+               for (int a = 0; a < 3; ++a) {
+                  boxes[6 * count + a] = t.lo[a];
+                  boxes[6 * count + 3 + a] = t.hi[a];
+               }
+            ++count;
+         } else if (t.state == 2) {
+            stack.push_back(t.right);
+            stack.push_back(t.left);
+         }
+      }
+      *nboxes = count;
+   });
+}
+
 int fac_ctx_create(fac_ctx **ctx, int dim, int device)
 {
    return guarded([&] {
@@ -3501,6 +4138,7 @@ int fac_set_bc(fac_ctx *ctx, const double *a, const double *b, const double *g)
          ctx->bc.b[l] = b[l];
          ctx->bc.g[l] = g[l];
       }
+      ctx->bc_object = true;
       // kernels take the coefficients by value: graphs captured with the
       // old ones are captured again
       ctx->drop_graph();
@@ -3543,7 +4181,10 @@ void set_stage_shape(fac_ctx *ctx, int bytes, int depth)
       CUDA_CHECK(cudaSetDevice(ctx->device));
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
       ctx->drop_graph();
-      for (int ln = 0; ln < ctx->nlev; ++ln) build_stage_units(ctx, ln);
+      for (int ln = 0; ln < ctx->nlev; ++ln) {
+         build_stage_units(ctx, ln);
+         build_res_units(ctx, ln);
+      }
       register_work_lists(ctx);
       launch_compact(ctx->stream, ctx->d_work_regs.p, (int)ctx->work_regs.size(),
                      ctx->active.p, nprob(ctx));
@@ -3675,6 +4316,7 @@ int fac_set_bc_faces(fac_ctx *ctx, int problem, int ln, int location, const doub
       ctx->bc.face_dom = ctx->face_dom_dev.p;
       ctx->bc.face_nprob = np;
       ctx->bc_faces = true;
+      ctx->bc_object = true;
       ctx->drop_graph();  // kernels take the coefficients by value
    });
 }
@@ -3976,13 +4618,18 @@ int fac_comp_residual(fac_ctx *ctx, int fid_r, int fid_u, int fid_f, int ln, int
       if (field_ghost(fid_u) != 1 || field_ghost(fid_r) != 0 || field_ghost(fid_f) != 0)
          throw FacError(FAC_ERR_ARG, "bad field kinds for the residual");
       // this entry point leaves the face fluxes in the flux side data, as
-      // the reference operator does; solves use the fused kernel
+      // the reference operator does; solves use the staged or fused kernels
       struct Restore {
          fac_ctx *c;
-         int v;
-         ~Restore() { c->fused_residual = v; }
-      } restore{ctx, ctx->fused_residual};
+         int v, st;
+         ~Restore()
+         {
+            c->fused_residual = v;
+            c->staged = st;
+         }
+      } restore{ctx, ctx->fused_residual, ctx->staged};
       ctx->fused_residual = 0;
+      ctx->staged = 0;
       comp_residual(ctx, fid_r, fid_u, fid_f, ln, error_equation ? 1 : 0);
       CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
    });

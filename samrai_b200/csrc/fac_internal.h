@@ -56,9 +56,6 @@ struct WorkReg {
    const Chunk *all;
    Chunk *list;
    const int *pcb;
-   // lists not in problem order (the staged units, largest first): the
-   // problem of every entry; the compaction keeps the order (pcb unused)
-   const int *prob;
    int n;
    int pad;
 };
@@ -297,6 +294,103 @@ struct UnitHdr {
    int off_push[6];        // per face id 2*axis+side: push targets, -1 if none
    int off_cff[6];         // Ewing fluxes of the same faces, -1 if none
 };
+
+// Shared-memory plan of one unit of the staged composite residual: the
+// 256-byte header, then u over the unit's slices and one slice either side
+// (ghosted rows, element size tu: FP64, or FP32 for the error of the mixed
+// cycle), f when the right-hand side is not zero, the side arrays of D and
+// C when variable (all FP64).
+FAC_HD inline StagePlan res_plan(int dim, int nx, int ny, int ns, int tu, bool hasf, bool dvar,
+                                 bool cvar)
+{
+   StagePlan sp;
+   const long long g1 = dim == 3 ? (long long)(nx + 2) * (ny + 2) : nx + 2;
+   const long long g0 = dim == 3 ? (long long)nx * ny : nx;
+   int r = 0;
+   sp.count[r] = (ns + 2) * g1;
+   sp.esize[r++] = tu;
+   if (hasf) {
+      sp.count[r] = ns * g0;
+      sp.esize[r++] = 8;
+   }
+   if (dvar) {
+      for (int a = 0; a < dim; ++a) {
+         long long n;
+         if (dim == 3) {
+            n = a == 0 ? (long long)ns * (nx + 1) * ny
+                       : (a == 1 ? (long long)ns * nx * (ny + 1) : (long long)(ns + 1) * nx * ny);
+         } else {
+            n = a == 0 ? (long long)ns * (nx + 1) : (long long)(ns + 1) * nx;
+         }
+         sp.count[r] = n;
+         sp.esize[r++] = 8;
+      }
+   }
+   if (cvar) {
+      sp.count[r] = ns * g0;
+      sp.esize[r++] = 8;
+   }
+   sp.nbase = sp.face0 = sp.cff0 = sp.nreg = r;
+   sp.nface = 0;
+   long long o = kStageHeader;
+   for (int k = 0; k < r; ++k) {
+      sp.off[k] = (int)o;
+      o += ((sp.count[k] * sp.esize[k] + 15) / 16) * 16 + 16;
+   }
+   for (int k = r; k < kStageMaxRegions; ++k) {
+      sp.off[k] = (int)o;
+      sp.count[k] = 0;
+      sp.esize[k] = 0;
+   }
+   sp.bytes = o > 0x3fffffff ? 0x3fffffff : (int)o;
+   return sp;
+}
+
+// Header of one unit of the staged residual.
+struct ResHdr {
+   int lo[3], hi[3];
+   int s0, ns;             // first slice (patch-relative) and slices of the unit
+   int ncells;             // cells of the unit, x fastest
+   int has_oflux;          // the level stores its patches' outer-side fluxes
+   unsigned mnx, mny;      // ceil(2^32 / d) for d = nx, ny (exact for q d < 2^32)
+   long long off0s;        // ghost-0 element of the unit's first cell
+   long long offo[3][2];   // outer-side flux arrays of the patch (axis, side)
+   double dxi[3];          // 1 / dx, FP64
+   int off_u, off_f, off_d[3], off_c;  // stage offsets of the regions (-1 none)
+};
+static_assert(sizeof(ResHdr) <= kStageHeader, "residual unit header");
+
+// Kinds of residual unit lists: the error or solution in FP64 with a
+// right-hand side, the same with a zero right-hand side (operator
+// application), the FP32 error of the mixed cycle with a right-hand side.
+enum ResKind : int { kResF64 = 0, kResF64Zero = 1, kResF32 = 2, kResKinds = 3 };
+
+// A cell of a patch (linear index x fastest) whose residual the staged pass
+// leaves to the fix-up pass: it has a coarse-fine face (Ewing) or a face
+// that takes a coarsened finer-level flux.
+struct CellRef {
+   int patch;
+   int lin;
+};
+
+// Berger-Rigoutsos node box on the device (3-D extents, 1 for unused axes)
+// and where its histograms start: x counts, then y, then z.
+struct BrNode {
+   int lo[3], hi[3];
+   long long hoff;
+};
+// A run of rows (along x) of one node box for one block of the histogram
+// kernel; rows are numbered y fastest, then z.
+struct BrItem {
+   int node;
+   int row0;
+   int nrows;
+   int pad;
+};
+// Block of the histogram kernel and x positions per thread: node boxes up
+// to kBrThreads * kBrMaxXPerThread cells along x.
+constexpr int kBrThreads = 256;
+constexpr int kBrMaxXPerThread = 4;
 
 // One bulk copy of a staged unit: nbytes (a multiple of 16) from byte
 // src_off (16-byte aligned) of source array src into the stage at dst_off.

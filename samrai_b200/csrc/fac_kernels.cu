@@ -671,6 +671,102 @@ k_residual(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
 // k_flux_coarsen put it, as the two-kernel sequence does.
 // ---------------------------------------------------------------------------
 
+// The residual of cell (li, lj, lk) of patch p (linear index lin) with its
+// fluxes formed on the spot; writes res and, where oflux is given, the
+// cell's patch-face fluxes.
+template <int DIM, bool DVAR, int CKIND, class TU>
+__device__ __forceinline__ void residual_cell(
+   const PatchDesc &p, int lin, int li, int lj, int lk, const double dai[3],
+   const TU *__restrict__ u, const double *__restrict__ dside, double dconst,
+   const unsigned char *__restrict__ cfmask, const EwingWeights &w, const int *ratio_to_coarser,
+   const unsigned char *__restrict__ fcmask, const double *__restrict__ fcflux,
+   const double *__restrict__ f, const double *__restrict__ cfield, double cconst,
+   double *__restrict__ res, double *__restrict__ oflux)
+{
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
+   const bool has_cf = (p.flags & 1) != 0;
+   // faces taking a coarsened finer-level flux exist on this patch
+   const bool has_fc = fcmask && (p.flags & 2) != 0;
+   const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
+   const TU *up = u + p.off1;
+   const int c = (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0);
+   const double uc = (double)up[c];
+   const int sx = li + (nx + 1) * (lj + ny * lk);
+   const int sy = li + nx * (lj + (ny + 1) * lk);
+   const int sz = li + nx * (lj + ny * lk);
+   // every face's loads are issued before any test of a mask: the plain
+   // fluxes first, then the Ewing fix on coarse-fine faces, then the
+   // coarsened finer-level fluxes over the faces that take them
+   double fl[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+   double dd[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+   for (int a = 0; a < DIM; ++a) {
+      const int st = a == 0 ? 1 : (a == 1 ? gx : gxy);
+      const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
+      const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+         const long long si = sbase + (s ? sup : 0);
+         const double d = DVAR ? dside[si] : dconst;
+         const double ulo = s ? uc : (double)up[c - st];
+         const double uhi = s ? (double)up[c + st] : uc;
+         dd[a][s] = d;
+         fl[a][s] = dai[a] * d * (uhi - ulo);
+      }
+   }
+   if (has_cf) {
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+         const int la = a == 0 ? li : (a == 1 ? lj : lk);
+         const int na = a == 0 ? nx : (a == 1 ? ny : nz);
+#pragma unroll
+         for (int s = 0; s < 2; ++s) {
+            if (!(s ? la == na - 1 : la == 0)) continue;
+            const int i = p.lo[0] + li, j = p.lo[1] + lj;
+            const int k = DIM == 3 ? p.lo[2] + lk : 0;
+            if (cfmask[oidx(p, a, s, i, j, k)])
+               fl[a][s] = ewing_face<DIM, TU>(p, u, a, s, i, j, k, fl[a][s], dd[a][s], w,
+                                              ratio_to_coarser);
+         }
+      }
+   }
+   if (has_fc) {
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+         const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
+         const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
+#pragma unroll
+         for (int s = 0; s < 2; ++s) {
+            const long long si = sbase + (s ? sup : 0);
+            if (fcmask[si]) fl[a][s] = fcflux[si];
+         }
+      }
+   }
+   const long long c0 = p.off0 + lin;
+   const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
+   double rv;
+   if (DIM == 2)
+      rv = f[c0] - (dai[0] * (fl[0][1] - fl[0][0]) + dai[1] * (fl[1][1] - fl[1][0])) - sf * uc;
+   else
+      rv = f[c0] - (dai[0] * (fl[0][1] - fl[0][0]) + dai[1] * (fl[1][1] - fl[1][0]) +
+                    dai[2] * (fl[2][1] - fl[2][0])) -
+           sf * uc;
+   res[c0] = rv;
+   if (oflux) {
+      const int i = p.lo[0] + li, j = p.lo[1] + lj, k = DIM == 3 ? p.lo[2] + lk : 0;
+      if (li == 0) oflux[oidx(p, 0, 0, i, j, k)] = fl[0][0];
+      if (li == nx - 1) oflux[oidx(p, 0, 1, i, j, k)] = fl[0][1];
+      if (lj == 0) oflux[oidx(p, 1, 0, i, j, k)] = fl[1][0];
+      if (lj == ny - 1) oflux[oidx(p, 1, 1, i, j, k)] = fl[1][1];
+      if (DIM == 3) {
+         if (lk == 0) oflux[oidx(p, 2, 0, i, j, k)] = fl[2][0];
+         if (lk == nz - 1) oflux[oidx(p, 2, 1, i, j, k)] = fl[2][1];
+      }
+   }
+}
+
 template <int DIM, bool DVAR, int CKIND, class TU>
 __global__ void __launch_bounds__(kThreads, 4)
 k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks,
@@ -686,94 +782,45 @@ k_residual_fused(const PatchDesc *__restrict__ patches, const Chunk *__restrict_
       if (run && !run[p.prob]) continue;
       const int nx = p.hi[0] - p.lo[0] + 1;
       const int ny = p.hi[1] - p.lo[1] + 1;
-      const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
-      const bool has_cf = (p.flags & 1) != 0;
-      // faces taking a coarsened finer-level flux exist on this patch
-      const bool has_fc = fcmask && (p.flags & 2) != 0;
-      const int gx = nx + 2, gxy = (nx + 2) * (ny + 2);
-      const TU *up = u + p.off1;
       const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const int lin = ch.begin + t;
          int li, lj, lk;
          patch_cell(p, lin, nx, ny, li, lj, lk);
-         const int c = (li + 1) + gx * (lj + 1) + (DIM == 3 ? gxy * (lk + 1) : 0);
-         const double uc = (double)up[c];
-         const int sx = li + (nx + 1) * (lj + ny * lk);
-         const int sy = li + nx * (lj + (ny + 1) * lk);
-         const int sz = li + nx * (lj + ny * lk);
-         // every face's loads are issued before any test of a mask: the
-         // plain fluxes first, then the Ewing fix on coarse-fine faces, then
-         // the coarsened finer-level fluxes over the faces that take them
-         double fl[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-         double dd[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll
-         for (int a = 0; a < DIM; ++a) {
-            const int st = a == 0 ? 1 : (a == 1 ? gx : gxy);
-            const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
-            const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
-#pragma unroll
-            for (int s = 0; s < 2; ++s) {
-               const long long si = sbase + (s ? sup : 0);
-               const double d = DVAR ? dside[si] : dconst;
-               const double ulo = s ? uc : (double)up[c - st];
-               const double uhi = s ? (double)up[c + st] : uc;
-               dd[a][s] = d;
-               fl[a][s] = dai[a] * d * (uhi - ulo);
-            }
-         }
-         if (has_cf) {
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) {
-               const int la = a == 0 ? li : (a == 1 ? lj : lk);
-               const int na = a == 0 ? nx : (a == 1 ? ny : nz);
-#pragma unroll
-               for (int s = 0; s < 2; ++s) {
-                  if (!(s ? la == na - 1 : la == 0)) continue;
-                  const int i = p.lo[0] + li, j = p.lo[1] + lj;
-                  const int k = DIM == 3 ? p.lo[2] + lk : 0;
-                  if (cfmask[oidx(p, a, s, i, j, k)])
-                     fl[a][s] = ewing_face<DIM, TU>(p, u, a, s, i, j, k, fl[a][s], dd[a][s], w,
-                                                    ratio_to_coarser);
-               }
-            }
-         }
-         if (has_fc) {
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) {
-               const long long sbase = p.offs[a] + (a == 0 ? sx : (a == 1 ? sy : sz));
-               const int sup = a == 0 ? 1 : (a == 1 ? nx : nx * ny);
-#pragma unroll
-               for (int s = 0; s < 2; ++s) {
-                  const long long si = sbase + (s ? sup : 0);
-                  if (fcmask[si]) fl[a][s] = fcflux[si];
-               }
-            }
-         }
-         const long long c0 = p.off0 + lin;
-         const double sf = CKIND == 2 ? cfield[c0] : (CKIND == 1 ? cconst : 0.0);
-         double rv;
-         if (DIM == 2)
-            rv = f[c0] - (dai[0] * (fl[0][1] - fl[0][0]) + dai[1] * (fl[1][1] - fl[1][0])) -
-                 sf * uc;
-         else
-            rv = f[c0] - (dai[0] * (fl[0][1] - fl[0][0]) + dai[1] * (fl[1][1] - fl[1][0]) +
-                          dai[2] * (fl[2][1] - fl[2][0])) -
-                 sf * uc;
-         res[c0] = rv;
-         if (oflux) {
-            const int i = p.lo[0] + li, j = p.lo[1] + lj, k = DIM == 3 ? p.lo[2] + lk : 0;
-            if (li == 0) oflux[oidx(p, 0, 0, i, j, k)] = fl[0][0];
-            if (li == nx - 1) oflux[oidx(p, 0, 1, i, j, k)] = fl[0][1];
-            if (lj == 0) oflux[oidx(p, 1, 0, i, j, k)] = fl[1][0];
-            if (lj == ny - 1) oflux[oidx(p, 1, 1, i, j, k)] = fl[1][1];
-            if (DIM == 3) {
-               if (lk == 0) oflux[oidx(p, 2, 0, i, j, k)] = fl[2][0];
-               if (lk == nz - 1) oflux[oidx(p, 2, 1, i, j, k)] = fl[2][1];
-            }
-         }
+         residual_cell<DIM, DVAR, CKIND, TU>(p, lin, li, lj, lk, dai, u, dside, dconst, cfmask, w,
+                                             ratio_to_coarser, fcmask, fcflux, f, cfield, cconst,
+                                             res, oflux);
       }
    }
+}
+
+// The fix-up after the staged residual: the listed cells (those with a
+// coarse-fine face or a face under a finer patch) as k_residual_fused
+// forms them, over the values the staged pass wrote.
+template <int DIM, bool DVAR, int CKIND, class TU>
+__global__ void __launch_bounds__(kThreads)
+k_residual_cells(const CellRef *__restrict__ cells, int ncells,
+                 const PatchDesc *__restrict__ patches, const TU *__restrict__ u,
+                 const double *__restrict__ dside, double dconst,
+                 const unsigned char *__restrict__ cfmask, EwingWeights w,
+                 const int *ratio_to_coarser, const unsigned char *__restrict__ fcmask,
+                 const double *__restrict__ fcflux, const double *__restrict__ f,
+                 const double *__restrict__ cfield, double cconst, double *__restrict__ res,
+                 double *__restrict__ oflux, const int *__restrict__ run)
+{
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= ncells) return;
+   const CellRef cr = cells[e];
+   const PatchDesc &p = patches[cr.patch];
+   if (run && !run[p.prob]) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   int li, lj, lk;
+   patch_cell(p, cr.lin, nx, ny, li, lj, lk);
+   const double dai[3] = {1. / p.dx[0], 1. / p.dx[1], DIM == 3 ? 1. / p.dx[2] : 0.0};
+   residual_cell<DIM, DVAR, CKIND, TU>(p, cr.lin, li, lj, lk, dai, u, dside, dconst, cfmask, w,
+                                       ratio_to_coarser, fcmask, fcflux, f, cfield, cconst, res,
+                                       oflux);
 }
 
 // ---------------------------------------------------------------------------
@@ -1453,37 +1500,6 @@ k_compact(const WorkReg *__restrict__ regs, const int *__restrict__ active, int 
 {
    const WorkReg r = regs[blockIdx.x];
    const int p = blockIdx.y;
-   if (r.prob) {
-      // a list in its own order: one block keeps the order of the active
-      // problems' entries (a straight copy when every problem is active)
-      if (p != 0) return;
-      int all = 1;
-      for (int q = threadIdx.x; q < nprob; q += blockDim.x) all &= active[q] != 0;
-      if (__syncthreads_and(all)) {
-         for (int t = threadIdx.x; t < r.n; t += blockDim.x) r.list[t] = r.all[t];
-         return;
-      }
-      __shared__ int wsum[kThreads / 32];
-      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-      int base = 0;
-      for (int t0 = 0; t0 < r.n; t0 += blockDim.x) {
-         const int t = t0 + threadIdx.x;
-         const bool keep = t < r.n && active[r.prob[t]] != 0;
-         const unsigned m = __ballot_sync(0xffffffffu, keep);
-         if (lane == 0) wsum[wid] = __popc(m);
-         __syncthreads();
-         int off = base, tot = 0;
-         for (int q = 0; q < kThreads / 32; ++q) {
-            if (q < wid) off += wsum[q];
-            tot += wsum[q];
-         }
-         if (keep) r.list[off + __popc(m & ((1u << lane) - 1u))] = r.all[t];
-         base += tot;
-         __syncthreads();
-      }
-      for (int t = base + threadIdx.x; t < r.n; t += blockDim.x) r.list[t] = Chunk{-1, 0, 0, 0};
-      return;
-   }
    int before = 0;
    for (int q = threadIdx.x; q < p; q += blockDim.x)
       if (active[q]) before += r.pcb[q + 1] - r.pcb[q];
@@ -2163,6 +2179,51 @@ void launch_residual_fused(cudaStream_t s, int dim, const PoissonSpec &spec, int
 }
 
 template <class TU>
+void launch_residual_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int ncells,
+                           const CellRef *cells, const PatchDesc *patches, const TU *u,
+                           const double *dside, const unsigned char *cfmask,
+                           const double *tranwt, const double *longwt,
+                           const int *ratio_to_coarser, const unsigned char *fcmask,
+                           const double *fcflux, const double *f, const double *cfield,
+                           double *res, double *oflux, const int *run)
+{
+   if (ncells <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   EwingWeights w;
+   for (int a = 0; a < 3; ++a) {
+      w.tranwt[a] = tranwt[a];
+      w.longwt[a] = longwt[a];
+   }
+   const int grid = (ncells + kThreads - 1) / kThreads;
+#define RC(D, V, C)                                                                          \
+   k_residual_cells<D, V, C, TU><<<grid, kThreads, 0, s>>>(                                   \
+      cells, ncells, patches, u, dside, spec.d_const, cfmask, w, ratio_to_coarser, fcmask,    \
+      fcflux, f, cfield, spec.c_const, res, oflux, run)
+   if (dim == 2) {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RC(2, true, 2);
+         else if (spec.c_kind == 1) RC(2, true, 1);
+         else RC(2, true, 0);
+      } else {
+         if (spec.c_kind == 2) RC(2, false, 2);
+         else if (spec.c_kind == 1) RC(2, false, 1);
+         else RC(2, false, 0);
+      }
+   } else {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RC(3, true, 2);
+         else if (spec.c_kind == 1) RC(3, true, 1);
+         else RC(3, true, 0);
+      } else {
+         if (spec.c_kind == 2) RC(3, false, 2);
+         else if (spec.c_kind == 1) RC(3, false, 1);
+         else RC(3, false, 0);
+      }
+   }
+#undef RC
+}
+
+template <class TU>
 void launch_residual(cudaStream_t s, int dim, const PoissonSpec &spec, int nchunks,
                      const PatchDesc *patches, const Chunk *chunks, const TU *u,
                      const double *f, const double *flux, const double *cfield,
@@ -2444,6 +2505,11 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
       const double *, const unsigned char *, const double *, const double *, const int *,   \
       const unsigned char *, const double *, const double *, const double *, double *,      \
       double *, const int *);                                                               \
+   template void launch_residual_cells<T>(                                                  \
+      cudaStream_t, int, const PoissonSpec &, int, const CellRef *, const PatchDesc *,        \
+      const T *, const double *, const unsigned char *, const double *, const double *,     \
+      const int *, const unsigned char *, const double *, const double *, const double *,   \
+      double *, double *, const int *);                                                     \
    template void launch_prolong_add<T>(cudaStream_t, int, const ProlongItem *,              \
                                        const Chunk *, int, const int *, const PatchDesc *, const T *, \
                                        const double *, const int *, T *, const int *);      \

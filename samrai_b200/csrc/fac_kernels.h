@@ -28,6 +28,40 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
                       const T *cfield, const T *cfflux, int offset, const int *pushmap,
                       const BcCoefs &bc, int *err, const WaitTest &wt = WaitTest());
 
+// Staged composite residual over a level's residual units (fac_stage.cu):
+// res = f - div flux - C u on every cell of the units, outer-side fluxes of
+// the patch faces when oflux is not null; u FP64 or FP32, the rest FP64.
+template <class TU>
+void launch_res_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nunits,
+                       int stage_bytes, int depth, const Chunk *units, const UnitCopy *copies,
+                       const unsigned char *headers, const TU *u, const double *f,
+                       const double *dside, const double *cfield, double *res, double *oflux,
+                       int *err, const WaitTest &wt = WaitTest());
+// The residual (and outer-side fluxes) of listed cells as the one-pass
+// kernel forms them, Ewing fix and coarsened finer fluxes included: the
+// fix-up after the staged residual.
+template <class TU>
+void launch_residual_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int ncells,
+                           const CellRef *cells, const PatchDesc *patches, const TU *u,
+                           const double *dside, const unsigned char *cfmask,
+                           const double *tranwt, const double *longwt,
+                           const int *ratio_to_coarser, const unsigned char *fcmask,
+                           const double *fcflux, const double *f, const double *cfield,
+                           double *res, double *oflux, const int *run);
+
+// Regrid step (fac_regrid.cu): tags (ghost-0 bytes) where the adaption
+// estimate of u (ghost-1, FP64) exceeds threshold, counts[prob] += tags;
+// one problem's tags into a dense array over [lo, lo + n); the tag
+// histograms of Berger-Rigoutsos node boxes.
+void launch_adaption_tags(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                          const Chunk *chunks, const double *u, double threshold,
+                          unsigned char *tags, unsigned long long *counts, const int *run);
+void launch_tags_dense(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
+                       const Chunk *chunks, const unsigned char *tags, int prob, const int *lo,
+                       const int *n, unsigned char *dense);
+void launch_br_histogram(cudaStream_t s, int nitems, const BrItem *items, const BrNode *nodes,
+                         const unsigned char *dense, const int *lo, const int *n, int *hist);
+
 // Krylov vector operations on composite vectors: ghost-0 level arrays, one
 // vector every vstride elements; per-problem coefficients; chunks are runs
 // of one problem's cells {problem, first cell, cells, chunk index} (partial

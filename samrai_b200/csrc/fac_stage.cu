@@ -372,11 +372,17 @@ __device__ __forceinline__ void stage_push(const unsigned char *stage, int tid,
    }
 }
 
-template <int DIM, bool DVAR, int CKIND, class T>
-__global__ void __launch_bounds__(kStageBlock)
-k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restrict__ copies,
-            StageBases bases, int stage_bytes, int depth, T *__restrict__ u, int offset,
-            T dconst, T cconst, BcCoefs bc, int *__restrict__ err, WaitTest wt)
+// The walk of a block over its units, shared by the staged passes: the
+// producer warp streams the units' copies into the ring, the consumer warps
+// run the pass's first phase on each unit, meet at a named barrier (where a
+// wait that ran out ends the walk for all of them), run its second phase
+// and free the stage.
+template <class Pass>
+__device__ __forceinline__ void staged_walk(const Chunk *__restrict__ chunks, int nwork,
+                                            const UnitCopy *__restrict__ copies,
+                                            const StageBases &bases, int stage_bytes, int depth,
+                                            int *__restrict__ err, const WaitTest &wt,
+                                            const Pass &pass)
 {
    extern __shared__ __align__(128) unsigned char smem[];
    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem);
@@ -385,16 +391,9 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
    unsigned long long *never_bar = reinterpret_cast<unsigned long long *>(
       smem + 2 * kStageDepthMax * 8 + sizeof(StageBases));
    unsigned char *stages = smem + kBarrierBytes;
-   // the list holds active problems only (compacted), largest units first;
-   // unit k of this block is entry k G + b in even rounds and k G + G-1-b in
-   // odd ones (G blocks, b this block): a snake, so that the blocks that
-   // take the larger unit of one round take the smaller of the next.  The
-   // walk ends at the first end marker (patch < 0) or past the list: later
-   // rounds lie wholly after it.
-   auto unit_at = [&](int k) {
-      const int b = (k & 1) ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
-      return k * (int)gridDim.x + b;
-   };
+   // the list holds active problems only (compacted), so unit k of this
+   // block is entry k G + b (G blocks, b this block) up to the end marker
+   auto unit_at = [&](int k) { return k * (int)gridDim.x + (int)blockIdx.x; };
    auto valid = [&](int w) { return w < nwork && chunks[w].patch >= 0; };
    if (threadIdx.x == 0) {
       for (int k = 0; k < depth; ++k) {
@@ -455,7 +454,7 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
       // (the test of the bounded wait waits on a barrier nothing arrives on)
       const bool ok = wt.never ? wait_phase(never_bar, 0u, wt.limit)
                                : wait_phase(&full[st], par, wt.limit);
-      if (ok) stage_update<DIM, DVAR, CKIND, T>(stage, tid, u, offset, dconst, cconst);
+      if (ok) pass.first(stage, tid);
       // every consumer passes here once per unit: all leave together when
       // any wait ran out, and the pushes read the updated stage
       if (consumers_any(!ok)) {
@@ -463,13 +462,196 @@ k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restr
          wait_phase(&full[st], par);  // copies still in flight land before the exit
          return;
       }
-      stage_push<DIM, T>(stage, tid, u, offset, bc);
+      pass.second(stage, tid);
       // the next copies into this stage (async proxy) follow the stores above
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);
       cur = nxt;
    }
+}
+
+// Red-black colour pass: update of the active colour, then the pushes.
+template <int DIM, bool DVAR, int CKIND, class T>
+struct ColourPass {
+   T *u;
+   int offset;
+   T dconst, cconst;
+   BcCoefs bc;
+   __device__ __forceinline__ void first(unsigned char *stage, int tid) const
+   {
+      stage_update<DIM, DVAR, CKIND, T>(stage, tid, u, offset, dconst, cconst);
+   }
+   __device__ __forceinline__ void second(unsigned char *stage, int tid) const
+   {
+      stage_push<DIM, T>(stage, tid, u, offset, bc);
+   }
+};
+
+template <int DIM, bool DVAR, int CKIND, class T>
+__global__ void __launch_bounds__(kStageBlock)
+k_rb_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restrict__ copies,
+            StageBases bases, int stage_bytes, int depth, ColourPass<DIM, DVAR, CKIND, T> pass,
+            int *__restrict__ err, WaitTest wt)
+{
+   staged_walk(chunks, nwork, copies, bases, stage_bytes, depth, err, wt, pass);
+}
+
+// One unit of the staged composite residual: for every cell of the unit,
+// the face fluxes from the staged u and D (computeFluxOnPatch, the
+// compflux* arithmetic: flux = (1/dx) D (u_hi - u_lo)) and the residual
+// r = f - div flux - C u (compres{var,con}sca{2,3}d), the operation order
+// of k_flux_cells + k_residual, FP64 throughout (--fmad=false); the fluxes
+// on the patch's faces go to the outer-side arrays.  Cells with a
+// coarse-fine face or a face under a finer patch are redone by the fix-up
+// pass afterwards.
+template <int DIM, bool DVAR, int CKIND, class TU>
+__device__ __forceinline__ void stage_residual(const unsigned char *stage, int tid, double dconst,
+                                               double cconst, double *__restrict__ res,
+                                               double *__restrict__ oflux)
+{
+   const ResHdr *h = reinterpret_cast<const ResHdr *>(stage);
+   const int s0 = h->s0;
+   const int lo0 = h->lo[0], lo1 = h->lo[1], lo2 = DIM == 3 ? h->lo[2] : 0;
+   const int nx = h->hi[0] - lo0 + 1;
+   const int ny = h->hi[1] - lo1 + 1;
+   const int nslow = DIM == 3 ? h->hi[2] - lo2 + 1 : ny;
+   const int gx = nx + 2, gy = ny + 2, sz = gx * gy;
+   const TU *su = reinterpret_cast<const TU *>(stage + h->off_u);
+   const bool hasf = h->off_f >= 0;
+   const double *sf = reinterpret_cast<const double *>(stage + (hasf ? h->off_f : 0));
+   const double *sdx = reinterpret_cast<const double *>(stage + h->off_d[0]);
+   const double *sdy = reinterpret_cast<const double *>(stage + h->off_d[1]);
+   const double *sdz = reinterpret_cast<const double *>(stage + h->off_d[2]);
+   const double *sc = reinterpret_cast<const double *>(stage + h->off_c);
+   const double dxi = h->dxi[0], dyi = h->dxi[1], dzi = DIM == 3 ? h->dxi[2] : 0.0;
+   double *gr = res + h->off0s;
+   const bool wo = oflux != nullptr && h->has_oflux;
+   const int n = h->ncells;
+   const unsigned mnx = h->mnx, mny = h->mny;
+   for (int t = tid; t < n; t += kConsumers) {
+      int li, lj, ls;
+      if (DIM == 3) {
+         const int row = udiv(t, mnx);
+         li = t - row * nx;
+         ls = udiv(row, mny);
+         lj = row - ls * ny;
+      } else {
+         ls = udiv(t, mnx);
+         li = t - ls * nx;
+         lj = s0 + ls;
+      }
+      const int c = DIM == 3 ? (li + 1) + gx * ((lj + 1) + gy * (ls + 1))
+                             : (li + 1) + gx * (ls + 1);
+      const double uc = (double)su[c];
+      double dx0, dx1, dy0, dy1, dz0 = 0.0, dz1 = 0.0;
+      if (DVAR) {
+         if (DIM == 3) {
+            const int bx = li + (nx + 1) * (lj + ny * ls);
+            dx0 = sdx[bx];
+            dx1 = sdx[bx + 1];
+            const int by = li + nx * (lj + (ny + 1) * ls);
+            dy0 = sdy[by];
+            dy1 = sdy[by + nx];
+            const int bz = li + nx * (lj + ny * ls);
+            dz0 = sdz[bz];
+            dz1 = sdz[bz + nx * ny];
+         } else {
+            const int bx = li + (nx + 1) * ls;
+            dx0 = sdx[bx];
+            dx1 = sdx[bx + 1];
+            const int by = li + nx * ls;
+            dy0 = sdy[by];
+            dy1 = sdy[by + nx];
+         }
+      } else {
+         dx0 = dx1 = dy0 = dy1 = dz0 = dz1 = dconst;
+      }
+      const double fxl = dxi * dx0 * (uc - (double)su[c - 1]);
+      const double fxh = dxi * dx1 * ((double)su[c + 1] - uc);
+      const double fyl = dyi * dy0 * (uc - (double)su[c - gx]);
+      const double fyh = dyi * dy1 * ((double)su[c + gx] - uc);
+      double fzl = 0.0, fzh = 0.0;
+      if (DIM == 3) {
+         fzl = dzi * dz0 * (uc - (double)su[c - sz]);
+         fzh = dzi * dz1 * ((double)su[c + sz] - uc);
+      }
+      const double scv = CKIND == 2 ? sc[t] : (CKIND == 1 ? cconst : 0.0);
+      const double fv = hasf ? sf[t] : 0.0;
+      double rv;
+      if (DIM == 2)
+         rv = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl)) - scv * uc;
+      else
+         rv = fv - (dxi * (fxh - fxl) + dyi * (fyh - fyl) + dzi * (fzh - fzl)) - scv * uc;
+      gr[t] = rv;
+      if (wo) {
+         const int kk = DIM == 3 ? s0 + ls : 0;  // slow-axis index in the patch (3-D)
+         if (li == 0) oflux[h->offo[0][0] + (DIM == 3 ? lj + ny * kk : lj)] = fxl;
+         if (li == nx - 1) oflux[h->offo[0][1] + (DIM == 3 ? lj + ny * kk : lj)] = fxh;
+         if (lj == 0) oflux[h->offo[1][0] + (DIM == 3 ? li + nx * kk : li)] = fyl;
+         if (lj == ny - 1) oflux[h->offo[1][1] + (DIM == 3 ? li + nx * kk : li)] = fyh;
+         if (DIM == 3) {
+            if (kk == 0) oflux[h->offo[2][0] + li + nx * lj] = fzl;
+            if (kk == nslow - 1) oflux[h->offo[2][1] + li + nx * lj] = fzh;
+         }
+      }
+   }
+}
+
+template <int DIM, bool DVAR, int CKIND, class TU>
+struct ResidualPass {
+   double dconst, cconst;
+   double *res, *oflux;
+   __device__ __forceinline__ void first(unsigned char *stage, int tid) const
+   {
+      stage_residual<DIM, DVAR, CKIND, TU>(stage, tid, dconst, cconst, res, oflux);
+   }
+   __device__ __forceinline__ void second(unsigned char *, int) const {}
+};
+
+template <int DIM, bool DVAR, int CKIND, class TU>
+__global__ void __launch_bounds__(kStageBlock)
+k_res_staged(const Chunk *__restrict__ chunks, int nwork, const UnitCopy *__restrict__ copies,
+             StageBases bases, int stage_bytes, int depth, ResidualPass<DIM, DVAR, CKIND, TU> pass,
+             int *__restrict__ err, WaitTest wt)
+{
+   staged_walk(chunks, nwork, copies, bases, stage_bytes, depth, err, wt, pass);
+}
+
+// Grid of a staged kernel: one wave of resident blocks, each walking its
+// share of the units.
+template <class K>
+int staged_grid(K *kernel, int nunits, int smem)
+{
+   static int nsm = 0;
+   if (nsm == 0) {
+      int dev = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+         nsm = 148;
+   }
+   int per_sm = 1;
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStageBlock, smem);
+   per_sm = per_sm < 1 ? 1 : per_sm;
+   return nunits < nsm * per_sm ? nunits : nsm * per_sm;
+}
+
+template <int DIM, bool DVAR, int CK, class TU>
+void res_staged_inst(cudaStream_t s, int nunits, int stage_bytes, int depth, const Chunk *units,
+                     const UnitCopy *copies, const StageBases &bases, double dconst,
+                     double cconst, double *res, double *oflux, int *err, const WaitTest &wt)
+{
+   static bool attr = false;
+   if (!attr) {
+      cudaFuncSetAttribute(k_res_staged<DIM, DVAR, CK, TU>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmemMax);
+      attr = true;
+   }
+   const int smem = kBarrierBytes + depth * stage_bytes;
+   const int grid = staged_grid(k_res_staged<DIM, DVAR, CK, TU>, nunits, smem);
+   const ResidualPass<DIM, DVAR, CK, TU> pass{dconst, cconst, res, oflux};
+   k_res_staged<DIM, DVAR, CK, TU><<<grid, kStageBlock, smem, s>>>(
+      units, nunits, copies, bases, stage_bytes, depth, pass, err, wt);
 }
 
 template <int DIM, bool DVAR, int CK, class T>
@@ -494,9 +676,9 @@ void staged_inst(cudaStream_t s, int nunits, int stage_bytes, int depth, const C
                                                  kStageBlock, smem);
    per_sm = per_sm < 1 ? 1 : per_sm;
    const int grid = nunits < nsm * per_sm ? nunits : nsm * per_sm;
+   const ColourPass<DIM, DVAR, CK, T> pass{u, offset, (T)dconst, (T)cconst, bc};
    k_rb_staged<DIM, DVAR, CK, T><<<grid, kStageBlock, smem, s>>>(
-      units, nunits, copies, bases, stage_bytes, depth, u, offset, (T)dconst, (T)cconst, bc,
-      err, wt);
+      units, nunits, copies, bases, stage_bytes, depth, pass, err, wt);
 }
 
 }  // namespace
@@ -553,5 +735,58 @@ void launch_rb_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nuni
 INST_STAGED(double)
 INST_STAGED(float)
 #undef INST_STAGED
+
+template <class TU>
+void launch_res_staged(cudaStream_t s, int dim, const PoissonSpec &spec, int nunits,
+                       int stage_bytes, int depth, const Chunk *units, const UnitCopy *copies,
+                       const unsigned char *headers, const TU *u, const double *f,
+                       const double *dside, const double *cfield, double *res, double *oflux,
+                       int *err, const WaitTest &wt)
+{
+   if (nunits <= 0) return;
+   add_kernel_launches(1);
+   StageBases bases;
+   for (int k = 0; k < kSrcCount; ++k) bases.p[k] = nullptr;
+   bases.p[kSrcU] = reinterpret_cast<const char *>(u);
+   bases.p[kSrcF] = reinterpret_cast<const char *>(f);
+   bases.p[kSrcD] = reinterpret_cast<const char *>(dside);
+   bases.p[kSrcC] = reinterpret_cast<const char *>(cfield);
+   bases.p[kSrcHdr] = reinterpret_cast<const char *>(headers);
+#define RG(D, V, C)                                                                        \
+   res_staged_inst<D, V, C, TU>(s, nunits, stage_bytes, depth, units, copies, bases,        \
+                                spec.d_const, spec.c_const, res, oflux, err, wt)
+   if (dim == 2) {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RG(2, true, 2);
+         else if (spec.c_kind == 1) RG(2, true, 1);
+         else RG(2, true, 0);
+      } else {
+         if (spec.c_kind == 2) RG(2, false, 2);
+         else if (spec.c_kind == 1) RG(2, false, 1);
+         else RG(2, false, 0);
+      }
+   } else {
+      if (spec.d_variable) {
+         if (spec.c_kind == 2) RG(3, true, 2);
+         else if (spec.c_kind == 1) RG(3, true, 1);
+         else RG(3, true, 0);
+      } else {
+         if (spec.c_kind == 2) RG(3, false, 2);
+         else if (spec.c_kind == 1) RG(3, false, 1);
+         else RG(3, false, 0);
+      }
+   }
+#undef RG
+}
+
+#define INST_RES_STAGED(TU)                                                                    \
+   template void launch_res_staged<TU>(cudaStream_t, int, const PoissonSpec &, int, int, int,  \
+                                       const Chunk *, const UnitCopy *, const unsigned char *, \
+                                       const TU *, const double *, const double *,             \
+                                       const double *, double *, double *, int *,              \
+                                       const WaitTest &);
+INST_RES_STAGED(double)
+INST_RES_STAGED(float)
+#undef INST_RES_STAGED
 
 }  // namespace samrai_b200

@@ -71,6 +71,12 @@ def load_library(build_if_missing=True):
         "fac_vec_linear_sum": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_int, dp,
                                               ctypes.c_int]),
         "fac_extend_coefficients": (ctypes.c_int, [vp]),
+        "fac_tag_gradient": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.POINTER(ctypes.c_longlong)]),
+        "fac_download_tags": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
+        "fac_cluster_tags": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, ip,
+                                            ip, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                            ip, ip]),
         "fac_set_poisson": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double]),
         "fac_set_bc": (ctypes.c_int, [vp, dp, dp, dp]),
@@ -503,6 +509,40 @@ class FacContext:
         a = np.ascontiguousarray(np.broadcast_to(a, self.nprob), dtype=np.float64)
         b = np.ascontiguousarray(np.broadcast_to(b, self.nprob), dtype=np.float64)
         _check(load_library().fac_vec_linear_sum(self.h, fz, _dp(a), fx, _dp(b), fy))
+
+    # regrid step -----------------------------------------------------------
+    def tag_gradient(self, fid, ln, threshold):
+        """Tag the cells of level ln where the adaption estimate of field
+        fid exceeds threshold (fac_tag_gradient); returns the count per
+        problem."""
+        cnt = np.zeros(self.nprob, dtype=np.int64)
+        _check(load_library().fac_tag_gradient(
+            self.h, fid, ln, float(threshold), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
+        return cnt
+
+    def download_tags(self, prob, ln):
+        out = np.empty(self.size(F, prob, ln), dtype=np.uint8)
+        _check(load_library().fac_download_tags(self.h, prob, ln, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def cluster_tags(self, prob, ln, bound, min_box, max_box=(0, 0, 0), efficiency=0.8,
+                     combine=0.8):
+        """Berger-Rigoutsos boxes (n, 6) over the tags of level ln of one
+        problem within the bound boxes (fac_cluster_tags)."""
+        bound = np.ascontiguousarray(np.asarray(bound, dtype=np.int32).reshape(-1, 6))
+        mn = np.ascontiguousarray(list(min_box) + [1] * (3 - len(min_box)), dtype=np.int32)
+        mx = np.ascontiguousarray(list(max_box) + [0] * (3 - len(max_box)), dtype=np.int32)
+        cap = 1024
+        while True:
+            out = np.zeros((cap, 6), dtype=np.int32)
+            nb = ctypes.c_int(0)
+            _check(load_library().fac_cluster_tags(self.h, prob, ln, len(bound), _ip(bound),
+                                                   _ip(mn), _ip(mx), float(efficiency),
+                                                   float(combine), cap, _ip(out),
+                                                   ctypes.byref(nb)))
+            if nb.value <= cap:
+                return out[:nb.value].copy()
+            cap = nb.value
 
     def timer_start(self):
         _check(load_library().fac_timer(self.h, 0, None))
