@@ -333,6 +333,7 @@ def regrid_measure(ctx, probs, target=0.02):
     The threshold is the one that tags about `target` of the cells (found
     by bisection before the timing).  Wall time of one tagging plus the
     clustering of every problem, synchronised."""
+    from samrai_b200 import fac
     ln = ctx.nlev - 1
     cells = sum(int(np.prod(p.levels[-1].boxes[:, 3:] - p.levels[-1].boxes[:, :3] + 1, axis=1).sum())
                 for p in probs)
@@ -411,6 +412,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-regrid", dest="regrid", action="store_false",
                     help="skip the regrid-step measurement (tagging and clustering)")
+    ap.add_argument("--no-cnn", dest="cnn", action="store_false",
+                    help="skip the learned part's training-throughput measurement")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the headline (multigrid-extended) variant")
     ap.add_argument("--smoother-only", type=int, default=0, metavar="SWEEPS",
@@ -621,6 +624,23 @@ def main():
         pctx.close()
 
     regrid = regrid_measure(ctx, probs) if args.regrid else None
+    cnn = None
+    if args.cnn:
+        # training throughput of the learned part's kernels (BF16 tensor
+        # cores, FP32 accumulation) against the measured BF16 GEMM peak
+        from samrai_b200 import learned
+        net = fac.CNN(max_batch=256, device=local_rank, seed=1)
+        cnn = learned.training_throughput(net, batch=256, steps=10, device=local_rank)
+        net.close()
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+                bf16 = float(json.load(fh)["bf16_tflops"])
+            cnn["peak_tflops"], cnn["peak_kind"] = bf16, "measured bf16 burst"
+        except Exception:
+            cnn["peak_tflops"], cnn["peak_kind"] = 1590.0, "fallback"
+        cnn["train_frac"] = round(cnn["train_tflops"] / cnn["peak_tflops"], 4)
+        for kk in ("train_ms", "forward_ms", "train_tflops", "forward_tflops"):
+            cnn[kk] = round(cnn[kk], 3)
     peak, peak_kind = measured_peaks()
     achieved = rb_bytes / (rb_ms * 1e-3) / 1e9 if rb_ms > 0 else 0.0
     out = {
@@ -682,6 +702,7 @@ def main():
         "stationary_fac": fac_only,
         "plain_fp64": plain,
         "regrid": regrid,
+        "cnn_training": cnn,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

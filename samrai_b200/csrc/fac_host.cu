@@ -443,6 +443,11 @@ struct fac_ctx {
    DevArray<double> kry_dots, kry_coef, kry_a;
    DevArray<double> vec_coef;  // per-problem scalars of fac_vec_linear_sum
    DevArray<unsigned long long> tag_counts;  // per-problem tag counts
+   // clustering scratch, grown as needed and kept between calls
+   DevArray<unsigned char> br_dense;
+   DevArray<BrNode> br_nodes;
+   DevArray<BrItem> br_items;
+   DevArray<int> br_hist;
    int krylov = 0;  // > 0: fac_solve runs FGMRES(krylov) around the FAC cycle
    // fac_set_coarse_extension: domain-covering coarser levels added below
    // every problem's level 0, and whether their coefficients need to be
@@ -1272,7 +1277,10 @@ void build_res_units(fac_ctx *c, int ln)
 // in patch order: a cell on a coarse-fine face of the level (the Ewing fix
 // changes that face's flux) and a cell next to a face that takes a
 // coarsened finer-level flux -- exactly the faces k_residual_fused treats
-// apart (patch flags bit 0 with cfmask, bit 1 with fcmask).
+// apart (patch flags bit 0 with cfmask, bit 1 with fcmask).  Cells under
+// the finer level count too: the V-cycle restricts their residual to the
+// coarser level (facCycle_Recursive's restrictResidual of the level's
+// whole residual).
 void build_residual_fixups(fac_ctx *c, int ln)
 {
    LevelState &L = c->L[ln];
@@ -1528,6 +1536,7 @@ void build_coarsen_tables(fac_ctx *c, int ln)
    for (int p = 0; p < np; ++p) {
       const int fb = Fl.prob_patch_begin[p], fe = Fl.prob_patch_begin[p + 1];
       const int cb = C.prob_patch_begin[p], ce = C.prob_patch_begin[p + 1];
+      std::vector<FluxCoarsenItem> fcs;  // this problem's, in the reference's order
       for (int ip = fb; ip < fe; ++ip) {
          const Box cbox = coarsen(Fl.box[ip], dim, r);
          for (int iq = cb; iq < ce; ++iq) {
@@ -1575,9 +1584,46 @@ void build_coarsen_tables(fac_ctx *c, int ln)
                   it.t1 = t1;
                   const int aux = r[t0] | ((t1 >= 0 ? r[t1] : 1) << 8);
                   it.ratio = aux;
-                  C.fcoarsen.add(it, ov.size());
+                  fcs.push_back(it);
                }
             }
+         }
+      }
+      // Two fine patches that share a face both coarsen it onto the same
+      // coarse faces.  Their values agree only as far as the two patches'
+      // copies of D on the shared face do; the reference's schedule writes
+      // the items in order and the last one stays (xfer/CoarsenSchedule.C:
+      // 275-330 over the fine patches in order, lower side before upper).
+      // Each item keeps only the faces no later item writes, so every
+      // coarse face has one writer and the result is the reference's.
+      for (size_t i = 0; i < fcs.size(); ++i) {
+         const FluxCoarsenItem &it = fcs[i];
+         Box bi;
+         for (int d = 0; d < 3; ++d) {
+            bi.lo[d] = it.lo[d];
+            bi.hi[d] = it.hi[d];
+         }
+         std::vector<Box> keep{bi};
+         for (size_t j = i + 1; j < fcs.size() && !keep.empty(); ++j) {
+            const FluxCoarsenItem &jt = fcs[j];
+            if (jt.coarse_patch != it.coarse_patch || jt.axis != it.axis ||
+                jt.lo[it.axis] != it.lo[it.axis])
+               continue;
+            Box bj;
+            for (int d = 0; d < 3; ++d) {
+               bj.lo[d] = jt.lo[d];
+               bj.hi[d] = jt.hi[d];
+            }
+            subtract_all(keep, bj);
+         }
+         for (const Box &k : keep) {
+            if (k.empty()) continue;
+            FluxCoarsenItem piece = it;
+            for (int d = 0; d < 3; ++d) {
+               piece.lo[d] = k.lo[d];
+               piece.hi[d] = k.hi[d];
+            }
+            C.fcoarsen.add(piece, k.size());
          }
       }
    }
@@ -3903,8 +3949,8 @@ int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *b
          n[a] = hi[a] - lo[a] + 1;
          cells *= n[a];
       }
-      DevArray<unsigned char> dense;
-      dense.alloc((size_t)cells);
+      DevArray<unsigned char> &dense = ctx->br_dense;
+      if (dense.n < (size_t)cells) dense.alloc((size_t)cells);
       CUDA_CHECK(cudaMemsetAsync(dense.p, 0, (size_t)cells, ctx->stream));
       launch_tags_dense(ctx->stream, d, (int)L.cell_chunks.size(), L.d_patches.p,
                         L.d_cell_chunks.p, L.tag.p, problem, lo, n, dense.p);
@@ -3922,9 +3968,16 @@ int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *b
          frontier.push_back((int)tree.size());
          tree.push_back(t);
       }
-      DevArray<BrNode> d_nodes;
-      DevArray<BrItem> d_items;
-      DevArray<int> d_hist;
+      DevArray<BrNode> &d_nodes = ctx->br_nodes;
+      DevArray<BrItem> &d_items = ctx->br_items;
+      DevArray<int> &d_hist = ctx->br_hist;
+      // upload into a buffer that grows only
+      auto put = [&](auto &dev, const auto &host) {
+         if (dev.n < host.size()) dev.alloc(host.size() * 2);
+         if (!host.empty())
+            CUDA_CHECK(cudaMemcpyAsync(dev.p, host.data(), host.size() * sizeof(host[0]),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+      };
       while (!frontier.empty()) {
          std::vector<BrNode> nodes;
          std::vector<BrItem> items;
@@ -3948,9 +4001,10 @@ int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *b
             const int per = std::max(1, 65536 / e[0]);
             for (int r0 = 0; r0 < rows; r0 += per) items.push_back({q, r0, std::min(per, rows - r0), 0});
          }
-         d_nodes.upload(nodes, ctx->stream);
-         d_items.upload(items, ctx->stream);
-         d_hist.alloc((size_t)std::max<long long>(1, hsize));
+         put(d_nodes, nodes);
+         put(d_items, items);
+         if (d_hist.n < (size_t)std::max<long long>(1, hsize))
+            d_hist.alloc((size_t)std::max<long long>(1, hsize) * 2);
          CUDA_CHECK(cudaMemsetAsync(d_hist.p, 0, (size_t)std::max<long long>(1, hsize) * sizeof(int),
                                     ctx->stream));
          launch_br_histogram(ctx->stream, (int)items.size(), d_items.p, d_nodes.p, dense.p, lo, n,

@@ -409,14 +409,21 @@ __device__ __forceinline__ void staged_walk(const Chunk *__restrict__ chunks, in
    if (warp == kConsumerWarps) {
       // producer warp: lane i issues copy i of a unit (the host-built copy
       // list, header first; its first entry carries the byte total)
+      // two units ahead of the copies it issues: the chunk of the unit after
+      // next and the copy entry of the next unit are loaded while this
+      // unit's stage comes free, so no dependent load waits per unit
+      const Chunk end = {-1, 0, 0, 0};
+      const UnitCopy none = {0, 0, 0, 0, 0};
       int w = unit_at(0);
-      Chunk ch = w < nwork ? chunks[w] : Chunk{-1, 0, 0, 0};
+      Chunk ch = w < nwork ? chunks[w] : end;
+      UnitCopy cp = ch.patch >= 0 && lane < ch.count ? copies[ch.begin + lane] : none;
+      w = unit_at(1);
+      Chunk chn = ch.patch >= 0 && w < nwork ? chunks[w] : end;
       int k = 0;  // units issued
       for (; ch.patch >= 0; ++k) {
-         const int wn = unit_at(k + 1);
-         const Chunk chn = wn < nwork ? chunks[wn] : Chunk{-1, 0, 0, 0};  // prefetch
-         UnitCopy cp = {0, 0, 0, 0, 0};
-         if (lane < ch.count) cp = copies[ch.begin + lane];
+         const UnitCopy cpn = chn.patch >= 0 && lane < chn.count ? copies[chn.begin + lane] : none;
+         const int w2 = unit_at(k + 2);
+         const Chunk chnn = chn.patch >= 0 && w2 < nwork ? chunks[w2] : end;
          const int st = k % depth;
          bool ok = true;
          if (k >= depth && lane == 0) ok = wait_phase(&empty[st], ((k / depth) & 1) ^ 1u);
@@ -430,8 +437,9 @@ __device__ __forceinline__ void staged_walk(const Chunk *__restrict__ chunks, in
          if (lane < ch.count)
             bulk_load(stage + cp.dst_off, sbases->p[cp.src] + cp.src_off, (unsigned)cp.nbytes,
                       &full[st]);
-         w = wn;
          ch = chn;
+         cp = cpn;
+         chn = chnn;
       }
       // the block's shared memory must outlive every copy issued into it:
       // the last `depth` units (one per stage; no later unit was issued

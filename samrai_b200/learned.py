@@ -166,3 +166,47 @@ def evaluate(problems: Sequence, level: int, net, params=None, precision="mixed"
         finally:
             ctx.close()
     return out
+
+
+# FLOPs per sample cell of one training step (forward, data gradients of
+# layers 4..2, weight gradients of all four layers; a multiply-add is two):
+# forward 2*27*(1*16 + 16*16 + 16*16 + 16*1), data backward the same minus
+# layer 1, weight gradients the same as forward.
+FWD_FLOP_PER_CELL = 2 * 27 * (16 + 256 + 256 + 16)
+TRAIN_FLOP_PER_CELL = 2 * FWD_FLOP_PER_CELL + 2 * 27 * (256 + 256 + 16)
+
+
+def training_throughput(net, batch=256, steps=20, device=0, seed=0):
+    """Training throughput of the project's kernels on random samples:
+    TFLOP/s of fac_cnn_train_step (wall time of `steps` steps of `batch`
+    samples between device synchronisations) and of the forward pass."""
+    import time
+
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    shape = (batch, S, S, S)
+    x = torch.randn(shape, generator=g).to(f"cuda:{device}")
+    t = torch.randn(shape, generator=g).to(f"cuda:{device}")
+    m = torch.ones(shape, device=f"cuda:{device}")
+    y = torch.empty(shape, device=f"cuda:{device}")
+    ms = float(m.sum())
+    for _ in range(3):
+        net.train_step(x.data_ptr(), t.data_ptr(), m.data_ptr(), batch, ms, 1e-4)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.train_step(x.data_ptr(), t.data_ptr(), m.data_ptr(), batch, ms, 1e-4)
+    torch.cuda.synchronize(device)
+    train_s = (time.perf_counter() - t0) / steps
+    for _ in range(3):
+        net.forward(x.data_ptr(), batch, y.data_ptr())
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.forward(x.data_ptr(), batch, y.data_ptr())
+    torch.cuda.synchronize(device)
+    fwd_s = (time.perf_counter() - t0) / steps
+    cells = batch * S3
+    return {"batch": batch, "train_ms": train_s * 1e3, "forward_ms": fwd_s * 1e3,
+            "train_tflops": cells * TRAIN_FLOP_PER_CELL / train_s / 1e12,
+            "forward_tflops": cells * FWD_FLOP_PER_CELL / fwd_s / 1e12}
