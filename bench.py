@@ -328,8 +328,9 @@ def regrid_measure(ctx, probs, target=0.02):
     """The regrid step on the finest level of every problem after the
     solve: device tagging of the solution by the adaption estimate
     (fac_tag_gradient) and Berger-Rigoutsos clustering of each problem's
-    tags within its level's bounding box (fac_cluster_tags: device
-    histograms, host decisions; min box 4, efficiency 0.8, combine 0.8).
+    tags within its level's bounding box (fac_cluster_tags_all: all
+    problems' trees walked together, device histograms, host decisions;
+    min box 4, efficiency 0.8, combine 0.8).
     The threshold is the one that tags about `target` of the cells (found
     by bisection before the timing).  Wall time of one tagging plus the
     clustering of every problem, synchronised."""
@@ -353,19 +354,16 @@ def regrid_measure(ctx, probs, target=0.02):
         bounds.append([[int(b[:, 0].min()), int(b[:, 1].min()), int(b[:, 2].min()),
                         int(b[:, 3].max()), int(b[:, 4].max()), int(b[:, 5].max())]])
     ctx.tag_gradient(fac.U, ln, thr)  # warm-up
-    for i in range(len(probs)):
-        ctx.cluster_tags(i, ln, bounds[i], (4, 4, 4))
+    ctx.cluster_tags_all(ln, bounds, (4, 4, 4))
     t0 = time.perf_counter()
     tags = ctx.tag_gradient(fac.U, ln, thr)
-    nbox = 0
-    for i in range(len(probs)):
-        nbox += len(ctx.cluster_tags(i, ln, bounds[i], (4, 4, 4)))
+    nbox = sum(len(b) for b in ctx.cluster_tags_all(ln, bounds, (4, 4, 4)))
     ms = (time.perf_counter() - t0) * 1e3
     return {"ms": round(ms, 2), "level": "finest", "cells": cells, "tagged": int(tags.sum()),
             "boxes": nbox, "threshold": thr,
             "what": "fac_tag_gradient (AdaptivePoisson adaption estimate > threshold) and "
-                    "fac_cluster_tags (Berger-Rigoutsos, min box 4, efficiency 0.8, combine "
-                    "0.8) of every problem's finest level, wall time"}
+                    "fac_cluster_tags_all (Berger-Rigoutsos, min box 4, efficiency 0.8, "
+                    "combine 0.8) of every problem's finest level, wall time"}
 
 
 def cpu_small_solves(names=("c1", "c3")):

@@ -492,6 +492,16 @@ int fac_download_tags(fac_ctx *ctx, int problem, int ln, unsigned char *host);
 int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *bound,
                      const int *min_box, const int *max_box, double efficiency,
                      double combine, int cap, int *boxes, int *nboxes);
+/* fac_cluster_tags for every problem of the context at once: problem p
+ * clusters inside its nbound[p] (>= 1) bound boxes, which follow problem
+ * p - 1's in bound.  The problems' trees are walked together, one histogram
+ * launch per depth for all of them, with the same decisions and boxes as
+ * fac_cluster_tags problem by problem.  The boxes go to boxes problem after
+ * problem (up to cap in all); counts[p] (host, one per problem) gets
+ * problem p's number, whether written or not. */
+int fac_cluster_tags_all(fac_ctx *ctx, int ln, const int *nbound, const int *bound,
+                         const int *min_box, const int *max_box, double efficiency,
+                         double combine, int cap, int *boxes, int *counts);
 
 /* ---- allocation-free norm.  No counterpart in the reference.
  *

@@ -2306,11 +2306,16 @@ bool fused_residual_on(const fac_ctx *c, int ln)
 }
 
 // The staged residual (TMA-staged units, then the fix-up of the special
-// cells) runs wherever the staged passes are on and the level's units fit
-// the shared memory; it gives the same bits as the other two forms.
+// cells) runs wherever the staged passes are on and two CTAs of the level's
+// largest unit fit an SM's shared memory; with one CTA per SM (FP64 slices
+// of 32 x 32 patches) it measured slower than the one-pass kernel.  It
+// gives the same bits as the other two forms.
 bool staged_residual_on(const fac_ctx *c, int ln, int kind)
 {
-   return c->staged && c->L[ln].runit_smem[kind] > 0 && !c->L[ln].runits[kind].empty();
+   const LevelState &L = c->L[ln];
+   if (!c->staged || L.runit_smem[kind] <= 0 || L.runits[kind].empty()) return false;
+   return 2LL * (kStageBarrierBytes + (long long)c->stage_depth * L.runit_smem[kind]) <=
+          kStageSmemMax;
 }
 
 void comp_residual(fac_ctx *c, int fid_r, int fid_u, int fid_f, int ln, int error_eq)
@@ -3902,31 +3907,30 @@ void decide(const BrParams &P, BrTree &n, int lchild[6], int rchild[6])
 
 }  // namespace
 
-int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *bound,
-                     const int *min_box, const int *max_box, double efficiency, double combine,
-                     int cap, int *boxes, int *nboxes)
+namespace {
+
+// Berger-Rigoutsos over the tags of level ln of the listed problems at once:
+// problem probs[q] clusters inside its nbound[q] bound boxes (back to back
+// in bound).  One dense tag array per problem; the trees are walked breadth
+// first together, one histogram launch per depth for all open nodes.
+// Boxes go out problem by problem (depth first, left before right);
+// counts[q] gets problem probs[q]'s number of boxes, the return value their
+// total (boxes beyond cap are counted, not written).
+long long cluster_levels(fac_ctx *ctx, int ln, const std::vector<int> &probs,
+                         const int *nbound, const int *bound, const BrParams &P, int cap,
+                         int *boxes, int *counts)
 {
-   return guarded([&] {
-      check_ops(ctx);
-      check_pl(ctx, problem, ln);
-      if (nbound < 1 || !bound || !min_box || !max_box || !nboxes || (cap > 0 && !boxes))
-         throw FacError(FAC_ERR_ARG, "bad clustering arguments");
-      if (!(efficiency >= 0.0 && efficiency <= 1.0) || !(combine >= 0.0 && combine <= 1.0))
-         throw FacError(FAC_ERR_ARG, "efficiency and combine efficiency must lie in [0, 1]");
-      LevelState &L = ctx->L[ln];
-      if (!L.tag.p) throw FacError(FAC_ERR_STATE, "no tags on this level (fac_tag_gradient)");
-      const int d = ctx->dim;
-      BrParams P;
-      P.dim = d;
-      P.efficiency = efficiency;
-      P.combine = combine;
-      for (int a = 0; a < 3; ++a) {
-         P.min_box[a] = a < d ? min_box[a] : 1;
-         P.max_box[a] = a < d && max_box[a] > 0 ? max_box[a] : std::numeric_limits<int>::max();
-         if (a < d && P.min_box[a] < 1) throw FacError(FAC_ERR_ARG, "min_box must be >= 1");
-      }
-      // dense tag array over the bounding box of the problem's patches and
-      // the bound boxes (cells outside the patches hold no tags)
+   LevelState &L = ctx->L[ln];
+   if (!L.tag.p) throw FacError(FAC_ERR_STATE, "no tags on this level (fac_tag_gradient)");
+   const int d = ctx->dim;
+   const int nq = (int)probs.size();
+   // dense tag arrays over the bounding box of each problem's patches and
+   // bound boxes (cells outside the patches hold no tags)
+   std::vector<std::array<int, 3> > dlo(nq), dn(nq);
+   std::vector<long long> doff(nq + 1, 0);
+   std::vector<int> boff(nq + 1, 0);
+   for (int q = 0; q < nq; ++q) boff[q + 1] = boff[q] + nbound[q];
+   for (int q = 0; q < nq; ++q) {
       int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
       auto grow = [&](const int *blo, const int *bhi) {
          for (int a = 0; a < 3; ++a) {
@@ -3935,149 +3939,220 @@ int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *b
             hi[a] = std::max(hi[a], h);
          }
       };
-      for (int ip = 0; ip < L.npatch; ++ip)
-         if (L.hp[ip].prob == problem) grow(L.hp[ip].lo, L.hp[ip].hi);
-      for (int b = 0; b < nbound; ++b) {
+      for (int ip = L.prob_patch_begin[probs[q]]; ip < L.prob_patch_begin[probs[q] + 1]; ++ip)
+         grow(L.hp[ip].lo, L.hp[ip].hi);
+      for (int b = boff[q]; b < boff[q + 1]; ++b) {
          const int *bb = bound + 6 * b;
          for (int a = 0; a < d; ++a)
             if (bb[3 + a] < bb[a]) throw FacError(FAC_ERR_ARG, "empty bound box");
          grow(bb, bb + 3);
       }
-      int n[3];
       long long cells = 1;
       for (int a = 0; a < 3; ++a) {
-         n[a] = hi[a] - lo[a] + 1;
-         cells *= n[a];
+         dlo[q][a] = lo[a];
+         dn[q][a] = hi[a] - lo[a] + 1;
+         cells *= dn[q][a];
       }
-      DevArray<unsigned char> &dense = ctx->br_dense;
-      if (dense.n < (size_t)cells) dense.alloc((size_t)cells);
-      CUDA_CHECK(cudaMemsetAsync(dense.p, 0, (size_t)cells, ctx->stream));
-      launch_tags_dense(ctx->stream, d, (int)L.cell_chunks.size(), L.d_patches.p,
-                        L.d_cell_chunks.p, L.tag.p, problem, lo, n, dense.p);
-      CUDA_CHECK(cudaGetLastError());
-      // breadth first over the tree: one histogram launch per depth
-      std::vector<BrTree> tree;
-      std::vector<int> roots, frontier;
-      for (int b = 0; b < nbound; ++b) {
+      doff[q + 1] = doff[q] + ((cells + 255) / 256) * 256;
+   }
+   DevArray<unsigned char> &dense = ctx->br_dense;
+   if (dense.n < (size_t)std::max<long long>(1, doff[nq])) dense.alloc((size_t)std::max<long long>(1, doff[nq]));
+   CUDA_CHECK(cudaMemsetAsync(dense.p, 0, (size_t)std::max<long long>(1, doff[nq]), ctx->stream));
+   for (int q = 0; q < nq; ++q) {
+      // the problem's own chunks of the full (uncompacted) cell list
+      const int ch0 = L.prob_cell_chunk_begin[probs[q]];
+      const int ch1 = L.prob_cell_chunk_begin[probs[q] + 1];
+      launch_tags_dense(ctx->stream, d, ch1 - ch0, L.d_patches.p, L.ws_cell.all.p + ch0, L.tag.p,
+                        probs[q], dlo[q].data(), dn[q].data(), dense.p + doff[q]);
+   }
+   CUDA_CHECK(cudaGetLastError());
+   std::vector<BrTree> tree;
+   std::vector<int> owner;  // problem slot q of each tree node
+   std::vector<int> frontier;
+   std::vector<std::vector<int> > roots(nq);
+   for (int q = 0; q < nq; ++q)
+      for (int b = boff[q]; b < boff[q + 1]; ++b) {
          BrTree t;
          for (int a = 0; a < 3; ++a) {
             t.lo[a] = a < d ? bound[6 * b + a] : 0;
             t.hi[a] = a < d ? bound[6 * b + 3 + a] : 0;
          }
-         roots.push_back((int)tree.size());
+         roots[q].push_back((int)tree.size());
          frontier.push_back((int)tree.size());
          tree.push_back(t);
+         owner.push_back(q);
       }
-      DevArray<BrNode> &d_nodes = ctx->br_nodes;
-      DevArray<BrItem> &d_items = ctx->br_items;
-      DevArray<int> &d_hist = ctx->br_hist;
-      // upload into a buffer that grows only
-      auto put = [&](auto &dev, const auto &host) {
-         if (dev.n < host.size()) dev.alloc(host.size() * 2);
-         if (!host.empty())
-            CUDA_CHECK(cudaMemcpyAsync(dev.p, host.data(), host.size() * sizeof(host[0]),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-      };
-      while (!frontier.empty()) {
-         std::vector<BrNode> nodes;
-         std::vector<BrItem> items;
-         long long hsize = 0;
-         for (int q = 0; q < (int)frontier.size(); ++q) {
-            const BrTree &t = tree[frontier[q]];
-            BrNode nd;
-            int e[3];
-            for (int a = 0; a < 3; ++a) {
-               nd.lo[a] = t.lo[a];
-               nd.hi[a] = t.hi[a];
-               e[a] = t.hi[a] - t.lo[a] + 1;
-            }
-            if (e[0] > kBrThreads * kBrMaxXPerThread)
-               throw FacError(FAC_ERR_ARG, "clustering box too long along x");
-            nd.hoff = hsize;
-            hsize += e[0] + e[1] + e[2];
-            nodes.push_back(nd);
-            // runs of rows of at most ~64k cells per block
-            const int rows = e[1] * e[2];
-            const int per = std::max(1, 65536 / e[0]);
-            for (int r0 = 0; r0 < rows; r0 += per) items.push_back({q, r0, std::min(per, rows - r0), 0});
+   DevArray<BrNode> &d_nodes = ctx->br_nodes;
+   DevArray<BrItem> &d_items = ctx->br_items;
+   DevArray<int> &d_hist = ctx->br_hist;
+   auto put = [&](auto &dev, const auto &host) {
+      if (dev.n < host.size()) dev.alloc(host.size() * 2);
+      if (!host.empty())
+         CUDA_CHECK(cudaMemcpyAsync(dev.p, host.data(), host.size() * sizeof(host[0]),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+   };
+   while (!frontier.empty()) {
+      std::vector<BrNode> nodes;
+      std::vector<BrItem> items;
+      long long hsize = 0;
+      for (int f = 0; f < (int)frontier.size(); ++f) {
+         const BrTree &t = tree[frontier[f]];
+         const int q = owner[frontier[f]];
+         BrNode nd;
+         int e[3];
+         for (int a = 0; a < 3; ++a) {
+            nd.lo[a] = t.lo[a];
+            nd.hi[a] = t.hi[a];
+            nd.dlo[a] = dlo[q][a];
+            nd.dn[a] = dn[q][a];
+            e[a] = t.hi[a] - t.lo[a] + 1;
          }
-         put(d_nodes, nodes);
-         put(d_items, items);
-         if (d_hist.n < (size_t)std::max<long long>(1, hsize))
-            d_hist.alloc((size_t)std::max<long long>(1, hsize) * 2);
-         CUDA_CHECK(cudaMemsetAsync(d_hist.p, 0, (size_t)std::max<long long>(1, hsize) * sizeof(int),
-                                    ctx->stream));
-         launch_br_histogram(ctx->stream, (int)items.size(), d_items.p, d_nodes.p, dense.p, lo, n,
-                             d_hist.p);
-         CUDA_CHECK(cudaGetLastError());
-         std::vector<int> hist((size_t)std::max<long long>(1, hsize));
-         CUDA_CHECK(cudaMemcpyAsync(hist.data(), d_hist.p, hist.size() * sizeof(int),
-                                    cudaMemcpyDeviceToHost, ctx->stream));
-         CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-         std::vector<int> next;
-         for (int q = 0; q < (int)frontier.size(); ++q) {
-            const int id = frontier[q];
-            const BrNode &nd = nodes[q];
-            long long o = nd.hoff;
-            for (int a = 0; a < 3; ++a) {
-               const int e = nd.hi[a] - nd.lo[a] + 1;
-               if (a < d) tree[id].h[a].assign(hist.begin() + o, hist.begin() + o + e);
-               o += e;
-            }
-            int lc[6], rc[6];
-            decide(P, tree[id], lc, rc);
-            if (tree[id].state == 2) {
-               for (int side = 0; side < 2; ++side) {
-                  const int *cb = side ? rc : lc;
-                  BrTree t;
-                  for (int a = 0; a < 3; ++a) {
-                     t.lo[a] = cb[a];
-                     t.hi[a] = cb[3 + a];
-                  }
-                  (side ? tree[id].right : tree[id].left) = (int)tree.size();
-                  next.push_back((int)tree.size());
-                  tree.push_back(t);
+         if (e[0] > kBrThreads * kBrMaxXPerThread)
+            throw FacError(FAC_ERR_ARG, "clustering box too long along x");
+         nd.hoff = hsize;
+         nd.doff = doff[q];
+         hsize += e[0] + e[1] + e[2];
+         nodes.push_back(nd);
+         // runs of rows of at most ~64k cells per block
+         const int rows = e[1] * e[2];
+         const int per = std::max(1, 65536 / e[0]);
+         for (int r0 = 0; r0 < rows; r0 += per) items.push_back({f, r0, std::min(per, rows - r0), 0});
+      }
+      put(d_nodes, nodes);
+      put(d_items, items);
+      const size_t hn = (size_t)std::max<long long>(1, hsize);
+      if (d_hist.n < hn) d_hist.alloc(hn * 2);
+      CUDA_CHECK(cudaMemsetAsync(d_hist.p, 0, hn * sizeof(int), ctx->stream));
+      launch_br_histogram(ctx->stream, (int)items.size(), d_items.p, d_nodes.p, dense.p, d_hist.p);
+      CUDA_CHECK(cudaGetLastError());
+      std::vector<int> hist(hn);
+      CUDA_CHECK(cudaMemcpyAsync(hist.data(), d_hist.p, hn * sizeof(int), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+      CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      std::vector<int> next;
+      for (int f = 0; f < (int)frontier.size(); ++f) {
+         const int id = frontier[f];
+         const BrNode &nd = nodes[f];
+         long long o = nd.hoff;
+         for (int a = 0; a < 3; ++a) {
+            const int e = nd.hi[a] - nd.lo[a] + 1;
+            if (a < d) tree[id].h[a].assign(hist.begin() + o, hist.begin() + o + e);
+            o += e;
+         }
+         int lc[6], rc[6];
+         decide(P, tree[id], lc, rc);
+         if (tree[id].state == 2) {
+            for (int side = 0; side < 2; ++side) {
+               const int *cb = side ? rc : lc;
+               BrTree t;
+               for (int a = 0; a < 3; ++a) {
+                  t.lo[a] = cb[a];
+                  t.hi[a] = cb[3 + a];
                }
+               (side ? tree[id].right : tree[id].left) = (int)tree.size();
+               next.push_back((int)tree.size());
+               tree.push_back(t);
+               owner.push_back(owner[id]);
             }
          }
-         frontier.swap(next);
       }
-      // recombination, children before parents (runChildren_check,
-      // mesh/BergerRigoutsosNode.C:719-790)
-      auto box_size = [&](const BrTree &t) {
-         long long s = 1;
-         for (int a = 0; a < d; ++a) s *= t.hi[a] - t.lo[a] + 1;
-         return s;
-      };
-      for (int id = (int)tree.size() - 1; id >= 0; --id) {
-         BrTree &t = tree[id];
-         if (t.state != 2) continue;
-         const BrTree &l = tree[t.left], &r = tree[t.right];
-         bool fits = true;
-         for (int a = 0; a < d; ++a) fits = fits && t.hi[a] - t.lo[a] + 1 <= P.max_box[a];
-         const double reduction = (double)(box_size(l) + box_size(r)) / (double)box_size(t);
-         if (l.state == 1 && r.state == 1 && fits && reduction >= P.combine) t.state = 1;
-      }
-      // the accepted boxes, depth first, left before right
+      frontier.swap(next);
+   }
+   // recombination, children before parents (runChildren_check,
+   // mesh/BergerRigoutsosNode.C:719-790)
+   auto box_size = [&](const BrTree &t) {
+      long long sz = 1;
+      for (int a = 0; a < d; ++a) sz *= t.hi[a] - t.lo[a] + 1;
+      return sz;
+   };
+   for (int id = (int)tree.size() - 1; id >= 0; --id) {
+      BrTree &t = tree[id];
+      if (t.state != 2) continue;
+      const BrTree &l = tree[t.left], &r = tree[t.right];
+      bool fits = true;
+      for (int a = 0; a < d; ++a) fits = fits && t.hi[a] - t.lo[a] + 1 <= P.max_box[a];
+      const double reduction = (double)(box_size(l) + box_size(r)) / (double)box_size(t);
+      if (l.state == 1 && r.state == 1 && fits && reduction >= P.combine) t.state = 1;
+   }
+   // the accepted boxes, problem by problem, depth first, left before right
+   long long total = 0;
+   for (int q = 0; q < nq; ++q) {
       int count = 0;
-      std::vector<int> stack(roots.rbegin(), roots.rend());
+      std::vector<int> stack(roots[q].rbegin(), roots[q].rend());
       while (!stack.empty()) {
          const int id = stack.back();
          stack.pop_back();
          const BrTree &t = tree[id];
          if (t.state == 1) {
-            if (count < cap)
+            if (total < cap)
                for (int a = 0; a < 3; ++a) {
-                  boxes[6 * count + a] = t.lo[a];
-                  boxes[6 * count + 3 + a] = t.hi[a];
+                  boxes[6 * total + a] = t.lo[a];
+                  boxes[6 * total + 3 + a] = t.hi[a];
                }
             ++count;
+            ++total;
          } else if (t.state == 2) {
             stack.push_back(t.right);
             stack.push_back(t.left);
          }
       }
+      counts[q] = count;
+   }
+   return total;
+}
+
+BrParams br_params(int d, const int *min_box, const int *max_box, double efficiency,
+                   double combine)
+{
+   if (!min_box || !max_box) throw FacError(FAC_ERR_ARG, "bad clustering arguments");
+   if (!(efficiency >= 0.0 && efficiency <= 1.0) || !(combine >= 0.0 && combine <= 1.0))
+      throw FacError(FAC_ERR_ARG, "efficiency and combine efficiency must lie in [0, 1]");
+   BrParams P;
+   P.dim = d;
+   P.efficiency = efficiency;
+   P.combine = combine;
+   for (int a = 0; a < 3; ++a) {
+      P.min_box[a] = a < d ? min_box[a] : 1;
+      P.max_box[a] = a < d && max_box[a] > 0 ? max_box[a] : std::numeric_limits<int>::max();
+      if (a < d && P.min_box[a] < 1) throw FacError(FAC_ERR_ARG, "min_box must be >= 1");
+   }
+   return P;
+}
+
+}  // namespace
+
+int fac_cluster_tags(fac_ctx *ctx, int problem, int ln, int nbound, const int *bound,
+                     const int *min_box, const int *max_box, double efficiency, double combine,
+                     int cap, int *boxes, int *nboxes)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, problem, ln);
+      if (nbound < 1 || !bound || !nboxes || (cap > 0 && !boxes))
+         throw FacError(FAC_ERR_ARG, "bad clustering arguments");
+      const BrParams P = br_params(ctx->dim, min_box, max_box, efficiency, combine);
+      int count = 0;
+      cluster_levels(ctx, ln, std::vector<int>{problem}, &nbound, bound, P, cap, boxes, &count);
       *nboxes = count;
+   });
+}
+
+int fac_cluster_tags_all(fac_ctx *ctx, int ln, const int *nbound, const int *bound,
+                         const int *min_box, const int *max_box, double efficiency,
+                         double combine, int cap, int *boxes, int *counts)
+{
+   return guarded([&] {
+      check_ops(ctx);
+      check_pl(ctx, 0, ln);
+      const int np = nprob(ctx);
+      if (!nbound || !bound || !counts || (cap > 0 && !boxes))
+         throw FacError(FAC_ERR_ARG, "bad clustering arguments");
+      for (int p = 0; p < np; ++p)
+         if (nbound[p] < 1) throw FacError(FAC_ERR_ARG, "every problem needs a bound box");
+      const BrParams P = br_params(ctx->dim, min_box, max_box, efficiency, combine);
+      std::vector<int> probs(np);
+      for (int p = 0; p < np; ++p) probs[p] = p;
+      cluster_levels(ctx, ln, probs, nbound, bound, P, cap, boxes, counts);
    });
 }
 

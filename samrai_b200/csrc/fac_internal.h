@@ -373,11 +373,14 @@ struct CellRef {
    int lin;
 };
 
-// Berger-Rigoutsos node box on the device (3-D extents, 1 for unused axes)
-// and where its histograms start: x counts, then y, then z.
+// Berger-Rigoutsos node box on the device (3-D extents, 1 for unused axes),
+// its problem's dense tag array and where its histograms start: x counts,
+// then y, then z.
 struct BrNode {
    int lo[3], hi[3];
+   int dlo[3], dn[3];   // the problem's dense tag array: lower corner, extents
    long long hoff;
+   long long doff;      // where that array starts
 };
 // A run of rows (along x) of one node box for one block of the histogram
 // kernel; rows are numbered y fastest, then z.

@@ -52,7 +52,8 @@ void launch_residual_cells(cudaStream_t s, int dim, const PoissonSpec &spec, int
 // Regrid step (fac_regrid.cu): tags (ghost-0 bytes) where the adaption
 // estimate of u (ghost-1, FP64) exceeds threshold, counts[prob] += tags;
 // one problem's tags into a dense array over [lo, lo + n); the tag
-// histograms of Berger-Rigoutsos node boxes.
+// histograms of Berger-Rigoutsos node boxes (each node names its problem's
+// dense array).
 void launch_adaption_tags(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                           const Chunk *chunks, const double *u, double threshold,
                           unsigned char *tags, unsigned long long *counts, const int *run);
@@ -60,7 +61,7 @@ void launch_tags_dense(cudaStream_t s, int dim, int nchunks, const PatchDesc *pa
                        const Chunk *chunks, const unsigned char *tags, int prob, const int *lo,
                        const int *n, unsigned char *dense);
 void launch_br_histogram(cudaStream_t s, int nitems, const BrItem *items, const BrNode *nodes,
-                         const unsigned char *dense, const int *lo, const int *n, int *hist);
+                         const unsigned char *dense, int *hist);
 
 // Krylov vector operations on composite vectors: ghost-0 level arrays, one
 // vector every vstride elements; per-problem coefficients; chunks are runs

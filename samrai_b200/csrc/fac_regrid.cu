@@ -114,12 +114,14 @@ k_tags_dense(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ ch
 // on the order.
 __global__ void __launch_bounds__(kBrThreads)
 k_br_histogram(const BrItem *__restrict__ items, const BrNode *__restrict__ nodes,
-               const unsigned char *__restrict__ dense, int3 lo, int3 n,
-               int *__restrict__ hist)
+               const unsigned char *__restrict__ dense_all, int *__restrict__ hist)
 {
    __shared__ int wsum[kBrThreads / 32];
    const BrItem it = items[blockIdx.x];
    const BrNode nd = nodes[it.node];
+   const unsigned char *dense = dense_all + nd.doff;
+   const int3 lo = make_int3(nd.dlo[0], nd.dlo[1], nd.dlo[2]);
+   const int3 n = make_int3(nd.dn[0], nd.dn[1], nd.dn[2]);
    const int ex = nd.hi[0] - nd.lo[0] + 1, ey = nd.hi[1] - nd.lo[1] + 1;
    int *hx = hist + nd.hoff, *hy = hx + ex, *hz = hy + ey;
    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -191,13 +193,11 @@ void launch_tags_dense(cudaStream_t s, int dim, int nchunks, const PatchDesc *pa
 }
 
 void launch_br_histogram(cudaStream_t s, int nitems, const BrItem *items, const BrNode *nodes,
-                         const unsigned char *dense, const int *lo, const int *n, int *hist)
+                         const unsigned char *dense, int *hist)
 {
    if (nitems <= 0) return;
    add_kernel_launches(1);
-   k_br_histogram<<<nitems, kBrThreads, 0, s>>>(items, nodes, dense,
-                                               make_int3(lo[0], lo[1], lo[2]),
-                                               make_int3(n[0], n[1], n[2]), hist);
+   k_br_histogram<<<nitems, kBrThreads, 0, s>>>(items, nodes, dense, hist);
 }
 
 }  // namespace samrai_b200

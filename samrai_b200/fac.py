@@ -77,6 +77,8 @@ def load_library(build_if_missing=True):
         "fac_cluster_tags": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, ip,
                                             ip, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                             ip, ip]),
+        "fac_cluster_tags_all": (ctypes.c_int, [vp, ctypes.c_int, ip, ip, ip, ip, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_int, ip, ip]),
         "fac_set_poisson": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double]),
         "fac_set_bc": (ctypes.c_int, [vp, dp, dp, dp]),
@@ -543,6 +545,32 @@ class FacContext:
             if nb.value <= cap:
                 return out[:nb.value].copy()
             cap = nb.value
+
+    def cluster_tags_all(self, ln, bounds, min_box, max_box=(0, 0, 0), efficiency=0.8,
+                         combine=0.8):
+        """cluster_tags for every problem at once (fac_cluster_tags_all):
+        bounds[p] are problem p's bound boxes; returns one (n, 6) array of
+        boxes per problem."""
+        bl = [np.asarray(b, dtype=np.int32).reshape(-1, 6) for b in bounds]
+        if len(bl) != self.nprob:
+            raise ValueError("one list of bound boxes per problem")
+        nbound = np.ascontiguousarray([len(b) for b in bl], dtype=np.int32)
+        bound = np.ascontiguousarray(np.concatenate(bl, axis=0))
+        mn = np.ascontiguousarray(list(min_box) + [1] * (3 - len(min_box)), dtype=np.int32)
+        mx = np.ascontiguousarray(list(max_box) + [0] * (3 - len(max_box)), dtype=np.int32)
+        counts = np.zeros(self.nprob, dtype=np.int32)
+        cap = 4096
+        while True:
+            out = np.zeros((cap, 6), dtype=np.int32)
+            _check(load_library().fac_cluster_tags_all(self.h, ln, _ip(nbound), _ip(bound),
+                                                       _ip(mn), _ip(mx), float(efficiency),
+                                                       float(combine), cap, _ip(out),
+                                                       _ip(counts)))
+            total = int(counts.sum())
+            if total <= cap:
+                ends = np.cumsum(counts)
+                return [out[e - c:e].copy() for c, e in zip(counts, ends)]
+            cap = total
 
     def timer_start(self):
         _check(load_library().fac_timer(self.h, 0, None))
