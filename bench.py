@@ -418,6 +418,9 @@ def main():
                     help="only run SWEEPS red-black sweeps on the largest level (for ncu)")
     ap.add_argument("--krylov", type=int, default=KRYLOV,
                     help="FGMRES restart length of the headline solve (0: stationary FAC)")
+    ap.add_argument("--cnn-only", type=int, default=0, metavar="BATCH",
+                    help="only time training steps of the learned part's network on BATCH "
+                         "samples (--steps of them, for kernel captures)")
     ap.add_argument("--cycles", type=int, default=0, metavar="N",
                     help="only run one solve of the headline variant stopped after N cycles "
                          "(a short, fixed launch sequence for kernel captures)")
@@ -441,6 +444,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
 
     from samrai_b200 import configs, fac
+    if args.cnn_only:
+        from samrai_b200 import learned
+        net = fac.CNN(max_batch=args.cnn_only, device=local_rank, seed=1)
+        r = learned.training_throughput(net, batch=args.cnn_only, steps=max(1, args.steps),
+                                        device=local_rank)
+        net.close()
+        print(json.dumps({"cnn_only": args.cnn_only, **r}), flush=True)
+        return 0
     probs, desc = make_workload(args.config, args.nprob, rank, world)
     mg = [configs.extend_hierarchy(p, k=MG_LEVELS[args.config]) for p in probs]
     ctx = fac.FacContext(mg, params=PARAMS_MG, device=local_rank, precision=args.precision)

@@ -523,7 +523,7 @@ int fac_cluster_tags_all(fac_ctx *ctx, int ln, const int *nbound, const int *bou
  * process exits; nothing is allocated or freed per call.  nseg above
  * FAC_NOALLOC_MAX_SEGMENTS returns FAC_ERR_ARG.  The first call on each
  * device looks up that device's address of the array (cudaGetSymbolAddress,
- * with the device current); make that first call before any stream capture.
+ * with the device current).
  * All calls share the array: calls whose work can overlap on the GPU (two
  * streams, or two host threads) race and must be serialised by the caller.
  * Every partial sum a call reads it first writes, so no clearing is needed.

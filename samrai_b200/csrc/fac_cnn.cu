@@ -7,14 +7,17 @@
 // FP32.  One sample is a patch plus a one-cell halo padded to an S^3 box
 // (S = 18: patches of up to 16^3 cells).
 //
-// The 16 -> 16 layers run as implicit GEMMs on the tensor cores
-// (mma.sync m16n8k16, BF16 in, FP32 accumulate): for each of the 27 taps a
-// warp multiplies a 16-cell x 16-channel activation tile (gathered at the
-// tap's offset) by the tap's 16 x 16 weight block.  The same kernel computes
-// the backward pass with respect to the data (taps reversed, weights
-// transposed, gated by the forward ReLU mask).  Weight gradients of the
-// 16 -> 16 layers are 27 small GEMMs reducing over all cells, one warp per
-// tap.  The 1 -> 16 and 16 -> 1 layers are tiny and run on the FP32 cores.
+// The 16 -> 16 layers run as implicit GEMMs on the 5th-generation tensor
+// cores (k_conv_mid_tc: tcgen05.mma, BF16 operands in shared memory, FP32
+// accumulators in tensor memory): a CTA stages a slab of z-planes of one
+// sample with a zero halo in shared memory, and for each 128-row tile of
+// the slab's cells one thread issues 27 MMAs (one per tap, M = 128 cells,
+// N = 16 output channels, K = 16 input channels), the tap being a shift of
+// the A operand's start address.  The same kernel computes the backward
+// pass with respect to the data (taps reversed, weights transposed, gated by
+// the forward ReLU mask).  Weight gradients of the 16 -> 16 layers are 27
+// small GEMMs reducing over all cells, one warp per tap (mma.sync).  The
+// 1 -> 16 and 16 -> 1 layers are tiny and run on the FP32 cores.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -53,11 +56,6 @@ __device__ __forceinline__ long long neighbour(long long cell, int x, int y, int
    if (x + dx < 0 || x + dx >= S || y + dy < 0 || y + dy >= S || z + dz < 0 || z + dz >= S)
       return -1;
    return cell + dz * S * S + dy * S + dx;
-}
-
-__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16 *p, long long idx)
-{
-   return *reinterpret_cast<const uint32_t *>(p + idx);
 }
 
 __device__ __forceinline__ void mma_bf16(float *d, const uint32_t *a, uint32_t b0, uint32_t b1)
@@ -100,71 +98,239 @@ __global__ void k_conv_in(const __nv_bfloat16 *__restrict__ x, const float *__re
 }
 
 // ---------------------------------------------------------------------------
-// layers 2, 3 (and their data gradients): 16 -> 16 on the tensor cores.
-// wt: [27][16 out][16 in] BF16.  mode 0: y = relu(acc); mode 1: y = acc *
-// (gate > 0) (ReLU backward with the forward activation as gate).
+// layers 2, 3 (and their data gradients) on tcgen05.
+//
+// A CTA takes slabs of kTcNz output z-planes of one sample in turn.  It
+// stages the slab's input planes z0-1 .. z0+kTcNz with a one-cell zero halo
+// in x and y (kTcPx x kTcPx cells per plane) in shared memory, channels
+// split in two planes of 8 (16 bytes per cell each): with cells as rows and
+// channels as K, that is the K-major canonical layout without swizzle (8
+// consecutive cells form a core matrix of 8 rows x 16 bytes; SBO = 128 bytes
+// between groups of 8 cells, LBO = the distance of the two channel planes).
+// Output row r (a padded cell index) needs input row r + off(tap), so tap t
+// is the same descriptor with its start moved by off(t) cells.  The padded
+// rows of halo positions are computed and dropped.  Weights: per tap the
+// 16 x 16 block as B (N = output channels, K = input channels, K-major).
+// Accumulators: tile i of 128 rows in tensor-memory columns 16 i .. 16 i +
+// 15, lane = row; warp w reads lanes 32 (w % 4) .. + 31.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
-k_conv_mid(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ wt,
-           __nv_bfloat16 *__restrict__ y, const __nv_bfloat16 *__restrict__ gate,
-           long long ncells, int mode)
+constexpr int kTcPx = S + 2;                         // padded row length
+constexpr int kTcPlane = kTcPx * kTcPx;              // padded plane
+constexpr int kTcNz = 3;                             // output planes per slab
+constexpr int kTcSlabs = S / kTcNz;                  // slabs per sample
+constexpr int kTcBox = (kTcNz + 2) * kTcPlane;       // staged cells
+constexpr int kTcTiles = (kTcNz * kTcPlane + 127) / 128;
+constexpr int kTcReach = 1 + kTcPx + kTcPlane;       // largest |tap offset|
+constexpr int kTcFront = 32;                         // cells before the box
+constexpr int kTcSpan = kTcFront + kTcBox + 128;     // cells per channel plane
+constexpr int kTcCols = 256;                         // tensor-memory columns
+constexpr int kTcPlaneBytes = kTcSpan * 16;
+constexpr int kTcWBytes = T * 512;
+constexpr int kTcSmem = 2 * kTcPlaneBytes + kTcWBytes + 16;
+constexpr int kTcThreads = 256;
+static_assert(S % kTcNz == 0, "whole slabs");
+static_assert(kTcFront + kTcPlane - kTcReach >= 0, "front guard");
+static_assert(kTcFront + kTcPlane + 128 * kTcTiles + kTcReach <= kTcSpan, "back guard");
+static_assert(16 * kTcTiles <= kTcCols, "accumulator columns");
+static_assert(kTcPlaneBytes % 16 == 0 && (kTcPlaneBytes >> 4) < (1 << 14), "LBO field");
+static_assert(3 * kTcSmem > 228 * 1024, "at most two CTAs per SM share the tensor memory");
+// instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), BF16
+// A and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at
+// bit 24
+constexpr unsigned kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
+                              ((128u >> 4) << 24);
+// a wait gives up after this many SM cycles (about 2 s)
+constexpr long long kTcWaitCycles = 4000000000ll;
+
+__device__ __forceinline__ unsigned tc_smem(const void *p)
 {
-   __shared__ __align__(16) __nv_bfloat16 w[T * C * C];
-   for (int i = threadIdx.x; i < T * C * C / 2; i += blockDim.x)
-      reinterpret_cast<uint32_t *>(w)[i] = reinterpret_cast<const uint32_t *>(wt)[i];
+   return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: start, leading and stride byte offsets
+// (16-byte units), descriptor version 1, no swizzle
+__device__ __forceinline__ unsigned long long tc_desc(unsigned addr, unsigned lbo, unsigned sbo)
+{
+   return (unsigned long long)((addr >> 4) & 0x3FFFu) |
+          ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+          ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(unsigned d, unsigned long long a, unsigned long long b,
+                                       unsigned idesc, unsigned accumulate)
+{
+   asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n"
+      "}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ bool tc_try_wait(unsigned bar, unsigned parity)
+{
+   unsigned ok;
+   asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+   return ok != 0;
+}
+
+__device__ __forceinline__ void tc_ld16(unsigned taddr, unsigned *v)
+{
+   asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// wt: [27][16 out][16 in] BF16.  mode 0: y = relu(acc); mode 1: y = acc *
+// (gate > 0).  A wait that runs out sets *err and ends the CTA's work.
+__global__ void __launch_bounds__(kTcThreads)
+k_conv_mid_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ wt,
+              __nv_bfloat16 *__restrict__ y, const __nv_bfloat16 *__restrict__ gate,
+              long long nsamp, int mode, int *__restrict__ err)
+{
+   extern __shared__ __align__(128) unsigned char tsm[];
+   uint4 *p0 = reinterpret_cast<uint4 *>(tsm);                   // channels 0..7
+   uint4 *p1 = reinterpret_cast<uint4 *>(tsm + kTcPlaneBytes);   // channels 8..15
+   unsigned char *ws = tsm + 2 * kTcPlaneBytes;
+   unsigned long long *bar = reinterpret_cast<unsigned long long *>(ws + kTcWBytes);
+   unsigned *tslot = reinterpret_cast<unsigned *>(bar + 1);
+   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+   // weights per tap as [in-channel half][out channel][8 in-channels]
+   for (int i = tid; i < T * C * 2; i += kTcThreads) {
+      const int half = i & 1, tco = i >> 1, t = tco / C, co = tco - t * C;
+      *reinterpret_cast<uint4 *>(ws + t * 512 + half * 256 + co * 16) =
+         *reinterpret_cast<const uint4 *>(wt + (size_t)tco * C + half * 8);
+   }
+   for (int i = tid; i < kTcSpan; i += kTcThreads) {
+      p0[i] = make_uint4(0u, 0u, 0u, 0u);
+      p1[i] = make_uint4(0u, 0u, 0u, 0u);
+   }
+   if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(bar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   if (warp == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                      tc_smem(tslot)),
+                   "r"(kTcCols)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+   }
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
    __syncthreads();
-   const int lane = threadIdx.x & 31;
-   const int g = lane >> 2, q = lane & 3;
-   const long long ntiles = (ncells + 15) / 16;
-   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-   for (long long tile = warp; tile < ntiles; tile += nwarps) {
-      const long long r0 = tile * 16 + g, r1 = r0 + 8;
-      int x0, y0, z0, x1, y1, z1;
-      cell_coords(r0, x0, y0, z0);
-      cell_coords(r1, x1, y1, z1);
-      const bool v0 = r0 < ncells, v1 = r1 < ncells;
-      float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-      for (int t = 0; t < T; ++t) {
-         const long long n0 = v0 ? neighbour(r0, x0, y0, z0, t) : -1;
-         const long long n1 = v1 ? neighbour(r1, x1, y1, z1, t) : -1;
-         uint32_t a[4];
-         a[0] = n0 >= 0 ? ld_pair(x, n0 * C + 2 * q) : 0u;
-         a[1] = n1 >= 0 ? ld_pair(x, n1 * C + 2 * q) : 0u;
-         a[2] = n0 >= 0 ? ld_pair(x, n0 * C + 2 * q + 8) : 0u;
-         a[3] = n1 >= 0 ? ld_pair(x, n1 * C + 2 * q + 8) : 0u;
-#pragma unroll
-         for (int j = 0; j < 2; ++j) {
-            const __nv_bfloat16 *wb = w + (t * C + 8 * j + g) * C + 2 * q;
-            const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wb);
-            const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wb + 8);
-            mma_bf16(acc[j], a, b0, b1);
+   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+   const unsigned tmem = *tslot;
+   const unsigned s0 = tc_smem(p0), s1 = tc_smem(p1), sw = tc_smem(ws), sb = tc_smem(bar);
+   unsigned phase = 0;
+   const long long nslab = nsamp * kTcSlabs;
+   for (long long slab = blockIdx.x; slab < nslab; slab += gridDim.x) {
+      const long long smp = slab / kTcSlabs;
+      const int z0 = (int)(slab - smp * kTcSlabs) * kTcNz;
+      const __nv_bfloat16 *xs = x + smp * (long long)S3 * C;
+      for (int i = tid; i < kTcBox; i += kTcThreads) {
+         const int zz = i / kTcPlane, r = i - zz * kTcPlane;
+         const int py = r / kTcPx, px = r - py * kTcPx;
+         const int cx = px - 1, cy = py - 1, cz = z0 - 1 + zz;
+         uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+         if (cx >= 0 && cx < S && cy >= 0 && cy < S && cz >= 0 && cz < S) {
+            const uint4 *src =
+               reinterpret_cast<const uint4 *>(xs + ((long long)cx + S * (cy + S * cz)) * C);
+            lo = src[0];
+            hi = src[1];
          }
+         p0[kTcFront + i] = lo;
+         p1[kTcFront + i] = hi;
       }
+      // the tensor cores read shared memory through the async proxy; the
+      // previous slab's accumulator reads come before these MMAs
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+         for (int i = 0; i < kTcTiles; ++i)
+            for (int t = 0; t < T; ++t) {
+               const int off = tap_dx(t) + kTcPx * tap_dy(t) + kTcPlane * tap_dz(t);
+               const unsigned row = (unsigned)(kTcFront + kTcPlane + 128 * i + off);
+               tc_mma(tmem + 16u * i, tc_desc(s0 + 16u * row, s1 - s0, 128u),
+                      tc_desc(sw + 512u * t, 256u, 128u), kTcIdesc, t > 0 ? 1u : 0u);
+            }
+         asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sb)
+            : "memory");
+      }
+      bool ok = true;
+      {
+         const long long t0 = clock64();
+         while (!tc_try_wait(sb, phase))
+            if (clock64() - t0 > kTcWaitCycles) {
+               ok = false;
+               break;
+            }
+      }
+      phase ^= 1u;
+      if (!__syncthreads_and(ok)) {
+         if (tid == 0) atomicExch(err, 1);
+         break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int q = warp & 3;
+      for (int i = warp >> 2; i < kTcTiles; i += kTcThreads / 128) {
+         unsigned v[16];
+         tc_ld16(tmem + ((unsigned)(32 * q) << 16) + 16u * i, v);
+         const int r = kTcPlane + 128 * i + 32 * q + lane;  // padded box row
+         const int zz = r / kTcPlane, rr = r - zz * kTcPlane;
+         const int py = rr / kTcPx, px = rr - py * kTcPx;
+         if (zz > kTcNz || px < 1 || px > S || py < 1 || py > S) continue;
+         const long long cell =
+            smp * S3 + (px - 1) + S * ((py - 1) + (long long)S * (z0 - 1 + zz));
+         float o[16];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-         const int c = 8 * j + 2 * q;
-         float o0 = acc[j][0], o1 = acc[j][1], o2 = acc[j][2], o3 = acc[j][3];
+         for (int c = 0; c < 16; ++c) o[c] = __uint_as_float(v[c]);
          if (mode == 0) {
-            o0 = fmaxf(o0, 0.f);
-            o1 = fmaxf(o1, 0.f);
-            o2 = fmaxf(o2, 0.f);
-            o3 = fmaxf(o3, 0.f);
+#pragma unroll
+            for (int c = 0; c < 16; ++c) o[c] = fmaxf(o[c], 0.f);
          } else {
-            if (v0) {
-               const __nv_bfloat162 gg = *reinterpret_cast<const __nv_bfloat162 *>(gate + r0 * C + c);
-               if (!(__bfloat162float(gg.x) > 0.f)) o0 = 0.f;
-               if (!(__bfloat162float(gg.y) > 0.f)) o1 = 0.f;
-            }
-            if (v1) {
-               const __nv_bfloat162 gg = *reinterpret_cast<const __nv_bfloat162 *>(gate + r1 * C + c);
-               if (!(__bfloat162float(gg.x) > 0.f)) o2 = 0.f;
-               if (!(__bfloat162float(gg.y) > 0.f)) o3 = 0.f;
-            }
+            const uint4 *gp = reinterpret_cast<const uint4 *>(gate + cell * C);
+            uint4 gg[2] = {gp[0], gp[1]};
+            const __nv_bfloat16 *g = reinterpret_cast<const __nv_bfloat16 *>(gg);
+#pragma unroll
+            for (int c = 0; c < 16; ++c)
+               if (!(__bfloat162float(g[c]) > 0.f)) o[c] = 0.f;
          }
-         if (v0) *reinterpret_cast<__nv_bfloat162 *>(y + r0 * C + c) = __floats2bfloat162_rn(o0, o1);
-         if (v1) *reinterpret_cast<__nv_bfloat162 *>(y + r1 * C + c) = __floats2bfloat162_rn(o2, o3);
+         uint4 out[2];
+         __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(out);
+#pragma unroll
+         for (int c = 0; c < 8; ++c) ob[c] = __floats2bfloat162_rn(o[2 * c], o[2 * c + 1]);
+         uint4 *dst = reinterpret_cast<uint4 *>(y + cell * C);
+         dst[0] = out[0];
+         dst[1] = out[1];
       }
+   }
+   // every accumulator read is done before the tensor memory is released
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+   __syncthreads();
+   if (warp == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"(kTcCols)
+                   : "memory");
    }
 }
 
@@ -403,6 +569,8 @@ struct fac_cnn {
    __nv_bfloat16 *x0 = nullptr, *a[3] = {nullptr}, *d[3] = {nullptr};
    float *y = nullptr, *dy = nullptr;
    double *loss = nullptr;
+   int *kerr = nullptr;                  // set by a tensor-core wait that ran out
+   int tc_grid = 0;                      // CTAs of k_conv_mid_tc (two per SM)
    int steps = 0;
    std::vector<void *> allocs;
 };
@@ -443,6 +611,27 @@ int pack(fac_cnn *n)
    return FAC_OK;
 }
 
+void conv_mid(fac_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *wt, __nv_bfloat16 *y,
+              const __nv_bfloat16 *gate, long long nsamp, int mode, cudaStream_t st)
+{
+   const long long slabs = nsamp * kTcSlabs;
+   const unsigned grid = (unsigned)std::min<long long>(slabs, n->tc_grid);
+   k_conv_mid_tc<<<grid, kTcThreads, kTcSmem, st>>>(x, wt, y, gate, nsamp, mode, n->kerr);
+}
+
+// the device error flag, after the stream has drained
+int device_status(fac_cnn *n)
+{
+   int e = 0;
+   CNN_CHECK(cudaMemcpyAsync(&e, n->kerr, sizeof(int), cudaMemcpyDeviceToHost, n->stream));
+   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   if (e) {
+      t_cnn_error = "a tensor-core wait ran out (k_conv_mid_tc)";
+      return FAC_ERR_DEVICE;
+   }
+   return FAC_OK;
+}
+
 int forward_on(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st)
 {
    const long long cells = nsamp * S3;
@@ -450,10 +639,8 @@ int forward_on(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st)
    const unsigned gb = (unsigned)((cells + tb - 1) / tb);
    k_to_bf16<<<gb, tb, 0, st>>>(x, n->x0, cells);
    k_conv_in<<<gb, tb, 0, st>>>(n->x0, n->w1r, n->a[0], cells);
-   const long long tiles = (cells + 15) / 16;
-   const unsigned mb = (unsigned)std::min<long long>((tiles + 7) / 8, 148 * 16);
-   k_conv_mid<<<mb, 256, 0, st>>>(n->a[0], n->wf[0], n->a[1], nullptr, cells, 0);
-   k_conv_mid<<<mb, 256, 0, st>>>(n->a[1], n->wf[1], n->a[2], nullptr, cells, 0);
+   conv_mid(n, n->a[0], n->wf[0], n->a[1], nullptr, nsamp, 0, st);
+   conv_mid(n, n->a[1], n->wf[1], n->a[2], nullptr, nsamp, 0, st);
    k_conv_out<<<gb, tb, 0, st>>>(n->a[2], n->w[3], n->y, cells);
    samrai_b200::add_kernel_launches(5);
    CNN_CHECK(cudaGetLastError());
@@ -479,11 +666,9 @@ int backward(fac_cnn *n, const float *target, const float *mask, long long nsamp
    k_bwd_weight_out<<<wb, T * C, 0, n->stream>>>(n->a[2], n->dy, n->gw[3], cells, per_block);
    k_bwd_out_data<<<gb, tb, 0, n->stream>>>(n->dy, n->w[3], n->a[2], n->d[2], cells);
    k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[1], n->d[2], n->gw[2], cells, per_block);
-   const long long tiles = (cells + 15) / 16;
-   const unsigned mb = (unsigned)std::min<long long>((tiles + 7) / 8, 148 * 16);
-   k_conv_mid<<<mb, 256, 0, n->stream>>>(n->d[2], n->wd[1], n->d[1], n->a[1], cells, 1);
+   conv_mid(n, n->d[2], n->wd[1], n->d[1], n->a[1], nsamp, 1, n->stream);
    k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[0], n->d[1], n->gw[1], cells, per_block);
-   k_conv_mid<<<mb, 256, 0, n->stream>>>(n->d[1], n->wd[0], n->d[0], n->a[0], cells, 1);
+   conv_mid(n, n->d[1], n->wd[0], n->d[0], n->a[0], nsamp, 1, n->stream);
    k_bwd_weight_in<<<wb, T * C, 0, n->stream>>>(n->x0, n->d[0], n->gw[0], cells, per_block);
    samrai_b200::add_kernel_launches(8);
    CNN_CHECK(cudaGetLastError());
@@ -560,8 +745,16 @@ int fac_cnn_create(fac_cnn **out, int device, int max_batch, unsigned long long 
       if ((rc = dalloc(n, &n->a[l], cells * C * 2)) || (rc = dalloc(n, &n->d[l], cells * C * 2)))
          return fail(rc);
    if ((rc = dalloc(n, &n->y, cells * 4)) || (rc = dalloc(n, &n->dy, cells * 4)) ||
-       (rc = dalloc(n, &n->loss, sizeof(double))))
+       (rc = dalloc(n, &n->loss, sizeof(double))) || (rc = dalloc(n, &n->kerr, sizeof(int))))
       return fail(rc);
+   int sms = 0;
+   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+       cudaFuncSetAttribute(k_conv_mid_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            kTcSmem) != cudaSuccess)
+      return fail(FAC_ERR_CUDA);
+   n->tc_grid = 2 * sms;
+   if (cudaMemsetAsync(n->kerr, 0, sizeof(int), n->stream) != cudaSuccess)
+      return fail(FAC_ERR_CUDA);
    // He initialisation from a seeded host generator (splitmix64 + Box-Muller)
    unsigned long long st = seed * 0x9E3779B97F4A7C15ull + 1;
    auto next = [&]() {
@@ -645,8 +838,7 @@ int fac_cnn_forward(fac_cnn *n, const float *x, long long nsamp, float *y)
    if ((rc = forward(n, x, nsamp))) return rc;
    CNN_CHECK(cudaMemcpyAsync(y, n->y, nsamp * S3 * sizeof(float), cudaMemcpyDeviceToDevice,
                              n->stream));
-   CNN_CHECK(cudaStreamSynchronize(n->stream));
-   return FAC_OK;
+   return device_status(n);
 }
 
 int fac_cnn_gradients(fac_cnn *n, const float *x, const float *target, const float *mask,
@@ -676,7 +868,7 @@ int fac_cnn_gradients(fac_cnn *n, const float *x, const float *target, const flo
       if (dst[k])
          CNN_CHECK(cudaMemcpyAsync(dst[k], n->gw[k], kSizes[k] * 4, cudaMemcpyDeviceToHost,
                                    n->stream));
-   CNN_CHECK(cudaStreamSynchronize(n->stream));
+   if ((rc = device_status(n))) return rc;
    if (loss) *loss = l / msum;
    return FAC_OK;
 }
@@ -703,7 +895,7 @@ int fac_cnn_train_step(fac_cnn *n, const float *x, const float *target, const fl
    if (loss) {
       double l = 0;
       CNN_CHECK(cudaMemcpyAsync(&l, n->loss, sizeof(double), cudaMemcpyDeviceToHost, n->stream));
-      CNN_CHECK(cudaStreamSynchronize(n->stream));
+      if ((rc = device_status(n))) return rc;
       *loss = l / mask_sum;
    }
    return FAC_OK;

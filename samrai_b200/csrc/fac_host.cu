@@ -3085,6 +3085,10 @@ void run_graph(fac_ctx *c, cudaGraphExec_t &exec, long long &launches, Body body
 
 }  // namespace
 
+// Relative size of the second Gram-Schmidt correction below which FGMRES
+// skips it (see the Gram-Schmidt step).
+constexpr double kReorthTol = 1e-10;
+
 void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *residual)
 {
    const int np = nprob(c);
@@ -3202,8 +3206,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             run_graph(c, c->apply_exec, c->apply_launches, apply_body);
          }
          // classical Gram-Schmidt, W = -TR - sum h_i V_i into slot j + 1,
-         // repeated once for the problems whose W lost more than half its
-         // norm (cancellation)
+         // repeated once for the problems that need it (below)
          const int K = j + 1;
          kry_dots(c, 0, 0, K, dots, FAC_TR, true);  // <TR, V_i>, i <= j, and <TR, TR>
          std::vector<double> before(np, 0.0);
@@ -3227,29 +3230,43 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             kry_combine(c, j + 1, a, 0, K, coef, &dots, FAC_TR);
             for (int p = 0; p < np; ++p) nw[p] = dots[p];
          }
+         // Second pass where it is needed.  With the fused pass the d_i are
+         // measured: the pass would move W' by ||d||, so it runs where
+         // ||d|| > kReorthTol ||W'||.  Skipping it leaves V_{j+1} that far from
+         // orthogonal to the V_i; the Arnoldi relation A Z = V H holds either
+         // way, and a basis that far from orthonormal changes the residual
+         // estimate only by a factor 1 + O(j kReorthTol).  Without the d_i:
+         // where W' lost more than half its norm (cancellation).
          bool again = false;
          std::vector<int> reo(np, 0);
-         for (int p = 0; p < np; ++p)
-            if (act[p] && nw[p] < 0.25 * before[p]) reo[p] = again = true;
          // squared norm of V_{j+1} before its normalisation, and -d_i of the
          // second pass (0 for the problems that need none)
          std::vector<double> hn2(nw), dcoef((size_t)np * K, 0.0);
-         bool exact = again && !fused;
-         if (again && fused) {
+         bool exact = false;
+         if (fused) {
             for (int p = 0; p < np; ++p) {
-               if (!reo[p]) continue;
+               if (!act[p]) continue;
                double s2 = 0.0;
+               for (int i = 0; i < K; ++i) {
+                  const double d = d2[(size_t)p * (K + 1) + i];
+                  s2 += d * d;
+               }
+               if (!(s2 > kReorthTol * kReorthTol * nw[p])) continue;
+               reo[p] = again = true;
                for (int i = 0; i < K; ++i) {
                   const double d = d2[(size_t)p * (K + 1) + i];
                   h[((size_t)p * H + i) * m + j] += d;
                   dcoef[(size_t)p * K + i] = -d;
-                  s2 += d * d;
                }
                // W' - sum d_i V_i is orthogonal to the V_i: its norm follows
                // from ||W'|| and the d_i while these are small against W'
                hn2[p] = nw[p] - s2;
                if (!(hn2[p] > 0.5 * nw[p])) exact = true;
             }
+         } else {
+            for (int p = 0; p < np; ++p)
+               if (act[p] && nw[p] < 0.25 * before[p]) reo[p] = again = true;
+            exact = again;
          }
          if (exact) {
             // second pass as its own combination, with the norm of the result

@@ -1620,20 +1620,25 @@ k_combine(const Chunk *__restrict__ chunks, int nwork, double *x, const double *
    WORK_LOOP(ch) {
       const double ap = a[ch.patch];
       const double *cp = coef + (long long)ch.patch * K;
+      // a problem's trailing zero coefficients add nothing: their vectors
+      // are not read (a problem that needs no second Gram-Schmidt pass
+      // reads only x)
+      int Kp = K;
+      while (Kp > 0 && cp[Kp - 1] == 0.0) --Kp;
       double sum = 0.0;
       // four cells of a thread at a time keep (K + 1) x 4 loads in flight
 #pragma unroll 4
       for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
          const long long c = (long long)ch.begin + t;
          double v = ap * xin[c];
-         for (int i0 = 0; i0 < K; i0 += kVecBlock) {
+         for (int i0 = 0; i0 < Kp; i0 += kVecBlock) {
             const double *vb = V + (long long)i0 * vstride + c;
             double vv[kVecBlock];
 #pragma unroll
-            for (int q = 0; q < kVecBlock; ++q) vv[q] = i0 + q < K ? vb[(long long)q * vstride] : 0.0;
+            for (int q = 0; q < kVecBlock; ++q) vv[q] = i0 + q < Kp ? vb[(long long)q * vstride] : 0.0;
 #pragma unroll
             for (int q = 0; q < kVecBlock; ++q)
-               if (i0 + q < K) v = v + cp[i0 + q] * vv[q];
+               if (i0 + q < Kp) v = v + cp[i0 + q] * vv[q];
          }
          x[c] = v;
          if (x2) x2[c] = v;

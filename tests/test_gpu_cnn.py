@@ -58,3 +58,23 @@ def test_training_lowers_loss(require_gpu):
               for _ in range(150)]
     assert losses[-1] < 0.3 * losses[0], (losses[0], losses[-1])
     net.close()
+
+
+def test_batch_walk_matches_single_samples(require_gpu):
+    """A batch of many samples (each CTA of the tensor-core convolution walks
+    several slabs, its accumulator barrier changing phase between them) gives
+    bit for bit what the same samples give alone."""
+    import torch
+    rng = np.random.default_rng(2)
+    n = 160
+    net = fac.CNN(max_batch=n, seed=7)
+    x = torch.from_numpy(rng.standard_normal((n, S, S, S)).astype(np.float32)).cuda()
+    y = torch.zeros_like(x)
+    net.forward(x.data_ptr(), n, y.data_ptr())
+    for first in (0, 77, n - 2):
+        xs = x[first:first + 2].contiguous()
+        ys = torch.zeros_like(xs)
+        net.forward(xs.data_ptr(), 2, ys.data_ptr())
+        assert torch.equal(ys, y[first:first + 2])
+    assert torch.isfinite(y).all()
+    net.close()
