@@ -16,8 +16,11 @@
 // the A operand's start address.  The same kernel computes the backward
 // pass with respect to the data (taps reversed, weights transposed, gated by
 // the forward ReLU mask).  Weight gradients of the 16 -> 16 layers are 27
-// small GEMMs reducing over all cells, one warp per tap (mma.sync).  The
-// 1 -> 16 and 16 -> 1 layers are tiny and run on the FP32 cores.
+// 16 x 16 GEMMs reducing over all cells, from the same staged slabs
+// (ldmatrix + mma.sync, three taps per warp).  Layer 4 (16 -> 1) runs on
+// the same tensor-core kernel with its weights padded to 16 output
+// channels; layer 1 (1 -> 16), its weight gradient and the other small
+// gradients run on the FP32 cores.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -197,11 +200,13 @@ __device__ __forceinline__ void tc_ld16(unsigned taddr, unsigned *v)
 }
 
 // wt: [27][16 out][16 in] BF16.  mode 0: y = relu(acc); mode 1: y = acc *
-// (gate > 0).  A wait that runs out sets *err and ends the CTA's work.
+// (gate > 0); mode 2 (layer 4, its weights padded to 16 output channels):
+// yf = output channel 0 in FP32.  A wait that runs out sets *err and ends
+// the CTA's work.
 __global__ void __launch_bounds__(kTcThreads)
 k_conv_mid_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ wt,
               __nv_bfloat16 *__restrict__ y, const __nv_bfloat16 *__restrict__ gate,
-              long long nsamp, int mode, int *__restrict__ err)
+              float *__restrict__ yf, long long nsamp, int mode, int *__restrict__ err)
 {
    extern __shared__ __align__(128) unsigned char tsm[];
    uint4 *p0 = reinterpret_cast<uint4 *>(tsm);                   // channels 0..7
@@ -300,6 +305,10 @@ k_conv_mid_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restri
          if (zz > kTcNz || px < 1 || px > S || py < 1 || py > S) continue;
          const long long cell =
             smp * S3 + (px - 1) + S * ((py - 1) + (long long)S * (z0 - 1 + zz));
+         if (mode == 2) {
+            yf[cell] = __uint_as_float(v[0]);
+            continue;
+         }
          float o[16];
 #pragma unroll
          for (int c = 0; c < 16; ++c) o[c] = __uint_as_float(v[c]);
@@ -332,34 +341,6 @@ k_conv_mid_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restri
                    "r"(kTcCols)
                    : "memory");
    }
-}
-
-// ---------------------------------------------------------------------------
-// layer 4: 16 -> 1 (FP32 output)
-// ---------------------------------------------------------------------------
-__global__ void k_conv_out(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ w4,
-                           float *__restrict__ y, long long ncells)
-{
-   __shared__ float w[T * C];
-   for (int i = threadIdx.x; i < T * C; i += blockDim.x)
-      w[i] = __bfloat162float(__float2bfloat16_rn(w4[i]));
-   __syncthreads();
-   const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (cell >= ncells) return;
-   int cx, cy, cz;
-   cell_coords(cell, cx, cy, cz);
-   float acc = 0.f;
-   for (int t = 0; t < T; ++t) {
-      const long long nb = neighbour(cell, cx, cy, cz, t);
-      if (nb < 0) continue;
-#pragma unroll
-      for (int c = 0; c < C; c += 2) {
-         const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162 *>(x + nb * C + c);
-         acc += w[t * C + c] * __bfloat162float(v.x);
-         acc += w[t * C + c + 1] * __bfloat162float(v.y);
-      }
-   }
-   y[cell] = acc;
 }
 
 // masked MSE: dy = 2/m * mask * (y - target); loss += sum(mask*(y-target)^2)
@@ -411,104 +392,257 @@ __global__ void k_bwd_out_data(const float *__restrict__ dy, const float *__rest
    }
 }
 
-// weight gradient of a 16 -> 16 layer: dw[t][ci][co] += sum_cells
-// x[cell + off_t][ci] * dy[cell][co].  27 warps per block, warp w = tap w,
-// each block reduces a run of `per_block` cells (a multiple of 16).
-__global__ void __launch_bounds__(T * 32)
-k_bwd_weight_mid(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ dy,
-                 float *__restrict__ dw, long long ncells, int per_block)
+// weight gradient of a 16 -> 16 layer: dw[t][ci][co] += sum over cells of
+// x[cell + off_t][ci] * dy[cell][co].  Slabs as in k_conv_mid_tc: the
+// slab's input box (zero halo) and the gradient at its output rows (zero at
+// the halo rows) are staged in shared memory in channel planes of 16 bytes
+// per cell; warp w owns taps 3w .. 3w + 2 (one x-row of taps) and multiplies
+// A = x^T (16 in-channels x 16 cells, ldmatrix.trans at the tap's shifted
+// rows) by B = dy (16 cells x 8 out-channels, ldmatrix.trans) with
+// mma.sync m16n8k16 over every 16 rows of the slab.  The tensor cores'
+// tcgen05 form needs M >= 64 output rows, and with 16 x 16 outputs per tap
+// and the tap as a row shift no operand layout gives that.  Each CTA sums
+// its slabs in registers and adds them once.
+constexpr int kWgWarps = T / 3;                      // 9 warps, 3 taps each
+constexpr int kWgThreads = 32 * kWgWarps;
+constexpr int kWgRows = 128 * kTcTiles;              // output rows per slab
+constexpr int kWgSmem = 2 * kTcPlaneBytes + 2 * kWgRows * 16;
+static_assert(T % 3 == 0, "three taps per warp");
+static_assert(kWgRows % 16 == 0, "whole k-steps");
+static_assert(kTcFront + kTcPlane + kWgRows + kTcReach <= kTcSpan, "x rows in the box");
+
+__device__ __forceinline__ void ldm_x4_trans(unsigned addr, uint32_t *r)
 {
-   const int t = threadIdx.x >> 5;
-   const int lane = threadIdx.x & 31;
-   const int g = lane >> 2, q = lane & 3;
-   const long long b0 = (long long)blockIdx.x * per_block;
-   const long long b1 = b0 + per_block < ncells ? b0 + per_block : ncells;
-   float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-   for (long long k0 = b0; k0 < b1; k0 += 16) {
-      // the four cells this thread touches: k0 + 2q, +1, +8, +9
-      long long cl[4] = {k0 + 2 * q, k0 + 2 * q + 1, k0 + 2 * q + 8, k0 + 2 * q + 9};
-      long long nb[4];
-      bool ok[4];
+   asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                : "r"(addr));
+}
+
+__global__ void __launch_bounds__(kWgThreads)
+k_bwd_weight_mid(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ dy,
+                 float *__restrict__ dw, long long nsamp)
+{
+   extern __shared__ __align__(128) unsigned char wsm[];
+   uint4 *x0 = reinterpret_cast<uint4 *>(wsm);
+   uint4 *x1 = reinterpret_cast<uint4 *>(wsm + kTcPlaneBytes);
+   uint4 *g0 = reinterpret_cast<uint4 *>(wsm + 2 * kTcPlaneBytes);
+   uint4 *g1 = g0 + kWgRows;
+   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+   for (int i = tid; i < kTcSpan; i += kWgThreads) {
+      x0[i] = make_uint4(0u, 0u, 0u, 0u);
+      x1[i] = make_uint4(0u, 0u, 0u, 0u);
+   }
+   const unsigned sx0 = tc_smem(x0), sx1 = tc_smem(x1), sg0 = tc_smem(g0), sg1 = tc_smem(g1);
+   // ldmatrix.x4: lanes 8j .. 8j + 7 give the rows of matrix j
+   const int mrow = lane & 7, mj = lane >> 3;
+   float acc[3][2][4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-         ok[i] = cl[i] < b1;
-         int cx, cy, cz;
-         cell_coords(cl[i], cx, cy, cz);
-         nb[i] = ok[i] ? neighbour(cl[i], cx, cy, cz, t) : -1;
+   for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+         for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+   int off[3];
+#pragma unroll
+   for (int a = 0; a < 3; ++a) {
+      const int t = 3 * warp + a;
+      off[a] = tap_dx(t) + kTcPx * tap_dy(t) + kTcPlane * tap_dz(t);
+   }
+   const long long nslab = nsamp * kTcSlabs;
+   for (long long slab = blockIdx.x; slab < nslab; slab += gridDim.x) {
+      const long long smp = slab / kTcSlabs;
+      const int z0 = (int)(slab - smp * kTcSlabs) * kTcNz;
+      const __nv_bfloat16 *xs = x + smp * (long long)S3 * C;
+      const __nv_bfloat16 *gs = dy + smp * (long long)S3 * C;
+      __syncthreads();  // the previous slab's reads are done
+      for (int i = tid; i < kTcBox; i += kWgThreads) {
+         const int zz = i / kTcPlane, r = i - zz * kTcPlane;
+         const int py = r / kTcPx, px = r - py * kTcPx;
+         const int cx = px - 1, cy = py - 1, cz = z0 - 1 + zz;
+         uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+         if (cx >= 0 && cx < S && cy >= 0 && cy < S && cz >= 0 && cz < S) {
+            const uint4 *src =
+               reinterpret_cast<const uint4 *>(xs + ((long long)cx + S * (cy + S * cz)) * C);
+            lo = src[0];
+            hi = src[1];
+         }
+         x0[kTcFront + i] = lo;
+         x1[kTcFront + i] = hi;
       }
-      // A[m=ci][k=cell] = x[cell + off_t][ci]
-      auto xa = [&](int i, int ci) -> __nv_bfloat16 {
-         return nb[i] >= 0 ? x[nb[i] * C + ci] : __float2bfloat16_rn(0.f);
-      };
-      uint32_t a[4];
-      {
-         __nv_bfloat162 p;
-         p = __halves2bfloat162(xa(0, g), xa(1, g));
-         a[0] = *reinterpret_cast<uint32_t *>(&p);
-         p = __halves2bfloat162(xa(0, g + 8), xa(1, g + 8));
-         a[1] = *reinterpret_cast<uint32_t *>(&p);
-         p = __halves2bfloat162(xa(2, g), xa(3, g));
-         a[2] = *reinterpret_cast<uint32_t *>(&p);
-         p = __halves2bfloat162(xa(2, g + 8), xa(3, g + 8));
-         a[3] = *reinterpret_cast<uint32_t *>(&p);
+      for (int i = tid; i < kWgRows; i += kWgThreads) {
+         const int rr = kTcPlane + i;  // padded box row of output row i
+         const int zz = rr / kTcPlane, r = rr - zz * kTcPlane;
+         const int py = r / kTcPx, px = r - py * kTcPx;
+         uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+         if (zz <= kTcNz && px >= 1 && px <= S && py >= 1 && py <= S) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(
+               gs + ((long long)(px - 1) + S * ((py - 1) + (long long)S * (z0 - 1 + zz))) * C);
+            lo = src[0];
+            hi = src[1];
+         }
+         g0[i] = lo;
+         g1[i] = hi;
       }
+      __syncthreads();
+      for (int k0 = 0; k0 < kWgRows; k0 += 16) {
+         // B: dy rows k0 .. k0 + 15; matrices (co 0-7, rows +0), (co 0-7,
+         // rows +8), (co 8-15, rows +0), (co 8-15, rows +8)
+         uint32_t b[4];
+         {
+            const unsigned base = (mj >> 1) ? sg1 : sg0;
+            ldm_x4_trans(base + 16u * (unsigned)(k0 + 8 * (mj & 1) + mrow), b);
+         }
+#pragma unroll
+         for (int a = 0; a < 3; ++a) {
+            // A = x^T at the tap's rows: matrices (ci 0-7, rows +0),
+            // (ci 8-15, rows +0), (ci 0-7, rows +8), (ci 8-15, rows +8)
+            uint32_t av[4];
+            const unsigned base = (mj & 1) ? sx1 : sx0;
+            const int row = kTcFront + kTcPlane + k0 + off[a] + 8 * (mj >> 1) + mrow;
+            ldm_x4_trans(base + 16u * (unsigned)row, av);
+            mma_bf16(acc[a][0], av, b[0], b[1]);
+            mma_bf16(acc[a][1], av, b[2], b[3]);
+         }
+      }
+   }
+   const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+   for (int a = 0; a < 3; ++a) {
+      const int t = 3 * warp + a;
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-         const int co = 8 * j + g;
-         auto db = [&](int i) -> __nv_bfloat16 {
-            return ok[i] ? dy[cl[i] * C + co] : __float2bfloat16_rn(0.f);
-         };
-         __nv_bfloat162 p0 = __halves2bfloat162(db(0), db(1));
-         __nv_bfloat162 p1 = __halves2bfloat162(db(2), db(3));
-         mma_bf16(acc[j], a, *reinterpret_cast<uint32_t *>(&p0), *reinterpret_cast<uint32_t *>(&p1));
+         const int co = 8 * j + 2 * q;
+         atomicAdd(&dw[(t * C + g) * C + co], acc[a][j][0]);
+         atomicAdd(&dw[(t * C + g) * C + co + 1], acc[a][j][1]);
+         atomicAdd(&dw[(t * C + g + 8) * C + co], acc[a][j][2]);
+         atomicAdd(&dw[(t * C + g + 8) * C + co + 1], acc[a][j][3]);
+      }
+   }
+}
+
+// Weight gradients of layers 1 and 4 from staged slabs (the slabs of
+// k_conv_mid_tc), on the FP32 cores: thread (tap t, row group g) sums rows
+// g, g + kSgGroups, ... of the slab's output rows into 16 accumulators, and
+// each CTA adds its sums once after all its slabs.
+//   layer 1: dw1[t][co] += sum_cells x0[cell + off_t] * d1[cell][co]
+//   layer 4: dw4[t][ci] += sum_cells a3[cell + off_t][ci] * dy[cell]
+constexpr int kSgGroups = 8;
+constexpr int kSgThreads = T * kSgGroups;            // 216
+constexpr int kSgInSmem = kTcSpan * 4 + kWgRows * 32;
+constexpr int kSgOutSmem = kTcSpan * 32 + kWgRows * 4;
+
+// padded box row i of the slab (z0, sample base) -> cell index in the
+// sample, or -1 outside it
+__device__ __forceinline__ int slab_box_cell(int i, int z0)
+{
+   const int zz = i / kTcPlane, r = i - zz * kTcPlane;
+   const int py = r / kTcPx, px = r - py * kTcPx;
+   const int cx = px - 1, cy = py - 1, cz = z0 - 1 + zz;
+   if (cx < 0 || cx >= S || cy < 0 || cy >= S || cz < 0 || cz >= S) return -1;
+   return cx + S * (cy + S * cz);
+}
+
+// output row i of the slab -> cell index in the sample, or -1 (halo row)
+__device__ __forceinline__ int slab_out_cell(int i, int z0)
+{
+   const int rr = kTcPlane + i;
+   const int zz = rr / kTcPlane, r = rr - zz * kTcPlane;
+   const int py = r / kTcPx, px = r - py * kTcPx;
+   if (zz > kTcNz || px < 1 || px > S || py < 1 || py > S) return -1;
+   return (px - 1) + S * ((py - 1) + S * (z0 - 1 + zz));
+}
+
+__global__ void __launch_bounds__(kSgThreads)
+k_bwd_weight_in(const __nv_bfloat16 *__restrict__ x0, const __nv_bfloat16 *__restrict__ d1,
+                float *__restrict__ dw1, long long nsamp)
+{
+   extern __shared__ __align__(128) unsigned char ssm[];
+   float *xs = reinterpret_cast<float *>(ssm);                       // kTcSpan
+   uint4 *ds = reinterpret_cast<uint4 *>(ssm + kTcSpan * 4);         // 2 per row
+   const int tid = threadIdx.x, t = tid / kSgGroups, g = tid - t * kSgGroups;
+   const int off = tap_dx(t) + kTcPx * tap_dy(t) + kTcPlane * tap_dz(t);
+   for (int i = tid; i < kTcSpan; i += kSgThreads) xs[i] = 0.f;
+   float acc[C];
+#pragma unroll
+   for (int c = 0; c < C; ++c) acc[c] = 0.f;
+   const long long nslab = nsamp * kTcSlabs;
+   for (long long slab = blockIdx.x; slab < nslab; slab += gridDim.x) {
+      const long long smp = slab / kTcSlabs;
+      const int z0 = (int)(slab - smp * kTcSlabs) * kTcNz;
+      __syncthreads();
+      for (int i = tid; i < kTcBox; i += kSgThreads) {
+         const int cell = slab_box_cell(i, z0);
+         xs[kTcFront + i] = cell >= 0 ? __bfloat162float(x0[smp * S3 + cell]) : 0.f;
+      }
+      for (int i = tid; i < kWgRows; i += kSgThreads) {
+         const int cell = slab_out_cell(i, z0);
+         uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+         if (cell >= 0) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(d1 + (smp * S3 + cell) * C);
+            lo = src[0];
+            hi = src[1];
+         }
+         ds[2 * i] = lo;
+         ds[2 * i + 1] = hi;
+      }
+      __syncthreads();
+      for (int k = g; k < kWgRows; k += kSgGroups) {
+         const float xv = xs[kTcFront + kTcPlane + k + off];
+         uint4 dd[2] = {ds[2 * k], ds[2 * k + 1]};
+         const __nv_bfloat16 *dv = reinterpret_cast<const __nv_bfloat16 *>(dd);
+#pragma unroll
+         for (int c = 0; c < C; ++c) acc[c] += xv * __bfloat162float(dv[c]);
       }
    }
 #pragma unroll
-   for (int j = 0; j < 2; ++j) {
-      const int co = 8 * j + 2 * q;
-      atomicAdd(&dw[(t * C + g) * C + co], acc[j][0]);
-      atomicAdd(&dw[(t * C + g) * C + co + 1], acc[j][1]);
-      atomicAdd(&dw[(t * C + g + 8) * C + co], acc[j][2]);
-      atomicAdd(&dw[(t * C + g + 8) * C + co + 1], acc[j][3]);
-   }
+   for (int c = 0; c < C; ++c) atomicAdd(&dw1[t * C + c], acc[c]);
 }
 
-// weight gradient of layer 1: dw1[t][co] += sum_cells x0[cell+off_t] * d1[cell][co]
-__global__ void k_bwd_weight_in(const __nv_bfloat16 *__restrict__ x0,
-                                const __nv_bfloat16 *__restrict__ d1, float *__restrict__ dw1,
-                                long long ncells, int per_block)
+__global__ void __launch_bounds__(kSgThreads)
+k_bwd_weight_out(const __nv_bfloat16 *__restrict__ a3, const float *__restrict__ dy,
+                 float *__restrict__ dw4, long long nsamp)
 {
-   const int t = threadIdx.x / C, co = threadIdx.x % C;  // 432 threads
-   const long long b0 = (long long)blockIdx.x * per_block;
-   const long long b1 = b0 + per_block < ncells ? b0 + per_block : ncells;
-   float acc = 0.f;
-   for (long long cell = b0; cell < b1; ++cell) {
-      int cx, cy, cz;
-      cell_coords(cell, cx, cy, cz);
-      const long long nb = neighbour(cell, cx, cy, cz, t);
-      if (nb < 0) continue;
-      acc += __bfloat162float(x0[nb]) * __bfloat162float(d1[cell * C + co]);
+   extern __shared__ __align__(128) unsigned char ssm[];
+   uint4 *as = reinterpret_cast<uint4 *>(ssm);                       // 2 per cell
+   float *ys = reinterpret_cast<float *>(ssm + kTcSpan * 32);        // kWgRows
+   const int tid = threadIdx.x, t = tid / kSgGroups, g = tid - t * kSgGroups;
+   const int off = tap_dx(t) + kTcPx * tap_dy(t) + kTcPlane * tap_dz(t);
+   for (int i = tid; i < 2 * kTcSpan; i += kSgThreads) as[i] = make_uint4(0u, 0u, 0u, 0u);
+   float acc[C];
+#pragma unroll
+   for (int c = 0; c < C; ++c) acc[c] = 0.f;
+   const long long nslab = nsamp * kTcSlabs;
+   for (long long slab = blockIdx.x; slab < nslab; slab += gridDim.x) {
+      const long long smp = slab / kTcSlabs;
+      const int z0 = (int)(slab - smp * kTcSlabs) * kTcNz;
+      __syncthreads();
+      for (int i = tid; i < kTcBox; i += kSgThreads) {
+         const int cell = slab_box_cell(i, z0);
+         uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+         if (cell >= 0) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(a3 + (smp * S3 + cell) * C);
+            lo = src[0];
+            hi = src[1];
+         }
+         as[2 * (kTcFront + i)] = lo;
+         as[2 * (kTcFront + i) + 1] = hi;
+      }
+      for (int i = tid; i < kWgRows; i += kSgThreads) {
+         const int cell = slab_out_cell(i, z0);
+         ys[i] = cell >= 0 ? dy[smp * S3 + cell] : 0.f;
+      }
+      __syncthreads();
+      for (int k = g; k < kWgRows; k += kSgGroups) {
+         const float yv = ys[k];
+         const int row = kTcFront + kTcPlane + k + off;
+         uint4 aa[2] = {as[2 * row], as[2 * row + 1]};
+         const __nv_bfloat16 *av = reinterpret_cast<const __nv_bfloat16 *>(aa);
+#pragma unroll
+         for (int c = 0; c < C; ++c) acc[c] += __bfloat162float(av[c]) * yv;
+      }
    }
-   atomicAdd(&dw1[t * C + co], acc);
-}
-
-// weight gradient of layer 4: dw4[t][ci] += sum_cells a3[cell+off_t][ci] * dy[cell]
-__global__ void k_bwd_weight_out(const __nv_bfloat16 *__restrict__ a3,
-                                 const float *__restrict__ dy, float *__restrict__ dw4,
-                                 long long ncells, int per_block)
-{
-   const int t = threadIdx.x / C, ci = threadIdx.x % C;
-   const long long b0 = (long long)blockIdx.x * per_block;
-   const long long b1 = b0 + per_block < ncells ? b0 + per_block : ncells;
-   float acc = 0.f;
-   for (long long cell = b0; cell < b1; ++cell) {
-      int cx, cy, cz;
-      cell_coords(cell, cx, cy, cz);
-      const long long nb = neighbour(cell, cx, cy, cz, t);
-      if (nb < 0) continue;
-      acc += __bfloat162float(a3[nb * C + ci]) * dy[cell];
-   }
-   atomicAdd(&dw4[t * C + ci], acc);
+#pragma unroll
+   for (int c = 0; c < C; ++c) atomicAdd(&dw4[t * C + c], acc[c]);
 }
 
 // BF16 copies of the 16 -> 16 weights: forward [t][co][ci] and data-gradient
@@ -522,6 +656,16 @@ __global__ void k_pack_mid(const float *__restrict__ w, __nv_bfloat16 *__restric
    const __nv_bfloat16 v = __float2bfloat16_rn(w[i]);
    wf[(t * C + co) * C + ci] = v;
    wd[((T - 1 - t) * C + ci) * C + co] = v;
+}
+
+// BF16 copy of the 16 -> 1 weights as a 16 -> 16 block [t][co][ci] whose
+// output channels 1..15 are zero (layer 4 on the tensor-core kernel)
+__global__ void k_pack_out(const float *__restrict__ w4, __nv_bfloat16 *__restrict__ wo)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= T * C * C) return;
+   const int t = i / (C * C), co = (i / C) % C, ci = i % C;
+   wo[i] = __float2bfloat16_rn(co == 0 ? w4[t * C + ci] : 0.f);
 }
 
 __global__ void k_round_bf16(const float *__restrict__ w, float *__restrict__ wr, int n)
@@ -566,6 +710,7 @@ struct fac_cnn {
    float *w[4] = {nullptr}, *gw[4] = {nullptr}, *m[4] = {nullptr}, *v[4] = {nullptr};
    float *w1r = nullptr;                 // BF16-rounded w1 for the first layer
    __nv_bfloat16 *wf[2] = {nullptr}, *wd[2] = {nullptr};  // layers 2, 3
+   __nv_bfloat16 *wo = nullptr;          // layer 4 padded to 16 x 16 per tap
    __nv_bfloat16 *x0 = nullptr, *a[3] = {nullptr}, *d[3] = {nullptr};
    float *y = nullptr, *dy = nullptr;
    double *loss = nullptr;
@@ -606,17 +751,27 @@ int pack(fac_cnn *n)
       k_pack_mid<<<(T * C * C + 255) / 256, 256, 0, n->stream>>>(n->w[l + 1], n->wf[l], n->wd[l]);
    }
    k_round_bf16<<<(T * C + 127) / 128, 128, 0, n->stream>>>(n->w[0], n->w1r, T * C);
-   samrai_b200::add_kernel_launches(3);
+   k_pack_out<<<(T * C * C + 255) / 256, 256, 0, n->stream>>>(n->w[3], n->wo);
+   samrai_b200::add_kernel_launches(4);
    CNN_CHECK(cudaGetLastError());
    return FAC_OK;
 }
 
 void conv_mid(fac_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *wt, __nv_bfloat16 *y,
-              const __nv_bfloat16 *gate, long long nsamp, int mode, cudaStream_t st)
+              const __nv_bfloat16 *gate, long long nsamp, int mode, cudaStream_t st,
+              float *yf = nullptr)
 {
    const long long slabs = nsamp * kTcSlabs;
    const unsigned grid = (unsigned)std::min<long long>(slabs, n->tc_grid);
-   k_conv_mid_tc<<<grid, kTcThreads, kTcSmem, st>>>(x, wt, y, gate, nsamp, mode, n->kerr);
+   k_conv_mid_tc<<<grid, kTcThreads, kTcSmem, st>>>(x, wt, y, gate, yf, nsamp, mode, n->kerr);
+}
+
+void weight_mid(fac_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *dw,
+                long long nsamp)
+{
+   const long long slabs = nsamp * kTcSlabs;
+   const unsigned grid = (unsigned)std::min<long long>(slabs, n->tc_grid);
+   k_bwd_weight_mid<<<grid, kWgThreads, kWgSmem, n->stream>>>(x, dy, dw, nsamp);
 }
 
 // the device error flag, after the stream has drained
@@ -641,7 +796,7 @@ int forward_on(fac_cnn *n, const float *x, long long nsamp, cudaStream_t st)
    k_conv_in<<<gb, tb, 0, st>>>(n->x0, n->w1r, n->a[0], cells);
    conv_mid(n, n->a[0], n->wf[0], n->a[1], nullptr, nsamp, 0, st);
    conv_mid(n, n->a[1], n->wf[1], n->a[2], nullptr, nsamp, 0, st);
-   k_conv_out<<<gb, tb, 0, st>>>(n->a[2], n->w[3], n->y, cells);
+   conv_mid(n, n->a[2], n->wo, nullptr, nullptr, nsamp, 2, st, n->y);
    samrai_b200::add_kernel_launches(5);
    CNN_CHECK(cudaGetLastError());
    return FAC_OK;
@@ -661,15 +816,14 @@ int backward(fac_cnn *n, const float *target, const float *mask, long long nsamp
       CNN_CHECK(cudaMemsetAsync(n->gw[l], 0, kSizes[l] * sizeof(float), n->stream));
    CNN_CHECK(cudaMemsetAsync(n->loss, 0, sizeof(double), n->stream));
    k_loss_grad<<<gb, tb, 0, n->stream>>>(n->y, target, mask, inv_m, n->dy, n->loss, cells);
-   const int per_block = 1024;
-   const unsigned wb = (unsigned)((cells + per_block - 1) / per_block);
-   k_bwd_weight_out<<<wb, T * C, 0, n->stream>>>(n->a[2], n->dy, n->gw[3], cells, per_block);
+   const unsigned sg = (unsigned)std::min<long long>(nsamp * kTcSlabs, n->tc_grid);
+   k_bwd_weight_out<<<sg, kSgThreads, kSgOutSmem, n->stream>>>(n->a[2], n->dy, n->gw[3], nsamp);
    k_bwd_out_data<<<gb, tb, 0, n->stream>>>(n->dy, n->w[3], n->a[2], n->d[2], cells);
-   k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[1], n->d[2], n->gw[2], cells, per_block);
+   weight_mid(n, n->a[1], n->d[2], n->gw[2], nsamp);
    conv_mid(n, n->d[2], n->wd[1], n->d[1], n->a[1], nsamp, 1, n->stream);
-   k_bwd_weight_mid<<<wb, T * 32, 0, n->stream>>>(n->a[0], n->d[1], n->gw[1], cells, per_block);
+   weight_mid(n, n->a[0], n->d[1], n->gw[1], nsamp);
    conv_mid(n, n->d[1], n->wd[0], n->d[0], n->a[0], nsamp, 1, n->stream);
-   k_bwd_weight_in<<<wb, T * C, 0, n->stream>>>(n->x0, n->d[0], n->gw[0], cells, per_block);
+   k_bwd_weight_in<<<sg, kSgThreads, kSgInSmem, n->stream>>>(n->x0, n->d[0], n->gw[0], nsamp);
    samrai_b200::add_kernel_launches(8);
    CNN_CHECK(cudaGetLastError());
    return FAC_OK;
@@ -736,7 +890,9 @@ int fac_cnn_create(fac_cnn **out, int device, int max_batch, unsigned long long 
           (rc = dalloc(n, &n->v[l], kSizes[l] * sizeof(float))))
          return fail(rc);
    }
-   if ((rc = dalloc(n, &n->w1r, T * C * sizeof(float)))) return fail(rc);
+   if ((rc = dalloc(n, &n->w1r, T * C * sizeof(float))) ||
+       (rc = dalloc(n, &n->wo, T * C * C * 2)))
+      return fail(rc);
    for (int l = 0; l < 2; ++l)
       if ((rc = dalloc(n, &n->wf[l], T * C * C * 2)) || (rc = dalloc(n, &n->wd[l], T * C * C * 2)))
          return fail(rc);
@@ -750,7 +906,13 @@ int fac_cnn_create(fac_cnn **out, int device, int max_batch, unsigned long long 
    int sms = 0;
    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
        cudaFuncSetAttribute(k_conv_mid_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            kTcSmem) != cudaSuccess)
+                            kTcSmem) != cudaSuccess ||
+       cudaFuncSetAttribute(k_bwd_weight_mid, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            kWgSmem) != cudaSuccess ||
+       cudaFuncSetAttribute(k_bwd_weight_out, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            kSgOutSmem) != cudaSuccess ||
+       cudaFuncSetAttribute(k_bwd_weight_in, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            kSgInSmem) != cudaSuccess)
       return fail(FAC_ERR_CUDA);
    n->tc_grid = 2 * sms;
    if (cudaMemsetAsync(n->kerr, 0, sizeof(int), n->stream) != cudaSuccess)

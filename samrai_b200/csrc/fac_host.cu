@@ -3085,6 +3085,50 @@ void run_graph(fac_ctx *c, cudaGraphExec_t &exec, long long &launches, Body body
 
 }  // namespace
 
+// The learned correction as the second stage of FGMRES's preconditioner:
+// the cycle's correction z (Krylov slot zslot) leaves the residual
+// s = v - A z of the error equation (v in R); the network's prediction of
+// the error for s on the learned level, carried to the coarser levels by
+// restriction, is added to z.  FGMRES takes whatever the preconditioner
+// returns, so this stage needs no step length of its own.
+void learned_precondition(fac_ctx *c, int zslot)
+{
+   OpTimer ot(c, "kry_learned", -1);
+   const int ln = c->learned_level;
+   const int lmax = c->nlev - 1;
+   LevelState &Lc = c->L[ln];
+   zero_field(c, FAC_E);
+   for (int l = 0; l < c->nlev; ++l) {
+      LevelState &L = c->L[l];
+      launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                      L.d_cell_chunks.p, kry_vec(c, l, zslot), L.e.p);
+   }
+   for (int l = lmax - 1; l >= 0; --l) restrict_op(c, FAC_E, FAC_E, l);
+   comp_residual(c, FAC_TR, FAC_E, FAC_R, lmax, 1);
+   for (int l = lmax - 1; l >= 0; --l) {
+      comp_residual(c, FAC_TR, FAC_E, FAC_R, l, 1);
+      restrict_op(c, FAC_TR, FAC_TR, l);
+   }
+   // the gather reads the residual from R of the learned level; v is kept
+   // in its Krylov slot
+   CUDA_CHECK(cudaMemcpyAsync(Lc.r.p, Lc.tr.p, Lc.r.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                              c->stream));
+   learned_gather(c, ln);
+   const float *y = nullptr;
+   if (cnn_forward_on_stream(c->cnn, c->cnn_in.p, Lc.npatch, c->stream, &y) != FAC_OK)
+      throw FacError(FAC_ERR_CUDA, "learned correction: network forward failed");
+   zero_field(c, FAC_E);
+   launch_scatter_samples(c->stream, c->dim, (int)Lc.cell_chunks.size(), Lc.d_patches.p,
+                          Lc.d_cell_chunks.p, y, c->cnn_scale.p, FAC_CNN_BOX, Lc.e.p);
+   for (int l = ln - 1; l >= 0; --l) restrict_op(c, FAC_E, FAC_E, l);
+   for (int l = 0; l <= ln; ++l) {
+      LevelState &L = c->L[l];
+      launch_g1_to_g0<double>(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                              L.d_cell_chunks.p, L.e.p, kry_vec(c, l, zslot), true);
+   }
+   CUDA_CHECK(cudaGetLastError());
+}
+
 // Relative size of the second Gram-Schmidt correction below which FGMRES
 // skips it (see the Gram-Schmidt step).
 constexpr double kReorthTol = 1e-10;
@@ -3194,6 +3238,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                                        L.d_patches.p, L.d_cell_chunks.p, L.e.p,
                                        kry_vec(c, ln, zslot0 + j));
          }
+         if (c->cnn) learned_precondition(c, zslot0 + j);
          // W = A Z_j = -(0 - A Z_j)
          zero_field(c, FAC_E);
          for (int ln = 0; ln < c->nlev; ++ln) {

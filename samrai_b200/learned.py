@@ -144,14 +144,21 @@ def train(net, pairs: PairSet, epochs=4, batch=64, lr=1e-3, seed=0, log=None):
     return losses
 
 
-def evaluate(problems: Sequence, level: int, net, params=None, precision="mixed", device=0):
+def evaluate(problems: Sequence, level: int, net, params=None, precision="mixed", device=0,
+             krylov=0):
     """Solve `problems` without and with the learned correction; returns
-    per-variant cycles, final residuals, residual histories and device ms."""
+    per-variant cycles, final residuals, residual histories and device ms.
+    With krylov > 0 the solves are FGMRES(krylov), the network being the
+    second stage of the preconditioner (after the FAC cycle); else the
+    stationary FAC loop with the network's minimal-residual step after every
+    cycle."""
     out = {}
     for name, use in (("plain", False), ("learned", True)):
         ctx = fac.FacContext(problems, params=dict(params or {}), device=device,
                              precision=precision)
         try:
+            if krylov:
+                ctx.set_krylov(krylov)
             if use:
                 ctx.set_learned(net, level)
             ctx.zero(fac.U)

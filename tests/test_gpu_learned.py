@@ -34,7 +34,14 @@ def test_training_lowers_loss_and_correction_never_hurts(require_gpu):
     # the minimal-residual step length is 0 whenever the prediction would not
     # lower the residual, so the correction never slows convergence down
     assert (lrn["cycles"] <= plain["cycles"] + 1).all()
+    # inside FGMRES(20): the network as the preconditioner's second stage;
+    # the flexible method converges whatever the stage returns
+    kev = learned.evaluate(held_out, level, net, params=PARAMS, krylov=20)
+    kp, kl = kev["plain"], kev["learned"]
+    assert kp["converged"].all() and kl["converged"].all()
     gain = {"loss_before": before, "loss_after": after, "epoch_losses": losses,
             "cycles_plain": plain["cycles"].tolist(), "cycles_learned": lrn["cycles"].tolist(),
-            "ms_plain": plain["ms"], "ms_learned": lrn["ms"]}
+            "ms_plain": plain["ms"], "ms_learned": lrn["ms"],
+            "fgmres_its_plain": kp["cycles"].tolist(), "fgmres_its_learned": kl["cycles"].tolist(),
+            "fgmres_ms_plain": kp["ms"], "fgmres_ms_learned": kl["ms"]}
     print(json.dumps(gain))
