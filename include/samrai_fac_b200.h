@@ -386,8 +386,8 @@ int fac_cnn_train_step(fac_cnn *net, const float *x, const float *target,
  * so the FAC residual never grows.  Under FGMRES (fac_set_krylov > 0) the
  * network is instead the second stage of the preconditioner: for the
  * residual s = v - A z that the FAC cycle's correction z leaves, its
- * prediction of the error is added to z (no step length; the flexible
- * method takes the combined correction).  Patches of `level` must have at most
+ * prediction e of the error goes into z += alpha e with the same
+ * minimal-residual alpha for s.  Patches of `level` must have at most
  * FAC_CNN_BOX-2 cells per side and the network a batch of at least the
  * level's patch count. */
 int fac_set_learned(fac_ctx *ctx, fac_cnn *net, int level);

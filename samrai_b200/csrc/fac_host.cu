@@ -1000,6 +1000,7 @@ void build_stage_units(fac_ctx *c, int ln)
       U.clear();
       int maxb = 0;
       bool decode_ok = true;
+      std::vector<int> ubytes;  // stage bytes of each unit
       for (int ip = 0; ip < L.npatch; ++ip) {
          const Box &b = L.box[ip];
          const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
@@ -1128,9 +1129,50 @@ void build_stage_units(fac_ctx *c, int ln)
             copies[first].total = (int)total;
             U.push_back({ip, first, (int)copies.size() - first, (int)hdrs.size()});
             hdrs.push_back(rec);
+            ubytes.push_back(sp.bytes);
             s0 += ns;
          }
          if (s0 != nslow) throw FacError(FAC_ERR_ARG, "staged units do not tile the patch");
+      }
+      // Small units share a stage: consecutive units of one problem are
+      // packed back to back (each at a 128-byte boundary) while the packed
+      // bytes stay within the stage budget and the copies within
+      // kStageMaxCopies; every header but the last gives the stage offset of
+      // the next.  Fewer, fuller stages: the per-stage cost of
+      // the barriers and the copy list is paid once for several patches.
+      {
+         std::vector<Chunk> P;
+         std::vector<UnitCopy> pc;
+         size_t u = 0;
+         while (u < U.size()) {
+            const int prob = L.hp[U[u].patch].prob;
+            const int first = (int)pc.size();
+            int base = 0, ncopy = 0, prev = -1;
+            long long total = 0;
+            size_t v = u;
+            for (; v < U.size() && L.hp[U[v].patch].prob == prob; ++v) {
+               const int nc = U[v].count;
+               if (v > u && (base + ubytes[v] > c->stage_budget || ncopy + nc > kStageMaxCopies))
+                  break;
+               for (int q = 0; q < nc; ++q) {
+                  UnitCopy cp = copies[U[v].begin + q];
+                  cp.dst_off += base;
+                  cp.total = 0;
+                  total += cp.nbytes;
+                  pc.push_back(cp);
+               }
+               if (prev >= 0) hdrs[prev].h.next = base;
+               prev = U[v].aux;
+               ncopy += nc;
+               maxb = std::max(maxb, base + ubytes[v]);
+               base += (ubytes[v] + 127) & ~127;
+            }
+            pc[first].total = (int)total;
+            P.push_back({U[u].patch, first, ncopy, U[u].aux});
+            u = v;
+         }
+         U.swap(P);
+         copies.swap(pc);
       }
       // stage_depth stages per CTA after the barriers and copy sources; a
       // level whose units do not fit runs the unstaged pass
@@ -2467,9 +2509,19 @@ void fac_cycle_recursive(fac_ctx *c, int ln)
    if (ln == 0) {
       solve_coarsest(c);
    } else {
-      smooth(c, FAC_E, FAC_R, ln, c->pre_sweeps, -1.0);
-      comp_residual(c, FAC_TR, FAC_E, FAC_R, ln, 1);
-      restrict_op(c, FAC_TR, FAC_R, ln - 1);
+      if (c->pre_sweeps > 0) {
+         smooth(c, FAC_E, FAC_R, ln, c->pre_sweeps, -1.0);
+         comp_residual(c, FAC_TR, FAC_E, FAC_R, ln, 1);
+         restrict_op(c, FAC_TR, FAC_R, ln - 1);
+      } else {
+         // Without pre-smoothing the error is still zero on this level and
+         // on the coarser ones (zeroed before the cycle, visited later), so
+         // the composite residual f - A 0 is f itself, bit for bit (every
+         // flux is D (0 - 0) = +0, and the finer level's saved fluxes, which
+         // nothing in this cycle reads, would be +0 too): f is restricted as
+         // it is.
+         restrict_op(c, FAC_R, FAC_R, ln - 1);
+      }
       fac_cycle_recursive(c, ln - 1);
       prolong_correct(c, FAC_E, FAC_E, ln);
       smooth(c, FAC_E, FAC_R, ln, c->post_sweeps, -1.0);
@@ -2675,11 +2727,17 @@ void fac_cycle_mixed(fac_ctx *c, int ln)
       return;
    }
    launch_convert<double, float>(c->stream, L.r.p, L.r32.p, (long long)L.r.n);
-   // every e32 is zeroed before the cycle, and coarser levels are reached
-   // only after this pre-smoothing
-   smooth32(c, ln, c->pre_sweeps, true);
-   comp_residual_mixed(c, ln);
-   restrict_op(c, FAC_TR, FAC_R, ln - 1);
+   if (c->pre_sweeps > 0) {
+      // every e32 is zeroed before the cycle, and coarser levels are reached
+      // only after this pre-smoothing
+      smooth32(c, ln, c->pre_sweeps, true);
+      comp_residual_mixed(c, ln);
+      restrict_op(c, FAC_TR, FAC_R, ln - 1);
+   } else {
+      // no pre-smoothing: the residual of the still zero error is f, bit
+      // for bit (fac_cycle_recursive)
+      restrict_op(c, FAC_R, FAC_R, ln - 1);
+   }
    fac_cycle_mixed(c, ln - 1);
    prolong32(c, ln);
    smooth32(c, ln, c->post_sweeps);
@@ -3086,33 +3144,50 @@ void run_graph(fac_ctx *c, cudaGraphExec_t &exec, long long &launches, Body body
 }  // namespace
 
 // The learned correction as the second stage of FGMRES's preconditioner:
-// the cycle's correction z (Krylov slot zslot) leaves the residual
-// s = v - A z of the error equation (v in R); the network's prediction of
-// the error for s on the learned level, carried to the coarser levels by
-// restriction, is added to z.  FGMRES takes whatever the preconditioner
-// returns, so this stage needs no step length of its own.
-void learned_precondition(fac_ctx *c, int zslot)
+// the cycle's correction z (Krylov slot zslot) for v (slot vslot) leaves
+// the residual s = v - A z of the error equation; the network predicts the
+// error e for s on the learned level (carried to the coarser levels by
+// restriction), and z += alpha e with the per-problem minimal-residual
+// alpha = <s, A e> / <A e, A e> (weighted; 0 when it would not lower the
+// residual), so the stage never makes the preconditioner's residual worse.
+void learned_precondition(fac_ctx *c, int vslot, int zslot)
 {
    OpTimer ot(c, "kry_learned", -1);
    const int ln = c->learned_level;
    const int lmax = c->nlev - 1;
+   const int np = nprob(c);
    LevelState &Lc = c->L[ln];
+   // the cycle left restricted residuals in R on the coarser levels: R = v
+   for (int l = 0; l < c->nlev; ++l) {
+      LevelState &L = c->L[l];
+      if (L.n0 > 0)
+         CUDA_CHECK(cudaMemcpyAsync(L.r.p, kry_vec(c, l, vslot), (size_t)L.n0 * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+   }
+   // composite residual of the error equation with rhs R into TR for the
+   // correction in E (finer values restricted onto covered cells first)
+   auto residual_of_e = [&]() {
+      for (int l = lmax - 1; l >= 0; --l) restrict_op(c, FAC_E, FAC_E, l);
+      comp_residual(c, FAC_TR, FAC_E, FAC_R, lmax, 1);
+      for (int l = lmax - 1; l >= 0; --l) {
+         comp_residual(c, FAC_TR, FAC_E, FAC_R, l, 1);
+         restrict_op(c, FAC_TR, FAC_TR, l);
+      }
+   };
    zero_field(c, FAC_E);
    for (int l = 0; l < c->nlev; ++l) {
       LevelState &L = c->L[l];
       launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
                       L.d_cell_chunks.p, kry_vec(c, l, zslot), L.e.p);
    }
-   for (int l = lmax - 1; l >= 0; --l) restrict_op(c, FAC_E, FAC_E, l);
-   comp_residual(c, FAC_TR, FAC_E, FAC_R, lmax, 1);
-   for (int l = lmax - 1; l >= 0; --l) {
-      comp_residual(c, FAC_TR, FAC_E, FAC_R, l, 1);
-      restrict_op(c, FAC_TR, FAC_TR, l);
+   residual_of_e();
+   // R = s
+   for (int l = 0; l < c->nlev; ++l) {
+      LevelState &L = c->L[l];
+      if (L.n0 > 0)
+         CUDA_CHECK(cudaMemcpyAsync(L.r.p, L.tr.p, (size_t)L.n0 * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
    }
-   // the gather reads the residual from R of the learned level; v is kept
-   // in its Krylov slot
-   CUDA_CHECK(cudaMemcpyAsync(Lc.r.p, Lc.tr.p, Lc.r.n * sizeof(double), cudaMemcpyDeviceToDevice,
-                              c->stream));
    learned_gather(c, ln);
    const float *y = nullptr;
    if (cnn_forward_on_stream(c->cnn, c->cnn_in.p, Lc.npatch, c->stream, &y) != FAC_OK)
@@ -3120,11 +3195,21 @@ void learned_precondition(fac_ctx *c, int zslot)
    zero_field(c, FAC_E);
    launch_scatter_samples(c->stream, c->dim, (int)Lc.cell_chunks.size(), Lc.d_patches.p,
                           Lc.d_cell_chunks.p, y, c->cnn_scale.p, FAC_CNN_BOX, Lc.e.p);
-   for (int l = ln - 1; l >= 0; --l) restrict_op(c, FAC_E, FAC_E, l);
-   for (int l = 0; l <= ln; ++l) {
+   // TR = s - A e, then alpha from <s, s - TR> and <s - TR, s - TR>
+   residual_of_e();
+   CUDA_CHECK(cudaMemsetAsync(c->dot_acc.p, 0, np * sizeof(double2), c->stream));
+   for (int l = 0; l < c->nlev; ++l) {
+      LevelState &L = c->L[l];
+      launch_dot_pair(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                      L.d_cell_chunks.p, L.r.p, L.tr.p, L.w.p, L.norm_partial.p,
+                      L.d_prob_cell_chunk_begin.p, np, c->dot_acc.p);
+   }
+   launch_alpha(c->stream, c->dot_acc.p, c->active.p, np, c->alpha.p);
+   for (int l = 0; l < c->nlev; ++l) {
       LevelState &L = c->L[l];
       launch_g1_to_g0<double>(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
-                              L.d_cell_chunks.p, L.e.p, kry_vec(c, l, zslot), true);
+                              L.d_cell_chunks.p, L.e.p, kry_vec(c, l, zslot), true,
+                              c->alpha.p);
    }
    CUDA_CHECK(cudaGetLastError());
 }
@@ -3238,7 +3323,7 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
                                        L.d_patches.p, L.d_cell_chunks.p, L.e.p,
                                        kry_vec(c, ln, zslot0 + j));
          }
-         if (c->cnn) learned_precondition(c, zslot0 + j);
+         if (c->cnn) learned_precondition(c, j, zslot0 + j);
          // W = A Z_j = -(0 - A Z_j)
          zero_field(c, FAC_E);
          for (int ln = 0; ln < c->nlev; ++ln) {

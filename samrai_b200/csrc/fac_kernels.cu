@@ -1727,7 +1727,8 @@ k_combine_dots(const Chunk *__restrict__ chunks, int nwork, double *x, const dou
 template <int DIM, class TS>
 __global__ void __launch_bounds__(kThreads)
 k_g1_to_g0(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
-           const TS *__restrict__ src, double *__restrict__ dst, int add)
+           const TS *__restrict__ src, double *__restrict__ dst, int add,
+           const double *__restrict__ scale)
 {
    WORK_LOOP(ch) {
       const PatchDesc &p = patches[ch.patch];
@@ -1740,7 +1741,8 @@ k_g1_to_g0(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
          const int i = p.lo[0] + ci;
          const int j = p.lo[1] + cj;
          const int k = DIM == 3 ? p.lo[2] + ck : 0;
-         const double v = (double)src[cidx<DIM>(p, p.off1, 1, i, j, k)];
+         double v = (double)src[cidx<DIM>(p, p.off1, 1, i, j, k)];
+         if (scale) v = scale[p.prob] * v;
          dst[p.off0 + lin] = add ? dst[p.off0 + lin] + v : v;
       }
    }
@@ -1890,21 +1892,22 @@ bool launch_combine_dots(cudaStream_t s, int nchunks, const Chunk *chunks, doubl
 
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
-                     const Chunk *chunks, const TS *src, double *dst, bool add)
+                     const Chunk *chunks, const TS *src, double *dst, bool add,
+                     const double *scale)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
       k_g1_to_g0<2, TS><<<work_grid(k_g1_to_g0<2, TS>, nchunks), kThreads, 0, s>>>(
-         patches, chunks, nchunks, src, dst, add ? 1 : 0);
+         patches, chunks, nchunks, src, dst, add ? 1 : 0, scale);
    else
       k_g1_to_g0<3, TS><<<work_grid(k_g1_to_g0<3, TS>, nchunks), kThreads, 0, s>>>(
-         patches, chunks, nchunks, src, dst, add ? 1 : 0);
+         patches, chunks, nchunks, src, dst, add ? 1 : 0, scale);
 }
 template void launch_g1_to_g0<double>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
-                                      const double *, double *, bool);
+                                      const double *, double *, bool, const double *);
 template void launch_g1_to_g0<float>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
-                                     const float *, double *, bool);
+                                     const float *, double *, bool, const double *);
 
 void launch_add_combination(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                             const Chunk *chunks, double *u, const double *Z, long long zstride,

@@ -232,6 +232,48 @@ def test_mg_extended_hierarchy_matches_oracle(require_gpu):
     assert (num / den) ** 0.5 <= 1e-9
 
 
+def test_no_presmoothing_matches_oracle(require_gpu):
+    """Without pre-smoothing the cycle restricts f instead of forming the
+    residual of the zero error (the same bits); the oracle forms it.  FP64
+    stationary solve on the extended hierarchy: the same cycle count and
+    residual history, the same solution."""
+    p = configs.extend_hierarchy(configs.config3())
+    prm = dict(coarse_tol=1e-300, coarse_max_it=40, pre_sweeps=0, post_sweeps=3)
+    o = Oracle(p, params=prm)
+    g = fac.FacContext([p], params=prm)
+    ok_o, it_o, res_o, hist_o = o.solve()
+    conv, its, res = g.solve()
+    assert ok_o and conv[0] and its[0] == it_o
+    assert rel_err(g.residual_history(0), hist_o) <= 1e-11
+    _solution_check(p, o, g)
+    g.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_no_presmoothing_fgmres_matches_oracle_solution(precision, require_gpu):
+    """FGMRES with the cycle without pre-smoothing, both precisions: the
+    solution of the oracle's converged plain solve."""
+    p = configs.config3()
+    x = configs.extend_hierarchy(p)
+    prm = dict(coarse_tol=1e-300, coarse_max_it=40, pre_sweeps=0, post_sweeps=3,
+               relative_residual_tol=1e-12, max_cycles=60)
+    g = fac.FacContext([x], params=prm, precision=precision)
+    g.set_krylov(20)
+    conv, its, res = g.solve()
+    assert conv[0]
+    op = Oracle(p, params=dict(coarse_tol=1e-10, relative_residual_tol=1e-12, max_cycles=200))
+    assert op.solve()[0]
+    k = x.virtual_levels
+    num = den = 0.0
+    for ln in range(p.nlev):
+        a = g.download(U, 0, ln + k)
+        b = op.get(U, ln)
+        num += float(np.sum((a - b) ** 2))
+        den += float(np.sum(b ** 2))
+    assert (num / den) ** 0.5 <= 1e-9
+    g.close()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_replay_matches_eager(precision, require_gpu):
     """fac_solve replays one captured CUDA graph per cycle; the eager launch
