@@ -380,6 +380,9 @@ struct LevelState {
    DevArray<double> dxc_prob;                        // per problem dx of level ln-1
    DevArray<unsigned long long> maxres_red, maxres_blk;
    bool one_patch_per_prob = false;  // patch p is problem p's only patch, <= 16384 cells
+   bool facemap_local = false;       // no face of the level has a same-level neighbour
+   int solve_smem = 0;               // shared bytes of the one-launch solve on shared
+                                     // copies (0: that form does not fit)
    DevArray<int> last_patch;
    std::vector<long long> dir_idx;
    DevArray<long long> d_dir_idx;
@@ -1456,6 +1459,9 @@ void build_facemap(fac_ctx *c, int ln)
          throw FacError(FAC_ERR_NESTING, "face table disagrees with the coarse-fine boundary");
    }
    L.fused_ok = ok;
+   L.facemap_local = true;
+   for (long long t = 0; t < L.no; ++t)
+      if (fmap[t] >= 0) L.facemap_local = false;
    L.facemap.upload(fmap, c->stream);
    L.pushmap.upload(pmap, c->stream);
    L.pushmap_h = std::move(pmap);
@@ -1533,6 +1539,20 @@ void build_chunks(fac_ctx *c, int ln)
    L.one_patch_per_prob = L.npatch == np;
    for (int ip = 0; ip < L.npatch; ++ip)
       if (L.hp[ip].prob != ip || L.box[ip].size() > 16384) L.one_patch_per_prob = false;
+   // the one-launch solve on shared copies of u, f, D and C (FP64)
+   L.solve_smem = 0;
+   if (L.one_patch_per_prob && L.facemap_local) {
+      long long most = 0;
+      for (int ip = 0; ip < L.npatch; ++ip) {
+         const Box &b = L.box[ip];
+         long long n = cell_count(c->dim, b, 1) + b.size();
+         if (c->spec.d_variable)
+            for (int a = 0; a < c->dim; ++a) n += side_box(b, a).size();
+         if (c->spec.c_kind == 2) n += b.size();
+         most = std::max(most, 8 * n);
+      }
+      if (most <= kSolveSmemMax) L.solve_smem = (int)most;
+   }
    // one colour pass reads u over the ghosted boxes, f at the active half,
    // writes u at the active half, and reads D on all faces when variable
    double n = 0, ng = 0;
@@ -2287,7 +2307,8 @@ void smooth(fac_ctx *c, int fid_e, int fid_r, int ln, int nsweeps, double tol)
       const int pi = prof_begin(c, 0, L.rb_bytes_prob, 2.0 * nsweeps);
       launch_rbgs_solve<double>(c->stream, c->dim, c->spec, L.npatch, L.d_patches.p, e, r,
                                 L.d.p, L.c.p, fmap, c->bc, nsweeps, tol, c->run.p,
-                                c->sweeps_call.p, L.maxres_red.p, L.maxres_blk.p);
+                                c->sweeps_call.p, L.maxres_red.p, L.maxres_blk.p,
+                                L.solve_smem);
       prof_end(c, pi);
    }
    for (int isweep = 0; isweep < (one_launch ? 0 : nsweeps); ++isweep) {
@@ -4313,6 +4334,10 @@ int fac_ctx_create(fac_ctx **ctx, int dim, int device)
          CUDA_CHECK(cudaGetDeviceCount(&ndev));
          if (device >= ndev) throw FacError(FAC_ERR_ARG, "bad device index");
          CUDA_CHECK(cudaSetDevice(device));
+         // outside any stream capture: the shared-memory limit of the
+         // one-launch coarsest solve (stays set for the process)
+         if (!allow_solve_smem(kSolveSmemMax))
+            throw FacError(FAC_ERR_CUDA, "shared-memory limit of the coarsest solve refused");
       }
       fac_ctx *c = new fac_ctx();
       c->dim = dim;

@@ -163,6 +163,9 @@ struct WaitTest {
 
 // Largest dynamic shared memory of one CTA of the staged colour pass.
 constexpr int kStageSmemMax = 227 * 1024;
+// dynamic shared memory of the one-launch coarsest solve on shared copies
+// (its static reduction array takes part of the per-block limit)
+constexpr int kSolveSmemMax = kStageSmemMax - 1024;
 // staged pass: mbarriers and copy sources ahead of the stages, and the
 // largest ring of stages a CTA holds
 constexpr int kStageBarrierBytes = 128;

@@ -443,6 +443,97 @@ k_rbgs_solve(const PatchDesc *__restrict__ patches, T *__restrict__ u, const T *
    }
 }
 
+// k_rbgs_solve with the patch held in shared memory: u (ghosted), f, the
+// side arrays of D and the C field are copied in once, every sweep runs on
+// the copies, and u is copied back.  rb_slot sees a patch descriptor whose
+// offsets point into the shared copies, so the arithmetic and the order of
+// the updates are those of k_rbgs_solve (the same bits).  For levels whose
+// face table has no same-level neighbour (one patch covering the domain),
+// patch by patch within the shared-memory limit.
+constexpr int kSolveSmemThreads = 512;
+
+template <int DIM, bool DVAR, int CKIND, class T>
+__global__ void __launch_bounds__(kSolveSmemThreads)
+k_rbgs_solve_smem(const PatchDesc *__restrict__ patches, T *__restrict__ u,
+                  const T *__restrict__ f, const T *__restrict__ dside,
+                  const T *__restrict__ cfield, T dconst, T cconst,
+                  const long long *__restrict__ facemap, BcCoefs bc, int nsweeps, double tol,
+                  int *__restrict__ run, long long *__restrict__ sweeps,
+                  unsigned long long *__restrict__ maxres_red,
+                  unsigned long long *__restrict__ maxres_blk)
+{
+   extern __shared__ __align__(16) unsigned char psm[];
+   const int ip = blockIdx.x;
+   const PatchDesc p = patches[ip];
+   const int pr = p.prob;
+   if (!run[pr]) return;
+   const int nx = p.hi[0] - p.lo[0] + 1;
+   const int ny = p.hi[1] - p.lo[1] + 1;
+   const int nz = DIM == 3 ? p.hi[2] - p.lo[2] + 1 : 1;
+   const long long n1 = (long long)(nx + 2) * (ny + 2) * (DIM == 3 ? nz + 2 : 1);
+   const long long n0 = (long long)nx * ny * nz;
+   long long ns[3] = {0, 0, 0};
+   for (int a = 0; a < DIM; ++a)
+      ns[a] = (long long)(nx + (a == 0)) * (ny + (a == 1)) * (DIM == 3 ? nz + (a == 2) : 1);
+   T *su = reinterpret_cast<T *>(psm);
+   T *sf = su + n1;
+   T *sd = sf + n0;
+   T *sc = sd + (DVAR ? ns[0] + ns[1] + ns[2] : 0);
+   for (long long q = threadIdx.x; q < n1; q += blockDim.x) su[q] = u[p.off1 + q];
+   for (long long q = threadIdx.x; q < n0; q += blockDim.x) sf[q] = f[p.off0 + q];
+   if (DVAR) {
+      long long o = 0;
+      for (int a = 0; a < DIM; ++a) {
+         for (long long q = threadIdx.x; q < ns[a]; q += blockDim.x) sd[o + q] = dside[p.offs[a] + q];
+         o += ns[a];
+      }
+   }
+   if (CKIND == 2)
+      for (long long q = threadIdx.x; q < n0; q += blockDim.x) sc[q] = cfield[p.off0 + q];
+   PatchDesc pl = p;
+   pl.off1 = 0;
+   pl.off0 = 0;
+   pl.offs[0] = 0;
+   pl.offs[1] = ns[0];
+   pl.offs[2] = ns[0] + ns[1];
+   __syncthreads();
+   const int hx = (nx + 1) >> 1;
+   const int nslots = hx * ny * nz;
+   const T one = (T)1;
+   const T dxi = one / (T)p.dx[0], dyi = one / (T)p.dx[1];
+   const T dzi = DIM == 3 ? one / (T)p.dx[2] : (T)0;
+   __shared__ double red[kSolveSmemThreads / 32];
+   bool going = true;
+   double mcol[2] = {0.0, 0.0};
+   for (int sw = 0; sw < nsweeps && going; ++sw) {
+      for (int color = 0; color < 2; ++color) {
+         double maxres = 0.0;
+         for (int t = threadIdx.x; t < nslots; t += blockDim.x)
+            rb_slot<DIM, DVAR, CKIND, T, true>(pl, t, nx, ny, hx, dxi, dyi, dzi, false, su, sf,
+                                               sd, sc, nullptr, nullptr, color, dconst, cconst,
+                                               facemap, bc, maxres);
+         for (int o = 16; o > 0; o >>= 1) {
+            const double other = __shfl_down_sync(0xffffffffu, maxres, o);
+            maxres = other > maxres ? other : maxres;
+         }
+         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxres;
+         __syncthreads();
+         double m = red[0];
+         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
+         mcol[color] = m;
+         __syncthreads();
+      }
+      if (threadIdx.x == 0) sweeps[pr] += 1;
+      if (tol >= 0.0) going = (mcol[0] > mcol[1] ? mcol[0] : mcol[1]) > tol;
+   }
+   for (long long q = threadIdx.x; q < n1; q += blockDim.x) u[p.off1 + q] = su[q];
+   if (threadIdx.x == 0) {
+      run[pr] = going ? 1 : 0;
+      maxres_red[ip] = (unsigned long long)__double_as_longlong(mcol[0]);
+      maxres_blk[ip] = (unsigned long long)__double_as_longlong(mcol[1]);
+   }
+}
+
 // ---------------------------------------------------------------------------
 // fluxes into side arrays, with the Ewing fix on coarse-fine faces
 // (computeFluxOnPatch, CellPoissonFACOps.C:2157-2267)
@@ -1945,20 +2036,52 @@ void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int
                                           homogeneous, bc, active);
 }
 
+bool allow_solve_smem(int bytes)
+{
+   bool ok = true;
+   auto set = [&](auto kern) {
+      ok = ok && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      bytes) == cudaSuccess;
+   };
+   set(k_rbgs_solve_smem<2, false, 0, double>);
+   set(k_rbgs_solve_smem<2, false, 1, double>);
+   set(k_rbgs_solve_smem<2, false, 2, double>);
+   set(k_rbgs_solve_smem<2, true, 0, double>);
+   set(k_rbgs_solve_smem<2, true, 1, double>);
+   set(k_rbgs_solve_smem<2, true, 2, double>);
+   set(k_rbgs_solve_smem<3, false, 0, double>);
+   set(k_rbgs_solve_smem<3, false, 1, double>);
+   set(k_rbgs_solve_smem<3, false, 2, double>);
+   set(k_rbgs_solve_smem<3, true, 0, double>);
+   set(k_rbgs_solve_smem<3, true, 1, double>);
+   set(k_rbgs_solve_smem<3, true, 2, double>);
+   return ok;
+}
+
 template <class T>
 void launch_rbgs_solve(cudaStream_t s, int dim, const PoissonSpec &spec, int npatch,
                        const PatchDesc *patches, T *u, const T *f, const T *dside,
                        const T *cfield, const long long *facemap, const BcCoefs &bc,
                        int nsweeps, double tol, int *run, long long *sweeps,
-                       unsigned long long *maxres_red, unsigned long long *maxres_blk)
+                       unsigned long long *maxres_red, unsigned long long *maxres_blk,
+                       int smem)
 {
    if (npatch <= 0 || nsweeps <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    const T dc = (T)spec.d_const, cc = (T)spec.c_const;
-#define RS(D, V, C)                                                                        \
-   k_rbgs_solve<D, V, C, T><<<npatch, kThreads, 0, s>>>(patches, u, f, dside, cfield, dc, cc, \
-                                                        facemap, bc, nsweeps, tol, run,      \
-                                                        sweeps, maxres_red, maxres_blk)
+#define RS(D, V, C)                                                                           \
+   do {                                                                                       \
+      if (smem > 0) {                                                                         \
+         k_rbgs_solve_smem<D, V, C, T><<<npatch, kSolveSmemThreads, smem, s>>>(               \
+            patches, u, f, dside, cfield, dc, cc, facemap, bc, nsweeps, tol, run, sweeps,     \
+            maxres_red, maxres_blk);                                                          \
+      } else {                                                                                \
+         k_rbgs_solve<D, V, C, T><<<npatch, kThreads, 0, s>>>(patches, u, f, dside, cfield,   \
+                                                              dc, cc, facemap, bc, nsweeps,   \
+                                                              tol, run, sweeps, maxres_red,   \
+                                                              maxres_blk);                    \
+      }                                                                                       \
+   } while (0)
    if (dim == 2) {
       if (spec.d_variable) {
          if (spec.c_kind == 2) RS(2, true, 2);
@@ -2481,7 +2604,7 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
                                       const PatchDesc *, T *, const T *, const T *,         \
                                       const T *, const long long *, const BcCoefs &, int,   \
                                       double, int *, long long *, unsigned long long *,     \
-                                      unsigned long long *);                                \
+                                      unsigned long long *, int);                           \
    template void launch_fill_gather<T>(cudaStream_t, long long, const unsigned *,           \
                                        const int *, const unsigned short *,                 \
                                        const FillItem *, const Chunk *, int, const int *,   \

@@ -119,12 +119,19 @@ void launch_fill(cudaStream_t s, const FillItem *items, const Chunk *chunks, int
 // without a coarser level and with one patch per problem (patch b of
 // problem patches[b].prob); run, sweeps and the per-patch red / black
 // residual maxima as the per-pass launches and the sweep check leave them.
+// smem > 0: every patch's arrays fit that many bytes of shared memory and
+// the face table has no same-level neighbour; the sweeps run on shared
+// copies (same bits).
+// Let the shared-memory form of the one-launch solve (FP64) take up to
+// `bytes` of dynamic shared memory on the current device; false if refused.
+bool allow_solve_smem(int bytes);
 template <class T>
 void launch_rbgs_solve(cudaStream_t s, int dim, const PoissonSpec &spec, int npatch,
                        const PatchDesc *patches, T *u, const T *f, const T *dside,
                        const T *cfield, const long long *facemap, const BcCoefs &bc,
                        int nsweeps, double tol, int *run, long long *sweeps,
-                       unsigned long long *maxres_red, unsigned long long *maxres_blk);
+                       unsigned long long *maxres_red, unsigned long long *maxres_blk,
+                       int smem = 0);
 // Ghost fill from a gather list of n elements (copies and constant refines,
 // see k_fill_gather) plus the physical-boundary items of the same fill.
 template <class T>
