@@ -91,7 +91,7 @@ __global__ void k_conv_in(const __nv_bfloat16 *__restrict__ x, const float *__re
       if (nb < 0) continue;
       const float v = __bfloat162float(x[nb]);
 #pragma unroll
-      for (int c = 0; c < C; ++c) acc[c] += w[t * C + c] * v;
+      for (int c = 0; c < C; ++c) acc[c] = __fmaf_rn(w[t * C + c], v, acc[c]);
    }
 #pragma unroll
    for (int c = 0; c < C; c += 2) {
@@ -381,7 +381,7 @@ __global__ void k_bwd_out_data(const float *__restrict__ dy, const float *__rest
       if (nb < 0) continue;
       const float g = dy[nb];
 #pragma unroll
-      for (int c = 0; c < C; ++c) acc[c] += w[t * C + c] * g;
+      for (int c = 0; c < C; ++c) acc[c] = __fmaf_rn(w[t * C + c], g, acc[c]);
    }
 #pragma unroll
    for (int c = 0; c < C; c += 2) {
@@ -521,9 +521,10 @@ k_bwd_weight_mid(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__res
 }
 
 // Weight gradients of layers 1 and 4 from staged slabs (the slabs of
-// k_conv_mid_tc), on the FP32 cores: thread (tap t, row group g) sums rows
-// g, g + kSgGroups, ... of the slab's output rows into 16 accumulators, and
-// each CTA adds its sums once after all its slabs.
+// k_conv_mid_tc), on the FP32 cores with fused multiply-adds (the network's
+// arithmetic needs no particular rounding): thread (tap t, row group g)
+// sums rows g, g + kSgGroups, ... of the slab's output rows into 16
+// accumulators, and each CTA adds its sums once after all its slabs.
 //   layer 1: dw1[t][co] += sum_cells x0[cell + off_t] * d1[cell][co]
 //   layer 4: dw4[t][ci] += sum_cells a3[cell + off_t][ci] * dy[cell]
 constexpr int kSgGroups = 8;
@@ -591,7 +592,7 @@ k_bwd_weight_in(const __nv_bfloat16 *__restrict__ x0, const __nv_bfloat16 *__res
          uint4 dd[2] = {ds[2 * k], ds[2 * k + 1]};
          const __nv_bfloat16 *dv = reinterpret_cast<const __nv_bfloat16 *>(dd);
 #pragma unroll
-         for (int c = 0; c < C; ++c) acc[c] += xv * __bfloat162float(dv[c]);
+         for (int c = 0; c < C; ++c) acc[c] = __fmaf_rn(xv, __bfloat162float(dv[c]), acc[c]);
       }
    }
 #pragma unroll
@@ -638,7 +639,7 @@ k_bwd_weight_out(const __nv_bfloat16 *__restrict__ a3, const float *__restrict__
          uint4 aa[2] = {as[2 * row], as[2 * row + 1]};
          const __nv_bfloat16 *av = reinterpret_cast<const __nv_bfloat16 *>(aa);
 #pragma unroll
-         for (int c = 0; c < C; ++c) acc[c] += __bfloat162float(av[c]) * yv;
+         for (int c = 0; c < C; ++c) acc[c] = __fmaf_rn(__bfloat162float(av[c]), yv, acc[c]);
       }
    }
 #pragma unroll
@@ -816,7 +817,8 @@ int backward(fac_cnn *n, const float *target, const float *mask, long long nsamp
       CNN_CHECK(cudaMemsetAsync(n->gw[l], 0, kSizes[l] * sizeof(float), n->stream));
    CNN_CHECK(cudaMemsetAsync(n->loss, 0, sizeof(double), n->stream));
    k_loss_grad<<<gb, tb, 0, n->stream>>>(n->y, target, mask, inv_m, n->dy, n->loss, cells);
-   const unsigned sg = (unsigned)std::min<long long>(nsamp * kTcSlabs, n->tc_grid);
+   // four CTAs per SM: the FP32-core weight gradients want the warps
+   const unsigned sg = (unsigned)std::min<long long>(nsamp * kTcSlabs, 2LL * n->tc_grid);
    k_bwd_weight_out<<<sg, kSgThreads, kSgOutSmem, n->stream>>>(n->a[2], n->dy, n->gw[3], nsamp);
    k_bwd_out_data<<<gb, tb, 0, n->stream>>>(n->dy, n->w[3], n->a[2], n->d[2], cells);
    weight_mid(n, n->a[1], n->d[2], n->gw[2], nsamp);

@@ -1003,7 +1003,6 @@ void build_stage_units(fac_ctx *c, int ln)
       U.clear();
       int maxb = 0;
       bool decode_ok = true;
-      std::vector<int> ubytes;  // stage bytes of each unit
       for (int ip = 0; ip < L.npatch; ++ip) {
          const Box &b = L.box[ip];
          const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
@@ -1132,50 +1131,9 @@ void build_stage_units(fac_ctx *c, int ln)
             copies[first].total = (int)total;
             U.push_back({ip, first, (int)copies.size() - first, (int)hdrs.size()});
             hdrs.push_back(rec);
-            ubytes.push_back(sp.bytes);
             s0 += ns;
          }
          if (s0 != nslow) throw FacError(FAC_ERR_ARG, "staged units do not tile the patch");
-      }
-      // Small units share a stage: consecutive units of one problem are
-      // packed back to back (each at a 128-byte boundary) while the packed
-      // bytes stay within the stage budget and the copies within
-      // kStageMaxCopies; every header but the last gives the stage offset of
-      // the next.  Fewer, fuller stages: the per-stage cost of
-      // the barriers and the copy list is paid once for several patches.
-      {
-         std::vector<Chunk> P;
-         std::vector<UnitCopy> pc;
-         size_t u = 0;
-         while (u < U.size()) {
-            const int prob = L.hp[U[u].patch].prob;
-            const int first = (int)pc.size();
-            int base = 0, ncopy = 0, prev = -1;
-            long long total = 0;
-            size_t v = u;
-            for (; v < U.size() && L.hp[U[v].patch].prob == prob; ++v) {
-               const int nc = U[v].count;
-               if (v > u && (base + ubytes[v] > c->stage_budget || ncopy + nc > kStageMaxCopies))
-                  break;
-               for (int q = 0; q < nc; ++q) {
-                  UnitCopy cp = copies[U[v].begin + q];
-                  cp.dst_off += base;
-                  cp.total = 0;
-                  total += cp.nbytes;
-                  pc.push_back(cp);
-               }
-               if (prev >= 0) hdrs[prev].h.next = base;
-               prev = U[v].aux;
-               ncopy += nc;
-               maxb = std::max(maxb, base + ubytes[v]);
-               base += (ubytes[v] + 127) & ~127;
-            }
-            pc[first].total = (int)total;
-            P.push_back({U[u].patch, first, ncopy, U[u].aux});
-            u = v;
-         }
-         U.swap(P);
-         copies.swap(pc);
       }
       // stage_depth stages per CTA after the barriers and copy sources; a
       // level whose units do not fit runs the unstaged pass

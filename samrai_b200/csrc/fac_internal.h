@@ -183,9 +183,6 @@ constexpr int kStageDepthMax = 4;
 // Each region is sized for its elements plus a 16-byte alignment shift;
 // off[r] is its start from the stage start (16-byte multiples).
 constexpr int kStageHeader = 256;
-// bulk copies of one stage (units packed into it included): the producer
-// warp issues them in rounds of 32
-constexpr int kStageMaxCopies = 128;
 constexpr int kStageMaxRegions = 18;
 
 struct StagePlan {
@@ -299,9 +296,6 @@ struct UnitHdr {
    int off_u, off_f, off_d[3], off_c;
    int off_push[6];        // per face id 2*axis+side: push targets, -1 if none
    int off_cff[6];         // Ewing fluxes of the same faces, -1 if none
-   int next;               // stage offset of the next unit packed into the
-                           // same stage, 0 if none (the offsets above are
-                           // relative to this unit's header)
 };
 
 // Shared-memory plan of one unit of the staged composite residual: the

@@ -407,9 +407,8 @@ __device__ __forceinline__ void staged_walk(const Chunk *__restrict__ chunks, in
    __syncthreads();
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
    if (warp == kConsumerWarps) {
-      // producer warp: lane i issues copies i, i + 32, ... of a unit (the
-      // host-built copy list, header first; its first entry carries the
-      // byte total)
+      // producer warp: lane i issues copy i of a unit (the host-built copy
+      // list, header first; its first entry carries the byte total)
       // two units ahead of the copies it issues: the chunk of the unit after
       // next and the copy entry of the next unit are loaded while this
       // unit's stage comes free, so no dependent load waits per unit
@@ -438,12 +437,6 @@ __device__ __forceinline__ void staged_walk(const Chunk *__restrict__ chunks, in
          if (lane < ch.count)
             bulk_load(stage + cp.dst_off, sbases->p[cp.src] + cp.src_off, (unsigned)cp.nbytes,
                       &full[st]);
-         // lists of packed units run past the warp: further rounds of 32
-         for (int i = lane + 32; i < ch.count; i += 32) {
-            const UnitCopy cq = copies[ch.begin + i];
-            bulk_load(stage + cq.dst_off, sbases->p[cq.src] + cq.src_off, (unsigned)cq.nbytes,
-                      &full[st]);
-         }
          ch = chn;
          cp = cpn;
          chn = chnn;
@@ -493,23 +486,13 @@ struct ColourPass {
    int offset;
    T dconst, cconst;
    BcCoefs bc;
-   // a stage holds one unit or several small ones packed back to back, each
-   // with its own header (UnitHdr::next chains them)
    __device__ __forceinline__ void first(unsigned char *stage, int tid) const
    {
-      int off = 0;
-      do {
-         stage_update<DIM, DVAR, CKIND, T>(stage + off, tid, u, offset, dconst, cconst);
-         off = reinterpret_cast<const UnitHdr *>(stage + off)->next;
-      } while (off > 0);
+      stage_update<DIM, DVAR, CKIND, T>(stage, tid, u, offset, dconst, cconst);
    }
    __device__ __forceinline__ void second(unsigned char *stage, int tid) const
    {
-      int off = 0;
-      do {
-         stage_push<DIM, T>(stage + off, tid, u, offset, bc);
-         off = reinterpret_cast<const UnitHdr *>(stage + off)->next;
-      } while (off > 0);
+      stage_push<DIM, T>(stage, tid, u, offset, bc);
    }
 };
 
