@@ -817,8 +817,7 @@ int backward(fac_cnn *n, const float *target, const float *mask, long long nsamp
       CNN_CHECK(cudaMemsetAsync(n->gw[l], 0, kSizes[l] * sizeof(float), n->stream));
    CNN_CHECK(cudaMemsetAsync(n->loss, 0, sizeof(double), n->stream));
    k_loss_grad<<<gb, tb, 0, n->stream>>>(n->y, target, mask, inv_m, n->dy, n->loss, cells);
-   // four CTAs per SM: the FP32-core weight gradients want the warps
-   const unsigned sg = (unsigned)std::min<long long>(nsamp * kTcSlabs, 2LL * n->tc_grid);
+   const unsigned sg = (unsigned)std::min<long long>(nsamp * kTcSlabs, n->tc_grid);
    k_bwd_weight_out<<<sg, kSgThreads, kSgOutSmem, n->stream>>>(n->a[2], n->dy, n->gw[3], nsamp);
    k_bwd_out_data<<<gb, tb, 0, n->stream>>>(n->dy, n->w[3], n->a[2], n->d[2], cells);
    weight_mid(n, n->a[1], n->d[2], n->gw[2], nsamp);
