@@ -1779,21 +1779,40 @@ k_combine_dots(const Chunk *__restrict__ chunks, int nwork, double *x, const dou
       double sum[KB + 1];
 #pragma unroll
       for (int q = 0; q <= KB; ++q) sum[q] = 0.0;
-      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
-         const long long c = (long long)ch.begin + t;
-         double vv[KB];
+      // UNR cells of a thread per round, all their loads issued before the
+      // first store (x may be xin, so a store would otherwise hold back the
+      // next cell's loads); the sums still take the cells in the order t,
+      // t + blockDim.x, ... of the one-cell loop
+      constexpr int UNR = KB <= 8 ? 2 : 1;
+      for (int t0 = threadIdx.x; t0 < ch.count; t0 += UNR * blockDim.x) {
+         double vv[UNR][KB], xi[UNR], wv[UNR];
 #pragma unroll
-         for (int q = 0; q < KB; ++q) vv[q] = q < K ? V[(long long)q * vstride + c] : 0.0;
-         double v = ap * xin[c];
+         for (int u = 0; u < UNR; ++u) {
+            const int t = t0 + u * (int)blockDim.x;
+            const long long c = (long long)ch.begin + t;
+            const bool in = t < ch.count;
 #pragma unroll
-         for (int q = 0; q < KB; ++q)
-            if (q < K) v = v + scoef[q] * vv[q];
-         x[c] = v;
-         const double wx = w[c] * v;
+            for (int q = 0; q < KB; ++q)
+               vv[u][q] = in && q < K ? V[(long long)q * vstride + c] : 0.0;
+            xi[u] = in ? xin[c] : 0.0;
+            wv[u] = in ? w[c] : 0.0;
+         }
 #pragma unroll
-         for (int q = 0; q < KB; ++q)
-            if (q < K) sum[q] += wx * vv[q];
-         sum[KB] += wx * v;
+         for (int u = 0; u < UNR; ++u) {
+            const int t = t0 + u * (int)blockDim.x;
+            if (t >= ch.count) break;
+            const long long c = (long long)ch.begin + t;
+            double v = ap * xi[u];
+#pragma unroll
+            for (int q = 0; q < KB; ++q)
+               if (q < K) v = v + scoef[q] * vv[u][q];
+            x[c] = v;
+            const double wx = wv[u] * v;
+#pragma unroll
+            for (int q = 0; q < KB; ++q)
+               if (q < K) sum[q] += wx * vv[u][q];
+            sum[KB] += wx * v;
+         }
       }
 #pragma unroll
       for (int q = 0; q <= KB; ++q) {
