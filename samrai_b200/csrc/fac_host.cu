@@ -376,6 +376,8 @@ struct LevelState {
    ItemList<FluxCoarsenItem> fcoarsen;               // from level ln+1 into this
    ItemList<FillItem> tmp_fill;                      // coarse interpolation arrays
    ItemList<ProlongItem> prolong;                    // from level ln-1 into this
+   ItemList<ProlongItem> prolong2;                   // the same, counted in coarse cells
+   bool prolong_r2 = false;                          // ratio 2 on every axis
    DevArray<double> tmp;
    DevArray<double> dxc_prob;                        // per problem dx of level ln-1
    DevArray<unsigned long long> maxres_red, maxres_blk;
@@ -1683,6 +1685,8 @@ void build_prolong_tables(fac_ctx *c, int ln)
    const int dim = c->dim;
    Fl.tmp_fill.clear();
    Fl.prolong.clear();
+   Fl.prolong2.clear();
+   Fl.prolong_r2 = Fl.ratio[0] == 2 && Fl.ratio[1] == 2 && (dim == 2 || Fl.ratio[2] == 2);
    auto sides = all_sides(dim);
    long long toff = 0;
    for (int ip = 0; ip < Fl.npatch; ++ip) {
@@ -1742,6 +1746,7 @@ void build_prolong_tables(fac_ctx *c, int ln)
       pi.fine_patch = ip;
       pi.tmp = T;
       Fl.prolong.add(pi, Fl.box[ip].size());
+      if (Fl.prolong_r2) Fl.prolong2.add(pi, Fl.box[ip].size() / (dim == 3 ? 8 : 4));
    }
    Fl.tmp.alloc(std::max<long long>(1, toff));
    if (c->mixed) {
@@ -1756,6 +1761,7 @@ void build_prolong_tables(fac_ctx *c, int ln)
    // every source of the interpolation array is on the coarser level
    build_fill_gather(c, Fl.tmp_fill, Fl.gather_tmp, toff, 0, C.n1);
    Fl.prolong.upload(c->stream);
+   Fl.prolong2.upload(c->stream);
    std::vector<double> dxc(3 * nprob(c));
    for (int p = 0; p < nprob(c); ++p)
       for (int a = 0; a < 3; ++a) dxc[3 * p + a] = C.dx[3 * p + a];
@@ -2103,6 +2109,7 @@ void register_work_lists(fac_ctx *c)
       register_items(c, L.tmp_fill);
       if (L.gather_tmp.ok) register_items(c, L.gather_tmp.bc);
       register_items(c, L.prolong);
+      register_items(c, L.prolong2);
       for (int t = 0; t < 2; ++t)
          register_work(c, L.ws_units[t], L.units[t], L.d_units[t].p, pp);
       for (int k = 0; k < kResKinds; ++k)
@@ -2428,9 +2435,15 @@ void prolong_correct(fac_ctx *c, int fid_src, int fid_dst, int dest_ln)
       launch_fill<double>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
                           Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp.p, nullptr,
                           field_ptr(C, fid_src), 1, c->bc, c->active.p);
-   launch_prolong_add(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
-                      Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp.p, Fl.dxc_prob.p, Fl.ratio,
-                      field_ptr(Fl, fid_dst), c->active.p);
+   if (Fl.prolong_r2)
+      launch_prolong_add_r2<double>(c->stream, c->dim, Fl.prolong2.d_items.p,
+                                    Fl.prolong2.d_chunks.p, Fl.prolong2.nchunks(),
+                                    Fl.prolong2.d_prefix.p, Fl.d_patches.p, Fl.tmp.p,
+                                    Fl.dxc_prob.p, field_ptr(Fl, fid_dst), c->active.p);
+   else
+      launch_prolong_add(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
+                         Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp.p,
+                         Fl.dxc_prob.p, Fl.ratio, field_ptr(Fl, fid_dst), c->active.p);
    CUDA_CHECK(cudaGetLastError());
 }
 
@@ -2691,9 +2704,15 @@ void prolong32(fac_ctx *c, int dest_ln)
       launch_fill<float>(c->stream, Fl.tmp_fill.d_items.p, Fl.tmp_fill.d_chunks.p,
                          Fl.tmp_fill.nchunks(), Fl.tmp_fill.d_prefix.p, Fl.tmp32.p, nullptr,
                          C.e32.p, 1, c->bc, c->active.p);
-   launch_prolong_add<float>(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
-                             Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p, Fl.tmp32.p, Fl.dxc_prob.p,
-                             Fl.ratio, Fl.e32.p, c->active.p);
+   if (Fl.prolong_r2)
+      launch_prolong_add_r2<float>(c->stream, c->dim, Fl.prolong2.d_items.p,
+                                   Fl.prolong2.d_chunks.p, Fl.prolong2.nchunks(),
+                                   Fl.prolong2.d_prefix.p, Fl.d_patches.p, Fl.tmp32.p,
+                                   Fl.dxc_prob.p, Fl.e32.p, c->active.p);
+   else
+      launch_prolong_add<float>(c->stream, c->dim, Fl.prolong.d_items.p, Fl.prolong.d_chunks.p,
+                                Fl.prolong.nchunks(), Fl.prolong.d_prefix.p, Fl.d_patches.p,
+                                Fl.tmp32.p, Fl.dxc_prob.p, Fl.ratio, Fl.e32.p, c->active.p);
    CUDA_CHECK(cudaGetLastError());
 }
 

@@ -1134,6 +1134,100 @@ k_prolong_add(const ProlongItem *__restrict__ items, const Chunk *__restrict__ c
    }
 }
 
+// k_prolong_add for ratio 2 on every axis: one thread per coarse cell of a
+// fine patch (fine patches are whole coarse cells), which loads the 3^DIM
+// values of the interpolation array around it once and updates its 2^DIM
+// fine cells.  Each fine cell takes the same corner values and weights as
+// in k_prolong_add (lower corner at the coarse cell plus the tabulated
+// shift, -1 for the lower fine cell and 0 for the upper one), so the same
+// bits; the loads are the union of those the fine cells read.
+template <int DIM, class T>
+__global__ void __launch_bounds__(kThreads)
+k_prolong_add_r2(const ProlongItem *__restrict__ items, const Chunk *__restrict__ chunks,
+                 int nwork, const int *__restrict__ prefix, const PatchDesc *__restrict__ fine,
+                 const T *__restrict__ tmp, const double *__restrict__ dxc_prob,
+                 T *__restrict__ e, const int *__restrict__ run)
+{
+   const T half = (T)0.5, one = (T)1;
+   __shared__ T s_x[3][2];
+   __shared__ int s_sh[3][2];
+   WORK_LOOP(ch) {
+      const int prob = items[ch.patch].prob;
+      if (run && !run[prob]) continue;
+      __syncthreads();  // the previous chunk's table is no longer read
+      if ((int)threadIdx.x < DIM * 2) {
+         const int a = threadIdx.x / 2, ir = threadIdx.x % 2;
+         const double *dxc = dxc_prob + 3 * prob;
+         const PatchDesc &p0 = fine[items[ch.patch].fine_patch];
+         const T deltax = ((T)ir + half) * (T)p0.dx[a] - (T)dxc[a] * half;
+         T x = deltax / (T)dxc[a];
+         int sh = 0;
+         if (x < 0.0) {
+            sh = -1;
+            x = x + one;
+         }
+         s_x[a][ir] = x;
+         s_sh[a][ir] = sh;
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+         int lin;
+         const ProlongItem &it = items[chunk_item(ch, prefix, t, lin)];
+         const PatchDesc &p = fine[it.fine_patch];
+         const int nxc = (p.hi[0] - p.lo[0] + 1) >> 1;
+         const int nyc = (p.hi[1] - p.lo[1] + 1) >> 1;
+         const int q = lin / nxc;
+         int c0[3];
+         c0[0] = coarsen_index(p.lo[0], 2) + (lin - q * nxc);
+         c0[1] = coarsen_index(p.lo[1], 2) + (DIM == 3 ? q % nyc : q);
+         c0[2] = DIM == 3 ? coarsen_index(p.lo[2], 2) + q / nyc : 0;
+         const ArrDesc &A = it.tmp;
+         const int sy = A.n[0];
+         const long long sz = (long long)A.n[0] * A.n[1];
+         const long long b = aidx(A, c0[0] - 1, c0[1] - 1, DIM == 3 ? c0[2] - 1 : 0);
+         constexpr int NZ = DIM == 3 ? 3 : 1;
+         T nb[NZ][3][3];
+#pragma unroll
+         for (int dz = 0; dz < NZ; ++dz)
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+               for (int dx = 0; dx < 3; ++dx) nb[dz][dy][dx] = tmp[b + dx + sy * dy + sz * dz];
+#pragma unroll
+         for (int iz = 0; iz < (DIM == 3 ? 2 : 1); ++iz)
+#pragma unroll
+            for (int iy = 0; iy < 2; ++iy)
+#pragma unroll
+               for (int ix = 0; ix < 2; ++ix) {
+                  const int ox = 1 + s_sh[0][ix], oy = 1 + s_sh[1][iy];
+                  const T xx = s_x[0][ix], y = s_x[1][iy];
+                  T v;
+                  if (DIM == 2) {
+                     const T c00 = nb[0][oy][ox], c10 = nb[0][oy][ox + 1];
+                     const T c01 = nb[0][oy + 1][ox], c11 = nb[0][oy + 1][ox + 1];
+                     v = (c00 + (c10 - c00) * xx) * (one - y) + (c01 + (c11 - c01) * xx) * y;
+                  } else {
+                     const int oz = 1 + s_sh[2][iz];
+                     const T z = s_x[2][iz];
+                     const T c000 = nb[oz][oy][ox], c100 = nb[oz][oy][ox + 1];
+                     const T c010 = nb[oz][oy + 1][ox], c110 = nb[oz][oy + 1][ox + 1];
+                     const T c001 = nb[oz + 1][oy][ox], c101 = nb[oz + 1][oy][ox + 1];
+                     const T c011 = nb[oz + 1][oy + 1][ox], c111 = nb[oz + 1][oy + 1][ox + 1];
+                     v = ((c000 + (c100 - c000) * xx) * (one - y) +
+                          (c010 + (c110 - c010) * xx) * y) *
+                            (one - z) +
+                         ((c001 + (c101 - c001) * xx) * (one - y) +
+                          (c011 + (c111 - c011) * xx) * y) *
+                            z;
+                  }
+                  const long long c = cidx<DIM>(p, p.off1, 1, 2 * c0[0] + ix, 2 * c0[1] + iy,
+                                                DIM == 3 ? 2 * c0[2] + iz : 0);
+                  e[c] = e[c] + v;
+               }
+      }
+   }
+}
+
 // ---------------------------------------------------------------------------
 // interior cell helpers
 // ---------------------------------------------------------------------------
@@ -2441,6 +2535,22 @@ void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const
 }
 
 template <class T>
+void launch_prolong_add_r2(cudaStream_t s, int dim, const ProlongItem *items,
+                           const Chunk *chunks, int nchunks, const int *prefix,
+                           const PatchDesc *fine, const T *tmp, const double *dxc_prob, T *e,
+                           const int *run)
+{
+   if (nchunks <= 0) return;
+   g_launches.fetch_add(1, std::memory_order_relaxed);
+   if (dim == 2)
+      k_prolong_add_r2<2, T><<<work_grid(k_prolong_add_r2<2, T>, nchunks), kThreads, 0, s>>>(
+         items, chunks, nchunks, prefix, fine, tmp, dxc_prob, e, run);
+   else
+      k_prolong_add_r2<3, T><<<work_grid(k_prolong_add_r2<3, T>, nchunks), kThreads, 0, s>>>(
+         items, chunks, nchunks, prefix, fine, tmp, dxc_prob, e, run);
+}
+
+template <class T>
 void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                          const Chunk *chunks, double *u, const T *e, const int *run)
 {
@@ -2666,6 +2776,9 @@ void launch_scatter(cudaStream_t s, const long long *idx, long long n, const dou
    template void launch_prolong_add<T>(cudaStream_t, int, const ProlongItem *,              \
                                        const Chunk *, int, const int *, const PatchDesc *, const T *, \
                                        const double *, const int *, T *, const int *);      \
+   template void launch_prolong_add_r2<T>(cudaStream_t, int, const ProlongItem *,           \
+                                          const Chunk *, int, const int *, const PatchDesc *, \
+                                          const T *, const double *, T *, const int *);     \
    template void launch_add_interior<T>(cudaStream_t, int, int, const PatchDesc *,          \
                                         const Chunk *, double *, const T *, const int *);
 INST_T(double)

@@ -208,6 +208,14 @@ template <class T>
 void launch_prolong_add(cudaStream_t s, int dim, const ProlongItem *items, const Chunk *chunks,
                         int nchunks, const int *prefix, const PatchDesc *fine, const T *tmp,
                         const double *dxc_prob, const int *ratio, T *e, const int *run);
+// the same for ratio 2 on every axis, over the coarse cells of the fine
+// patches (items counted in coarse cells): same bits, one load of each
+// interpolation value per coarse cell
+template <class T>
+void launch_prolong_add_r2(cudaStream_t s, int dim, const ProlongItem *items,
+                           const Chunk *chunks, int nchunks, const int *prefix,
+                           const PatchDesc *fine, const T *tmp, const double *dxc_prob, T *e,
+                           const int *run);
 
 template <class T>
 void launch_add_interior(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
