@@ -3310,25 +3310,32 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             OpTimer ot(c, "kry_precondition", -1);
             run_graph(c, c->prec_exec, c->prec_launches, prec_body);
          }
+         // Z_j into its slot and into E (ghosts zero) for W = A Z_j; the
+         // mixed cycle's correction is in e32, so one pass writes both
+         const bool both = c->mixed && !c->cnn;
+         if (both) zero_field(c, FAC_E);
          for (int ln = 0; ln < c->nlev; ++ln) {
             LevelState &L = c->L[ln];
             if (c->mixed)
                launch_g1_to_g0<float>(c->stream, c->dim, (int)L.cell_chunks.size(),
                                       L.d_patches.p, L.d_cell_chunks.p, L.e32.p,
-                                      kry_vec(c, ln, zslot0 + j));
+                                      kry_vec(c, ln, zslot0 + j), false, nullptr,
+                                      both ? L.e.p : nullptr);
             else
                launch_g1_to_g0<double>(c->stream, c->dim, (int)L.cell_chunks.size(),
                                        L.d_patches.p, L.d_cell_chunks.p, L.e.p,
                                        kry_vec(c, ln, zslot0 + j));
          }
          if (c->cnn) learned_precondition(c, j, zslot0 + j);
-         // W = A Z_j = -(0 - A Z_j)
-         zero_field(c, FAC_E);
-         for (int ln = 0; ln < c->nlev; ++ln) {
-            LevelState &L = c->L[ln];
-            launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
-                            L.d_cell_chunks.p, kry_vec(c, ln, zslot0 + j), L.e.p);
+         if (!both) {
+            zero_field(c, FAC_E);
+            for (int ln = 0; ln < c->nlev; ++ln) {
+               LevelState &L = c->L[ln];
+               launch_g0_to_g1(c->stream, c->dim, (int)L.cell_chunks.size(), L.d_patches.p,
+                               L.d_cell_chunks.p, kry_vec(c, ln, zslot0 + j), L.e.p);
+            }
          }
+         // W = A Z_j = -(0 - A Z_j)
          {
             OpTimer ot(c, "kry_apply", -1);
             run_graph(c, c->apply_exec, c->apply_launches, apply_body);

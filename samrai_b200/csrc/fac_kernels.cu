@@ -1932,7 +1932,7 @@ template <int DIM, class TS>
 __global__ void __launch_bounds__(kThreads)
 k_g1_to_g0(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chunks, int nwork,
            const TS *__restrict__ src, double *__restrict__ dst, int add,
-           const double *__restrict__ scale)
+           const double *__restrict__ scale, double *__restrict__ dst1)
 {
    WORK_LOOP(ch) {
       const PatchDesc &p = patches[ch.patch];
@@ -1945,9 +1945,11 @@ k_g1_to_g0(const PatchDesc *__restrict__ patches, const Chunk *__restrict__ chun
          const int i = p.lo[0] + ci;
          const int j = p.lo[1] + cj;
          const int k = DIM == 3 ? p.lo[2] + ck : 0;
-         double v = (double)src[cidx<DIM>(p, p.off1, 1, i, j, k)];
+         const long long c1 = cidx<DIM>(p, p.off1, 1, i, j, k);
+         double v = (double)src[c1];
          if (scale) v = scale[p.prob] * v;
          dst[p.off0 + lin] = add ? dst[p.off0 + lin] + v : v;
+         if (dst1) dst1[c1] = v;
       }
    }
 }
@@ -2097,21 +2099,21 @@ bool launch_combine_dots(cudaStream_t s, int nchunks, const Chunk *chunks, doubl
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                      const Chunk *chunks, const TS *src, double *dst, bool add,
-                     const double *scale)
+                     const double *scale, double *dst1)
 {
    if (nchunks <= 0) return;
    g_launches.fetch_add(1, std::memory_order_relaxed);
    if (dim == 2)
       k_g1_to_g0<2, TS><<<work_grid(k_g1_to_g0<2, TS>, nchunks), kThreads, 0, s>>>(
-         patches, chunks, nchunks, src, dst, add ? 1 : 0, scale);
+         patches, chunks, nchunks, src, dst, add ? 1 : 0, scale, dst1);
    else
       k_g1_to_g0<3, TS><<<work_grid(k_g1_to_g0<3, TS>, nchunks), kThreads, 0, s>>>(
-         patches, chunks, nchunks, src, dst, add ? 1 : 0, scale);
+         patches, chunks, nchunks, src, dst, add ? 1 : 0, scale, dst1);
 }
 template void launch_g1_to_g0<double>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
-                                      const double *, double *, bool, const double *);
+                                      const double *, double *, bool, const double *, double *);
 template void launch_g1_to_g0<float>(cudaStream_t, int, int, const PatchDesc *, const Chunk *,
-                                     const float *, double *, bool, const double *);
+                                     const float *, double *, bool, const double *, double *);
 
 void launch_add_combination(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                             const Chunk *chunks, double *u, const double *Z, long long zstride,

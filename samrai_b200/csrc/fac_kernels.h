@@ -98,11 +98,12 @@ bool launch_combine_dots(cudaStream_t s, int nchunks, const Chunk *chunks, doubl
                          const int *prob_chunk_begin, int nprob, const int *active, double *out,
                          const double *xin = nullptr);
 // dst (ghost-0) = interior of src (ghost-1), converted to FP64, times
-// scale[problem] when scale is given (with add: dst += it)
+// scale[problem] when scale is given (with add: dst += it); with dst1 (a
+// ghost-1 FP64 field, not src) the same values also go to its interior
 template <class TS>
 void launch_g1_to_g0(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                      const Chunk *chunks, const TS *src, double *dst, bool add = false,
-                     const double *scale = nullptr);
+                     const double *scale = nullptr, double *dst1 = nullptr);
 // u interior += sum_i y[p*K+i] Z_i
 void launch_add_combination(cudaStream_t s, int dim, int nchunks, const PatchDesc *patches,
                             const Chunk *chunks, double *u, const double *Z, long long zstride,
