@@ -3310,10 +3310,12 @@ void fgmres_solve(fac_ctx *c, int m, int *converged, int *iterations, double *re
             OpTimer ot(c, "kry_precondition", -1);
             run_graph(c, c->prec_exec, c->prec_launches, prec_body);
          }
-         // Z_j into its slot and into E (ghosts zero) for W = A Z_j; the
-         // mixed cycle's correction is in e32, so one pass writes both
+         // Z_j into its slot and into E for W = A Z_j; the mixed cycle's
+         // correction is in e32, so one pass writes both.  E's interior is
+         // then Z_j on every level, and its ghost cells need no zeroing: the
+         // operator fills every face ghost of a level before its residual
+         // reads it, and edge and corner ghosts are not read
          const bool both = c->mixed && !c->cnn;
-         if (both) zero_field(c, FAC_E);
          for (int ln = 0; ln < c->nlev; ++ln) {
             LevelState &L = c->L[ln];
             if (c->mixed)
